@@ -1,0 +1,206 @@
+/*
+ * windstencil_b200.h -- C ABI of the B200 (sm_100a) BF3W inviscid RHS library.
+ *
+ * libwindstencil_b200.so replaces WindStencil's inviscid hot path: the fused
+ * BF3W kernel (src/kernels/OCFD_split.cpp:36-3918), its driver and boundary
+ * ring kernel (src/solver/OCFD_NS_Jacobian3d.cpp:24-414, :828-2530), the sound
+ * speed / prim<->cons / RK-stage kernels around it, and the host-staged halo
+ * exchange (src/mpi/OCFD_mpi_dev.cpp:123-290) on one GPU.
+ *
+ * Conventions (all entry points):
+ *   - plain C types, device pointers in ws_field / ws_soa, sizes in elements;
+ *   - the return value is WS_OK (0) or a WS_ERR_* code; nothing aborts and the
+ *     message of the last failure on the calling thread is in ws_last_error();
+ *   - work is enqueued on the given stream (NULL = legacy default stream) and
+ *     no entry point synchronises the host, except where its comment says so;
+ *   - LAP fields are [nz+8][ny+8][pitch >= nx+8] doubles, x fastest, 4 ghost
+ *     layers on every side; SoA arrays are [5][length_Z][length_Y][pitch]
+ *     doubles (reference index macros, include/windstencil/cuda_utility.h:16-27).
+ */
+#ifndef WINDSTENCIL_B200_H
+#define WINDSTENCIL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(WS_BUILDING_LIB) && defined(__GNUC__)
+#define WS_API __attribute__((visibility("default")))
+#else
+#define WS_API
+#endif
+
+#define WS_LAP 4
+#define WS_NVARS 5
+#define WS_ABI_VERSION 1
+
+/* cudaStream_t without including the CUDA headers */
+typedef struct CUstream_st* ws_stream_t;
+
+/* == cudaField (include/windstencil/cuda_commen.h:48-54, HIP layout). */
+typedef struct ws_field {
+    double* ptr;        /* device pointer to element (0,0,0) of the LAP array */
+    uint32_t pitch;     /* row pitch in elements                              */
+    uint32_t dummy0;
+} ws_field;
+
+/* == cudaSoA (include/windstencil/cuda_commen.h:64-72). */
+typedef struct ws_soa {
+    double* ptr;        /* device pointer to element (0,0,0) of variable 0    */
+    uint32_t pitch;     /* row pitch in elements                              */
+    uint32_t length_Y;  /* rows per plane                                      */
+    uint32_t length_Z;  /* planes per variable                                 */
+    uint32_t dummy0;
+} ws_soa;
+
+typedef struct ws_dim3 { uint32_t x, y, z; } ws_dim3;
+
+/* == cudaJobPackage (include/windstencil/cuda_commen.h:98-106): the cells
+ * [start, end) in LAP coordinates (interior = [4, n+4)). */
+typedef struct ws_job { ws_dim3 start, end; } ws_job;
+
+enum ws_face_kind {
+    WS_FACE_PERIODIC = 0,   /* ghosts wrap (the reference's periodic self-exchange) */
+    WS_FACE_EXTRAP = 1      /* zero-gradient ghosts (copy of the boundary cell)     */
+};
+
+enum ws_precision {
+    WS_FP64 = 0,            /* the drop-in: every operation in FP64                  */
+    WS_MIXED = 1            /* FP32 split, smoothness indicators, weights and
+                               candidates; FP64 state, face difference and RK3      */
+};
+
+enum ws_status {
+    WS_OK = 0,
+    WS_ERR_INVALID = 1,     /* bad argument (sizes, job, pitch, alignment)  */
+    WS_ERR_CUDA = 2,        /* a CUDA runtime call failed                    */
+    WS_ERR_ALLOC = 3,       /* device or host allocation failed              */
+    WS_ERR_UNSUPPORTED = 4, /* configuration this build does not implement   */
+    WS_ERR_NONFINITE = 5,   /* device status: non-finite value, rho<=0, p<=0 */
+    WS_ERR_TIMEOUT = 6,     /* a bounded device wait gave up                 */
+    WS_ERR_BUDGET = 7,      /* admission would exceed the HBM budget         */
+    WS_ERR_BUSY = 8,        /* object in use / queue full                    */
+    WS_ERR_NOT_FOUND = 9    /* unknown request id                            */
+};
+
+/* Grid and physics constants.  Replaces the reference's __constant__ set
+ * (src/runtime/parameters_d.cpp:12-35) and the derived constants of
+ * OCFD_init.cpp:379-407 (Cv, split_C1, split_C3 are derived from gamma, ama). */
+typedef struct ws_grid {
+    uint32_t nx, ny, nz;      /* interior extents                                */
+    uint32_t lap;             /* ghost width; must be WS_LAP                      */
+    double hx, hy, hz;        /* grid spacing (reference default 1/(N-1))         */
+    double gamma;             /* Gamma                                            */
+    double ama;               /* Ama (reference Mach number)                      */
+    double epsl_sw;           /* EPSL_SW, Steger-Warming entropy fix              */
+    int32_t face_kind[6];     /* x-, x+, y-, y+, z-, z+ : enum ws_face_kind       */
+    int32_t precision;        /* enum ws_precision                                */
+    int32_t metrics_uniform;  /* 1: Cartesian metrics xi=(1,0,0), eta=(0,1,0),
+                                 zeta=(0,0,1) and J=1; metric fields not read    */
+} ws_grid;
+
+/* Metric fields (LAP), the reference's pAkx_d..pAsz_d and pAjac_d
+ * (include/windstencil/parameters_d.h:37-63). */
+typedef struct ws_metrics {
+    ws_field akx, aky, akz;   /* xi   gradient */
+    ws_field aix, aiy, aiz;   /* eta  gradient */
+    ws_field asx, asy, asz;   /* zeta gradient */
+    ws_field ajac;            /* Jacobian J    */
+} ws_metrics;
+
+/* Kernel tile shape: (tile_x x tile_y) columns swept along z in chunks of
+ * scan_z planes; threads per CTA.  Zeroes select the tuned default. */
+typedef struct ws_tile {
+    int32_t tile_x, tile_y, scan_z, threads;
+} ws_tile;
+
+/* ------------------------------------------------------------------------ */
+/* Library                                                                   */
+/* ------------------------------------------------------------------------ */
+WS_API int  ws_abi_version(void);
+/* Copies the message of the last failure on this thread (NUL-terminated). */
+WS_API int  ws_last_error(char* buf, size_t n);
+/* Bytes of the LAP-field pitch this library allocates for extent nx+8. */
+WS_API uint32_t ws_lap_pitch(uint32_t nx);
+
+/* ------------------------------------------------------------------------ */
+/* Drop-in kernels (explicit arguments)                                      */
+/* ------------------------------------------------------------------------ */
+
+/* cc = sqrt(T)/Ama over the job extended by 4 ghost layers.
+ * Replaces du_invis_Jacobian3d_init (OCFD_NS_Jacobian3d.cpp:24-33) and
+ * sound_speed_kernel (commen_kernel.cpp:145-154). */
+WS_API int ws_du_invis_jacobian3d_init(const ws_grid* g, ws_job job, ws_field T, ws_field cc,
+                                ws_stream_t stream);
+
+/* du (SoA, written with `=`) = BF3W inviscid RHS on the job's cells from the
+ * LAP primitives d,u,v,w and sound speed cc (ghosts filled).  metrics may be
+ * NULL when g->metrics_uniform is 1.  du(x,y,z) is addressed relative to
+ * job.start.  Replaces du_invis_Jacobian3d_x (OCFD_NS_Jacobian3d.cpp:133-414:
+ * the fused kernel OCFD_split.cpp:36-3918 plus the boundary ring kernel
+ * :828-2530); needs no workspace and allocates nothing. */
+WS_API int ws_du_invis_jacobian3d(const ws_grid* g, ws_job job, ws_field d, ws_field u,
+                           ws_field v, ws_field w, ws_field cc, const ws_metrics* metrics,
+                           ws_soa du, ws_stream_t stream);
+
+/* Same, with an explicit tile shape (autotuner and tests). */
+WS_API int ws_du_invis_jacobian3d_tiled(const ws_grid* g, ws_job job, ws_field d, ws_field u,
+                                 ws_field v, ws_field w, ws_field cc,
+                                 const ws_metrics* metrics, ws_soa du, ws_tile tile,
+                                 ws_stream_t stream);
+
+/* In-place ghost fill (4 layers) of nfields LAP fields by g->face_kind.
+ * Replaces exchange_boundary_xyz_packed_dev (OCFD_mpi_dev.cpp:123-290) on one
+ * GPU: no host staging, no MPI. */
+WS_API int ws_ghost_fill(const ws_grid* g, const ws_field* fields, int nfields, ws_stream_t stream);
+
+/* Conserved (SoA f) -> LAP interiors of d,u,v,w,T and P (P.ptr may be NULL).
+ * Replaces get_duvwT / cons_to_pri_kernel (commen_kernel.cpp:78-119). */
+WS_API int ws_cons_to_prim(const ws_grid* g, ws_soa f, ws_field d, ws_field u, ws_field v,
+                    ws_field w, ws_field T, ws_field P, ws_stream_t stream);
+
+/* LAP primitives -> conserved SoA f.
+ * Replaces pri_to_cons_kernel_warp (commen_kernel.cpp:33-73). */
+WS_API int ws_prim_to_cons(const ws_grid* g, ws_field d, ws_field u, ws_field v, ws_field w,
+                    ws_field T, ws_soa f, ws_stream_t stream);
+
+/* SSP-RK3 stage krk in {1,2,3}: f <- stage(fn, f, dt*du).
+ * Replaces OCFD_time_advance (OCFD_time.cpp:15-91). */
+WS_API int ws_time_advance(const ws_grid* g, int krk, double dt, ws_soa f, ws_soa fn, ws_soa du,
+                    ws_stream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* One grid, device-resident, SSP-RK3 step as one CUDA graph                 */
+/* Replaces the time loop NS_solver_real (OCFD_NS_Solver.cpp:64-90) with all  */
+/* three RK stages.                                                           */
+/* ------------------------------------------------------------------------ */
+typedef struct ws_solver ws_solver;
+
+/* Allocates the state (f, fn, du SoA; d,u,v,w,T,cc LAP) on the current device. */
+WS_API int  ws_solver_create(const ws_grid* g, ws_solver** out);
+WS_API void ws_solver_destroy(ws_solver* s);
+/* Uploads a dense conserved state [5][nz][ny][nx] from host memory. */
+WS_API int  ws_solver_set_state(ws_solver* s, const double* f_host, ws_stream_t stream);
+/* Downloads the conserved state; synchronises `stream`. */
+WS_API int  ws_solver_get_state(ws_solver* s, double* f_host, ws_stream_t stream);
+/* Downloads du of the last ws_solver_rhs(); synchronises `stream`. */
+WS_API int  ws_solver_get_rhs(ws_solver* s, double* du_host, ws_stream_t stream);
+/* Device descriptors of the state (f, du SoA; d,u,v,w,T,cc LAP). */
+WS_API int  ws_solver_fields(ws_solver* s, ws_soa* f, ws_soa* du, ws_field prims[6]);
+/* CFL time step of the current state; synchronises `stream`. */
+WS_API int  ws_solver_compute_dt(ws_solver* s, double cfl, double* dt, ws_stream_t stream);
+/* du of the current state (prims, ghost fill, cc, RHS). */
+WS_API int  ws_solver_rhs(ws_solver* s, ws_stream_t stream);
+/* nsteps SSP-RK3 steps with time step dt, replayed from one CUDA graph. */
+WS_API int  ws_solver_step(ws_solver* s, double dt, int nsteps, ws_stream_t stream);
+/* Device status word (0 or WS_ERR_NONFINITE); synchronises `stream`. */
+WS_API int  ws_solver_status(ws_solver* s, int* status, ws_stream_t stream);
+WS_API int  ws_solver_set_tile(ws_solver* s, ws_tile tile);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WINDSTENCIL_B200_H */

@@ -1,0 +1,330 @@
+#!/usr/bin/env python3
+"""Build the reference's own scalar kernels for the host (test infrastructure).
+
+The reference (WindStencil) is HIP-only and cannot be built here as a whole:
+hipcc, ROCm and MPI are absent and its fused kernel assumes 64-lane
+wavefronts.  Its per-point arithmetic, however, is plain C inside a handful of
+functions.  This recipe reads those functions *where they lie* in the mounted
+reference tree, places them behind a small shim that maps the HIP qualifiers
+and the index macros to host C++, compiles them with g++ into
+``oracle/_ref/libwsref.so`` and deletes the generated translation unit, so no
+reference source is kept (``oracle/_ref/`` is git-ignored).
+
+Functions taken from the reference (path within the WindStencil tree):
+  src/kernels/OCFD_Schemes.cpp        OCFD_weno7_SYMBO_kernel_P_opt, _M_opt
+  src/solver/OCFD_NS_Jacobian3d.cpp   split_Jac3d_Stager_Warming_ker_origin
+  src/kernels/commen_kernel.cpp       cons_to_pri_kernel, pri_to_cons_kernel,
+                                      sound_speed_kernel
+  src/solver/OCFD_time.cpp            OCFD_time_advance_ker1/2/3
+  include/windstencil/cuda_utility.h  get_Field / get_Field_LAP / get_SoA /
+                                      get_SoA_LAP index macros
+
+The host drivers below (``ref_*``) are this project's code: they set the
+HIP thread coordinates for every point and call the reference function, and
+``ref_du_invis`` assembles the decomposed RHS from the reference's split and
+WENO functions with the loop of oracle/oracle.cpp (or_du_invis).
+
+Only tests/ and bench.py's CPU-baseline legs use the result, as the checker.
+Usage:  python oracle/build_ref.py [--ref /path/to/reference] [--native]
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import re
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT_DIR = os.path.join(HERE, "_ref")
+DEFAULT_REF = "/root/reference"
+
+FUNCS = [
+    ("src/kernels/OCFD_Schemes.cpp", "OCFD_weno7_SYMBO_kernel_P_opt"),
+    ("src/kernels/OCFD_Schemes.cpp", "OCFD_weno7_SYMBO_kernel_M_opt"),
+    ("src/solver/OCFD_NS_Jacobian3d.cpp", "split_Jac3d_Stager_Warming_ker_origin"),
+    ("src/kernels/commen_kernel.cpp", "pri_to_cons_kernel"),
+    ("src/kernels/commen_kernel.cpp", "cons_to_pri_kernel"),
+    ("src/kernels/commen_kernel.cpp", "sound_speed_kernel"),
+    ("src/solver/OCFD_time.cpp", "OCFD_time_advance_ker1"),
+    ("src/solver/OCFD_time.cpp", "OCFD_time_advance_ker2"),
+    ("src/solver/OCFD_time.cpp", "OCFD_time_advance_ker3"),
+]
+MACROS = [("include/windstencil/cuda_utility.h",
+           ["get_Field", "get_Field_LAP", "get_SoA", "get_SoA_LAP"])]
+
+SHIM_HEAD = r"""
+// ---- host shim for HIP device code (generated; not committed) ----
+#include <cmath>
+#include <cstring>
+#include <vector>
+using std::sqrt; using std::fmax; using std::fmin;
+typedef double REAL;
+#define LAP 4
+#define __device__
+#define __global__
+#define __host__
+#define __forceinline__ inline
+struct dim3 { unsigned x, y, z;
+  dim3(unsigned a = 1, unsigned b = 1, unsigned c = 1) : x(a), y(b), z(c) {} };
+static thread_local dim3 threadIdx(0, 0, 0), blockIdx(0, 0, 0), blockDim(1, 1, 1);
+struct cudaField { REAL* ptr; unsigned pitch; unsigned dummy0; };
+struct cudaSoA { REAL* ptr; unsigned pitch, length_Y, length_Z, dummy0; };
+struct cudaJobPackage { dim3 start, end;
+  cudaJobPackage() {}
+  cudaJobPackage(const dim3& s, const dim3& e) : start(s), end(e) {} };
+static thread_local REAL epsl_sw_d, Gamma_d, split_C1_d, split_C3_d, Cv_d, Ama_d, dt_d;
+static thread_local unsigned ny_d, nz_d, ny_2lap_d, nz_2lap_d;
+"""
+
+DRIVERS = r"""
+// ---- host drivers (this project's code) ----
+namespace {
+void set_consts(double gamma, double ama, double eps) {
+  Gamma_d = gamma; Ama_d = ama; epsl_sw_d = eps;
+  // derived constants as the reference forms them (OCFD_init.cpp:380-386)
+  Cv_d = 1.0 / (gamma * (gamma - 1.0) * ama * ama);
+  split_C1_d = 2.0 * (gamma - 1.0);
+  split_C3_d = (3.0 - gamma) / (2.0 * (gamma - 1.0));
+}
+void set_dims(int nx, int ny, int nz) {
+  ny_d = ny; nz_d = nz; ny_2lap_d = ny + 2 * LAP; nz_2lap_d = nz + 2 * LAP; (void)nx;
+}
+cudaField fld(double* p, int nx) { cudaField f; f.ptr = p; f.pitch = nx + 2 * LAP; f.dummy0 = 0; return f; }
+cudaSoA soa(double* p, int nx, int ny, int nz) {
+  cudaSoA s; s.ptr = p; s.pitch = nx; s.length_Y = ny; s.length_Z = nz; s.dummy0 = 0; return s; }
+}
+
+extern "C" {
+double ref_weno_p(const double* s) { REAL t[8]; std::memcpy(t, s, sizeof t);
+  return OCFD_weno7_SYMBO_kernel_P_opt(t); }
+double ref_weno_m(const double* s) { REAL t[8]; std::memcpy(t, s, sizeof t);
+  return OCFD_weno7_SYMBO_kernel_M_opt(t); }
+void ref_weno_p_batch(const double* s, long n, double* out) {
+  #pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; ++i) out[i] = ref_weno_p(s + 8 * i); }
+void ref_weno_m_batch(const double* s, long n, double* out) {
+  #pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; ++i) out[i] = ref_weno_m(s + 8 * i); }
+
+// one-point fields: pitch 1 and unit padded extents make every index 0 (+var)
+void ref_split_batch(const double* in, long n, double gamma, double eps,
+                     double* fp, double* fm) {
+  #pragma omp parallel
+  {
+    set_consts(gamma, 1.0, eps);
+    ny_2lap_d = 1; nz_2lap_d = 1;
+    #pragma omp for schedule(static)
+    for (long i = 0; i < n; ++i) {
+      double p[8]; std::memcpy(p, in + 8 * i, sizeof p);
+      cudaField f[8];
+      for (int k = 0; k < 8; ++k) { f[k].ptr = p + k; f[k].pitch = 1; f[k].dummy0 = 0; }
+      cudaSoA sp{fp + 5 * i, 1, 1, 1, 0}, sm{fm + 5 * i, 1, 1, 1, 0};
+      threadIdx = dim3(0, 0, 0); blockIdx = dim3(0, 0, 0); blockDim = dim3(1, 1, 1);
+      cudaJobPackage job(dim3(0, 0, 0), dim3(1, 1, 1));
+      split_Jac3d_Stager_Warming_ker_origin(f[0], f[1], f[2], f[3], f[4], sp, sm,
+                                            f[5], f[6], f[7], job);
+    }
+  }
+}
+
+void ref_cons_to_prim(int nx, int ny, int nz, double gamma, double ama, double* f,
+                      double* d, double* u, double* v, double* w, double* T, double* P) {
+  #pragma omp parallel
+  {
+    set_consts(gamma, ama, 0.0); set_dims(nx, ny, nz);
+    cudaJobPackage job(dim3(0, 0, 0), dim3(nx, ny, nz));
+    #pragma omp for collapse(2) schedule(static)
+    for (int k = 0; k < nz; ++k) for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i) {
+      threadIdx = dim3(i, j, k);
+      cons_to_pri_kernel(soa(f, nx, ny, nz), fld(d, nx), fld(u, nx), fld(v, nx), fld(w, nx),
+                         fld(T, nx), fld(P, nx), job);
+    }
+  }
+}
+
+void ref_prim_to_cons(int nx, int ny, int nz, double gamma, double ama, double* d,
+                      double* u, double* v, double* w, double* T, double* f) {
+  #pragma omp parallel
+  {
+    set_consts(gamma, ama, 0.0); set_dims(nx, ny, nz);
+    cudaJobPackage job(dim3(0, 0, 0), dim3(nx, ny, nz));
+    #pragma omp for collapse(2) schedule(static)
+    for (int k = 0; k < nz; ++k) for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i) {
+      threadIdx = dim3(i, j, k);
+      pri_to_cons_kernel(soa(f, nx, ny, nz), fld(d, nx), fld(u, nx), fld(v, nx), fld(w, nx),
+                         fld(T, nx), job);
+    }
+  }
+}
+
+void ref_sound_speed(int nx, int ny, int nz, double ama, double* T, double* cc) {
+  #pragma omp parallel
+  {
+    set_consts(1.4, ama, 0.0); set_dims(nx, ny, nz);
+    cudaJobPackage job(dim3(0, 0, 0), dim3(nx + 2 * LAP, ny + 2 * LAP, nz + 2 * LAP));
+    #pragma omp for collapse(2) schedule(static)
+    for (int k = 0; k < nz + 2 * LAP; ++k) for (int j = 0; j < ny + 2 * LAP; ++j)
+      for (int i = 0; i < nx + 2 * LAP; ++i) {
+        threadIdx = dim3(i, j, k);
+        sound_speed_kernel(fld(T, nx), fld(cc, nx), job);
+      }
+  }
+}
+
+// f_lap may be NULL (stage 3 then writes into a scratch LAP copy)
+void ref_time_advance(int krk, double dt, int nx, int ny, int nz, double* f, double* fn,
+                      double* du) {
+  std::vector<double> lap;
+  if (krk == 3) lap.assign((size_t)5 * (nx + 2 * LAP) * (ny + 2 * LAP) * (nz + 2 * LAP), 0.0);
+  #pragma omp parallel
+  {
+    set_dims(nx, ny, nz); dt_d = dt;
+    cudaJobPackage job(dim3(0, 0, 0), dim3(nx, ny, nz));
+    cudaSoA sl{lap.empty() ? nullptr : lap.data(), (unsigned)(nx + 2 * LAP),
+               (unsigned)(ny + 2 * LAP), (unsigned)(nz + 2 * LAP), 0};
+    #pragma omp for collapse(2) schedule(static)
+    for (int k = 0; k < nz; ++k) for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i) {
+      threadIdx = dim3(i, j, k);
+      if (krk == 1) OCFD_time_advance_ker1(soa(f, nx, ny, nz), soa(fn, nx, ny, nz), soa(du, nx, ny, nz), job);
+      else if (krk == 2) OCFD_time_advance_ker2(soa(f, nx, ny, nz), soa(fn, nx, ny, nz), soa(du, nx, ny, nz), job);
+      else OCFD_time_advance_ker3(soa(f, nx, ny, nz), soa(fn, nx, ny, nz), soa(du, nx, ny, nz), sl, job);
+    }
+  }
+}
+
+// Decomposed inviscid RHS from the reference's split and WENO functions; the
+// loop structure is or_du_invis() of oracle/oracle.cpp.  Cartesian metrics
+// when metrics == NULL, J = 1 when ajac == NULL.  face_kind is not needed:
+// ghosts must be filled by the caller.
+void ref_du_invis(int nx, int ny, int nz, double hx, double hy, double hz, double gamma,
+                  double eps, const double* d, const double* u, const double* v,
+                  const double* w, const double* cc, const double* const* metrics,
+                  const double* ajac, double* du) {
+  const long px = nx + 2 * LAP, py = ny + 2 * LAP;
+  auto lap = [&](long i, long j, long k) { return (i + LAP) + px * ((j + LAP) + py * (k + LAP)); };
+  const double h[3] = {hx, hy, hz};
+  const long ext[3] = {nx, ny, nz};
+  std::memset(du, 0, sizeof(double) * 5 * (size_t)nx * ny * nz);
+  for (int dir = 0; dir < 3; ++dir) {
+    const long n = ext[dir];
+    const long na = dir == 0 ? ny : nx, nb = dir == 2 ? ny : nz;
+    #pragma omp parallel
+    {
+      set_consts(gamma, 1.0, eps);
+      ny_2lap_d = 1; nz_2lap_d = 1;
+      std::vector<double> fp(5 * (n + 2 * LAP)), fm(5 * (n + 2 * LAP)), face(n + 1);
+      #pragma omp for collapse(2) schedule(static)
+      for (long b = 0; b < nb; ++b) for (long a = 0; a < na; ++a) {
+        auto at = [&](long s) { return dir == 0 ? lap(s, a, b) : dir == 1 ? lap(a, s, b) : lap(a, b, s); };
+        auto cell = [&](long s, long var) {
+          long i = dir == 0 ? s : a, j = dir == 1 ? s : (dir == 0 ? a : b), k = dir == 2 ? s : b;
+          return i + nx * (j + ny * (k + nz * var)); };
+        for (long s = -LAP; s < n + LAP; ++s) {
+          const long p = at(s);
+          double in[8] = {d[p], u[p], v[p], w[p], cc[p],
+                          metrics ? metrics[3 * dir][p] : (dir == 0 ? 1.0 : 0.0),
+                          metrics ? metrics[3 * dir + 1][p] : (dir == 1 ? 1.0 : 0.0),
+                          metrics ? metrics[3 * dir + 2][p] : (dir == 2 ? 1.0 : 0.0)};
+          double pp[5], mm[5];
+          cudaField f[8];
+          for (int q = 0; q < 8; ++q) { f[q].ptr = in + q; f[q].pitch = 1; f[q].dummy0 = 0; }
+          cudaSoA sp{pp, 1, 1, 1, 0}, sm{mm, 1, 1, 1, 0};
+          threadIdx = dim3(0, 0, 0);
+          cudaJobPackage job(dim3(0, 0, 0), dim3(1, 1, 1));
+          split_Jac3d_Stager_Warming_ker_origin(f[0], f[1], f[2], f[3], f[4], sp, sm, f[5], f[6], f[7], job);
+          for (int var = 0; var < 5; ++var) {
+            fp[var * (n + 2 * LAP) + s + LAP] = pp[var];
+            fm[var * (n + 2 * LAP) + s + LAP] = mm[var];
+          }
+        }
+        for (int pm = 0; pm < 2; ++pm) for (int var = 0; var < 5; ++var) {
+          double* line = (pm == 0 ? fp.data() : fm.data()) + var * (n + 2 * LAP);
+          for (long i = -1; i < n; ++i) {
+            REAL* st = line + (i - 3 + LAP);
+            face[i + 1] = pm == 0 ? OCFD_weno7_SYMBO_kernel_P_opt(st) : OCFD_weno7_SYMBO_kernel_M_opt(st);
+          }
+          for (long i = 0; i < n; ++i) {
+            const double J = ajac ? ajac[at(i)] : 1.0;
+            du[cell(i, var)] += -J * (face[i + 1] - face[i]) / h[dir];
+          }
+        }
+      }
+    }
+  }
+}
+}  // extern "C"
+"""
+
+
+def extract_function(text: str, name: str) -> str:
+    """Return the full definition of function `name` (signature + body)."""
+    m = re.search(r"^[^\n;{}]*\b" + re.escape(name) + r"\s*\(", text, re.M)
+    while m:
+        # skip commented-out lines and prototypes
+        start = m.start()
+        line = text[start:text.find("\n", start)]
+        if not line.lstrip().startswith("//"):
+            i = text.find("{", m.end())
+            semi = text.find(";", m.end())
+            if i != -1 and (semi == -1 or i < semi):
+                depth, j = 0, i
+                while j < len(text):
+                    if text[j] == "{":
+                        depth += 1
+                    elif text[j] == "}":
+                        depth -= 1
+                        if depth == 0:
+                            return text[start:j + 1]
+                    j += 1
+        m = re.compile(r"^[^\n;{}]*\b" + re.escape(name) + r"\s*\(", re.M).search(text, m.end())
+    raise RuntimeError(f"function {name} not found")
+
+
+def extract_macro(text: str, name: str) -> str:
+    m = re.search(r"^#define\s+" + re.escape(name) + r"\(.*$", text, re.M)
+    if not m:
+        raise RuntimeError(f"macro {name} not found")
+    return m.group(0)
+
+
+def build(ref: str, native: bool = False) -> str:
+    os.makedirs(OUT_DIR, exist_ok=True)
+    parts = [SHIM_HEAD]
+    for hdr, names in MACROS:
+        txt = open(os.path.join(ref, hdr), encoding="utf-8", errors="replace").read()
+        parts += [extract_macro(txt, n) for n in names]
+    for src, name in FUNCS:
+        txt = open(os.path.join(ref, src), encoding="utf-8", errors="replace").read()
+        parts.append(extract_function(txt, name))
+    parts.append(DRIVERS)
+    tu = os.path.join(OUT_DIR, "wsref_tu.cpp")
+    so = os.path.join(OUT_DIR, "libwsref.so")
+    with open(tu, "w") as f:
+        f.write("\n\n".join(parts))
+    cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+    arch = "-march=native" if native else "-march=x86-64-v2"
+    cmd = [cxx, "-O3", "-std=c++17", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off",
+           "-fno-fast-math", arch, "-w", "-o", so, tu]
+    try:
+        subprocess.run(cmd, check=True)
+    finally:
+        os.remove(tu)          # keep no reference source on disk
+    return so
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default=os.environ.get("WS_REFERENCE", DEFAULT_REF))
+    ap.add_argument("--native", action="store_true")
+    a = ap.parse_args()
+    if not os.path.isdir(os.path.join(a.ref, "src")):
+        print(f"reference tree not found at {a.ref}; nothing built", file=sys.stderr)
+        return 1
+    print(build(a.ref, a.native))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

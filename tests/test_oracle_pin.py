@@ -1,0 +1,99 @@
+"""Pins the CPU oracle to the reference's own code.
+
+The reference ships no golden vectors or known-answer tests for this path.
+oracle/build_ref.py builds the reference's own scalar kernels for the host;
+these tests require the oracle (oracle/oracle.cpp) to agree with them
+bit-for-bit (both built with -ffp-contract=off).
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle import LAP, make_grid
+
+
+def _stencils(n, seed):
+    rng = np.random.default_rng(seed)
+    s = rng.standard_normal((n, 8)) * rng.uniform(1e-3, 30.0, (n, 1)) + rng.uniform(-5, 5, (n, 1))
+    # smooth, constant, step, spike and zero stencils
+    x = np.linspace(0, 1, 8)
+    s[:100] = np.sin(2 * np.pi * x * rng.uniform(0.1, 2, (100, 1)))
+    s[100:200] = rng.uniform(-3, 3, (100, 1))
+    s[200:300] = np.where(x > rng.uniform(0, 1, (100, 1)), 1.0, 0.125)
+    s[300:400] = 0.0
+    s[300:400, 3] = rng.uniform(-1, 1, 100)
+    s[400:500] = 0.0
+    return s
+
+
+def test_weno_p_m_bitexact(oracle, reffn):
+    s = _stencils(300_000, 11)
+    assert np.array_equal(oracle.weno_p(s), reffn.weno_p(s))
+    assert np.array_equal(oracle.weno_m(s), reffn.weno_m(s))
+
+
+def test_weno_mirror(oracle):
+    s = _stencils(50_000, 12)
+    assert np.array_equal(oracle.weno_m(s), oracle.weno_p(s[:, ::-1]))
+
+
+def test_split_bitexact(oracle, reffn):
+    rng = np.random.default_rng(13)
+    n = 50_000
+    pts = np.column_stack([
+        rng.uniform(0.05, 5.0, n), rng.normal(0, 2, n), rng.normal(0, 1, n), rng.normal(0, 1, n),
+        rng.uniform(0.1, 3.0, n), rng.normal(0, 1, (n, 3))])
+    pts[:1000, 5:] = [1.0, 0.0, 0.0]
+    pts[1000:2000, 5:] = [0.0, 1.0, 0.0]
+    for gamma, eps in [(1.4, 1e-6), (1.67, 0.0), (1.3, 0.1)]:
+        fp, fm = oracle.split(pts, gamma, eps)
+        rfp, rfm = reffn.split(pts, gamma, eps)
+        assert np.array_equal(fp, rfp) and np.array_equal(fm, rfm)
+
+
+def _prims(g, seed):
+    rng = np.random.default_rng(seed)
+    shp = (g.nz + 2 * LAP, g.ny + 2 * LAP, g.nx + 2 * LAP)
+    d = rng.uniform(0.5, 2.0, shp)
+    u = rng.normal(0.3, 0.5, shp)
+    v = rng.normal(0, 0.3, shp)
+    w = rng.normal(0, 0.3, shp)
+    T = rng.uniform(0.5, 1.5, shp)
+    return d, u, v, w, T
+
+
+def test_field_kernels_bitexact(oracle, reffn):
+    g = make_grid(13, 9, 7, gamma=1.4, ama=0.8)
+    d, u, v, w, T = _prims(g, 14)
+    f = oracle.prim_to_cons(g, d, u, v, w, T)
+    assert np.array_equal(f, reffn.prim_to_cons(g, d, u, v, w, T))
+    a = oracle.cons_to_prim(g, f)
+    b = reffn.cons_to_prim(g, f)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+    assert np.array_equal(oracle.sound_speed(g, T), reffn.sound_speed(g, T))
+    rng = np.random.default_rng(15)
+    for krk in (1, 2, 3):
+        f0 = rng.normal(size=f.shape)
+        fn = rng.normal(size=f.shape)
+        du = rng.normal(size=f.shape)
+        a1, b1 = f0.copy(), f0.copy()
+        oracle.time_advance(krk, 1.7e-3, a1, fn, du)
+        reffn.time_advance(krk, 1.7e-3, g, b1, fn, du)
+        assert np.array_equal(a1, b1)
+
+
+@pytest.mark.parametrize("general", [False, True])
+def test_du_invis_bitexact(oracle, reffn, general):
+    g = make_grid(19, 11, 9)
+    d, u, v, w, T = _prims(g, 16)
+    cc = oracle.sound_speed(g, T)
+    metrics = ajac = None
+    if general:
+        rng = np.random.default_rng(17)
+        shp = d.shape
+        metrics = [np.ascontiguousarray(rng.uniform(0.5, 1.5, shp) if i % 4 == 0 else
+                                        rng.uniform(-0.3, 0.3, shp)) for i in range(9)]
+        ajac = rng.uniform(0.7, 1.3, shp)
+    a = oracle.du_invis(g, d, u, v, w, cc, metrics, ajac)
+    b = reffn.du_invis(g, d, u, v, w, cc, metrics, ajac)
+    assert np.array_equal(a, b)

@@ -1,0 +1,248 @@
+"""windstencil_b200 -- B200 (sm_100a) BF3W inviscid RHS behind a C ABI.
+
+Python mirror of include/windstencil_b200.h for tests, benchmarks and
+Python callers.  Device memory comes from torch (plumbing only); every
+computation runs in libwindstencil_b200.so, and importing the compute entry
+points fails loudly when the library has not been built.
+
+Reference interface this mirrors (WindStencil, src/):
+  du_invis_Jacobian3d_init  solver/OCFD_NS_Jacobian3d.cpp:24-33   -> du_invis_jacobian3d_init
+  du_invis_Jacobian3d_x     solver/OCFD_NS_Jacobian3d.cpp:133-414 -> du_invis_jacobian3d
+  exchange_boundary_xyz_packed_dev  mpi/OCFD_mpi_dev.cpp:123-290 -> ghost_fill
+  get_duvwT / cons_to_pri_kernel     kernels/commen_kernel.cpp:78-119 -> cons_to_prim
+  pri_to_cons_kernel_warp            kernels/commen_kernel.cpp:33-73  -> prim_to_cons
+  OCFD_time_advance                  solver/OCFD_time.cpp:15-91        -> time_advance
+  NS_solver_real (time loop)         solver/OCFD_NS_Solver.cpp:64-90   -> Solver
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+from ._abi import (FACE_EXTRAP, FACE_PERIODIC, FP64, LAP, MIXED, WsDim3, WsError, WsField,
+                   WsGrid, WsJob, WsMetrics, WsSoa, WsTile, check, header_symbols, last_error,
+                   load)
+
+__all__ = [
+    "FACE_EXTRAP", "FACE_PERIODIC", "FP64", "MIXED", "LAP", "WsError", "Grid", "make_grid",
+    "lap_tensor", "soa_tensor", "field_desc", "soa_desc", "interior_job", "du_invis_jacobian3d",
+    "du_invis_jacobian3d_init", "ghost_fill", "cons_to_prim", "prim_to_cons", "time_advance",
+    "Solver", "load", "header_symbols", "last_error",
+]
+
+
+@dataclass
+class Grid:
+    """Grid and physics constants (ws_grid).  h defaults to 1/(N-1), the
+    reference's convention (OCFD_init.cpp:29-31)."""
+    nx: int
+    ny: int
+    nz: int
+    hx: float | None = None
+    hy: float | None = None
+    hz: float | None = None
+    gamma: float = 1.4
+    ama: float = 1.0
+    epsl_sw: float = 1e-6
+    faces: tuple = (FACE_PERIODIC,) * 6
+    precision: int = FP64
+    metrics_uniform: bool = True
+
+    def __post_init__(self):
+        self.hx = self.hx if self.hx is not None else 1.0 / (self.nx - 1.0)
+        self.hy = self.hy if self.hy is not None else 1.0 / (self.ny - 1.0)
+        self.hz = self.hz if self.hz is not None else 1.0 / (self.nz - 1.0)
+
+    def c(self) -> WsGrid:
+        g = WsGrid()
+        g.nx, g.ny, g.nz, g.lap = self.nx, self.ny, self.nz, LAP
+        g.hx, g.hy, g.hz = self.hx, self.hy, self.hz
+        g.gamma, g.ama, g.epsl_sw = self.gamma, self.ama, self.epsl_sw
+        for i, k in enumerate(self.faces):
+            g.face_kind[i] = int(k)
+        g.precision = int(self.precision)
+        g.metrics_uniform = 1 if self.metrics_uniform else 0
+        return g
+
+    @property
+    def cells(self) -> int:
+        return self.nx * self.ny * self.nz
+
+
+def make_grid(nx, ny, nz, **kw) -> Grid:
+    return Grid(nx, ny, nz, **kw)
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def lap_pitch(nx: int) -> int:
+    return int(load().ws_lap_pitch(nx))
+
+
+def lap_tensor(g: Grid, n: int | None = None, device="cuda", fill=0.0):
+    """LAP field(s): (nz+8, ny+8, pitch) float64, pitch = ws_lap_pitch(nx)."""
+    torch = _torch()
+    shape = (g.nz + 2 * LAP, g.ny + 2 * LAP, lap_pitch(g.nx))
+    if n is not None:
+        shape = (n,) + shape
+    return torch.full(shape, fill, dtype=torch.float64, device=device)
+
+
+def soa_tensor(g: Grid, device="cuda"):
+    torch = _torch()
+    return torch.zeros((5, g.nz, g.ny, g.nx), dtype=torch.float64, device=device)
+
+
+def field_desc(t) -> WsField:
+    """ws_field of a (nz+8, ny+8, pitch) float64 tensor (contiguous rows)."""
+    assert t.dtype.itemsize == 8 and t.dim() == 3 and t.stride(-1) == 1
+    assert t.stride(0) == t.stride(1) * t.shape[1], "planes must be contiguous"
+    return WsField(t.data_ptr(), t.stride(1), 0)
+
+
+def soa_desc(t) -> WsSoa:
+    """ws_soa of a (5, Lz, Ly, pitch) float64 tensor."""
+    assert t.dtype.itemsize == 8 and t.dim() == 4 and t.stride(-1) == 1
+    assert t.stride(1) == t.stride(2) * t.shape[2] and t.stride(0) == t.stride(1) * t.shape[1]
+    return WsSoa(t.data_ptr(), t.stride(2), t.shape[2], t.shape[1], 0)
+
+
+def interior_job(g: Grid) -> WsJob:
+    """The reference's job for the whole interior (OCFD_Stream.cpp:193)."""
+    return WsJob(WsDim3(LAP, LAP, LAP), WsDim3(g.nx + LAP, g.ny + LAP, g.nz + LAP))
+
+
+def _stream(stream):
+    if stream is None:
+        return _torch().cuda.current_stream().cuda_stream
+    return getattr(stream, "cuda_stream", stream)
+
+
+def _metrics(m):
+    if m is None:
+        return None
+    if isinstance(m, WsMetrics):
+        return C.byref(m)
+    mm = WsMetrics(*[field_desc(t) for t in m])   # 10 tensors: akx..asz, ajac
+    return C.byref(mm)
+
+
+def du_invis_jacobian3d_init(g: Grid, job: WsJob, T, cc, stream=None) -> None:
+    gc = g.c()
+    check(load().ws_du_invis_jacobian3d_init(C.byref(gc), job, field_desc(T), field_desc(cc),
+                                             _stream(stream)))
+
+
+def du_invis_jacobian3d(g: Grid, job: WsJob, d, u, v, w, cc, du, metrics=None, tile=None,
+                        stream=None) -> None:
+    """du = BF3W inviscid RHS (ws_du_invis_jacobian3d / _tiled)."""
+    gc = g.c()
+    fs = [field_desc(t) for t in (d, u, v, w, cc)]
+    if metrics is not None:
+        mm = metrics if isinstance(metrics, WsMetrics) else WsMetrics(
+            *[field_desc(t) for t in metrics])
+        mp = C.byref(mm)
+    else:
+        mp = None
+    if tile is None:
+        rc = load().ws_du_invis_jacobian3d(C.byref(gc), job, *fs, mp, soa_desc(du),
+                                           _stream(stream))
+    else:
+        rc = load().ws_du_invis_jacobian3d_tiled(C.byref(gc), job, *fs, mp, soa_desc(du),
+                                                 WsTile(*tile), _stream(stream))
+    check(rc)
+
+
+def ghost_fill(g: Grid, fields, stream=None) -> None:
+    gc = g.c()
+    arr = (WsField * len(fields))(*[field_desc(t) for t in fields])
+    check(load().ws_ghost_fill(C.byref(gc), arr, len(fields), _stream(stream)))
+
+
+def cons_to_prim(g: Grid, f, d, u, v, w, T, P=None, stream=None) -> None:
+    gc = g.c()
+    pd = field_desc(P) if P is not None else WsField(None, 0, 0)
+    check(load().ws_cons_to_prim(C.byref(gc), soa_desc(f), *[field_desc(t) for t in
+                                                              (d, u, v, w, T)], pd,
+                                 _stream(stream)))
+
+
+def prim_to_cons(g: Grid, d, u, v, w, T, f, stream=None) -> None:
+    gc = g.c()
+    check(load().ws_prim_to_cons(C.byref(gc), *[field_desc(t) for t in (d, u, v, w, T)],
+                                 soa_desc(f), _stream(stream)))
+
+
+def time_advance(g: Grid, krk: int, dt: float, f, fn, du, stream=None) -> None:
+    gc = g.c()
+    check(load().ws_time_advance(C.byref(gc), krk, dt, soa_desc(f), soa_desc(fn), soa_desc(du),
+                                 _stream(stream)))
+
+
+class Solver:
+    """One device-resident grid stepped by SSP-RK3 CUDA graphs (ws_solver_*)."""
+
+    def __init__(self, g: Grid):
+        self.g = g
+        self._gc = g.c()
+        h = C.c_void_p()
+        check(load().ws_solver_create(C.byref(self._gc), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            load().ws_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, f_host, stream=None):
+        """f_host: C-contiguous float64 numpy (5, nz, ny, nx)."""
+        import numpy as np
+        a = np.ascontiguousarray(f_host, dtype=np.float64)
+        self._keep = a
+        check(load().ws_solver_set_state(self.h, a.ctypes.data, _stream(stream)))
+
+    def get_state(self, stream=None):
+        import numpy as np
+        out = np.empty((5, self.g.nz, self.g.ny, self.g.nx))
+        check(load().ws_solver_get_state(self.h, out.ctypes.data, _stream(stream)))
+        return out
+
+    def get_rhs(self, stream=None):
+        import numpy as np
+        out = np.empty((5, self.g.nz, self.g.ny, self.g.nx))
+        check(load().ws_solver_get_rhs(self.h, out.ctypes.data, _stream(stream)))
+        return out
+
+    def fields(self):
+        f, du = WsSoa(), WsSoa()
+        prims = (WsField * 6)()
+        check(load().ws_solver_fields(self.h, C.byref(f), C.byref(du), prims))
+        return f, du, list(prims)
+
+    def compute_dt(self, cfl: float, stream=None) -> float:
+        dt = C.c_double()
+        check(load().ws_solver_compute_dt(self.h, cfl, C.byref(dt), _stream(stream)))
+        return dt.value
+
+    def rhs(self, stream=None):
+        check(load().ws_solver_rhs(self.h, _stream(stream)))
+
+    def step(self, dt: float, nsteps: int = 1, stream=None):
+        check(load().ws_solver_step(self.h, dt, nsteps, _stream(stream)))
+
+    def status(self, stream=None) -> int:
+        s = C.c_int()
+        check(load().ws_solver_status(self.h, C.byref(s), _stream(stream)))
+        return s.value
+
+    def set_tile(self, tile):
+        check(load().ws_solver_set_tile(self.h, WsTile(*tile)))

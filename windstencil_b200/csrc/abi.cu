@@ -1,0 +1,231 @@
+// abi.cu -- extern "C" entry points of libwindstencil_b200.so.
+//
+// Argument checking, error reporting and the one-grid solver whose SSP-RK3
+// step is one captured CUDA graph (ghost fill -> RHS -> stage update, three
+// times).  Reference counterparts are named in include/windstencil_b200.h.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "ws_internal.h"
+
+namespace ws {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+int cuda_fail(cudaError_t e, const char* what) {
+    g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? WS_ERR_ALLOC : WS_ERR_CUDA;
+}
+
+namespace {
+
+int check_grid(const ws_grid* g) {
+    if (!g) return fail(WS_ERR_INVALID, "grid is NULL");
+    if (g->lap != WS_LAP) return fail(WS_ERR_INVALID, "grid.lap must be 4");
+    if (g->nx < 4 || g->ny < 4 || g->nz < 4)
+        return fail(WS_ERR_INVALID, "grid extents must be >= 4 in every direction");
+    if (g->nx > (1u << 20) || g->ny > (1u << 20) || g->nz > (1u << 20))
+        return fail(WS_ERR_INVALID, "grid extent too large");
+    if (!(g->hx > 0 && g->hy > 0 && g->hz > 0)) return fail(WS_ERR_INVALID, "h must be > 0");
+    if (!(g->gamma > 1.0) || !(g->ama > 0) || !(g->epsl_sw >= 0))
+        return fail(WS_ERR_INVALID, "need gamma > 1, ama > 0, epsl_sw >= 0");
+    for (int i = 0; i < 6; ++i)
+        if (g->face_kind[i] != WS_FACE_PERIODIC && g->face_kind[i] != WS_FACE_EXTRAP)
+            return fail(WS_ERR_INVALID, "face_kind must be WS_FACE_PERIODIC or WS_FACE_EXTRAP");
+    if (g->precision != WS_FP64 && g->precision != WS_MIXED)
+        return fail(WS_ERR_INVALID, "precision must be WS_FP64 or WS_MIXED");
+    return WS_OK;
+}
+
+int check_field(const ws_grid* g, ws_field f, const char* name) {
+    if (!f.ptr) return fail(WS_ERR_INVALID, std::string(name) + ": NULL pointer");
+    if (f.pitch < g->nx + 8) return fail(WS_ERR_INVALID, std::string(name) + ": pitch < nx+8");
+    if ((reinterpret_cast<uintptr_t>(f.ptr) & 7) != 0)
+        return fail(WS_ERR_INVALID, std::string(name) + ": pointer not 8-byte aligned");
+    return WS_OK;
+}
+
+int check_soa(ws_soa s, uint32_t ex, uint32_t ey, uint32_t ez, const char* name) {
+    if (!s.ptr) return fail(WS_ERR_INVALID, std::string(name) + ": NULL pointer");
+    if (s.pitch < ex || s.length_Y < ey || s.length_Z < ez)
+        return fail(WS_ERR_INVALID, std::string(name) + ": SoA smaller than the job");
+    if ((reinterpret_cast<uintptr_t>(s.ptr) & 7) != 0)
+        return fail(WS_ERR_INVALID, std::string(name) + ": pointer not 8-byte aligned");
+    return WS_OK;
+}
+
+int check_job(const ws_grid* g, ws_job j) {
+    if (j.start.x < 4 || j.start.y < 4 || j.start.z < 4 || j.end.x > g->nx + 4 ||
+        j.end.y > g->ny + 4 || j.end.z > g->nz + 4)
+        return fail(WS_ERR_INVALID, "job must lie inside the interior [4, n+4)");
+    return WS_OK;
+}
+
+bool job_empty(ws_job j) {
+    return j.end.x <= j.start.x || j.end.y <= j.start.y || j.end.z <= j.start.z;
+}
+
+// default tile: the autotuner's choice when present, else configuration 0
+int default_cfg() { return 0; }
+int default_scan(const ws_grid*) { return 32; }
+
+}  // namespace
+
+// Fill RhsArgs and launch; shared by the drop-in entry and the solver.
+int rhs_enqueue(const ws_grid* g, ws_job job, const ws_field prims[5], const ws_metrics* m,
+                ws_soa du, ws_tile tile, cudaStream_t st) {
+    int cfg = default_cfg();
+    if (tile.tile_x || tile.tile_y || tile.threads) {
+        cfg = find_tile_cfg(tile.tile_x, tile.tile_y, tile.threads);
+        if (cfg < 0) return fail(WS_ERR_UNSUPPORTED, "tile shape not compiled in this build");
+    }
+    const TileCfg c = tile_cfg(cfg);
+    const int scan = tile.scan_z > 0 ? tile.scan_z : default_scan(g);
+    RhsArgs a{};
+    for (int i = 0; i < 5; ++i) {
+        a.prim[i] = prims[i].ptr;
+        a.ppitch[i] = prims[i].pitch;
+    }
+    const bool uni = g->metrics_uniform != 0;
+    if (!uni) {
+        const ws_field* mf = &m->akx;
+        for (int i = 0; i < 10; ++i) {
+            a.met[i] = mf[i].ptr;
+            a.mpitch[i] = mf[i].pitch;
+        }
+    }
+    a.du = du.ptr;
+    a.du_pitch = du.pitch;
+    a.du_ly = du.length_Y;
+    a.du_lz = du.length_Z;
+    a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
+    a.sx = job.start.x; a.sy = job.start.y; a.sz = job.start.z;
+    a.ex = job.end.x; a.ey = job.end.y; a.ez = job.end.z;
+    a.ntx = (a.ex - a.sx + c.bx - 1) / c.bx;
+    a.nty = (a.ey - a.sy + c.by - 1) / c.by;
+    a.zc = scan;
+    a.nzc = (a.ez - a.sz + scan - 1) / scan;
+    a.rhx = 1.0 / g->hx; a.rhy = 1.0 / g->hy; a.rhz = 1.0 / g->hz;
+    a.eps2 = g->epsl_sw * g->epsl_sw;
+    a.hrg = 0.5 / g->gamma;
+    a.c1 = 2.0 * (g->gamma - 1.0);
+    a.c3 = (3.0 - g->gamma) / (2.0 * (g->gamma - 1.0));
+    a.gm1 = g->gamma - 1.0;
+    const long nwork = (long)a.ntx * a.nty * a.nzc;
+    int ctas = rhs_max_ctas(g->precision, uni, cfg);
+    if (ctas <= 0) return fail(WS_ERR_CUDA, "cannot size the persistent grid");
+    if (nwork < ctas) ctas = (int)nwork;
+    return launch_rhs(a, g->precision, uni, cfg, ctas, st);
+}
+
+}  // namespace ws
+
+using namespace ws;
+
+// ============================================================================
+extern "C" {
+
+int ws_abi_version(void) { return WS_ABI_VERSION; }
+
+int ws_last_error(char* buf, size_t n) {
+    if (!buf || n == 0) return WS_ERR_INVALID;
+    std::snprintf(buf, n, "%s", g_last_error.c_str());
+    return WS_OK;
+}
+
+uint32_t ws_lap_pitch(uint32_t nx) { return lap_pitch(nx); }
+
+int ws_du_invis_jacobian3d_init(const ws_grid* g, ws_job job, ws_field T, ws_field cc,
+                                ws_stream_t stream) {
+    int rc;
+    if ((rc = check_grid(g))) return rc;
+    if ((rc = check_job(g, job))) return rc;
+    if ((rc = check_field(g, T, "T")) || (rc = check_field(g, cc, "cc"))) return rc;
+    if (job_empty(job)) return WS_OK;
+    return launch_sound_speed(g, job, T, cc, (cudaStream_t)stream);
+}
+
+int ws_du_invis_jacobian3d_tiled(const ws_grid* g, ws_job job, ws_field d, ws_field u,
+                                 ws_field v, ws_field w, ws_field cc,
+                                 const ws_metrics* metrics, ws_soa du, ws_tile tile,
+                                 ws_stream_t stream) {
+    int rc;
+    if ((rc = check_grid(g))) return rc;
+    if ((rc = check_job(g, job))) return rc;
+    const ws_field prims[5] = {d, u, v, w, cc};
+    const char* names[5] = {"d", "u", "v", "w", "cc"};
+    for (int i = 0; i < 5; ++i)
+        if ((rc = check_field(g, prims[i], names[i]))) return rc;
+    if (!g->metrics_uniform) {
+        if (!metrics) return fail(WS_ERR_INVALID, "metrics required when metrics_uniform == 0");
+        const ws_field* mf = &metrics->akx;
+        for (int i = 0; i < 10; ++i)
+            if ((rc = check_field(g, mf[i], "metric field"))) return rc;
+    }
+    if (job_empty(job)) return WS_OK;
+    if ((rc = check_soa(du, job.end.x - job.start.x, job.end.y - job.start.y,
+                        job.end.z - job.start.z, "du")))
+        return rc;
+    return rhs_enqueue(g, job, prims, metrics, du, tile, (cudaStream_t)stream);
+}
+
+int ws_du_invis_jacobian3d(const ws_grid* g, ws_job job, ws_field d, ws_field u, ws_field v,
+                           ws_field w, ws_field cc, const ws_metrics* metrics, ws_soa du,
+                           ws_stream_t stream) {
+    ws_tile t{0, 0, 0, 0};
+    return ws_du_invis_jacobian3d_tiled(g, job, d, u, v, w, cc, metrics, du, t, stream);
+}
+
+int ws_ghost_fill(const ws_grid* g, const ws_field* fields, int nfields, ws_stream_t stream) {
+    int rc;
+    if ((rc = check_grid(g))) return rc;
+    if (!fields || nfields < 1 || nfields > 8)
+        return fail(WS_ERR_INVALID, "ghost fill takes 1..8 fields");
+    for (int i = 0; i < nfields; ++i)
+        if ((rc = check_field(g, fields[i], "field"))) return rc;
+    return launch_ghost_fill(g, fields, nfields, (cudaStream_t)stream);
+}
+
+int ws_cons_to_prim(const ws_grid* g, ws_soa f, ws_field d, ws_field u, ws_field v, ws_field w,
+                    ws_field T, ws_field P, ws_stream_t stream) {
+    int rc;
+    if ((rc = check_grid(g))) return rc;
+    if ((rc = check_soa(f, g->nx, g->ny, g->nz, "f"))) return rc;
+    const ws_field fs[5] = {d, u, v, w, T};
+    for (int i = 0; i < 5; ++i)
+        if ((rc = check_field(g, fs[i], "primitive"))) return rc;
+    if (P.ptr && (rc = check_field(g, P, "P"))) return rc;
+    return launch_cons_to_prim(g, f, d, u, v, w, T, P, nullptr, (cudaStream_t)stream);
+}
+
+int ws_prim_to_cons(const ws_grid* g, ws_field d, ws_field u, ws_field v, ws_field w, ws_field T,
+                    ws_soa f, ws_stream_t stream) {
+    int rc;
+    if ((rc = check_grid(g))) return rc;
+    if ((rc = check_soa(f, g->nx, g->ny, g->nz, "f"))) return rc;
+    const ws_field fs[5] = {d, u, v, w, T};
+    for (int i = 0; i < 5; ++i)
+        if ((rc = check_field(g, fs[i], "primitive"))) return rc;
+    return launch_prim_to_cons(g, d, u, v, w, T, f, (cudaStream_t)stream);
+}
+
+int ws_time_advance(const ws_grid* g, int krk, double dt, ws_soa f, ws_soa fn, ws_soa du,
+                    ws_stream_t stream) {
+    int rc;
+    if ((rc = check_grid(g))) return rc;
+    if (krk < 1 || krk > 3) return fail(WS_ERR_INVALID, "krk must be 1, 2 or 3");
+    if ((rc = check_soa(f, g->nx, g->ny, g->nz, "f")) ||
+        (rc = check_soa(fn, g->nx, g->ny, g->nz, "fn")) ||
+        (rc = check_soa(du, g->nx, g->ny, g->nz, "du")))
+        return rc;
+    return launch_time_advance(g, krk, dt, f, fn, du, (cudaStream_t)stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,318 @@
+// field_kernels.cu -- bandwidth kernels around the RHS: sound speed, ghost
+// fill, prim<->cons, SSP-RK3 stage updates.
+//
+// Reference counterparts:
+//   sound speed    src/kernels/commen_kernel.cpp:145-154 (launched over the
+//                  LAP-extended job by OCFD_NS_Jacobian3d.cpp:24-33)
+//   ghost fill     src/mpi/OCFD_mpi_dev.cpp:123-290 (host-staged periodic
+//                  self-exchange; here an in-place device copy)
+//   cons->prim     src/kernels/commen_kernel.cpp:78-119
+//   prim->cons     src/kernels/commen_kernel.cpp:33-73
+//   RK3 stages     src/solver/OCFD_time.cpp:15-91
+#include "ws_internal.h"
+
+namespace ws {
+
+namespace {
+
+__device__ __forceinline__ size_t lap_idx(int i, int j, int k, uint32_t pitch, int ny) {
+    return (size_t)i + (size_t)pitch * ((size_t)j + (size_t)(ny + 8) * (size_t)k);
+}
+__device__ __forceinline__ size_t soa_idx(int i, int j, int k, int var, const ws_soa& s) {
+    return (size_t)i + (size_t)s.pitch * ((size_t)j + (size_t)s.length_Y *
+                                          ((size_t)k + (size_t)s.length_Z * (size_t)var));
+}
+
+// source interior index of a (possibly ghost) LAP index along one axis
+__device__ __forceinline__ int ghost_src(int i, int n, int lo_kind, int hi_kind) {
+    if (i < 4) return lo_kind == WS_FACE_PERIODIC ? i + n : 4;
+    if (i >= n + 4) return hi_kind == WS_FACE_PERIODIC ? i - n : n + 3;
+    return i;
+}
+
+struct GhostArgs {
+    double* ptr[8];
+    uint32_t pitch[8];
+    int nf;
+    int nx, ny, nz;
+    int kind[6];
+};
+
+// One thread per ghost point (all of the 4-layer shell, edges and corners
+// included): value = interior value at the wrapped / clamped coordinates.
+// Because the source is always an interior point, one launch fills every face.
+__global__ void ghost_fill_kernel(const __grid_constant__ GhostArgs a) {
+    const long px = a.nx + 8, py = a.ny + 8;
+    const long nzs = 8 * px * py;              // z slabs (full xy planes)
+    const long nys = 8 * px * (long)a.nz;      // y slabs, interior z
+    const long nxs = 8 * (long)a.ny * a.nz;    // x slabs, interior y,z
+    const long total = nzs + nys + nxs;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total;
+         t += (long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        if (t < nzs) {
+            const long pl = t / (px * py), r = t - pl * (px * py);
+            k = pl < 4 ? (int)pl : (int)(a.nz + pl);          // 0..3, nz+4..nz+7
+            j = (int)(r / px);
+            i = (int)(r - (long)j * px);
+        } else if (t < nzs + nys) {
+            const long t2 = t - nzs;
+            const long row = t2 / px;
+            i = (int)(t2 - row * px);
+            const int rj = (int)(row % 8);
+            k = 4 + (int)(row / 8);
+            j = rj < 4 ? rj : a.ny + rj;
+        } else {
+            const long t3 = t - nzs - nys;
+            const long line = t3 / 8;
+            const int ri = (int)(t3 - line * 8);
+            i = ri < 4 ? ri : a.nx + ri;
+            j = 4 + (int)(line % a.ny);
+            k = 4 + (int)(line / a.ny);
+        }
+        const int si = ghost_src(i, a.nx, a.kind[0], a.kind[1]);
+        const int sj = ghost_src(j, a.ny, a.kind[2], a.kind[3]);
+        const int sk = ghost_src(k, a.nz, a.kind[4], a.kind[5]);
+        for (int f = 0; f < a.nf; ++f) {
+            double* p = a.ptr[f];
+            p[lap_idx(i, j, k, a.pitch[f], a.ny)] = p[lap_idx(si, sj, sk, a.pitch[f], a.ny)];
+        }
+    }
+}
+
+__global__ void sound_speed_kernel(ws_field T, ws_field cc, int i0, int j0, int k0, int ni,
+                                   int nj, int nk, int ny, double ama) {
+    const long n = (long)ni * nj * nk;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n;
+         t += (long)gridDim.x * blockDim.x) {
+        const int i = i0 + (int)(t % ni);
+        const long r = t / ni;
+        const int j = j0 + (int)(r % nj), k = k0 + (int)(r / nj);
+        cc.ptr[lap_idx(i, j, k, cc.pitch, ny)] = sqrt(T.ptr[lap_idx(i, j, k, T.pitch, ny)]) / ama;
+    }
+}
+
+struct PrimArgs {
+    ws_soa f;
+    ws_field d, u, v, w, T, P;
+    int nx, ny, nz;
+    double cv, gamma;
+    int* status;
+};
+
+__global__ void cons_to_prim_kernel(const __grid_constant__ PrimArgs a) {
+    const long n = (long)a.nx * a.ny * a.nz;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n;
+         t += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % a.nx);
+        const long r = t / a.nx;
+        const int j = (int)(r % a.ny), k = (int)(r / a.ny);
+        const double d1 = a.f.ptr[soa_idx(i, j, k, 0, a.f)];
+        const double u1 = a.f.ptr[soa_idx(i, j, k, 1, a.f)] / d1;
+        const double v1 = a.f.ptr[soa_idx(i, j, k, 2, a.f)] / d1;
+        const double w1 = a.f.ptr[soa_idx(i, j, k, 3, a.f)] / d1;
+        double t1 = a.f.ptr[soa_idx(i, j, k, 4, a.f)];
+        t1 = t1 - 0.5 * d1 * (u1 * u1 + v1 * v1 + w1 * w1);
+        const int I = i + 4, J = j + 4, K = k + 4;
+        a.d.ptr[lap_idx(I, J, K, a.d.pitch, a.ny)] = d1;
+        a.u.ptr[lap_idx(I, J, K, a.u.pitch, a.ny)] = u1;
+        a.v.ptr[lap_idx(I, J, K, a.v.pitch, a.ny)] = v1;
+        a.w.ptr[lap_idx(I, J, K, a.w.pitch, a.ny)] = w1;
+        const double T1 = t1 / (d1 * a.cv);
+        a.T.ptr[lap_idx(I, J, K, a.T.pitch, a.ny)] = T1;
+        if (a.P.ptr) a.P.ptr[lap_idx(I, J, K, a.P.pitch, a.ny)] = (t1 / d1) * (a.gamma - 1.0);
+        if (a.status && !(d1 > 0.0 && T1 > 0.0 && T1 < INFINITY)) atomicOr(a.status, 1);
+    }
+}
+
+__global__ void prim_to_cons_kernel(const __grid_constant__ PrimArgs a) {
+    const long n = (long)a.nx * a.ny * a.nz;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n;
+         t += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % a.nx);
+        const long r = t / a.nx;
+        const int j = (int)(r % a.ny), k = (int)(r / a.ny);
+        const int I = i + 4, J = j + 4, K = k + 4;
+        const double d1 = a.d.ptr[lap_idx(I, J, K, a.d.pitch, a.ny)];
+        const double u1 = a.u.ptr[lap_idx(I, J, K, a.u.pitch, a.ny)];
+        const double v1 = a.v.ptr[lap_idx(I, J, K, a.v.pitch, a.ny)];
+        const double w1 = a.w.ptr[lap_idx(I, J, K, a.w.pitch, a.ny)];
+        const double T1 = a.T.ptr[lap_idx(I, J, K, a.T.pitch, a.ny)];
+        a.f.ptr[soa_idx(i, j, k, 0, a.f)] = d1;
+        a.f.ptr[soa_idx(i, j, k, 1, a.f)] = u1 * d1;
+        a.f.ptr[soa_idx(i, j, k, 2, a.f)] = v1 * d1;
+        a.f.ptr[soa_idx(i, j, k, 3, a.f)] = w1 * d1;
+        a.f.ptr[soa_idx(i, j, k, 4, a.f)] = d1 * ((u1 * u1 + v1 * v1 + w1 * w1) * 0.5 + a.cv * T1);
+    }
+}
+
+// RK3 stage coefficients, OCFD_time.cpp:15-65: f = a*fn + b*(f + dt*du),
+// stage 1 f = fn + dt*du.
+__device__ __forceinline__ double rk_stage(int krk, double fn, double f, double du, double dt) {
+    if (krk == 1) return fn + dt * du;
+    if (krk == 2) return (3.0 / 4.0) * fn + (1.0 / 4.0) * (f + dt * du);
+    return (1.0 / 3.0) * fn + (2.0 / 3.0) * (f + dt * du);
+}
+
+struct StageArgs {
+    ws_soa f, fn, du;
+    int nx, ny, nz, krk;
+    double dt;
+};
+
+__global__ void time_advance_kernel(const __grid_constant__ StageArgs a) {
+    const long n = (long)a.nx * a.ny * a.nz;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n;
+         t += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % a.nx);
+        const long r = t / a.nx;
+        const int j = (int)(r % a.ny), k = (int)(r / a.ny);
+#pragma unroll
+        for (int var = 0; var < 5; ++var) {
+            const size_t p = soa_idx(i, j, k, var, a.f);
+            const double fo = a.f.ptr[p];
+            const double fnv = a.fn.ptr[soa_idx(i, j, k, var, a.fn)];
+            const double duv = a.du.ptr[soa_idx(i, j, k, var, a.du)];
+            a.f.ptr[p] = rk_stage(a.krk, fnv, fo, duv, a.dt);
+        }
+    }
+}
+
+// Stage update fused with cons->prim and the interior sound speed.
+struct StagePrimArgs {
+    StageArgs s;
+    ws_field d, u, v, w, T, cc;
+    double cv, ama;
+    int* status;
+};
+
+__global__ void stage_update_kernel(const __grid_constant__ StagePrimArgs a) {
+    const int nx = a.s.nx, ny = a.s.ny, nz = a.s.nz;
+    const long n = (long)nx * ny * nz;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n;
+         t += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % nx);
+        const long r = t / nx;
+        const int j = (int)(r % ny), k = (int)(r / ny);
+        double q[5];
+#pragma unroll
+        for (int var = 0; var < 5; ++var) {
+            const size_t p = soa_idx(i, j, k, var, a.s.f);
+            const double fo = a.s.f.ptr[p];
+            const double fnv = a.s.fn.ptr[soa_idx(i, j, k, var, a.s.fn)];
+            const double duv = a.s.du.ptr[soa_idx(i, j, k, var, a.s.du)];
+            q[var] = rk_stage(a.s.krk, fnv, fo, duv, a.s.dt);
+            a.s.f.ptr[p] = q[var];
+        }
+        const double d1 = q[0];
+        const double u1 = q[1] / d1, v1 = q[2] / d1, w1 = q[3] / d1;
+        const double t1 = q[4] - 0.5 * d1 * (u1 * u1 + v1 * v1 + w1 * w1);
+        const double T1 = t1 / (d1 * a.cv);
+        const int I = i + 4, J = j + 4, K = k + 4;
+        a.d.ptr[lap_idx(I, J, K, a.d.pitch, ny)] = d1;
+        a.u.ptr[lap_idx(I, J, K, a.u.pitch, ny)] = u1;
+        a.v.ptr[lap_idx(I, J, K, a.v.pitch, ny)] = v1;
+        a.w.ptr[lap_idx(I, J, K, a.w.pitch, ny)] = w1;
+        a.T.ptr[lap_idx(I, J, K, a.T.pitch, ny)] = T1;
+        a.cc.ptr[lap_idx(I, J, K, a.cc.pitch, ny)] = sqrt(T1) / a.ama;
+        if (a.status && !(d1 > 0.0 && T1 > 0.0 && T1 < INFINITY)) atomicOr(a.status, 1);
+    }
+}
+
+int grid_for(long n, int threads) {
+    long b = (n + threads - 1) / threads;
+    const long cap = 148L * 16;
+    if (b > cap) b = cap;
+    return (int)(b < 1 ? 1 : b);
+}
+
+}  // namespace
+
+int launch_ghost_fill(const ws_grid* g, const ws_field* f, int nf, cudaStream_t st) {
+    if (nf < 1 || nf > 8) return fail(WS_ERR_INVALID, "ghost fill: 1..8 fields");
+    GhostArgs a{};
+    for (int i = 0; i < nf; ++i) {
+        a.ptr[i] = f[i].ptr;
+        a.pitch[i] = f[i].pitch;
+    }
+    a.nf = nf;
+    a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
+    for (int i = 0; i < 6; ++i) a.kind[i] = g->face_kind[i];
+    const long px = g->nx + 8, py = g->ny + 8;
+    const long total = 8 * px * py + 8 * px * (long)g->nz + 8 * (long)g->ny * g->nz;
+    ghost_fill_kernel<<<grid_for(total, 256), 256, 0, st>>>(a);
+    WS_CUDA(cudaGetLastError());
+    return WS_OK;
+}
+
+int launch_sound_speed(const ws_grid* g, ws_job job, ws_field T, ws_field cc, cudaStream_t st) {
+    const int i0 = (int)job.start.x - 4, j0 = (int)job.start.y - 4, k0 = (int)job.start.z - 4;
+    const int ni = (int)(job.end.x - job.start.x) + 8, nj = (int)(job.end.y - job.start.y) + 8,
+              nk = (int)(job.end.z - job.start.z) + 8;
+    const long n = (long)ni * nj * nk;
+    sound_speed_kernel<<<grid_for(n, 256), 256, 0, st>>>(T, cc, i0, j0, k0, ni, nj, nk, g->ny,
+                                                          g->ama);
+    WS_CUDA(cudaGetLastError());
+    return WS_OK;
+}
+
+int launch_cons_to_prim(const ws_grid* g, ws_soa f, ws_field d, ws_field u, ws_field v,
+                        ws_field w, ws_field T, ws_field P, int* status, cudaStream_t st) {
+    PrimArgs a{};
+    a.f = f; a.d = d; a.u = u; a.v = v; a.w = w; a.T = T; a.P = P;
+    a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
+    a.cv = 1.0 / (g->gamma * (g->gamma - 1.0) * g->ama * g->ama);
+    a.gamma = g->gamma;
+    a.status = status;
+    cons_to_prim_kernel<<<grid_for((long)g->nx * g->ny * g->nz, 256), 256, 0, st>>>(a);
+    WS_CUDA(cudaGetLastError());
+    return WS_OK;
+}
+
+int launch_prim_to_cons(const ws_grid* g, ws_field d, ws_field u, ws_field v, ws_field w,
+                        ws_field T, ws_soa f, cudaStream_t st) {
+    PrimArgs a{};
+    a.f = f; a.d = d; a.u = u; a.v = v; a.w = w; a.T = T;
+    a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
+    a.cv = 1.0 / (g->gamma * (g->gamma - 1.0) * g->ama * g->ama);
+    a.gamma = g->gamma;
+    prim_to_cons_kernel<<<grid_for((long)g->nx * g->ny * g->nz, 256), 256, 0, st>>>(a);
+    WS_CUDA(cudaGetLastError());
+    return WS_OK;
+}
+
+int launch_time_advance(const ws_grid* g, int krk, double dt, ws_soa f, ws_soa fn, ws_soa du,
+                        cudaStream_t st) {
+    StageArgs a{};
+    a.f = f; a.fn = fn; a.du = du;
+    a.nx = g->nx; a.ny = g->ny; a.nz = g->nz; a.krk = krk; a.dt = dt;
+    time_advance_kernel<<<grid_for((long)g->nx * g->ny * g->nz, 256), 256, 0, st>>>(a);
+    WS_CUDA(cudaGetLastError());
+    return WS_OK;
+}
+
+int launch_stage_update(const ws_grid* g, int krk, double dt, ws_soa f, ws_soa fn, ws_soa du,
+                        const ws_field prims[6], int* status, cudaStream_t st) {
+    StagePrimArgs a{};
+    a.s.f = f; a.s.fn = fn; a.s.du = du;
+    a.s.nx = g->nx; a.s.ny = g->ny; a.s.nz = g->nz; a.s.krk = krk; a.s.dt = dt;
+    a.d = prims[0]; a.u = prims[1]; a.v = prims[2]; a.w = prims[3]; a.T = prims[4];
+    a.cc = prims[5];
+    a.cv = 1.0 / (g->gamma * (g->gamma - 1.0) * g->ama * g->ama);
+    a.ama = g->ama;
+    a.status = status;
+    stage_update_kernel<<<grid_for((long)g->nx * g->ny * g->nz, 256), 256, 0, st>>>(a);
+    WS_CUDA(cudaGetLastError());
+    return WS_OK;
+}
+
+int launch_ghost_fill_prims(const ws_grid* g, const ws_field prims[6], cudaStream_t st) {
+    return launch_ghost_fill(g, prims, 6, st);
+}
+
+uint32_t lap_pitch(uint32_t nx) {
+    // rows padded to a multiple of 32 doubles (256 B)
+    return ((nx + 8 + 31) / 32) * 32;
+}
+
+}  // namespace ws
