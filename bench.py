@@ -49,7 +49,7 @@ BYTES_PER_CELL = 80.0       # 5 FP64 primitives in + 5 FP64 du out (Cartesian me
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nx", type=int, default=600)
@@ -82,7 +82,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
@@ -281,7 +281,7 @@ def run_ours(a, rank, world, dist):
         host.copy_(torch.from_numpy(f0))
         hp = host.numpy()
         ptr = hp.ctypes.data
-        n_e2e = max(2, min(a.steps, 5))
+        n_e2e = max(2, min(a.steps, 10))
         for _ in range(1):
             ws._abi.check(lib.ws_solver_set_state(s.h, ptr, stream.cuda_stream))
             s.step(dt, 1, stream=stream)

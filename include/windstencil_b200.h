@@ -111,8 +111,10 @@ typedef struct ws_metrics {
     ws_field ajac;            /* Jacobian J    */
 } ws_metrics;
 
-/* Kernel tile shape: (tile_x x tile_y) columns swept along z in chunks of
- * scan_z planes; threads per CTA.  Zeroes select the tuned default. */
+/* Kernel tile shape: a CTA of `threads` threads owns tile_x x tile_y columns
+ * and sweeps them along z; scan_z caps the planes of one sweep (0: no cap,
+ * each persistent CTA sweeps its whole share of planes).  Zeroes in tile_x,
+ * tile_y, threads select the tuned default. */
 typedef struct ws_tile {
     int32_t tile_x, tile_y, scan_z, threads;
 } ws_tile;
@@ -123,8 +125,14 @@ typedef struct ws_tile {
 WS_API int  ws_abi_version(void);
 /* Copies the message of the last failure on this thread (NUL-terminated). */
 WS_API int  ws_last_error(char* buf, size_t n);
-/* Bytes of the LAP-field pitch this library allocates for extent nx+8. */
+/* Elements of the LAP-field row pitch this library allocates for extent nx+8
+ * (a multiple of 32). */
 WS_API uint32_t ws_lap_pitch(uint32_t nx);
+/* Attainable FMA throughput of the current device in TFLOP/s (independent
+ * FMA chains on every SM; the roofline denominator of the RHS kernels).
+ * Synchronises `stream`.  No reference counterpart (measurement utility). */
+WS_API int ws_probe_fp64_peak(double* tflops, ws_stream_t stream);
+WS_API int ws_probe_fp32_peak(double* tflops, ws_stream_t stream);
 
 /* ------------------------------------------------------------------------ */
 /* Drop-in kernels (explicit arguments)                                      */

@@ -74,7 +74,8 @@ bool job_empty(ws_job j) {
 
 // default tile: the autotuner's choice when present, else configuration 0
 int default_cfg() { return 0; }
-int default_scan(const ws_grid*) { return 32; }
+// sweep length cap: unlimited (each persistent CTA sweeps its whole share)
+int default_scan(const ws_grid*) { return 1 << 30; }
 
 }  // namespace
 

@@ -9,10 +9,11 @@
 //           OCFD_NS_Jacobian3d.cpp:251);
 //   WENO  : src/kernels/OCFD_Schemes.cpp:306-368 (P) and :491-553 (M); the M
 //           form equals the P form on the reversed stencil.
-// The FP64 code keeps the reference's terms; it lets the compiler contract
-// multiply-adds and reassociates two products (the leave-one-out weight
-// products and the P+M face sum), which changes results at the 1e-16 level
-// only.  Parity with the reference is 1e-12 relative (tests/test_gpu_parity.py).
+// The split keeps the reference's terms.  The WENO is an exact algebraic
+// rewrite on stencil differences (below); with FMA contraction and the shared
+// P/M division the results differ from the reference's evaluation order at
+// the 1e-15 level only.  Parity with the reference is 1e-12 relative
+// (tests/test_gpu_parity.py).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -114,90 +115,93 @@ __device__ __forceinline__ void sw_split_gen(T d, T u, T v, T w, T c, T a1, T a2
 
 // ---------------------------------------------------------------------------
 // WENO7-SYMBO face value from t[0..7] = points i-3..i+4 (P orientation),
-// returned as numerator/denominator so that the caller can combine the P and
-// M faces with one division.  FP64: the reference's product weights
-// w_k = d_k * prod_{j != k}(eps + beta_j), formed with shared partial
-// products.  FP32: the equivalent normalised weights d_k / (eps + beta_k),
-// which cannot overflow the FP32 range the way a product of four indicators
-// can.
+// evaluated on the first, second and third differences of the stencil:
+//   D_j = t_{j+1}-t_j,  S_j = D_{j+1}-D_j,  T_j = S_{j+1}-S_j.
+// In these variables the reference's three derivative rounds of candidate k
+// are a 3-term first-difference form r_k, 6 x a 1-2 term second-difference
+// form s_k, and 6 x T_k, so (all indicators divided by 720, eps likewise)
+//   beta_k/720 = r_k^2 + 39 s_k^2 + 39.05 T_k^2
+// and, because each candidate's coefficients sum to 12,
+//   q_k = 12 t_3 + l_k(D),   face = t_3 + sum w_k l_k / (12 sum w_k).
+// Both are exact algebraic rewrites of OCFD_Schemes.cpp:306-368; they remove
+// about a fifth of the FP64 operations and agree with the reference form to
+// ~1e-15 relative.  The result is returned as t_3 + num/den so that the P and
+// M faces of one flux can share a single division.
+// FP64: the reference's product weights w_k = d_k * prod_{j != k}(eps + beta_j)
+// from shared partial products.  FP32 (mixed form): the equivalent normalised
+// weights d_k / (eps + beta_k), which cannot overflow the FP32 range the way a
+// product of four indicators can.
 // ---------------------------------------------------------------------------
+template <typename T>
+struct WenoDiffs {
+    T D0, D1, D2, D3, D4, D5, D6;
+    T b0, b1, b2, b3, b4;
+};
+
+template <typename T>
+__device__ __forceinline__ void weno7_indicators(const T t[8], WenoDiffs<T>& o) {
+    o.D0 = t[1] - t[0]; o.D1 = t[2] - t[1]; o.D2 = t[3] - t[2]; o.D3 = t[4] - t[3];
+    o.D4 = t[5] - t[4]; o.D5 = t[6] - t[5]; o.D6 = t[7] - t[6];
+    const T S0 = o.D1 - o.D0, S1 = o.D2 - o.D1, S2 = o.D3 - o.D2, S3 = o.D4 - o.D3;
+    const T S4 = o.D5 - o.D4, S5 = o.D6 - o.D5;
+    const T T0 = S1 - S0, T1 = S2 - S1, T2 = S3 - S2, T3 = S4 - S3, T4 = S5 - S4;
+    const T c2 = T(39.0), c3 = T(39.05);
+    T r, s;
+    r = T(2) * o.D0 - T(7) * o.D1 + T(11) * o.D2;    s = T(2) * S1 - S0;
+    o.b0 = (c3 * T0) * T0 + ((c2 * s) * s + r * r);
+    r = T(5) * o.D2 - o.D1 + T(2) * o.D3;            s = S2;
+    o.b1 = (c3 * T1) * T1 + ((c2 * s) * s + r * r);
+    r = T(2) * o.D2 + T(5) * o.D3 - o.D4;            s = S3;
+    o.b2 = (c3 * T2) * T2 + ((c2 * s) * s + r * r);
+    r = T(11) * o.D3 - T(7) * o.D4 + T(2) * o.D5;    s = T(2) * S3 - S4;
+    o.b3 = (c3 * T3) * T3 + ((c2 * s) * s + r * r);
+    r = T(26) * o.D4 - T(31) * o.D5 + T(11) * o.D6;  s = T(3) * S4 - T(2) * S5;
+    o.b4 = (c3 * T4) * T4 + ((c2 * s) * s + r * r);
+}
+
+template <typename T>
+__device__ __forceinline__ void weno7_candidates(const WenoDiffs<T>& o, T w0, T w1, T w2, T w3,
+                                                 T w4, T& num, T& den) {
+    const T l0 = T(3) * o.D0 - T(10) * o.D1 + T(13) * o.D2;
+    const T l1 = T(4) * o.D2 - o.D1 + T(3) * o.D3;
+    const T l2 = o.D2 + T(6) * o.D3 - o.D4;
+    const T l3 = T(9) * o.D3 - T(4) * o.D4 + o.D5;
+    const T l4 = T(12) * o.D3 - T(13) * o.D4 + T(10) * o.D5 - T(3) * o.D6;
+    num = w0 * l0 + w1 * l1 + w2 * l2 + w3 * l3 + w4 * l4;
+    den = T(12) * (w0 + w1 + w2 + w3 + w4);
+}
+
+// face value = t[3] + num/den
 template <typename T>
 __device__ __forceinline__ void weno7_symbo_nd(const T t[8], T& num, T& den);
 
 template <>
 __device__ __forceinline__ void weno7_symbo_nd<double>(const double t[8], double& num,
                                                        double& den) {
-    double q, b0, b1, b2, b3, b4;
-    q = -2.0 * t[0] + 9.0 * t[1] - 18.0 * t[2] + 11.0 * t[3];   b0 = 720.0 * q * q;
-    q = t[1] - 6.0 * t[2] + 3.0 * t[3] + 2.0 * t[4];             b1 = 720.0 * q * q;
-    q = -2.0 * t[2] - 3.0 * t[3] + 6.0 * t[4] - t[5];            b2 = 720.0 * q * q;
-    q = -11.0 * t[3] + 18.0 * t[4] - 9.0 * t[5] + 2.0 * t[6];    b3 = 720.0 * q * q;
-    q = -26.0 * t[4] + 57.0 * t[5] - 42.0 * t[6] + 11.0 * t[7]; b4 = 720.0 * q * q;
-    q = -6.0 * t[0] + 24.0 * t[1] - 30.0 * t[2] + 12.0 * t[3];  b0 += 780.0 * q * q;
-    q = 6.0 * t[2] - 12.0 * t[3] + 6.0 * t[4];                   b1 += 780.0 * q * q;
-    q = 6.0 * t[3] - 12.0 * t[4] + 6.0 * t[5];                   b2 += 780.0 * q * q;
-    q = 12.0 * t[3] - 30.0 * t[4] + 24.0 * t[5] - 6.0 * t[6];    b3 += 780.0 * q * q;
-    q = 18.0 * t[4] - 48.0 * t[5] + 42.0 * t[6] - 12.0 * t[7];   b4 += 780.0 * q * q;
-    q = -6.0 * t[0] + 18.0 * (t[1] - t[2]) + 6.0 * t[3];         b0 += 781.0 * q * q;
-    q = -6.0 * t[1] + 18.0 * (t[2] - t[3]) + 6.0 * t[4];         b1 += 781.0 * q * q;
-    q = -6.0 * t[2] + 18.0 * (t[3] - t[4]) + 6.0 * t[5];         b2 += 781.0 * q * q;
-    q = -6.0 * t[3] + 18.0 * (t[4] - t[5]) + 6.0 * t[6];         b3 += 781.0 * q * q;
-    q = -6.0 * t[4] + 18.0 * (t[5] - t[6]) + 6.0 * t[7];         b4 += 781.0 * q * q;
-    b4 = fmax(fmax(fmax(b0, b1), fmax(b2, b3)), b4);
-    const double e = 2.592e-6;
-    const double e0 = e + b0, e1 = e + b1, e2 = e + b2, e3 = e + b3, e4 = e + b4;
-    // leave-one-out products from prefix / suffix partial products
+    WenoDiffs<double> o;
+    weno7_indicators<double>(t, o);
+    const double b4 = fmax(fmax(fmax(o.b0, o.b1), fmax(o.b2, o.b3)), o.b4);
+    const double e = 2.592e-6 / 720.0;
+    const double e0 = e + o.b0, e1 = e + o.b1, e2 = e + o.b2, e3 = e + o.b3, e4 = e + b4;
     const double p01 = e0 * e1, p34 = e3 * e4;
     const double p012 = p01 * e2, p234 = e2 * p34;
-    const double w0 = 0.0401954833730 * (e1 * p234);
-    const double w1 = 0.2493800006710 * (e0 * p234);
-    const double w2 = 0.4802686256260 * (p01 * p34);
-    const double w3 = 0.2009775476730 * (p012 * e4);
-    const double w4 = 0.0291783426580 * (p012 * e3);
-    double acc;
-    q = -3.0 * t[0] + 13.0 * t[1] - 23.0 * t[2] + 25.0 * t[3];  acc = w0 * q;
-    q = t[1] - 5.0 * t[2] + 13.0 * t[3] + 3.0 * t[4];            acc += w1 * q;
-    q = -t[2] + 7.0 * t[3] + 7.0 * t[4] - t[5];                  acc += w2 * q;
-    q = 3.0 * t[3] + 13.0 * t[4] - 5.0 * t[5] + t[6];            acc += w3 * q;
-    q = 25.0 * t[4] - 23.0 * t[5] + 13.0 * t[6] - 3.0 * t[7];    acc += w4 * q;
-    num = acc;
-    den = 12.0 * (w0 + w1 + w2 + w3 + w4);
+    weno7_candidates<double>(o, 0.0401954833730 * (e1 * p234), 0.2493800006710 * (e0 * p234),
+                             0.4802686256260 * (p01 * p34), 0.2009775476730 * (p012 * e4),
+                             0.0291783426580 * (p012 * e3), num, den);
 }
 
 template <>
 __device__ __forceinline__ void weno7_symbo_nd<float>(const float t[8], float& num,
                                                       float& den) {
-    float q, b0, b1, b2, b3, b4;
-    q = -2.0f * t[0] + 9.0f * t[1] - 18.0f * t[2] + 11.0f * t[3];   b0 = 720.0f * q * q;
-    q = t[1] - 6.0f * t[2] + 3.0f * t[3] + 2.0f * t[4];              b1 = 720.0f * q * q;
-    q = -2.0f * t[2] - 3.0f * t[3] + 6.0f * t[4] - t[5];             b2 = 720.0f * q * q;
-    q = -11.0f * t[3] + 18.0f * t[4] - 9.0f * t[5] + 2.0f * t[6];    b3 = 720.0f * q * q;
-    q = -26.0f * t[4] + 57.0f * t[5] - 42.0f * t[6] + 11.0f * t[7]; b4 = 720.0f * q * q;
-    q = -6.0f * t[0] + 24.0f * t[1] - 30.0f * t[2] + 12.0f * t[3];  b0 += 780.0f * q * q;
-    q = 6.0f * t[2] - 12.0f * t[3] + 6.0f * t[4];                    b1 += 780.0f * q * q;
-    q = 6.0f * t[3] - 12.0f * t[4] + 6.0f * t[5];                    b2 += 780.0f * q * q;
-    q = 12.0f * t[3] - 30.0f * t[4] + 24.0f * t[5] - 6.0f * t[6];   b3 += 780.0f * q * q;
-    q = 18.0f * t[4] - 48.0f * t[5] + 42.0f * t[6] - 12.0f * t[7];  b4 += 780.0f * q * q;
-    q = -6.0f * t[0] + 18.0f * (t[1] - t[2]) + 6.0f * t[3];         b0 += 781.0f * q * q;
-    q = -6.0f * t[1] + 18.0f * (t[2] - t[3]) + 6.0f * t[4];         b1 += 781.0f * q * q;
-    q = -6.0f * t[2] + 18.0f * (t[3] - t[4]) + 6.0f * t[5];         b2 += 781.0f * q * q;
-    q = -6.0f * t[3] + 18.0f * (t[4] - t[5]) + 6.0f * t[6];         b3 += 781.0f * q * q;
-    q = -6.0f * t[4] + 18.0f * (t[5] - t[6]) + 6.0f * t[7];         b4 += 781.0f * q * q;
-    b4 = fmaxf(fmaxf(fmaxf(b0, b1), fmaxf(b2, b3)), b4);
-    const float e = 2.592e-6f;
-    const float w0 = __fdividef(0.0401954833730f, e + b0);
-    const float w1 = __fdividef(0.2493800006710f, e + b1);
-    const float w2 = __fdividef(0.4802686256260f, e + b2);
-    const float w3 = __fdividef(0.2009775476730f, e + b3);
-    const float w4 = __fdividef(0.0291783426580f, e + b4);
-    float acc;
-    q = -3.0f * t[0] + 13.0f * t[1] - 23.0f * t[2] + 25.0f * t[3];  acc = w0 * q;
-    q = t[1] - 5.0f * t[2] + 13.0f * t[3] + 3.0f * t[4];             acc += w1 * q;
-    q = -t[2] + 7.0f * t[3] + 7.0f * t[4] - t[5];                    acc += w2 * q;
-    q = 3.0f * t[3] + 13.0f * t[4] - 5.0f * t[5] + t[6];             acc += w3 * q;
-    q = 25.0f * t[4] - 23.0f * t[5] + 13.0f * t[6] - 3.0f * t[7];    acc += w4 * q;
-    num = acc;
-    den = 12.0f * (w0 + w1 + w2 + w3 + w4);
+    WenoDiffs<float> o;
+    weno7_indicators<float>(t, o);
+    const float b4 = fmaxf(fmaxf(fmaxf(o.b0, o.b1), fmaxf(o.b2, o.b3)), o.b4);
+    const float e = 2.592e-6f / 720.0f;
+    weno7_candidates<float>(o, __fdividef(0.0401954833730f, e + o.b0),
+                            __fdividef(0.2493800006710f, e + o.b1),
+                            __fdividef(0.4802686256260f, e + o.b2),
+                            __fdividef(0.2009775476730f, e + o.b3),
+                            __fdividef(0.0291783426580f, e + b4), num, den);
 }
 
 // ---------------------------------------------------------------------------
