@@ -3,6 +3,7 @@
 // Argument checking, error reporting and the one-grid solver whose SSP-RK3
 // step is one captured CUDA graph (ghost fill -> RHS -> stage update, three
 // times).  Reference counterparts are named in include/windstencil_b200.h.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -119,10 +120,14 @@ int rhs_enqueue(const ws_grid* g, ws_job job, const ws_field prims[5], const ws_
     a.c1 = 2.0 * (g->gamma - 1.0);
     a.c3 = (3.0 - g->gamma) / (2.0 * (g->gamma - 1.0));
     a.gm1 = g->gamma - 1.0;
-    const long nwork = (long)a.ntx * a.nty * a.nzc;
+    // persistent grid: one CTA per resident slot, but no more than keeps
+    // every CTA at >= 16 planes of work once the tile columns run out
+    const long ntile = (long)a.ntx * a.nty;
+    const long planes = ntile * (a.ez - a.sz);
     int ctas = rhs_max_ctas(g->precision, uni, cfg);
     if (ctas <= 0) return fail(WS_ERR_CUDA, "cannot size the persistent grid");
-    if (nwork < ctas) ctas = (int)nwork;
+    const long want = ntile >= ctas ? ctas : std::max(ntile, planes / 16);
+    if (want < ctas) ctas = (int)std::max(1L, want);
     return launch_rhs(a, g->precision, uni, cfg, ctas, st);
 }
 

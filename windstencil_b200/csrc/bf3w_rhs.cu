@@ -25,10 +25,13 @@
 //   * Primitive planes are staged with cp.async, double-buffered one plane
 //     ahead: the buffer of plane z holds its (BX+8) x (BY+8) box and the
 //     BX x BY centre of plane z+5.
-//   * Persistent grid, one CTA per SM; the linearised (tile, plane) space of
-//     the job is cut into equal contiguous ranges, one per CTA, so every CTA
-//     gets the same number of planes (a range that crosses a tile boundary
-//     starts a new sweep with its own 9-plane prologue).
+//   * Persistent grid, one CTA per SM.  Whole tile columns are swept round
+//     robin (CTA b takes tiles b, b+G, ...), so the CTAs resident together
+//     sweep neighbouring columns at the same z and their halo re-reads hit
+//     L2; the (tile, plane) space of the tiles left over is then cut into
+//     equal contiguous ranges, one per CTA, so every CTA ends with the same
+//     number of planes (a range that crosses a tile boundary starts a new
+//     sweep with its own 9-plane prologue).
 //   * No tensor cores: nothing on this path is a contraction.  The bound is
 //     the FP64 pipe (7266 algorithmic FLOP per cell).
 #include <cstdio>
@@ -108,20 +111,19 @@ __device__ __forceinline__ double face_flux<double>(const double* bp, int pmoff,
     return (p3 + m3) + (np * dm + nm * dp) / (dp * dm);
 }
 
+// mixed form: P and M in the two lanes of packed FP32x2 arithmetic; the face
+// value is summed in FP32 and widened once (the face difference is FP64)
 template <>
 __device__ __forceinline__ double face_flux<float>(const float* bp, int pmoff, int stride,
                                                    int kw, int wrap) {
-    float t[8], np, dp, nm, dm;
+    float2 t[8], n, d;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) t[k] = bp[k * stride - (k >= kw ? wrap : 0)];
-    weno7_symbo_nd<float>(t, np, dp);
-    const float p3 = t[3];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) t[k] = bp[pmoff + (7 - k) * stride - ((7 - k) >= kw ? wrap : 0)];
-    weno7_symbo_nd<float>(t, nm, dm);
-    const float m3 = t[3];
-    return ((double)p3 + (double)m3) +
-           ((double)__fdividef(np, dp) + (double)__fdividef(nm, dm));
+    for (int k = 0; k < 8; ++k)
+        t[k] = make_float2(bp[k * stride - (k >= kw ? wrap : 0)],
+                           bp[pmoff + (7 - k) * stride - ((7 - k) >= kw ? wrap : 0)]);
+    weno7_symbo_pm_f32x2(t, n, d);
+    const float q = (n.x * d.y + n.y * d.x) * rcp_approx(d.x * d.y);
+    return (double)((t[3].x + t[3].y) + q);
 }
 
 // cp.async the primitive box of plane z (x: x0-4..x0+BX+3, y: y0-4..y0+BY+3)
@@ -302,18 +304,29 @@ template <int BX, int BY, int NT, bool UNI, typename CT>
 __global__ void __launch_bounds__(NT, 1) bf3w_rhs_kernel(const __grid_constant__ RhsArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const SplitK<CT> k = {CT(a.eps2), CT(a.hrg), CT(a.c1), CT(a.c3), CT(a.gm1)};
+    const int G = gridDim.x, b = blockIdx.x;
     const long nzj = a.ez - a.sz;
-    const long total = (long)a.ntx * a.nty * nzj;
-    const long lo = total * blockIdx.x / gridDim.x;
-    const long hi = total * (blockIdx.x + 1) / gridDim.x;
+    const int ntile = a.ntx * a.nty;
+    // 1) whole-column sweeps, round robin: the CTAs running together sweep
+    //    neighbouring tiles at the same z, so the halo re-reads hit L2
+    const int full = ntile / G;
+    for (int r = 0; r < full; ++r) {
+        const int tile = b + r * G;
+        const int x0 = a.sx + (tile % a.ntx) * BX, y0 = a.sy + (tile / a.ntx) * BY;
+        for (int z = a.sz; z < a.ez; z += a.zc)
+            sweep<BX, BY, NT, UNI, CT>(a, k, smem_raw, x0, y0, z, min(z + a.zc, a.ez));
+    }
+    // 2) the remaining tiles' (tile, plane) space cut into equal ranges
+    const long total = (long)(ntile - full * G) * nzj;
+    const long lo = total * b / G, hi = total * (b + 1) / G;
     long pos = lo;
     while (pos < hi) {
-        const long tile = pos / nzj;
-        const int zoff = (int)(pos - tile * nzj);
+        const long tr = pos / nzj;
+        const int zoff = (int)(pos - tr * nzj);
         const int len = (int)min(min(nzj - zoff, hi - pos), (long)a.zc);
-        const int tx = (int)(tile % a.ntx), ty = (int)(tile / a.ntx);
-        sweep<BX, BY, NT, UNI, CT>(a, k, smem_raw, a.sx + tx * BX, a.sy + ty * BY, a.sz + zoff,
-                                   a.sz + zoff + len);
+        const int tile = full * G + (int)tr;
+        sweep<BX, BY, NT, UNI, CT>(a, k, smem_raw, a.sx + (tile % a.ntx) * BX,
+                                   a.sy + (tile / a.ntx) * BY, a.sz + zoff, a.sz + zoff + len);
         pos += len;
     }
 }

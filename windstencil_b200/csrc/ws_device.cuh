@@ -190,18 +190,75 @@ __device__ __forceinline__ void weno7_symbo_nd<double>(const double t[8], double
                              0.0291783426580 * (p012 * e3), num, den);
 }
 
-template <>
-__device__ __forceinline__ void weno7_symbo_nd<float>(const float t[8], float& num,
-                                                      float& den) {
-    WenoDiffs<float> o;
-    weno7_indicators<float>(t, o);
-    const float b4 = fmaxf(fmaxf(fmaxf(o.b0, o.b1), fmaxf(o.b2, o.b3)), o.b4);
-    const float e = 2.592e-6f / 720.0f;
-    weno7_candidates<float>(o, __fdividef(0.0401954833730f, e + o.b0),
-                            __fdividef(0.2493800006710f, e + o.b1),
-                            __fdividef(0.4802686256260f, e + o.b2),
-                            __fdividef(0.2009775476730f, e + o.b3),
-                            __fdividef(0.0291783426580f, e + b4), num, den);
+// ---------------------------------------------------------------------------
+// Mixed form: the P and M reconstructions of one face are the same arithmetic
+// on two stencils, so they run as the two lanes of Blackwell's packed FP32x2
+// instructions (FFMA2/FADD2/FMUL2): t[k] = (P stencil k, M stencil k).  The
+// normalised weights d_k/(eps+beta_k) take their reciprocals in pairs,
+// 1/a = b/(ab) and 1/b = a/(ab), from the approximate hardware reciprocal;
+// ab stays inside the FP32 range for any indicator below ~1e19.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 f2(float c) { return make_float2(c, c); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(f2(-1.f), b, a); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float2 rcp2(float2 x) {
+    return make_float2(rcp_approx(x.x), rcp_approx(x.y));
+}
+
+// face value of lane L = t[3].L + num.L / den.L
+__device__ __forceinline__ void weno7_symbo_pm_f32x2(const float2 t[8], float2& num,
+                                                     float2& den) {
+    const float2 D0 = sub2(t[1], t[0]), D1 = sub2(t[2], t[1]), D2 = sub2(t[3], t[2]);
+    const float2 D3 = sub2(t[4], t[3]), D4 = sub2(t[5], t[4]), D5 = sub2(t[6], t[5]);
+    const float2 D6 = sub2(t[7], t[6]);
+    const float2 S0 = sub2(D1, D0), S1 = sub2(D2, D1), S2 = sub2(D3, D2), S3 = sub2(D4, D3);
+    const float2 S4 = sub2(D5, D4), S5 = sub2(D6, D5);
+    const float2 T0 = sub2(S1, S0), T1 = sub2(S2, S1), T2 = sub2(S3, S2), T3 = sub2(S4, S3);
+    const float2 T4 = sub2(S5, S4);
+    const float2 c2 = f2(39.0f), c3 = f2(39.05f);
+    auto beta = [&](float2 r, float2 s, float2 T) {
+        return fma2(mul2(c3, T), T, fma2(mul2(c2, s), s, mul2(r, r)));
+    };
+    float2 r, s;
+    r = fma2(f2(11.f), D2, fma2(f2(-7.f), D1, mul2(f2(2.f), D0)));
+    s = fma2(f2(2.f), S1, mul2(f2(-1.f), S0));
+    const float2 b0 = beta(r, s, T0);
+    r = fma2(f2(2.f), D3, fma2(f2(5.f), D2, mul2(f2(-1.f), D1)));
+    const float2 b1 = beta(r, S2, T1);
+    r = fma2(f2(-1.f), D4, fma2(f2(5.f), D3, mul2(f2(2.f), D2)));
+    const float2 b2 = beta(r, S3, T2);
+    r = fma2(f2(2.f), D5, fma2(f2(-7.f), D4, mul2(f2(11.f), D3)));
+    s = fma2(f2(2.f), S3, mul2(f2(-1.f), S4));
+    const float2 b3 = beta(r, s, T3);
+    r = fma2(f2(11.f), D6, fma2(f2(-31.f), D5, mul2(f2(26.f), D4)));
+    s = fma2(f2(3.f), S4, mul2(f2(-2.f), S5));
+    float2 b4 = beta(r, s, T4);
+    b4.x = fmaxf(fmaxf(fmaxf(b0.x, b1.x), fmaxf(b2.x, b3.x)), b4.x);
+    b4.y = fmaxf(fmaxf(fmaxf(b0.y, b1.y), fmaxf(b2.y, b3.y)), b4.y);
+    const float2 e = f2(2.592e-6f / 720.0f);
+    const float2 e0 = add2(e, b0), e1 = add2(e, b1), e2 = add2(e, b2), e3 = add2(e, b3);
+    const float2 e4 = add2(e, b4);
+    const float2 r01 = rcp2(mul2(e0, e1)), r23 = rcp2(mul2(e2, e3)), r4 = rcp2(e4);
+    const float2 w0 = mul2(mul2(f2(0.0401954833730f), e1), r01);
+    const float2 w1 = mul2(mul2(f2(0.2493800006710f), e0), r01);
+    const float2 w2 = mul2(mul2(f2(0.4802686256260f), e3), r23);
+    const float2 w3 = mul2(mul2(f2(0.2009775476730f), e2), r23);
+    const float2 w4 = mul2(f2(0.0291783426580f), r4);
+    const float2 l0 = fma2(f2(13.f), D2, fma2(f2(-10.f), D1, mul2(f2(3.f), D0)));
+    const float2 l1 = fma2(f2(3.f), D3, fma2(f2(4.f), D2, mul2(f2(-1.f), D1)));
+    const float2 l2 = fma2(f2(-1.f), D4, fma2(f2(6.f), D3, D2));
+    const float2 l3 = fma2(f2(-4.f), D4, fma2(f2(9.f), D3, D5));
+    const float2 l4 =
+        fma2(f2(-3.f), D6, fma2(f2(10.f), D5, fma2(f2(-13.f), D4, mul2(f2(12.f), D3))));
+    num = fma2(w4, l4, fma2(w3, l3, fma2(w2, l2, fma2(w1, l1, mul2(w0, l0)))));
+    den = mul2(f2(12.f), add2(add2(add2(w0, w1), add2(w2, w3)), w4));
 }
 
 // ---------------------------------------------------------------------------
