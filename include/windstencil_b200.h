@@ -208,6 +208,87 @@ WS_API int  ws_solver_step(ws_solver* s, double dt, int nsteps, ws_stream_t stre
 WS_API int  ws_solver_status(ws_solver* s, int* status, ws_stream_t stream);
 WS_API int  ws_solver_set_tile(ws_solver* s, ws_tile tile);
 
+/* ------------------------------------------------------------------------ */
+/* Many independent grids, device-resident, stepped together: per RK stage   */
+/* one batched ghost fill, one persistent fused-RHS launch over all grids,   */
+/* one batched stage update; the step is replayed from a CUDA graph.  No     */
+/* reference counterpart (the reference solves one grid per MPI rank).       */
+/* All grids: Cartesian (metrics_uniform = 1) and one precision.             */
+/* ------------------------------------------------------------------------ */
+typedef struct ws_batch ws_batch;
+
+WS_API int  ws_batch_create(const ws_grid* grids, int n, ws_batch** out);
+WS_API void ws_batch_destroy(ws_batch* b);
+WS_API int  ws_batch_size(ws_batch* b);
+/* dense conserved state [5][nz][ny][nx] of grid i */
+WS_API int  ws_batch_set_state(ws_batch* b, int i, const double* f_host, ws_stream_t stream);
+WS_API int  ws_batch_get_state(ws_batch* b, int i, double* f_host, ws_stream_t stream);
+WS_API int  ws_batch_get_rhs(ws_batch* b, int i, double* du_host, ws_stream_t stream);
+/* CFL time step of every grid (dt_out[n]); synchronises `stream` */
+WS_API int  ws_batch_compute_dt(ws_batch* b, double cfl, double* dt_out, ws_stream_t stream);
+WS_API int  ws_batch_set_dt(ws_batch* b, const double* dt);
+WS_API int  ws_batch_set_tile(ws_batch* b, ws_tile tile);
+WS_API int  ws_batch_get_tile(ws_batch* b, ws_tile* tile);
+/* du of every grid's current state */
+WS_API int  ws_batch_rhs(ws_batch* b, ws_stream_t stream);
+/* nsteps SSP-RK3 steps of every grid */
+WS_API int  ws_batch_step(ws_batch* b, int nsteps, ws_stream_t stream);
+/* per-grid status (0 or WS_ERR_NONFINITE); synchronises `stream` */
+WS_API int  ws_batch_status(ws_batch* b, int* status, ws_stream_t stream);
+/* times the compiled tile shapes on this batch's RHS and keeps the fastest */
+WS_API int  ws_batch_autotune(ws_batch* b, ws_tile* chosen, ws_stream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* Continuous-batching solve server.  No reference counterpart.  A host      */
+/* thread admits queued requests while the HBM state budget and the slot     */
+/* limit allow, keeps their state on the device, advances every active grid  */
+/* one SSP-RK3 step per tick (one batched launch per kernel per stage and    */
+/* precision) and retires grids that reached their step count.               */
+/* ------------------------------------------------------------------------ */
+typedef struct ws_server ws_server;
+
+typedef struct ws_server_config {
+    size_t hbm_budget_bytes;  /* device memory for request states (0: 80 GiB) */
+    int32_t max_active;       /* concurrent grids (0: 4096)                    */
+    ws_tile tile;             /* kernel tile shape (zeroes: default)           */
+} ws_server_config;
+
+typedef struct ws_request {
+    ws_grid grid;             /* Cartesian, FP64 or mixed                      */
+    int32_t nsteps;           /* SSP-RK3 steps                                 */
+    double cfl;               /* dt = cfl / max wave speed of the initial state */
+    double dt;                /* > 0: use this dt instead of cfl               */
+    const double* f0_host;    /* dense conserved initial state [5][nz][ny][nx];
+                                 read at admission, keep it valid until then;
+                                 NULL: seeded synthetic state (below)          */
+    uint64_t synth_seed;      /* periodic Sod-type state: rho 1 | 0.125,       */
+    double synth_mach;        /* p 1/gamma | 0.1/gamma, u = mach, 1% noise     */
+    double synth_x_jump;      /* jump position as a fraction of nx             */
+    double* result_host;      /* final conserved state is copied here (or NULL) */
+} ws_request;
+
+typedef struct ws_server_stats {
+    long submitted, queued, active, completed, failed, ticks, max_active;
+    size_t hbm_in_use;
+    double p50_latency_s, p99_latency_s, mean_latency_s;  /* submit -> result */
+    double served_cell_rhs;    /* cell-RHS evaluations of completed requests  */
+    double busy_s, elapsed_s;
+} ws_server_stats;
+
+enum ws_request_state { WS_RQ_QUEUED = 0, WS_RQ_RUNNING = 1, WS_RQ_DONE = 2, WS_RQ_FAILED = 3 };
+
+WS_API int  ws_server_create(const ws_server_config* cfg, ws_server** out);
+/* stops the loop, frees every request's device state */
+WS_API void ws_server_destroy(ws_server* s);
+WS_API int  ws_server_submit(ws_server* s, const ws_request* r, uint64_t* id);
+/* state = enum ws_request_state; latency (submit -> done) or -1 */
+WS_API int  ws_server_poll(ws_server* s, uint64_t id, int* state, double* latency_s);
+/* blocks until the request is done (WS_ERR_TIMEOUT after timeout_s > 0) */
+WS_API int  ws_server_wait(ws_server* s, uint64_t id, double timeout_s);
+WS_API int  ws_server_get_stats(ws_server* s, ws_server_stats* out);
+/* forgets a finished request */
+WS_API int  ws_server_release(ws_server* s, uint64_t id);
+
 #ifdef __cplusplus
 }
 #endif

@@ -246,3 +246,148 @@ class Solver:
 
     def set_tile(self, tile):
         check(load().ws_solver_set_tile(self.h, WsTile(*tile)))
+
+
+class Batch:
+    """Many device-resident grids stepped together (ws_batch_*)."""
+
+    def __init__(self, grids):
+        self.grids = list(grids)
+        arr = (WsGrid * len(self.grids))(*[g.c() for g in self.grids])
+        h = C.c_void_p()
+        check(load().ws_batch_create(arr, len(self.grids), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            load().ws_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self):
+        return len(self.grids)
+
+    def set_state(self, i, f_host, stream=None):
+        import numpy as np
+        a = np.ascontiguousarray(f_host, dtype=np.float64)
+        check(load().ws_batch_set_state(self.h, i, a.ctypes.data, _stream(stream)))
+        _abi_sync(stream)
+
+    def get_state(self, i, stream=None):
+        import numpy as np
+        g = self.grids[i]
+        out = np.empty((5, g.nz, g.ny, g.nx))
+        check(load().ws_batch_get_state(self.h, i, out.ctypes.data, _stream(stream)))
+        return out
+
+    def get_rhs(self, i, stream=None):
+        import numpy as np
+        g = self.grids[i]
+        out = np.empty((5, g.nz, g.ny, g.nx))
+        check(load().ws_batch_get_rhs(self.h, i, out.ctypes.data, _stream(stream)))
+        return out
+
+    def compute_dt(self, cfl, stream=None):
+        import numpy as np
+        out = np.empty(len(self.grids))
+        check(load().ws_batch_compute_dt(self.h, cfl, out.ctypes.data_as(C.POINTER(C.c_double)),
+                                         _stream(stream)))
+        return out
+
+    def set_dt(self, dts):
+        import numpy as np
+        a = np.ascontiguousarray(dts, dtype=np.float64)
+        check(load().ws_batch_set_dt(self.h, a.ctypes.data_as(C.POINTER(C.c_double))))
+
+    def set_tile(self, tile):
+        check(load().ws_batch_set_tile(self.h, WsTile(*tile)))
+
+    def rhs(self, stream=None):
+        check(load().ws_batch_rhs(self.h, _stream(stream)))
+
+    def step(self, nsteps=1, stream=None):
+        check(load().ws_batch_step(self.h, nsteps, _stream(stream)))
+
+    def status(self, stream=None):
+        arr = (C.c_int * len(self.grids))()
+        check(load().ws_batch_status(self.h, arr, _stream(stream)))
+        return list(arr)
+
+    def autotune(self, stream=None):
+        t = WsTile()
+        check(load().ws_batch_autotune(self.h, C.byref(t), _stream(stream)))
+        return (t.tile_x, t.tile_y, t.scan_z, t.threads)
+
+
+class Server:
+    """Continuous-batching solve server (ws_server_*)."""
+
+    def __init__(self, hbm_budget_bytes=80 << 30, max_active=4096, tile=(0, 0, 0, 0)):
+        from ._abi import WsServerConfig
+        cfg = WsServerConfig(hbm_budget_bytes, max_active, WsTile(*tile))
+        h = C.c_void_p()
+        check(load().ws_server_create(C.byref(cfg), C.byref(h)))
+        self.h = h
+        self._keep = {}
+
+    def close(self):
+        if self.h:
+            load().ws_server_destroy(self.h)
+            self.h = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, grid: Grid, nsteps, cfl=0.5, dt=0.0, f0=None, seed=0, mach=1.0,
+               x_jump=0.5, want_result=True):
+        """Queue a solve; returns the request id.  f0: dense conserved state
+        (numpy) or None for the seeded synthetic state on the device."""
+        import numpy as np
+        from ._abi import WsRequest
+        res = np.empty((5, grid.nz, grid.ny, grid.nx)) if want_result else None
+        f0a = None if f0 is None else np.ascontiguousarray(f0, dtype=np.float64)
+        r = WsRequest(grid.c(), nsteps, cfl, dt, None if f0a is None else f0a.ctypes.data,
+                      seed, mach, x_jump, None if res is None else res.ctypes.data)
+        rid = C.c_uint64()
+        check(load().ws_server_submit(self.h, C.byref(r), C.byref(rid)))
+        self._keep[rid.value] = (f0a, res)
+        return rid.value
+
+    def poll(self, rid):
+        st, lat = C.c_int(), C.c_double()
+        rc = load().ws_server_poll(self.h, rid, C.byref(st), C.byref(lat))
+        return st.value, lat.value, rc
+
+    def wait(self, rid, timeout=0.0):
+        check(load().ws_server_wait(self.h, rid, timeout))
+        return self._keep[rid][1]
+
+    def result(self, rid):
+        return self._keep[rid][1]
+
+    def release(self, rid):
+        check(load().ws_server_release(self.h, rid))
+        self._keep.pop(rid, None)
+
+    def stats(self) -> dict:
+        from ._abi import WsServerStats
+        s = WsServerStats()
+        check(load().ws_server_get_stats(self.h, C.byref(s)))
+        return {n: getattr(s, n) for n, _ in WsServerStats._fields_}
+
+
+def _abi_sync(stream):
+    """Host buffers handed to an asynchronous upload must outlive it."""
+    if stream is None:
+        _torch().cuda.current_stream().synchronize()
+    else:
+        getattr(stream, "synchronize", lambda: None)()

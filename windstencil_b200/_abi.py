@@ -59,6 +59,25 @@ class WsTile(C.Structure):
                 ("threads", C.c_int32)]
 
 
+class WsServerConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_size_t), ("max_active", C.c_int32), ("tile", WsTile)]
+
+
+class WsRequest(C.Structure):
+    _fields_ = [("grid", WsGrid), ("nsteps", C.c_int32), ("cfl", C.c_double),
+                ("dt", C.c_double), ("f0_host", C.c_void_p), ("synth_seed", C.c_uint64),
+                ("synth_mach", C.c_double), ("synth_x_jump", C.c_double),
+                ("result_host", C.c_void_p)]
+
+
+class WsServerStats(C.Structure):
+    _fields_ = [(n, C.c_long) for n in ("submitted", "queued", "active", "completed", "failed",
+                                        "ticks", "max_active")] + [
+        ("hbm_in_use", C.c_size_t), ("p50_latency_s", C.c_double),
+        ("p99_latency_s", C.c_double), ("mean_latency_s", C.c_double),
+        ("served_cell_rhs", C.c_double), ("busy_s", C.c_double), ("elapsed_s", C.c_double)]
+
+
 _P = C.c_void_p
 _I = C.c_int
 SIGNATURES = {
@@ -87,6 +106,27 @@ SIGNATURES = {
     "ws_solver_step": (_I, [_P, C.c_double, _I, _P]),
     "ws_solver_status": (_I, [_P, C.POINTER(_I), _P]),
     "ws_solver_set_tile": (_I, [_P, WsTile]),
+    "ws_batch_create": (_I, [C.POINTER(WsGrid), _I, C.POINTER(_P)]),
+    "ws_batch_destroy": (None, [_P]),
+    "ws_batch_size": (_I, [_P]),
+    "ws_batch_set_state": (_I, [_P, _I, _P, _P]),
+    "ws_batch_get_state": (_I, [_P, _I, _P, _P]),
+    "ws_batch_get_rhs": (_I, [_P, _I, _P, _P]),
+    "ws_batch_compute_dt": (_I, [_P, C.c_double, C.POINTER(C.c_double), _P]),
+    "ws_batch_set_dt": (_I, [_P, C.POINTER(C.c_double)]),
+    "ws_batch_set_tile": (_I, [_P, WsTile]),
+    "ws_batch_get_tile": (_I, [_P, C.POINTER(WsTile)]),
+    "ws_batch_rhs": (_I, [_P, _P]),
+    "ws_batch_step": (_I, [_P, _I, _P]),
+    "ws_batch_status": (_I, [_P, C.POINTER(_I), _P]),
+    "ws_batch_autotune": (_I, [_P, C.POINTER(WsTile), _P]),
+    "ws_server_create": (_I, [C.POINTER(WsServerConfig), C.POINTER(_P)]),
+    "ws_server_destroy": (None, [_P]),
+    "ws_server_submit": (_I, [_P, C.POINTER(WsRequest), C.POINTER(C.c_uint64)]),
+    "ws_server_poll": (_I, [_P, C.c_uint64, C.POINTER(_I), C.POINTER(C.c_double)]),
+    "ws_server_wait": (_I, [_P, C.c_uint64, C.c_double]),
+    "ws_server_get_stats": (_I, [_P, C.POINTER(WsServerStats)]),
+    "ws_server_release": (_I, [_P, C.c_uint64]),
 }
 
 _lib = None

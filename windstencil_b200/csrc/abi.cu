@@ -80,16 +80,9 @@ int default_scan(const ws_grid*) { return 1 << 30; }
 
 }  // namespace
 
-// Fill RhsArgs and launch; shared by the drop-in entry and the solver.
-int rhs_enqueue(const ws_grid* g, ws_job job, const ws_field prims[5], const ws_metrics* m,
-                ws_soa du, ws_tile tile, cudaStream_t st) {
-    int cfg = default_cfg();
-    if (tile.tile_x || tile.tile_y || tile.threads) {
-        cfg = find_tile_cfg(tile.tile_x, tile.tile_y, tile.threads);
-        if (cfg < 0) return fail(WS_ERR_UNSUPPORTED, "tile shape not compiled in this build");
-    }
+RhsArgs make_rhs_args(const ws_grid* g, ws_job job, const ws_field prims[5],
+                      const ws_metrics* m, ws_soa du, int cfg, int scan) {
     const TileCfg c = tile_cfg(cfg);
-    const int scan = tile.scan_z > 0 ? tile.scan_z : default_scan(g);
     RhsArgs a{};
     for (int i = 0; i < 5; ++i) {
         a.prim[i] = prims[i].ptr;
@@ -120,6 +113,20 @@ int rhs_enqueue(const ws_grid* g, ws_job job, const ws_field prims[5], const ws_
     a.c1 = 2.0 * (g->gamma - 1.0);
     a.c3 = (3.0 - g->gamma) / (2.0 * (g->gamma - 1.0));
     a.gm1 = g->gamma - 1.0;
+    return a;
+}
+
+// Fill RhsArgs and launch; shared by the drop-in entry and the solver.
+int rhs_enqueue(const ws_grid* g, ws_job job, const ws_field prims[5], const ws_metrics* m,
+                ws_soa du, ws_tile tile, cudaStream_t st) {
+    int cfg = default_cfg();
+    if (tile.tile_x || tile.tile_y || tile.threads) {
+        cfg = find_tile_cfg(tile.tile_x, tile.tile_y, tile.threads);
+        if (cfg < 0) return fail(WS_ERR_UNSUPPORTED, "tile shape not compiled in this build");
+    }
+    const int scan = tile.scan_z > 0 ? tile.scan_z : default_scan(g);
+    const bool uni = g->metrics_uniform != 0;
+    const RhsArgs a = make_rhs_args(g, job, prims, m, du, cfg, scan);
     // persistent grid: one CTA per resident slot, but no more than keeps
     // every CTA at >= 16 planes of work once the tile columns run out
     const long ntile = (long)a.ntx * a.nty;

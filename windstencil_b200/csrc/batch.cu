@@ -1,0 +1,487 @@
+// batch.cu -- many independent grids stepped together.
+//
+// The reference solves one grid per MPI rank (src/solver/OCFD_NS_Solver.cpp);
+// this file adds what it does not have: device-resident states of many
+// uneven grids, advanced by SSP-RK3 with one batched launch per kernel per
+// stage (ghost fill, fused RHS, stage update), the step replayed from a CUDA
+// graph, and an autotuner that times the compiled tile shapes on the batch.
+#include <algorithm>
+#include <cstring>
+#include <memory>
+
+#include "ws_internal.h"
+
+namespace ws {
+
+namespace {
+size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+__global__ void max_speed_kernel(ws_field u, ws_field v, ws_field w, ws_field cc, int nx,
+                                 int ny, int nz, double rx, double ry, double rz,
+                                 unsigned long long* out) {
+    const long n = (long)nx * ny * nz;
+    const double rr = sqrt(rx * rx + ry * ry + rz * rz);
+    double m = 0.0;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n;
+         t += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % nx) + 4;
+        const long r = t / nx;
+        const int j = (int)(r % ny) + 4, k = (int)(r / ny) + 4;
+        auto at = [&](const ws_field& f) {
+            return f.ptr[(size_t)i + (size_t)f.pitch * ((size_t)j + (size_t)(ny + 8) * k)];
+        };
+        const double s = fabs(at(u)) * rx + fabs(at(v)) * ry + fabs(at(w)) * rz + at(cc) * rr;
+        m = fmax(m, s);
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+}  // namespace
+
+// max over the interior of |u|/hx + |v|/hy + |w|/hz + c*sqrt(hx^-2+hy^-2+hz^-2)
+// as the bits of a non-negative double, atomically max-ed into *out
+int launch_max_speed(const ws_grid* g, const ws_field prims[6], unsigned long long* out,
+                     cudaStream_t st) {
+    const long n = (long)g->nx * g->ny * g->nz;
+    int blocks = (int)std::min<long>((n + 255) / 256, 148L * 8);
+    max_speed_kernel<<<std::max(blocks, 1), 256, 0, st>>>(prims[1], prims[2], prims[3], prims[5],
+                                                          g->nx, g->ny, g->nz, 1.0 / g->hx,
+                                                          1.0 / g->hy, 1.0 / g->hz, out);
+    WS_CUDA(cudaGetLastError());
+    return WS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// GridState
+// ---------------------------------------------------------------------------
+size_t grid_state_bytes(const ws_grid& g) {
+    const size_t ncell = (size_t)g.nx * g.ny * g.nz;
+    const size_t nlap = (size_t)lap_pitch(g.nx) * (g.ny + 8) * (g.nz + 8);
+    return 3 * align256(5 * ncell * sizeof(double)) + 6 * align256(nlap * sizeof(double)) + 256;
+}
+
+int grid_state_alloc(GridState& s, const ws_grid& g, cudaStream_t st) {
+    s.g = g;
+    s.bytes = grid_state_bytes(g);
+    WS_CUDA(cudaMallocAsync(&s.mem, s.bytes, st));
+    WS_CUDA(cudaMemsetAsync(s.mem, 0, s.bytes, st));
+    const size_t ncell = (size_t)g.nx * g.ny * g.nz;
+    const uint32_t lp = lap_pitch(g.nx);
+    const size_t nlap = (size_t)lp * (g.ny + 8) * (g.nz + 8);
+    unsigned char* p = static_cast<unsigned char*>(s.mem);
+    for (int b = 0; b < 3; ++b) {
+        ws_soa q{reinterpret_cast<double*>(p), g.nx, g.ny, g.nz, 0};
+        if (b < 2) s.f[b] = q; else s.du = q;
+        p += align256(5 * ncell * sizeof(double));
+    }
+    for (int i = 0; i < 6; ++i) {
+        s.prims[i] = ws_field{reinterpret_cast<double*>(p), lp, 0};
+        p += align256(nlap * sizeof(double));
+    }
+    s.status = reinterpret_cast<int*>(p);
+    s.cur = 0;
+    return WS_OK;
+}
+
+void grid_state_free(GridState& s, cudaStream_t st) {
+    if (s.mem) cudaFreeAsync(s.mem, st);
+    s.mem = nullptr;
+}
+
+int grid_state_upload(GridState& s, const double* f_host, cudaStream_t st) {
+    const size_t n = (size_t)5 * s.g.nx * s.g.ny * s.g.nz;
+    WS_CUDA(cudaMemcpyAsync(s.f[s.cur].ptr, f_host, n * sizeof(double), cudaMemcpyHostToDevice,
+                            st));
+    int rc = launch_cons_to_prim(&s.g, s.f[s.cur], s.prims[0], s.prims[1], s.prims[2],
+                                 s.prims[3], s.prims[4], ws_field{nullptr, 0, 0}, s.status, st);
+    if (rc) return rc;
+    ws_job job{{4, 4, 4}, {s.g.nx + 4, s.g.ny + 4, s.g.nz + 4}};
+    return launch_sound_speed(&s.g, job, s.prims[4], s.prims[5], st);
+}
+
+int grid_state_download(GridState& s, double* f_host, cudaStream_t st) {
+    const size_t n = (size_t)5 * s.g.nx * s.g.ny * s.g.nz;
+    WS_CUDA(cudaMemcpyAsync(f_host, s.f[s.cur].ptr, n * sizeof(double), cudaMemcpyDeviceToHost,
+                            st));
+    return WS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// BatchRunner
+// ---------------------------------------------------------------------------
+BatchRunner::~BatchRunner() { release(nullptr); }
+
+void BatchRunner::drop_graphs() {
+    for (auto& e : exec_)
+        if (e) {
+            cudaGraphExecDestroy(e);
+            e = nullptr;
+        }
+}
+
+void BatchRunner::release(cudaStream_t st) {
+    drop_graphs();
+    if (dev_) cudaFreeAsync(dev_, st);
+    dev_ = nullptr;
+    dev_bytes_ = 0;
+    if (cap_) cudaStreamDestroy(cap_);
+    cap_ = nullptr;
+    grids_.clear();
+}
+
+int BatchRunner::build(const std::vector<GridState*>& grids, int cfg, int zc, cudaStream_t st) {
+    drop_graphs();
+    grids_ = grids;
+    cfg_ = cfg;
+    zc_ = zc > 0 ? zc : (1 << 30);
+    parity_ = 0;
+    const int n = (int)grids.size();
+    if (n == 0) return WS_OK;
+    precision_ = grids[0]->g.precision;
+    for (auto* s : grids)
+        if (s->g.precision != precision_ || !s->g.metrics_uniform)
+            return fail(WS_ERR_INVALID, "a batch holds Cartesian grids of one precision");
+    const size_t gsz = ghost_args_size(), ssz = stage_args_size();
+    long n_gtab = 0, n_stab = 0;
+    for (auto* s : grids) {
+        n_gtab += ghost_chunks(&s->g);
+        n_stab += cell_chunks(&s->g);
+    }
+    if (n_gtab > (1L << 30) || n_stab > (1L << 30)) return fail(WS_ERR_INVALID, "batch too large");
+    n_gtab_ = (int)n_gtab;
+    n_stab_ = (int)n_stab;
+    // layout of the device tables
+    const size_t o_rhs = 0;
+    const size_t o_cum = align256(o_rhs + n * sizeof(RhsArgs));
+    const size_t o_gh = align256(o_cum + (n + 1) * sizeof(long));
+    const size_t o_gt = align256(o_gh + n * gsz);
+    const size_t o_s0 = align256(o_gt + n_gtab * sizeof(int2));
+    const size_t o_s1 = align256(o_s0 + n * ssz);
+    const size_t o_st = align256(o_s1 + n * ssz);
+    const size_t bytes = align256(o_st + n_stab * sizeof(int2));
+    host_.assign(bytes, 0);
+    unsigned char* h = host_.data();
+    RhsArgs* hr = reinterpret_cast<RhsArgs*>(h + o_rhs);
+    long* hc = reinterpret_cast<long*>(h + o_cum);
+    int2* hgt = reinterpret_cast<int2*>(h + o_gt);
+    int2* hst = reinterpret_cast<int2*>(h + o_st);
+    hc[0] = 0;
+    long gi = 0, si = 0;
+    for (int i = 0; i < n; ++i) {
+        GridState* s = grids[i];
+        ws_job job{{4, 4, 4}, {s->g.nx + 4, s->g.ny + 4, s->g.nz + 4}};
+        const ws_field p5[5] = {s->prims[0], s->prims[1], s->prims[2], s->prims[3], s->prims[5]};
+        hr[i] = make_rhs_args(&s->g, job, p5, nullptr, s->du, cfg, zc_);
+        hc[i + 1] = hc[i] + (long)hr[i].ntx * hr[i].nty * s->g.nz;
+        fill_ghost_args(h + o_gh + i * gsz, &s->g, s->prims);
+        for (long c = 0; c < ghost_chunks(&s->g); ++c) hgt[gi++] = make_int2(i, (int)c);
+        for (long c = 0; c < cell_chunks(&s->g); ++c) hst[si++] = make_int2(i, (int)c);
+    }
+    if (bytes > dev_bytes_) {
+        if (dev_) cudaFreeAsync(dev_, st);
+        dev_ = nullptr;
+        WS_CUDA(cudaMallocAsync(&dev_, bytes, st));
+        dev_bytes_ = bytes;
+    }
+    unsigned char* d = static_cast<unsigned char*>(dev_);
+    d_rhs_ = reinterpret_cast<RhsArgs*>(d + o_rhs);
+    d_cum_ = reinterpret_cast<long*>(d + o_cum);
+    d_ghost_ = d + o_gh;
+    d_gtab_ = reinterpret_cast<int2*>(d + o_gt);
+    d_stage_[0] = d + o_s0;
+    d_stage_[1] = d + o_s1;
+    d_stab_ = reinterpret_cast<int2*>(d + o_st);
+    int rc = upload_stage_tables(st);   // fills the stage blocks of host_ and uploads all
+    if (rc) return rc;
+    const int maxc = rhs_max_ctas(precision_, true, cfg_);
+    if (maxc <= 0) return fail(WS_ERR_CUDA, "cannot size the persistent grid");
+    const long planes = hc[n];
+    ctas_ = (int)std::max(1L, std::min<long>(maxc, std::max<long>(1, planes / 16)));
+    return WS_OK;
+}
+
+int BatchRunner::upload_stage_tables(cudaStream_t st) {
+    const int n = (int)grids_.size();
+    if (n == 0) return WS_OK;
+    const size_t ssz = stage_args_size();
+    unsigned char* h = host_.data();
+    const size_t o0 = static_cast<unsigned char*>(d_stage_[0]) - static_cast<unsigned char*>(dev_);
+    const size_t o1 = static_cast<unsigned char*>(d_stage_[1]) - static_cast<unsigned char*>(dev_);
+    for (int p = 0; p < 2; ++p)
+        for (int i = 0; i < n; ++i) {
+            GridState* s = grids_[i];
+            const int src = s->cur ^ p;
+            fill_stage_args(h + (p ? o1 : o0) + i * ssz, &s->g, s->dt, s->f[1 - src], s->f[src],
+                            s->du, s->prims, s->status);
+        }
+    WS_CUDA(cudaMemcpyAsync(dev_, host_.data(), host_.size(), cudaMemcpyHostToDevice, st));
+    // host_ must stay unchanged until the copy has read it
+    WS_CUDA(cudaStreamSynchronize(st));
+    return WS_OK;
+}
+
+int BatchRunner::enqueue_rhs(cudaStream_t st) {
+    if (grids_.empty()) return WS_OK;
+    int rc = launch_ghost_fill_batch(d_ghost_, d_gtab_, n_gtab_, st);
+    if (rc) return rc;
+    return launch_rhs_batch(d_rhs_, d_cum_, (int)grids_.size(), zc_, precision_, true, cfg_,
+                            ctas_, st);
+}
+
+int BatchRunner::enqueue_step(cudaStream_t st) {
+    for (int krk = 1; krk <= 3; ++krk) {
+        int rc = enqueue_rhs(st);
+        if (rc) return rc;
+        rc = launch_stage_update_batch(d_stage_[parity_], d_stab_, n_stab_, krk, st);
+        if (rc) return rc;
+    }
+    return WS_OK;
+}
+
+int BatchRunner::step(int nsteps, cudaStream_t st) {
+    if (grids_.empty() || nsteps <= 0) return WS_OK;
+    if (!exec_[0]) {
+        if (!cap_) WS_CUDA(cudaStreamCreateWithFlags(&cap_, cudaStreamNonBlocking));
+        const int keep = parity_;
+        for (int p = 0; p < 2; ++p) {
+            parity_ = p;
+            cudaGraph_t graph = nullptr;
+            WS_CUDA(cudaStreamBeginCapture(cap_, cudaStreamCaptureModeThreadLocal));
+            int rc = enqueue_step(cap_);
+            cudaError_t e = cudaStreamEndCapture(cap_, &graph);
+            if (rc) {
+                if (graph) cudaGraphDestroy(graph);
+                parity_ = keep;
+                return rc;
+            }
+            if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+            e = cudaGraphInstantiate(&exec_[p], graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+        }
+        parity_ = keep;
+    }
+    for (int i = 0; i < nsteps; ++i) {
+        WS_CUDA(cudaGraphLaunch(exec_[parity_], st));
+        parity_ ^= 1;
+        for (auto* s : grids_) s->cur ^= 1;
+    }
+    return WS_OK;
+}
+
+}  // namespace ws
+
+using namespace ws;
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+struct ws_batch {
+    std::vector<GridState> states;
+    BatchRunner runner;
+    ws_tile tile{0, 0, 0, 0};
+    bool dirty = true;
+};
+
+namespace {
+int batch_ready(ws_batch* b, cudaStream_t st) {
+    if (!b->dirty) return WS_OK;
+    std::vector<GridState*> ptrs;
+    for (auto& s : b->states) ptrs.push_back(&s);
+    int cfg = 0;
+    if (b->tile.tile_x || b->tile.tile_y || b->tile.threads) {
+        cfg = find_tile_cfg(b->tile.tile_x, b->tile.tile_y, b->tile.threads);
+        if (cfg < 0) return fail(WS_ERR_UNSUPPORTED, "tile shape not compiled in this build");
+    }
+    int rc = b->runner.build(ptrs, cfg, b->tile.scan_z, st);
+    if (rc == WS_OK) b->dirty = false;
+    return rc;
+}
+}  // namespace
+
+extern "C" {
+
+int ws_batch_create(const ws_grid* grids, int n, ws_batch** out) {
+    if (!out) return fail(WS_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!grids || n <= 0) return fail(WS_ERR_INVALID, "need at least one grid");
+    for (int i = 0; i < n; ++i) {
+        const ws_grid& g = grids[i];
+        if (g.lap != WS_LAP || g.nx < 4 || g.ny < 4 || g.nz < 4 || !g.metrics_uniform ||
+            (g.precision != WS_FP64 && g.precision != WS_MIXED) ||
+            g.precision != grids[0].precision)
+            return fail(WS_ERR_INVALID, "batch grids: Cartesian, n >= 4, one precision");
+    }
+    std::unique_ptr<ws_batch> b(new (std::nothrow) ws_batch());
+    if (!b) return fail(WS_ERR_ALLOC, "host allocation failed");
+    b->states.resize(n);
+    for (int i = 0; i < n; ++i) {
+        int rc = grid_state_alloc(b->states[i], grids[i], nullptr);
+        if (rc) {
+            for (auto& s : b->states) grid_state_free(s, nullptr);
+            return rc;
+        }
+    }
+    WS_CUDA(cudaStreamSynchronize(nullptr));
+    *out = b.release();
+    return WS_OK;
+}
+
+void ws_batch_destroy(ws_batch* b) {
+    if (!b) return;
+    cudaDeviceSynchronize();
+    b->runner.release(nullptr);
+    for (auto& s : b->states) grid_state_free(s, nullptr);
+    cudaStreamSynchronize(nullptr);
+    delete b;
+}
+
+int ws_batch_size(ws_batch* b) { return b ? (int)b->states.size() : 0; }
+
+int ws_batch_set_state(ws_batch* b, int i, const double* f_host, ws_stream_t stream) {
+    if (!b || !f_host || i < 0 || i >= (int)b->states.size())
+        return fail(WS_ERR_INVALID, "bad batch index or NULL state");
+    return grid_state_upload(b->states[i], f_host, (cudaStream_t)stream);
+}
+
+int ws_batch_get_state(ws_batch* b, int i, double* f_host, ws_stream_t stream) {
+    if (!b || !f_host || i < 0 || i >= (int)b->states.size())
+        return fail(WS_ERR_INVALID, "bad batch index or NULL state");
+    int rc = grid_state_download(b->states[i], f_host, (cudaStream_t)stream);
+    if (rc) return rc;
+    WS_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    return WS_OK;
+}
+
+int ws_batch_get_rhs(ws_batch* b, int i, double* du_host, ws_stream_t stream) {
+    if (!b || !du_host || i < 0 || i >= (int)b->states.size())
+        return fail(WS_ERR_INVALID, "bad batch index or NULL buffer");
+    const GridState& s = b->states[i];
+    const size_t n = (size_t)5 * s.g.nx * s.g.ny * s.g.nz;
+    cudaStream_t st = (cudaStream_t)stream;
+    WS_CUDA(cudaMemcpyAsync(du_host, s.du.ptr, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    WS_CUDA(cudaStreamSynchronize(st));
+    return WS_OK;
+}
+
+int ws_batch_compute_dt(ws_batch* b, double cfl, double* dt_out, ws_stream_t stream) {
+    if (!b || !dt_out) return fail(WS_ERR_INVALID, "NULL argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int n = (int)b->states.size();
+    unsigned long long* d = nullptr;
+    WS_CUDA(cudaMallocAsync(&d, n * sizeof(unsigned long long), st));
+    WS_CUDA(cudaMemsetAsync(d, 0, n * sizeof(unsigned long long), st));
+    for (int i = 0; i < n; ++i) {
+        int rc = launch_max_speed(&b->states[i].g, b->states[i].prims, d + i, st);
+        if (rc) return rc;
+    }
+    std::vector<unsigned long long> h(n);
+    WS_CUDA(cudaMemcpyAsync(h.data(), d, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                            st));
+    WS_CUDA(cudaFreeAsync(d, st));
+    WS_CUDA(cudaStreamSynchronize(st));
+    for (int i = 0; i < n; ++i) {
+        double m;
+        std::memcpy(&m, &h[i], sizeof m);
+        if (!(m > 0)) return fail(WS_ERR_NONFINITE, "maximum wave speed is not positive");
+        dt_out[i] = cfl / m;
+    }
+    return WS_OK;
+}
+
+int ws_batch_set_dt(ws_batch* b, const double* dt) {
+    if (!b || !dt) return fail(WS_ERR_INVALID, "NULL argument");
+    for (size_t i = 0; i < b->states.size(); ++i) {
+        if (!(dt[i] > 0)) return fail(WS_ERR_INVALID, "dt must be > 0");
+        b->states[i].dt = dt[i];
+    }
+    b->dirty = true;
+    return WS_OK;
+}
+
+int ws_batch_set_tile(ws_batch* b, ws_tile tile) {
+    if (!b) return fail(WS_ERR_INVALID, "batch is NULL");
+    if ((tile.tile_x || tile.tile_y || tile.threads) &&
+        find_tile_cfg(tile.tile_x, tile.tile_y, tile.threads) < 0)
+        return fail(WS_ERR_UNSUPPORTED, "tile shape not compiled in this build");
+    b->tile = tile;
+    b->dirty = true;
+    return WS_OK;
+}
+
+int ws_batch_get_tile(ws_batch* b, ws_tile* tile) {
+    if (!b || !tile) return fail(WS_ERR_INVALID, "NULL argument");
+    *tile = b->tile;
+    return WS_OK;
+}
+
+int ws_batch_rhs(ws_batch* b, ws_stream_t stream) {
+    if (!b) return fail(WS_ERR_INVALID, "batch is NULL");
+    int rc = batch_ready(b, (cudaStream_t)stream);
+    if (rc) return rc;
+    return b->runner.enqueue_rhs((cudaStream_t)stream);
+}
+
+int ws_batch_step(ws_batch* b, int nsteps, ws_stream_t stream) {
+    if (!b) return fail(WS_ERR_INVALID, "batch is NULL");
+    for (auto& s : b->states)
+        if (!(s.dt > 0)) return fail(WS_ERR_INVALID, "set dt (ws_batch_set_dt) before stepping");
+    int rc = batch_ready(b, (cudaStream_t)stream);
+    if (rc) return rc;
+    return b->runner.step(nsteps, (cudaStream_t)stream);
+}
+
+int ws_batch_status(ws_batch* b, int* status, ws_stream_t stream) {
+    if (!b || !status) return fail(WS_ERR_INVALID, "NULL argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    for (size_t i = 0; i < b->states.size(); ++i)
+        WS_CUDA(cudaMemcpyAsync(&status[i], b->states[i].status, sizeof(int),
+                                cudaMemcpyDeviceToHost, st));
+    WS_CUDA(cudaStreamSynchronize(st));
+    for (size_t i = 0; i < b->states.size(); ++i) status[i] = status[i] ? WS_ERR_NONFINITE : WS_OK;
+    return WS_OK;
+}
+
+// Times every compiled tile shape (and two sweep caps) on one batched RHS of
+// this batch and keeps the fastest; returns it in *chosen.
+int ws_batch_autotune(ws_batch* b, ws_tile* chosen, ws_stream_t stream) {
+    if (!b) return fail(WS_ERR_INVALID, "batch is NULL");
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaEvent_t e0, e1;
+    WS_CUDA(cudaEventCreate(&e0));
+    WS_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    ws_tile best_tile{0, 0, 0, 0};
+    const int caps[2] = {0, 32};
+    for (int c = 0; c < num_tile_cfgs(); ++c)
+        for (int cap : caps) {
+            const TileCfg tc = tile_cfg(c);
+            b->tile = ws_tile{tc.bx, tc.by, cap, tc.threads};
+            b->dirty = true;
+            int rc = batch_ready(b, st);
+            if (rc == WS_OK) rc = b->runner.enqueue_rhs(st);    // warm-up
+            if (rc) {
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                return rc;
+            }
+            cudaEventRecord(e0, st);
+            for (int r = 0; r < 2; ++r) b->runner.enqueue_rhs(st);
+            cudaEventRecord(e1, st);
+            WS_CUDA(cudaEventSynchronize(e1));
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best) {
+                best = ms;
+                best_tile = b->tile;
+            }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b->tile = best_tile;
+    b->dirty = true;
+    if (chosen) *chosen = best_tile;
+    return batch_ready(b, st);
+}
+
+}  // extern "C"

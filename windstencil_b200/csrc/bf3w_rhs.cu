@@ -331,6 +331,41 @@ __global__ void __launch_bounds__(NT, 1) bf3w_rhs_kernel(const __grid_constant__
     }
 }
 
+// Batched form: many independent grids, one persistent launch.  The work
+// space is the concatenation over grids of (tile, plane) in tile-major order;
+// cum[g] is the number of tile-planes before grid g.  Each CTA takes an equal
+// contiguous range, so a CTA sweeps neighbouring columns of one grid in turn
+// and every CTA ends with the same number of planes.
+template <int BX, int BY, int NT, bool UNI, typename CT>
+__global__ void __launch_bounds__(NT, 1)
+    bf3w_rhs_batch_kernel(const RhsArgs* __restrict__ grids, const long* __restrict__ cum,
+                          int ngrids, int zc) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const long total = cum[ngrids];
+    const long lo = total * blockIdx.x / gridDim.x, hi = total * (blockIdx.x + 1) / gridDim.x;
+    if (lo >= hi) return;
+    int g = 0, top = ngrids;          // last g with cum[g] <= lo
+    while (top - g > 1) {
+        const int mid = (g + top) >> 1;
+        if (cum[mid] <= lo) g = mid; else top = mid;
+    }
+    long pos = lo;
+    while (pos < hi) {
+        while (cum[g + 1] <= pos) ++g;
+        const RhsArgs& a = grids[g];
+        const SplitK<CT> k = {CT(a.eps2), CT(a.hrg), CT(a.c1), CT(a.c3), CT(a.gm1)};
+        const long nzj = a.ez - a.sz;
+        const long local = pos - cum[g];
+        const long tile = local / nzj;
+        const int zoff = (int)(local - tile * nzj);
+        const int len = (int)min(min(nzj - zoff, hi - pos), (long)zc);
+        sweep<BX, BY, NT, UNI, CT>(a, k, smem_raw, a.sx + (int)(tile % a.ntx) * BX,
+                                   a.sy + (int)(tile / a.ntx) * BY, a.sz + zoff,
+                                   a.sz + zoff + len);
+        pos += len;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Compiled tile shapes and host launch
 // ---------------------------------------------------------------------------
@@ -365,7 +400,32 @@ struct Launcher {
         WS_CUDA(cudaGetLastError());
         return WS_OK;
     }
+    static int launch_batch(const RhsArgs* grids, const long* cum, int n, int zc, int ctas,
+                            cudaStream_t st) {
+        static int prepared[64] = {0};
+        int dev = 0;
+        WS_CUDA(cudaGetDevice(&dev));
+        if (dev >= 0 && dev < 64 && !prepared[dev]) {
+            WS_CUDA(cudaFuncSetAttribute(bf3w_rhs_batch_kernel<BX, BY, NT, UNI, CT>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem()));
+            prepared[dev] = 1;
+        }
+        bf3w_rhs_batch_kernel<BX, BY, NT, UNI, CT><<<ctas, NT, smem(), st>>>(grids, cum, n, zc);
+        WS_CUDA(cudaGetLastError());
+        return WS_OK;
+    }
 };
+
+template <int BX, int BY, int NT>
+int dispatch_batch(const RhsArgs* grids, const long* cum, int n, int zc, int precision, bool uni,
+                   int ctas, cudaStream_t st) {
+    if (precision == WS_MIXED)
+        return uni ? Launcher<BX, BY, NT, true, float>::launch_batch(grids, cum, n, zc, ctas, st)
+                   : Launcher<BX, BY, NT, false, float>::launch_batch(grids, cum, n, zc, ctas, st);
+    return uni ? Launcher<BX, BY, NT, true, double>::launch_batch(grids, cum, n, zc, ctas, st)
+               : Launcher<BX, BY, NT, false, double>::launch_batch(grids, cum, n, zc, ctas, st);
+}
 
 template <int BX, int BY, int NT>
 int dispatch_launch(const RhsArgs& a, int precision, bool uni, int ctas, cudaStream_t st) {
@@ -400,6 +460,16 @@ int launch_rhs(const RhsArgs& a, int precision, bool uniform, int cfg, int ctas,
         case 0: return dispatch_launch<16, 8, 512>(a, precision, uniform, ctas, st);
         case 1: return dispatch_launch<16, 8, 256>(a, precision, uniform, ctas, st);
         case 2: return dispatch_launch<16, 8, 448>(a, precision, uniform, ctas, st);
+        default: return fail(WS_ERR_INVALID, "unknown tile configuration");
+    }
+}
+
+int launch_rhs_batch(const RhsArgs* grids, const long* cum, int n, int zc, int precision,
+                     bool uniform, int cfg, int ctas, cudaStream_t st) {
+    switch (cfg) {
+        case 0: return dispatch_batch<16, 8, 512>(grids, cum, n, zc, precision, uniform, ctas, st);
+        case 1: return dispatch_batch<16, 8, 256>(grids, cum, n, zc, precision, uniform, ctas, st);
+        case 2: return dispatch_batch<16, 8, 448>(grids, cum, n, zc, precision, uniform, ctas, st);
         default: return fail(WS_ERR_INVALID, "unknown tile configuration");
     }
 }

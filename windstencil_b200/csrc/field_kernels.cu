@@ -1,5 +1,5 @@
 // field_kernels.cu -- bandwidth kernels around the RHS: sound speed, ghost
-// fill, prim<->cons, SSP-RK3 stage updates.
+// fill, prim<->cons, SSP-RK3 stage updates; single-grid and batched forms.
 //
 // Reference counterparts:
 //   sound speed    src/kernels/commen_kernel.cpp:145-154 (launched over the
@@ -30,6 +30,39 @@ __device__ __forceinline__ int ghost_src(int i, int n, int lo_kind, int hi_kind)
     return i;
 }
 
+__host__ __device__ __forceinline__ long ghost_count(int nx, int ny, int nz) {
+    const long px = nx + 8, py = ny + 8;
+    return 8 * px * py + 8 * px * (long)nz + 8 * (long)ny * nz;
+}
+
+// t-th point of the 4-layer ghost shell (edges and corners included):
+// z slabs (full xy planes), then y slabs at interior z, then x slabs.
+__device__ __forceinline__ void ghost_point(long t, int nx, int ny, int nz, int& i, int& j,
+                                            int& k) {
+    const long px = nx + 8, py = ny + 8;
+    const long nzs = 8 * px * py, nys = 8 * px * (long)nz;
+    if (t < nzs) {
+        const long pl = t / (px * py), r = t - pl * (px * py);
+        k = pl < 4 ? (int)pl : (int)(nz + pl);
+        j = (int)(r / px);
+        i = (int)(r - (long)j * px);
+    } else if (t < nzs + nys) {
+        const long t2 = t - nzs;
+        const long row = t2 / px;
+        i = (int)(t2 - row * px);
+        const int rj = (int)(row % 8);
+        k = 4 + (int)(row / 8);
+        j = rj < 4 ? rj : ny + rj;
+    } else {
+        const long t3 = t - nzs - nys;
+        const long line = t3 / 8;
+        const int ri = (int)(t3 - line * 8);
+        i = ri < 4 ? ri : nx + ri;
+        j = 4 + (int)(line % ny);
+        k = 4 + (int)(line / ny);
+    }
+}
+
 struct GhostArgs {
     double* ptr[8];
     uint32_t pitch[8];
@@ -38,46 +71,26 @@ struct GhostArgs {
     int kind[6];
 };
 
-// One thread per ghost point (all of the 4-layer shell, edges and corners
-// included): value = interior value at the wrapped / clamped coordinates.
-// Because the source is always an interior point, one launch fills every face.
-__global__ void ghost_fill_kernel(const __grid_constant__ GhostArgs a) {
-    const long px = a.nx + 8, py = a.ny + 8;
-    const long nzs = 8 * px * py;              // z slabs (full xy planes)
-    const long nys = 8 * px * (long)a.nz;      // y slabs, interior z
-    const long nxs = 8 * (long)a.ny * a.nz;    // x slabs, interior y,z
-    const long total = nzs + nys + nxs;
-    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total;
-         t += (long)gridDim.x * blockDim.x) {
-        int i, j, k;
-        if (t < nzs) {
-            const long pl = t / (px * py), r = t - pl * (px * py);
-            k = pl < 4 ? (int)pl : (int)(a.nz + pl);          // 0..3, nz+4..nz+7
-            j = (int)(r / px);
-            i = (int)(r - (long)j * px);
-        } else if (t < nzs + nys) {
-            const long t2 = t - nzs;
-            const long row = t2 / px;
-            i = (int)(t2 - row * px);
-            const int rj = (int)(row % 8);
-            k = 4 + (int)(row / 8);
-            j = rj < 4 ? rj : a.ny + rj;
-        } else {
-            const long t3 = t - nzs - nys;
-            const long line = t3 / 8;
-            const int ri = (int)(t3 - line * 8);
-            i = ri < 4 ? ri : a.nx + ri;
-            j = 4 + (int)(line % a.ny);
-            k = 4 + (int)(line / a.ny);
-        }
-        const int si = ghost_src(i, a.nx, a.kind[0], a.kind[1]);
-        const int sj = ghost_src(j, a.ny, a.kind[2], a.kind[3]);
-        const int sk = ghost_src(k, a.nz, a.kind[4], a.kind[5]);
-        for (int f = 0; f < a.nf; ++f) {
-            double* p = a.ptr[f];
-            p[lap_idx(i, j, k, a.pitch[f], a.ny)] = p[lap_idx(si, sj, sk, a.pitch[f], a.ny)];
-        }
+// value at a ghost point = interior value at the wrapped / clamped
+// coordinates; the source is always an interior point, so one pass fills
+// every face without ordering between them.
+__device__ __forceinline__ void ghost_fill_point(const GhostArgs& a, long t) {
+    int i, j, k;
+    ghost_point(t, a.nx, a.ny, a.nz, i, j, k);
+    const int si = ghost_src(i, a.nx, a.kind[0], a.kind[1]);
+    const int sj = ghost_src(j, a.ny, a.kind[2], a.kind[3]);
+    const int sk = ghost_src(k, a.nz, a.kind[4], a.kind[5]);
+    for (int f = 0; f < a.nf; ++f) {
+        double* p = a.ptr[f];
+        p[lap_idx(i, j, k, a.pitch[f], a.ny)] = p[lap_idx(si, sj, sk, a.pitch[f], a.ny)];
     }
+}
+
+__global__ void ghost_fill_kernel(const __grid_constant__ GhostArgs a) {
+    const long total = ghost_count(a.nx, a.ny, a.nz);
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total;
+         t += (long)gridDim.x * blockDim.x)
+        ghost_fill_point(a, t);
 }
 
 __global__ void sound_speed_kernel(ws_field T, ws_field cc, int i0, int j0, int k0, int ni,
@@ -178,6 +191,8 @@ __global__ void time_advance_kernel(const __grid_constant__ StageArgs a) {
     }
 }
 
+}  // namespace
+
 // Stage update fused with cons->prim and the interior sound speed.
 struct StagePrimArgs {
     StageArgs s;
@@ -186,37 +201,71 @@ struct StagePrimArgs {
     int* status;
 };
 
-__global__ void stage_update_kernel(const __grid_constant__ StagePrimArgs a) {
-    const int nx = a.s.nx, ny = a.s.ny, nz = a.s.nz;
-    const long n = (long)nx * ny * nz;
-    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n;
-         t += (long)gridDim.x * blockDim.x) {
-        const int i = (int)(t % nx);
-        const long r = t / nx;
-        const int j = (int)(r % ny), k = (int)(r / ny);
-        double q[5];
+namespace {
+
+// stage update of cell t (interior, x fastest) for stage krk
+template <int KRK>
+__device__ __forceinline__ void stage_cell(const StagePrimArgs& a, long t) {
+    const int nx = a.s.nx, ny = a.s.ny;
+    const int i = (int)(t % nx);
+    const long r = t / nx;
+    const int j = (int)(r % ny), k = (int)(r / ny);
+    double q[5];
 #pragma unroll
-        for (int var = 0; var < 5; ++var) {
-            const size_t p = soa_idx(i, j, k, var, a.s.f);
-            const double fo = a.s.f.ptr[p];
-            const double fnv = a.s.fn.ptr[soa_idx(i, j, k, var, a.s.fn)];
-            const double duv = a.s.du.ptr[soa_idx(i, j, k, var, a.s.du)];
-            q[var] = rk_stage(a.s.krk, fnv, fo, duv, a.s.dt);
-            a.s.f.ptr[p] = q[var];
-        }
-        const double d1 = q[0];
-        const double u1 = q[1] / d1, v1 = q[2] / d1, w1 = q[3] / d1;
-        const double t1 = q[4] - 0.5 * d1 * (u1 * u1 + v1 * v1 + w1 * w1);
-        const double T1 = t1 / (d1 * a.cv);
-        const int I = i + 4, J = j + 4, K = k + 4;
-        a.d.ptr[lap_idx(I, J, K, a.d.pitch, ny)] = d1;
-        a.u.ptr[lap_idx(I, J, K, a.u.pitch, ny)] = u1;
-        a.v.ptr[lap_idx(I, J, K, a.v.pitch, ny)] = v1;
-        a.w.ptr[lap_idx(I, J, K, a.w.pitch, ny)] = w1;
-        a.T.ptr[lap_idx(I, J, K, a.T.pitch, ny)] = T1;
-        a.cc.ptr[lap_idx(I, J, K, a.cc.pitch, ny)] = sqrt(T1) / a.ama;
-        if (a.status && !(d1 > 0.0 && T1 > 0.0 && T1 < INFINITY)) atomicOr(a.status, 1);
+    for (int var = 0; var < 5; ++var) {
+        const size_t p = soa_idx(i, j, k, var, a.s.f);
+        const double fo = KRK == 1 ? 0.0 : a.s.f.ptr[p];   // stage 1 does not read f
+        const double fnv = a.s.fn.ptr[soa_idx(i, j, k, var, a.s.fn)];
+        const double duv = a.s.du.ptr[soa_idx(i, j, k, var, a.s.du)];
+        q[var] = rk_stage(KRK, fnv, fo, duv, a.s.dt);
+        a.s.f.ptr[p] = q[var];
     }
+    const double d1 = q[0];
+    const double u1 = q[1] / d1, v1 = q[2] / d1, w1 = q[3] / d1;
+    const double t1 = q[4] - 0.5 * d1 * (u1 * u1 + v1 * v1 + w1 * w1);
+    const double T1 = t1 / (d1 * a.cv);
+    const int I = i + 4, J = j + 4, K = k + 4;
+    a.d.ptr[lap_idx(I, J, K, a.d.pitch, ny)] = d1;
+    a.u.ptr[lap_idx(I, J, K, a.u.pitch, ny)] = u1;
+    a.v.ptr[lap_idx(I, J, K, a.v.pitch, ny)] = v1;
+    a.w.ptr[lap_idx(I, J, K, a.w.pitch, ny)] = w1;
+    a.T.ptr[lap_idx(I, J, K, a.T.pitch, ny)] = T1;
+    a.cc.ptr[lap_idx(I, J, K, a.cc.pitch, ny)] = sqrt(T1) / a.ama;
+    if (a.status && !(d1 > 0.0 && T1 > 0.0 && T1 < INFINITY)) atomicOr(a.status, 1);
+}
+
+template <int KRK>
+__global__ void stage_update_kernel(const __grid_constant__ StagePrimArgs a) {
+    const long n = (long)a.s.nx * a.s.ny * a.s.nz;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n;
+         t += (long)gridDim.x * blockDim.x)
+        stage_cell<KRK>(a, t);
+}
+
+// ---- batched forms: block b works on grid tab[b].x, chunk tab[b].y of
+// kBatchChunk points (a host-built table; no search on the device)
+constexpr int kBatchThreads = 256;
+constexpr long kBatchChunk = 256L * 8;
+
+__global__ void ghost_fill_batch_kernel(const GhostArgs* __restrict__ grids,
+                                        const int2* __restrict__ tab) {
+    const int2 e = tab[blockIdx.x];
+    const GhostArgs& a = grids[e.x];
+    const long total = ghost_count(a.nx, a.ny, a.nz);
+    const long t0 = (long)e.y * kBatchChunk;
+    const long t1 = min(total, t0 + kBatchChunk);
+    for (long t = t0 + threadIdx.x; t < t1; t += blockDim.x) ghost_fill_point(a, t);
+}
+
+template <int KRK>
+__global__ void stage_update_batch_kernel(const StagePrimArgs* __restrict__ grids,
+                                          const int2* __restrict__ tab) {
+    const int2 e = tab[blockIdx.x];
+    const StagePrimArgs& a = grids[e.x];
+    const long total = (long)a.s.nx * a.s.ny * a.s.nz;
+    const long t0 = (long)e.y * kBatchChunk;
+    const long t1 = min(total, t0 + kBatchChunk);
+    for (long t = t0 + threadIdx.x; t < t1; t += blockDim.x) stage_cell<KRK>(a, t);
 }
 
 int grid_for(long n, int threads) {
@@ -238,9 +287,7 @@ int launch_ghost_fill(const ws_grid* g, const ws_field* f, int nf, cudaStream_t 
     a.nf = nf;
     a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
     for (int i = 0; i < 6; ++i) a.kind[i] = g->face_kind[i];
-    const long px = g->nx + 8, py = g->ny + 8;
-    const long total = 8 * px * py + 8 * px * (long)g->nz + 8 * (long)g->ny * g->nz;
-    ghost_fill_kernel<<<grid_for(total, 256), 256, 0, st>>>(a);
+    ghost_fill_kernel<<<grid_for(ghost_count(g->nx, g->ny, g->nz), 256), 256, 0, st>>>(a);
     WS_CUDA(cudaGetLastError());
     return WS_OK;
 }
@@ -291,8 +338,8 @@ int launch_time_advance(const ws_grid* g, int krk, double dt, ws_soa f, ws_soa f
     return WS_OK;
 }
 
-int launch_stage_update(const ws_grid* g, int krk, double dt, ws_soa f, ws_soa fn, ws_soa du,
-                        const ws_field prims[6], int* status, cudaStream_t st) {
+StagePrimArgs make_stage_args(const ws_grid* g, int krk, double dt, ws_soa f, ws_soa fn,
+                              ws_soa du, const ws_field prims[6], int* status) {
     StagePrimArgs a{};
     a.s.f = f; a.s.fn = fn; a.s.du = du;
     a.s.nx = g->nx; a.s.ny = g->ny; a.s.nz = g->nz; a.s.krk = krk; a.s.dt = dt;
@@ -301,13 +348,69 @@ int launch_stage_update(const ws_grid* g, int krk, double dt, ws_soa f, ws_soa f
     a.cv = 1.0 / (g->gamma * (g->gamma - 1.0) * g->ama * g->ama);
     a.ama = g->ama;
     a.status = status;
-    stage_update_kernel<<<grid_for((long)g->nx * g->ny * g->nz, 256), 256, 0, st>>>(a);
+    return a;
+}
+
+int launch_stage_update(const ws_grid* g, int krk, double dt, ws_soa f, ws_soa fn, ws_soa du,
+                        const ws_field prims[6], int* status, cudaStream_t st) {
+    const StagePrimArgs a = make_stage_args(g, krk, dt, f, fn, du, prims, status);
+    const int blocks = grid_for((long)g->nx * g->ny * g->nz, 256);
+    if (krk == 1) stage_update_kernel<1><<<blocks, 256, 0, st>>>(a);
+    else if (krk == 2) stage_update_kernel<2><<<blocks, 256, 0, st>>>(a);
+    else stage_update_kernel<3><<<blocks, 256, 0, st>>>(a);
     WS_CUDA(cudaGetLastError());
     return WS_OK;
 }
 
 int launch_ghost_fill_prims(const ws_grid* g, const ws_field prims[6], cudaStream_t st) {
     return launch_ghost_fill(g, prims, 6, st);
+}
+
+// ---- batched launches ----------------------------------------------------
+size_t ghost_args_size() { return sizeof(GhostArgs); }
+size_t stage_args_size() { return sizeof(StagePrimArgs); }
+
+void fill_ghost_args(void* out, const ws_grid* g, const ws_field prims[6]) {
+    GhostArgs a{};
+    for (int i = 0; i < 6; ++i) {
+        a.ptr[i] = prims[i].ptr;
+        a.pitch[i] = prims[i].pitch;
+    }
+    a.nf = 6;
+    a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
+    for (int i = 0; i < 6; ++i) a.kind[i] = g->face_kind[i];
+    *reinterpret_cast<GhostArgs*>(out) = a;
+}
+
+void fill_stage_args(void* out, const ws_grid* g, double dt, ws_soa f, ws_soa fn, ws_soa du,
+                     const ws_field prims[6], int* status) {
+    *reinterpret_cast<StagePrimArgs*>(out) = make_stage_args(g, 0, dt, f, fn, du, prims, status);
+}
+
+long ghost_chunks(const ws_grid* g) {
+    return (ghost_count(g->nx, g->ny, g->nz) + kBatchChunk - 1) / kBatchChunk;
+}
+long cell_chunks(const ws_grid* g) {
+    return ((long)g->nx * g->ny * g->nz + kBatchChunk - 1) / kBatchChunk;
+}
+
+int launch_ghost_fill_batch(const void* grids, const int2* tab, int nblocks, cudaStream_t st) {
+    if (nblocks <= 0) return WS_OK;
+    ghost_fill_batch_kernel<<<nblocks, kBatchThreads, 0, st>>>(
+        reinterpret_cast<const GhostArgs*>(grids), tab);
+    WS_CUDA(cudaGetLastError());
+    return WS_OK;
+}
+
+int launch_stage_update_batch(const void* grids, const int2* tab, int nblocks, int krk,
+                              cudaStream_t st) {
+    if (nblocks <= 0) return WS_OK;
+    const StagePrimArgs* g = reinterpret_cast<const StagePrimArgs*>(grids);
+    if (krk == 1) stage_update_batch_kernel<1><<<nblocks, kBatchThreads, 0, st>>>(g, tab);
+    else if (krk == 2) stage_update_batch_kernel<2><<<nblocks, kBatchThreads, 0, st>>>(g, tab);
+    else stage_update_batch_kernel<3><<<nblocks, kBatchThreads, 0, st>>>(g, tab);
+    WS_CUDA(cudaGetLastError());
+    return WS_OK;
 }
 
 uint32_t lap_pitch(uint32_t nx) {

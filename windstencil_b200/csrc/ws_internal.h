@@ -4,6 +4,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/windstencil_b200.h"
 
@@ -46,6 +47,13 @@ int find_tile_cfg(int bx, int by, int threads);   // index or -1
 int launch_rhs(const RhsArgs& a, int precision, bool uniform, int cfg, int ctas,
                cudaStream_t st);
 int rhs_max_ctas(int precision, bool uniform, int cfg);   // resident CTAs on the device
+// Batched RHS over n grids (device array of RhsArgs, cum[n+1] tile-plane
+// prefix sums); all grids share precision, metric kind and tile shape.
+int launch_rhs_batch(const RhsArgs* grids, const long* cum, int n, int zc, int precision,
+                     bool uniform, int cfg, int ctas, cudaStream_t st);
+// Host-side RhsArgs of one grid and job (tile shape cfg, sweep cap scan).
+RhsArgs make_rhs_args(const ws_grid* g, ws_job job, const ws_field prims[5],
+                      const ws_metrics* m, ws_soa du, int cfg, int scan);
 
 // Field kernels (field_kernels.cu).
 struct FieldArgs {
@@ -67,5 +75,79 @@ int launch_stage_update(const ws_grid* g, int krk, double dt, ws_soa f, ws_soa f
 int launch_ghost_fill_prims(const ws_grid* g, const ws_field prims[6], cudaStream_t st);
 
 uint32_t lap_pitch(uint32_t nx);
+
+// Batched field kernels: per-grid argument blocks (opaque, sizes below) in
+// device memory and a block table int2{grid, chunk}.
+size_t ghost_args_size();
+size_t stage_args_size();
+void fill_ghost_args(void* out, const ws_grid* g, const ws_field prims[6]);
+void fill_stage_args(void* out, const ws_grid* g, double dt, ws_soa f, ws_soa fn, ws_soa du,
+                     const ws_field prims[6], int* status);
+long ghost_chunks(const ws_grid* g);
+long cell_chunks(const ws_grid* g);
+int launch_ghost_fill_batch(const void* grids, const int2* tab, int nblocks, cudaStream_t st);
+int launch_stage_update_batch(const void* grids, const int2* tab, int nblocks, int krk,
+                              cudaStream_t st);
+
+// Device-resident state of one grid (used by the solver, batches and the
+// server): f[2] and du SoA, d,u,v,w,T,cc LAP fields and a status word, in
+// one allocation.
+struct GridState {
+    ws_grid g{};
+    void* mem = nullptr;
+    size_t bytes = 0;
+    ws_soa f[2]{}, du{};
+    ws_field prims[6]{};
+    int* status = nullptr;
+    int cur = 0;            // buffer holding the current state
+    double dt = 0.0;
+};
+size_t grid_state_bytes(const ws_grid& g);
+// stream-ordered allocation from the device's default memory pool
+int grid_state_alloc(GridState& s, const ws_grid& g, cudaStream_t st);
+void grid_state_free(GridState& s, cudaStream_t st);
+// upload a dense conserved state and derive d,u,v,w,T,cc on the interior
+int grid_state_upload(GridState& s, const double* f_host, cudaStream_t st);
+int grid_state_download(GridState& s, double* f_host, cudaStream_t st);   // no sync
+
+// A set of grids stepped together: one batched launch per kernel per stage.
+class BatchRunner {
+  public:
+    BatchRunner() = default;
+    ~BatchRunner();
+    BatchRunner(const BatchRunner&) = delete;
+    BatchRunner& operator=(const BatchRunner&) = delete;
+    // (re)build the device tables for `grids` (all of one precision);
+    // invalidates captured graphs
+    int build(const std::vector<GridState*>& grids, int cfg, int zc, cudaStream_t st);
+    int enqueue_rhs(cudaStream_t st);
+    // one SSP-RK3 step of every grid from its current buffer into the other
+    int enqueue_step(cudaStream_t st);
+    // nsteps steps (graph replay); flips every grid's current buffer
+    int step(int nsteps, cudaStream_t st);
+    int size() const { return (int)grids_.size(); }
+    int cfg() const { return cfg_; }
+    int zc() const { return zc_; }
+    void release(cudaStream_t st);
+
+  private:
+    int upload_stage_tables(cudaStream_t st);
+    std::vector<GridState*> grids_;
+    int precision_ = 0, cfg_ = 0, zc_ = 1 << 30, ctas_ = 0;
+    void* dev_ = nullptr;           // device tables
+    size_t dev_bytes_ = 0;
+    RhsArgs* d_rhs_ = nullptr;
+    long* d_cum_ = nullptr;
+    void* d_ghost_ = nullptr;
+    int2* d_gtab_ = nullptr;
+    void* d_stage_[2] = {nullptr, nullptr};   // parity 0: cur -> other; 1: swapped
+    int2* d_stab_ = nullptr;
+    int n_gtab_ = 0, n_stab_ = 0;
+    int parity_ = 0;
+    cudaStream_t cap_ = nullptr;
+    cudaGraphExec_t exec_[2] = {nullptr, nullptr};
+    void drop_graphs();
+    std::vector<unsigned char> host_;
+};
 
 }  // namespace ws
