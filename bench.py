@@ -1,7 +1,7 @@
 #!/usr/bin/env python3
 """Benchmark of the BF3W inviscid RHS on B200 (one JSON line on rank 0).
 
-Workload (default): plain FP64 fused RHS on the 600x128x128 grid of the
+Headline workload: plain FP64 fused RHS on the 600x128x128 grid of the
 benchmark configuration "Plain FP64 fused RHS at 600x128x128 and 480x512x64":
 4 ghost cells, periodic in y and z, zero-gradient extrapolation in x, seeded
 Sod state (left rho=1, p=1; right rho=0.125, p=0.1; 1% noise), SSP-RK3 at
@@ -9,23 +9,31 @@ CFL 0.5.  One bench step = one SSP-RK3 time step = 3 RHS evaluations
 (ghost fill -> fused RHS -> stage update, x3), replayed from a CUDA graph.
 
   value          Gcell-RHS/s = cells x 3 x K / device time of K steps
-                 (CUDA events, max over ranks; state 1.2 GB > L2, no flush
-                 needed)
+                 (CUDA events, max over ranks; the state is 1.2 GB > L2, so
+                 no flush is needed)
   e2e            the same metric through the C ABI with host buffers: every
                  step uploads the conserved state from pinned host memory,
                  steps, and downloads it again
   roofline       the fused RHS kernel alone, timed with CUDA events on its
-                 launch stream; algorithmic FLOP = WS_FLOP_PER_CELL x cells;
-                 FP64-pipe bound, peak = FP64 FMA throughput measured in this
-                 run by a DFMA microkernel (MEASURED_PEAKS.json has no FP64
-                 figure); HBM fraction against MEASURED_PEAKS hbm_gbs
+                 launch stream; algorithmic FLOP = 7266 per cell (the
+                 oracle's operation count); FP64-pipe bound, peak = FP64 FMA
+                 throughput measured in this run by a DFMA microkernel
+                 (MEASURED_PEAKS.json has no FP64 figure); the HBM side uses
+                 MEASURED_PEAKS hbm_gbs
   cpu_baseline   the reference's own scalar kernels built for the host
                  (oracle/_ref), else the oracle port, on this machine's cores
+  mixed          the mixed-precision form on the 600x128x128 Fourier
+                 workload: kernel speed-up over FP64 and state error after
+                 100 steps (rel. L2 / L-inf per conserved field)
+  batched        256 uneven periodic grids, 50 SSP-RK3 steps, FP64 and mixed,
+                 against one-grid-at-a-time FP64 solves of the same grids
+  served         Poisson arrivals of solve requests into the continuous-
+                 batching server; p50/p99 latency and served throughput
 
---impl reference runs only the CPU reference arm (rank 0) on the same
+--impl reference runs only the CPU reference arm (rank 0) on the headline
 workload and metric.  --gpus N > 1 runs N independent replicas (one grid per
-rank, weak scaling; the single-grid path has no exchange step at one grid per
-GPU).
+rank, weak scaling: the single-grid path has no exchange step at one grid
+per GPU).
 """
 from __future__ import annotations
 
@@ -34,7 +42,6 @@ import json
 import os
 import subprocess
 import sys
-import threading
 import time
 
 import numpy as np
@@ -42,7 +49,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-FLOP_PER_CELL = 7266.0      # oracle.or_op_counts(): algorithmic FLOP per cell-RHS
+FLOP_PER_CELL = 7266.0      # oracle or_op_counts(): algorithmic FLOP per cell-RHS
 BYTES_PER_CELL = 80.0       # 5 FP64 primitives in + 5 FP64 du out (Cartesian metrics)
 
 
@@ -55,10 +62,19 @@ def parse():
     ap.add_argument("--nx", type=int, default=600)
     ap.add_argument("--ny", type=int, default=128)
     ap.add_argument("--nz", type=int, default=128)
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--batch-grids", type=int, default=256)
+    ap.add_argument("--batch-steps", type=int, default=50)
+    ap.add_argument("--serial-grids", type=int, default=32)
+    ap.add_argument("--serve-rate", type=float, default=200.0)
+    ap.add_argument("--serve-rate-low", type=float, default=6.0)
+    ap.add_argument("--serve-seconds", type=float, default=20.0)
+    ap.add_argument("--serve-drain", type=float, default=20.0)
     return ap.parse_args()
 
 
@@ -100,7 +116,7 @@ class ClockSampler:
     def summary(self):
         if not self.out:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm, smax, reasons = [], [], set()
+        sm, smax, pw, reasons = [], [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.out.strip().splitlines():
             p = [x.strip() for x in line.split(",")]
@@ -109,6 +125,7 @@ class ClockSampler:
             try:
                 sm.append(float(p[1]))
                 smax.append(float(p[2]))
+                pw.append(float(p[3]))
             except ValueError:
                 continue
             for n, v in zip(names, p[5:9]):
@@ -116,68 +133,58 @@ class ClockSampler:
                     reasons.add(n)
         return {"sm_mhz": float(np.median(sm)) if sm else None,
                 "sm_max_mhz": max(smax) if smax else None,
+                "power_w_max": max(pw) if pw else None,
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_arm(a, seconds, reference_preferred=True):
-    """Time the CPU inviscid RHS on the workload's grid (bounded sample)."""
+# ---------------------------------------------------------------------------
+# CPU arms (the oracle is the checker / reported baseline, never the product)
+# ---------------------------------------------------------------------------
+def _cpu_rhs_setup(nx, ny, nz, hz=None):
     from oracle.oracle import Oracle, RefFunctions, make_grid
     from windstencil_b200 import workloads as wl
     o = Oracle()
-    kind = "port"
-    rhs = o.du_invis
-    if reference_preferred and RefFunctions.available():
-        r = RefFunctions()
-        rhs = r.du_invis
-        kind = "reference"
-    og = make_grid(a.nx, a.ny, a.nz, face_kind=(1, 1, 0, 0, 0, 0))
-    f = wl.sod_state(a.nx, a.ny, a.nz, seed=2)
+    kind, rhs = "port", o.du_invis
+    if RefFunctions.available():
+        kind, rhs = "reference", RefFunctions().du_invis
+    og = make_grid(nx, ny, nz, hz=hz, face_kind=(1, 1, 0, 0, 0, 0))
+    f = wl.sod_state(nx, ny, nz, seed=2)
     d, u, v, w, T, _ = o.cons_to_prim(og, f)
     for x in (d, u, v, w, T):
         o.ghost_fill(og, x)
     cc = o.sound_speed(og, T)
-    cores = o.threads()
-    rhs(og, d, u, v, w, cc)         # warm-up (page-in, thread pool)
-    n = 0
-    t0 = time.perf_counter()
+    return o, kind, (lambda: rhs(og, d, u, v, w, cc))
+
+
+def cpu_arm(a, seconds):
+    """Bounded sample: full RHS evaluations of the headline grid for ~`seconds`."""
+    o, kind, run = _cpu_rhs_setup(a.nx, a.ny, a.nz)
+    run()                           # warm-up (page-in, thread pool)
+    n, t0 = 0, time.perf_counter()
     while True:
-        rhs(og, d, u, v, w, cc)
+        run()
         n += 1
         el = time.perf_counter() - t0
         if el >= seconds or n >= 50:
             break
-    value = a.nx * a.ny * a.nz * n / el / 1e9
-    sample = (f"{n} full inviscid RHS evaluation(s) of the {a.nx}x{a.ny}x{a.nz} grid in "
-              f"{el:.1f} s ({'reference scalar kernels built for the host' if kind == 'reference' else 'oracle port'}, "
-              f"OpenMP over {cores} threads)")
-    return {"value": value, "unit": "Gcell-RHS/s", "cores": cores, "kind": kind,
-            "sample": sample}
+    what = ("reference scalar kernels built for the host" if kind == "reference"
+            else "oracle port")
+    return {"value": a.nx * a.ny * a.nz * n / el / 1e9, "unit": "Gcell-RHS/s",
+            "cores": o.threads(), "kind": kind,
+            "sample": f"{n} full inviscid RHS evaluation(s) of the {a.nx}x{a.ny}x{a.nz} grid "
+                      f"in {el:.1f} s ({what}, OpenMP over {o.threads()} threads)"}
 
 
 def run_reference(a, rank, world):
     if rank != 0:
         return
-    from oracle.oracle import Oracle, RefFunctions, make_grid
-    from windstencil_b200 import workloads as wl
-    o = Oracle()
-    kind = "port"
-    rhs = o.du_invis
-    if RefFunctions.available():
-        rhs = RefFunctions().du_invis
-        kind = "reference"
-    # each step: one inviscid RHS on a 16-plane z-slab of the grid (bounded sample)
-    nzs = min(a.nz, 16)
-    og = make_grid(a.nx, a.ny, nzs, hz=1.0 / (a.nz - 1.0), face_kind=(1, 1, 0, 0, 0, 0))
-    f = wl.sod_state(a.nx, a.ny, nzs, seed=2)
-    d, u, v, w, T, _ = o.cons_to_prim(og, f)
-    for x in (d, u, v, w, T):
-        o.ghost_fill(og, x)
-    cc = o.sound_speed(og, T)
+    nzs = min(a.nz, 16)       # each step: one RHS on a 16-plane slab (bounded sample)
+    o, kind, run = _cpu_rhs_setup(a.nx, a.ny, nzs, hz=1.0 / (a.nz - 1.0))
     for _ in range(a.warmup):
-        rhs(og, d, u, v, w, cc)
+        run()
     t0 = time.perf_counter()
     for _ in range(a.steps):
-        rhs(og, d, u, v, w, cc)
+        run()
     el = time.perf_counter() - t0
     value = a.nx * a.ny * nzs * a.steps / el / 1e9
     sample = (f"each step: one inviscid RHS on a {a.nx}x{a.ny}x{nzs} slab of the workload "
@@ -195,6 +202,201 @@ def run_reference(a, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# GPU arms
+# ---------------------------------------------------------------------------
+def _events(torch):
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _peak(ws, name):
+    import ctypes as C
+    out = C.c_double()
+    ws._abi.check(getattr(ws.load(), name)(C.byref(out), None))
+    return out.value
+
+
+def time_rhs_kernel(torch, ws, g, solver, stream, reps):
+    """Mean device time of the fused RHS through the drop-in entry point."""
+    import ctypes as C
+    _, du_desc, prims = solver.fields()
+    gc = g.c()
+    lib = ws.load()
+    job = ws.interior_job(g)
+    p5 = [prims[0], prims[1], prims[2], prims[3], prims[5]]
+    call = lambda: ws._abi.check(lib.ws_du_invis_jacobian3d(   # noqa: E731
+        C.byref(gc), job, *p5, None, du_desc, stream.cuda_stream))
+    for _ in range(2):
+        call()
+    e0, e1 = _events(torch)
+    e0.record(stream)
+    for _ in range(reps):
+        call()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def bench_mixed(a, torch, ws, wl, stream):
+    """Mixed form vs FP64 on the 600x128x128 Fourier workload, 100 steps."""
+    nx, ny, nz = a.nx, a.ny, a.nz
+    f0 = wl.fourier_state(nx, ny, nz, seed=1)
+    res = {"workload": f"{nx}x{ny}x{nz} periodic Fourier state with contact, 100 SSP-RK3 "
+                       "steps at CFL 0.5",
+           "error_measure": "per conserved field: rel. L2 = |a-b|_2/|b|_2, "
+                            "rel. L-inf = max|a-b|/max|b|, mixed vs FP64 on this GPU"}
+    out = {}
+    for name, prec in (("fp64", ws.FP64), ("mixed", ws.MIXED)):
+        g = ws.Grid(nx, ny, nz, precision=prec)
+        s = ws.Solver(g)
+        s.set_state(f0, stream=stream)
+        if name == "fp64":
+            dt = s.compute_dt(0.5, stream=stream)
+        out[name + "_kernel_ms"] = time_rhs_kernel(torch, ws, g, s, stream, 10)
+        s.step(dt, 2, stream=stream)
+        s.set_state(f0, stream=stream)
+        e0, e1 = _events(torch)
+        e0.record(stream)
+        s.step(dt, 100, stream=stream)
+        e1.record(stream)
+        e1.synchronize()
+        out[name + "_step_ms"] = e0.elapsed_time(e1) / 100
+        out[name + "_state"] = s.get_state(stream=stream)
+        s.close()
+    a64, a32 = out["fp64_state"], out["mixed_state"]
+    l2 = [float(np.linalg.norm(a32[i] - a64[i]) / np.linalg.norm(a64[i])) for i in range(5)]
+    li = [float(np.max(np.abs(a32[i] - a64[i])) / np.max(np.abs(a64[i]))) for i in range(5)]
+    cells = nx * ny * nz
+    peak32 = _peak(ws, "ws_probe_fp32_peak")
+    res.update({
+        "kernel_ms_fp64": out["fp64_kernel_ms"], "kernel_ms_mixed": out["mixed_kernel_ms"],
+        "kernel_speedup_vs_fp64": out["fp64_kernel_ms"] / out["mixed_kernel_ms"],
+        "value": cells * 3 / (out["mixed_step_ms"] * 1e-3) / 1e9,
+        "value_fp64_same_workload": cells * 3 / (out["fp64_step_ms"] * 1e-3) / 1e9,
+        "unit": "Gcell-RHS/s",
+        "step_speedup_vs_fp64": out["fp64_step_ms"] / out["mixed_step_ms"],
+        "state_rel_l2": l2, "state_rel_linf": li, "max_rel_l2": max(l2),
+        "fp32_peak_tflops_measured": peak32,
+        "rhs_gcell_s": cells / (out["mixed_kernel_ms"] * 1e-3) / 1e9})
+    return res
+
+
+def bench_batch(a, torch, ws, wl, stream):
+    specs = wl.batch_specs(a.batch_grids, seed=4)
+    cells = sum(s.cells for s in specs)
+    states = [wl.batch_state(s) for s in specs]
+    res = {"workload": f"{len(specs)} periodic grids, nx log-U[32,256], ny,nz log-U[16,128], "
+                       "Mach U[0.3,3], Sod jump at a seeded x, 1% noise; "
+                       f"{a.batch_steps} SSP-RK3 steps at CFL 0.5",
+           "grids": len(specs), "cells": cells}
+    dts = None
+    for name, prec in (("fp64", ws.FP64), ("mixed", ws.MIXED)):
+        b = ws.Batch([ws.Grid(s.nx, s.ny, s.nz, precision=prec) for s in specs])
+        for i, f in enumerate(states):
+            b.set_state(i, f, stream=stream)
+        if dts is None:
+            dts = b.compute_dt(0.5, stream=stream)
+        b.set_dt(dts)
+        tile = b.autotune(stream=stream)
+        b.step(2, stream=stream)
+        for i, f in enumerate(states):       # same stream: ordered after the warm-up
+            b.set_state(i, f, stream=stream)
+        stream.synchronize()
+        e0, e1 = _events(torch)
+        e0.record(stream)
+        b.step(a.batch_steps, stream=stream)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        st = b.status()
+        b.close()
+        res[name] = {"value": cells * 3 * a.batch_steps / (ms * 1e-3) / 1e9,
+                     "unit": "Gcell-RHS/s", "ms_per_step": ms / a.batch_steps,
+                     "tile": list(tile), "nonfinite_grids": int(sum(1 for x in st if x)),
+                     "launches_per_step": 9}
+    # one grid at a time, FP64, same grids (a sample of them), same steps
+    nser = min(a.serial_grids, len(specs))
+    tot_ms, ser_cells = 0.0, 0
+    for i in range(nser):
+        s = specs[i]
+        sol = ws.Solver(ws.Grid(s.nx, s.ny, s.nz))
+        sol.set_state(states[i], stream=stream)
+        sol.step(dts[i], 1, stream=stream)
+        sol.set_state(states[i], stream=stream)
+        e0, e1 = _events(torch)
+        e0.record(stream)
+        sol.step(dts[i], a.batch_steps, stream=stream)
+        e1.record(stream)
+        e1.synchronize()
+        tot_ms += e0.elapsed_time(e1)
+        ser_cells += s.cells
+        sol.close()
+    serial = ser_cells * 3 * a.batch_steps / (tot_ms * 1e-3) / 1e9
+    res["one_grid_at_a_time_fp64"] = {
+        "value": serial, "unit": "Gcell-RHS/s",
+        "sample": f"grids 0..{nser - 1} of the batch, each solved alone with ws_solver "
+                  f"({a.batch_steps} steps, graph-captured)"}
+    res["speedup_fp64_vs_one_at_a_time"] = res["fp64"]["value"] / serial
+    res["speedup_mixed_vs_one_at_a_time"] = res["mixed"]["value"] / serial
+    return res, serial
+
+
+def bench_serve(a, ws, wl, serial_rate, rate, seconds, drain, seed=5):
+    """Poisson arrivals into the continuous-batching server (bounded run)."""
+    rng = np.random.default_rng(seed)
+    specs = wl.batch_specs(int(rate * seconds * 1.2) + 16, seed=seed)
+    srv = ws.Server(hbm_budget_bytes=80 << 30)
+    t0 = time.perf_counter()
+    t_next = 0.0
+    ids, offered_work = [], 0.0
+    i = 0
+    while True:
+        now = time.perf_counter() - t0
+        if now >= seconds:
+            break
+        if now < t_next:
+            time.sleep(min(t_next - now, 0.01))
+            continue
+        s = specs[i % len(specs)]
+        nsteps = int(rng.integers(50, 501))
+        prec = ws.FP64 if rng.random() < 0.5 else ws.MIXED
+        g = ws.Grid(s.nx, s.ny, s.nz, precision=prec)
+        ids.append(srv.submit(g, nsteps, cfl=0.5, seed=s.seed, mach=s.mach, x_jump=s.x_jump,
+                              want_result=False))
+        offered_work += 3.0 * nsteps * s.cells
+        i += 1
+        t_next += rng.exponential(1.0 / rate)
+    deadline = time.perf_counter() + drain
+    while time.perf_counter() < deadline:
+        st = srv.stats()
+        if st["completed"] + st["failed"] >= len(ids):
+            break
+        time.sleep(0.2)
+    st = srv.stats()
+    wall = time.perf_counter() - t0
+    srv.close()
+    served = st["served_cell_rhs"] / wall / 1e9
+    executed = st["executed_cell_rhs"] / wall / 1e9
+    return {
+        "arrivals": "Poisson", "rate_per_s": rate, "arrival_window_s": seconds,
+        "offered_requests": len(ids), "completed": st["completed"], "failed": st["failed"],
+        "unfinished_at_stop": len(ids) - st["completed"] - st["failed"],
+        "wall_s": wall, "p50_latency_s": st["p50_latency_s"],
+        "p99_latency_s": st["p99_latency_s"], "mean_latency_s": st["mean_latency_s"],
+        "latency_over": "completed requests (submit -> result on the device)",
+        "max_concurrent_grids": st["max_active"], "ticks": st["ticks"],
+        "offered_gcell_rhs_s": offered_work / seconds / 1e9,
+        "served_gcell_rhs_s": served, "executed_gcell_rhs_s": executed, "unit": "Gcell-RHS/s",
+        "served_vs_one_at_a_time_fp64": served / serial_rate if serial_rate else None,
+        "executed_vs_one_at_a_time_fp64": executed / serial_rate if serial_rate else None,
+        "requests": "grid as the batched workload, steps U[50,500], FP64 or mixed 50/50, "
+                    "80 GiB state budget, seeded initial state generated on the device",
+        "note": "admission: FIFO under the HBM budget and a 3.2e7 active-cell cap; "
+                "arrivals stop at the end of the window, latency percentiles cover the "
+                "requests finished by the drain deadline; served counts finished requests' "
+                "work, executed all device work in the window"}
+
+
 def run_ours(a, rank, world, dist):
     import torch
     import windstencil_b200 as ws
@@ -202,9 +404,8 @@ def run_ours(a, rank, world, dist):
 
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    prec = ws.MIXED if a.precision == "mixed" else ws.FP64
     faces = (ws.FACE_EXTRAP, ws.FACE_EXTRAP, 0, 0, 0, 0)
-    g = ws.Grid(a.nx, a.ny, a.nz, faces=faces, precision=prec)
+    g = ws.Grid(a.nx, a.ny, a.nz, faces=faces)
     cells = g.cells
     f0 = wl.sod_state(a.nx, a.ny, a.nz, seed=2 + rank)
     s = ws.Solver(g)
@@ -221,7 +422,7 @@ def run_ours(a, rank, world, dist):
     stream.synchronize()
     barrier()
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0, e1 = _events(torch)
     with ClockSampler(local) as clk:
         e0.record(stream)
         s.step(dt, a.steps, stream=stream)
@@ -237,63 +438,46 @@ def run_ours(a, rank, world, dist):
     status = s.status(stream=stream)
     value = world * cells * 3 * a.steps / (ms * 1e-3) / 1e9
 
-    # ---- dominant kernel alone: the fused RHS through the drop-in entry point
-    f_desc, du_desc, prims = s.fields()
-    gc = g.c()
-    lib = ws.load()
-    import ctypes as C
-    job = ws.interior_job(g)
-    p5 = [prims[0], prims[1], prims[2], prims[3], prims[5]]
-    nrhs = max(3, a.steps)
-    for _ in range(2):
-        ws._abi.check(lib.ws_du_invis_jacobian3d(C.byref(gc), job, *p5, None, du_desc,
-                                                 stream.cuda_stream))
-    k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    k0.record(stream)
-    for _ in range(nrhs):
-        ws._abi.check(lib.ws_du_invis_jacobian3d(C.byref(gc), job, *p5, None, du_desc,
-                                                 stream.cuda_stream))
-    k1.record(stream)
-    k1.synchronize()
-    rhs_ms = k0.elapsed_time(k1) / nrhs
-    peak = fp64_peak_tflops(torch, stream)
+    # ---- dominant kernel alone (drop-in entry point, same stream)
+    rhs_ms = time_rhs_kernel(torch, ws, g, s, stream, max(3, min(a.steps, 20)))
+    peak = _peak(ws, "ws_probe_fp64_peak")
     achieved = FLOP_PER_CELL * cells / (rhs_ms * 1e-3) / 1e12
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
         pass
-    hbm = peaks.get("hbm_gbs")
-    traffic = measured_traffic(a)
     roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-            "frac": achieved / peak if peak else None, "traffic": traffic,
-            "kernel": "bf3w_rhs_kernel", "kernel_ms": rhs_ms,
+            "frac": achieved / peak if peak else None, "traffic": measured_traffic(a),
+            "kernel": "bf3w_rhs_kernel<16,8,512,1,double>", "kernel_ms": rhs_ms,
             "peak_source": "DFMA microkernel measured in this run (of measured)",
             "algorithmic_flop_per_cell": FLOP_PER_CELL,
             "algorithmic_bytes_per_cell": BYTES_PER_CELL,
+            "rhs_gcell_s": cells / (rhs_ms * 1e-3) / 1e9,
             "hbm_achieved_gbs": BYTES_PER_CELL * cells / (rhs_ms * 1e-3) / 1e9,
-            "hbm_peak_gbs": hbm}
+            "hbm_peak_gbs": peaks.get("hbm_gbs"), "hbm_peak_source": "MEASURED_PEAKS.json"}
 
     # ---- end to end through the C ABI with host buffers
     e2e = None
     if not a.no_e2e:
+        import ctypes as C  # noqa: F401
+        lib = ws.load()
         host = torch.empty((5, a.nz, a.ny, a.nx), dtype=torch.float64).pin_memory()
         host.copy_(torch.from_numpy(f0))
-        hp = host.numpy()
-        ptr = hp.ctypes.data
+        ptr = host.numpy().ctypes.data
         n_e2e = max(2, min(a.steps, 10))
-        for _ in range(1):
+
+        def one():
             ws._abi.check(lib.ws_solver_set_state(s.h, ptr, stream.cuda_stream))
             s.step(dt, 1, stream=stream)
             ws._abi.check(lib.ws_solver_get_state(s.h, ptr, stream.cuda_stream))
+        one()
         barrier()
-        q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        q0, q1 = _events(torch)
         w0 = time.perf_counter()
         q0.record(stream)
         for _ in range(n_e2e):
-            ws._abi.check(lib.ws_solver_set_state(s.h, ptr, stream.cuda_stream))
-            s.step(dt, 1, stream=stream)
-            ws._abi.check(lib.ws_solver_get_state(s.h, ptr, stream.cuda_stream))
+            one()
         q1.record(stream)
         q1.synchronize()
         wall = time.perf_counter() - w0
@@ -308,43 +492,39 @@ def run_ours(a, rank, world, dist):
                "steps": n_e2e, "wall_s": wall,
                "note": "every step: pinned host state -> device, one SSP-RK3 step, "
                        "state -> pinned host, through ws_solver_set_state/step/get_state"}
+    s.close()
 
+    extra = {}
+    if rank == 0 and world == 1:
+        if not a.no_mixed:
+            extra["mixed"] = bench_mixed(a, torch, ws, wl, stream)
+        serial = None
+        if not a.no_batch:
+            extra["batched"], serial = bench_batch(a, torch, ws, wl, stream)
+        if not a.no_serve:
+            # the configuration's offered load (200/s, far above one GPU) and a
+            # load one B200 sustains, where latency is not queueing-bound
+            extra["served"] = bench_serve(a, ws, wl, serial, a.serve_rate, a.serve_seconds,
+                                          a.serve_drain)
+            extra["served_sustainable"] = bench_serve(a, ws, wl, serial, a.serve_rate_low,
+                                                      a.serve_seconds, a.serve_drain, seed=6)
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
         cpu = cpu_arm(a, a.cpu_seconds)
 
-    s.close()
     if rank == 0:
         line = {"metric": "Gcell-RHS/s", "value": value, "unit": "Gcell-RHS/s", "n_gpus": world,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms / a.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64" if prec == ws.FP64 else "f64 state / f32 flux",
-                "data": "synthetic",
-                "config": {"workload": workload_name(a) if prec == ws.FP64 else
-                           workload_name(a).replace("fp64", "mixed"),
-                           "grid": [a.nx, a.ny, a.nz], "rhs_per_step": 3, "cfl": 0.5,
-                           "dt": dt, "inputs_exceed_l2": True,
-                           "parallelism": f"replicas{world}"},
+                "dtype": "f64", "data": "synthetic",
+                "config": {"workload": workload_name(a), "grid": [a.nx, a.ny, a.nz],
+                           "rhs_per_step": 3, "cfl": 0.5, "dt": dt,
+                           "inputs_exceed_l2": True, "parallelism": f"replicas{world}"},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": 9 * a.steps, "clocks": clk.summary(),
                 "device_status": status}
+        line.update(extra)
         print(json.dumps(line), flush=True)
-
-
-_PEAK = None
-
-
-def fp64_peak_tflops(torch, stream):
-    import ctypes as C
-    import windstencil_b200 as ws
-    lib = ws.load()
-    if not hasattr(lib, "ws_probe_fp64_peak"):
-        return None
-    lib.ws_probe_fp64_peak.restype = C.c_int
-    lib.ws_probe_fp64_peak.argtypes = [C.POINTER(C.c_double), C.c_void_p]
-    out = C.c_double()
-    ws._abi.check(lib.ws_probe_fp64_peak(C.byref(out), stream.cuda_stream))
-    return out.value
 
 
 def measured_traffic(a):

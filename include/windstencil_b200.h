@@ -251,6 +251,8 @@ typedef struct ws_server_config {
     size_t hbm_budget_bytes;  /* device memory for request states (0: 80 GiB) */
     int32_t max_active;       /* concurrent grids (0: 4096)                    */
     ws_tile tile;             /* kernel tile shape (zeroes: default)           */
+    double max_active_cells;  /* cells stepped per tick; admission waits above
+                                 it once the device is full (0: 3.2e7)         */
 } ws_server_config;
 
 typedef struct ws_request {
@@ -272,6 +274,7 @@ typedef struct ws_server_stats {
     size_t hbm_in_use;
     double p50_latency_s, p99_latency_s, mean_latency_s;  /* submit -> result */
     double served_cell_rhs;    /* cell-RHS evaluations of completed requests  */
+    double executed_cell_rhs;  /* cell-RHS evaluations run, finished or not   */
     double busy_s, elapsed_s;
 } ws_server_stats;
 

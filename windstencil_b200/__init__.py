@@ -327,9 +327,10 @@ class Batch:
 class Server:
     """Continuous-batching solve server (ws_server_*)."""
 
-    def __init__(self, hbm_budget_bytes=80 << 30, max_active=4096, tile=(0, 0, 0, 0)):
+    def __init__(self, hbm_budget_bytes=80 << 30, max_active=4096, tile=(0, 0, 0, 0),
+                 max_active_cells=0.0):
         from ._abi import WsServerConfig
-        cfg = WsServerConfig(hbm_budget_bytes, max_active, WsTile(*tile))
+        cfg = WsServerConfig(hbm_budget_bytes, max_active, WsTile(*tile), max_active_cells)
         h = C.c_void_p()
         check(load().ws_server_create(C.byref(cfg), C.byref(h)))
         self.h = h

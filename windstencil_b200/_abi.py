@@ -60,7 +60,8 @@ class WsTile(C.Structure):
 
 
 class WsServerConfig(C.Structure):
-    _fields_ = [("hbm_budget_bytes", C.c_size_t), ("max_active", C.c_int32), ("tile", WsTile)]
+    _fields_ = [("hbm_budget_bytes", C.c_size_t), ("max_active", C.c_int32), ("tile", WsTile),
+                ("max_active_cells", C.c_double)]
 
 
 class WsRequest(C.Structure):
@@ -75,7 +76,8 @@ class WsServerStats(C.Structure):
                                         "ticks", "max_active")] + [
         ("hbm_in_use", C.c_size_t), ("p50_latency_s", C.c_double),
         ("p99_latency_s", C.c_double), ("mean_latency_s", C.c_double),
-        ("served_cell_rhs", C.c_double), ("busy_s", C.c_double), ("elapsed_s", C.c_double)]
+        ("served_cell_rhs", C.c_double), ("executed_cell_rhs", C.c_double),
+        ("busy_s", C.c_double), ("elapsed_s", C.c_double)]
 
 
 _P = C.c_void_p

@@ -112,16 +112,28 @@ struct ws_server {
     bool rebuild = true;
     // statistics
     std::vector<double> latencies;
-    double served_cell_rhs = 0, t_start = 0, t_last = 0;
+    double served_cell_rhs = 0, executed_cell_rhs = 0, t_start = 0, t_last = 0;
     long ticks = 0, admitted = 0, completed = 0, failed = 0, max_active_seen = 0;
     double busy_s = 0;
+    double active_cells = 0;
 };
 
 namespace {
 
+double cells_of(const Req* q) {
+    return (double)q->r.grid.nx * q->r.grid.ny * q->r.grid.nz;
+}
+
+// FIFO admission: memory (HBM budget) and compute (active cells) both cap the
+// running set; the compute cap keeps a tick short once the device is full,
+// so admitted requests finish sooner instead of all slowing down together.
 int admit_locked(ws_server* s, std::vector<Req*>& fresh) {
+    double cells = s->active_cells;
+    for (Req* q : fresh) cells += cells_of(q);
     while (!s->queue.empty() && (int)s->active.size() + (int)fresh.size() < s->cfg.max_active) {
         Req* q = s->reqs[s->queue.front()].get();
+        const bool idle = s->active.empty() && fresh.empty();
+        if (!idle && cells + cells_of(q) > (double)s->cfg.max_active_cells) break;
         if (s->used + q->bytes > s->cfg.hbm_budget_bytes) {
             if (s->active.empty() && fresh.empty()) {       // can never fit
                 q->state = RQ_FAILED;
@@ -135,6 +147,7 @@ int admit_locked(ws_server* s, std::vector<Req*>& fresh) {
         }
         s->queue.pop_front();
         s->used += q->bytes;
+        cells += cells_of(q);
         q->state = RQ_RUNNING;
         q->t_admit = now_s();
         fresh.push_back(q);
@@ -232,6 +245,7 @@ void loop(ws_server* s) {
                     finish(s, q, rc ? rc : WS_ERR_NONFINITE);
                 } else {
                     s->active.push_back(q);
+                    s->active_cells += cells_of(q);
                     s->admitted++;
                 }
             }
@@ -256,6 +270,7 @@ void loop(ws_server* s) {
         for (int p = 0; p < 2; ++p) s->runner[p].step(1, st);
         cudaStreamSynchronize(st);
         s->ticks++;
+        s->executed_cell_rhs += 3.0 * s->active_cells;
         std::vector<Req*> done;
         for (Req* q : s->active)
             if (++q->steps_done >= q->r.nsteps) done.push_back(q);
@@ -276,6 +291,7 @@ void loop(ws_server* s) {
                 Req* q = done[i];
                 grid_state_free(q->st, st);
                 s->active.erase(std::find(s->active.begin(), s->active.end(), q));
+                s->active_cells -= cells_of(q);
                 finish(s, q, err ? err : (status[i] ? WS_ERR_NONFINITE : WS_OK));
             }
             s->rebuild = true;
@@ -300,6 +316,7 @@ int ws_server_create(const ws_server_config* cfg, ws_server** out) {
     if (cfg) s->cfg = *cfg;
     if (s->cfg.hbm_budget_bytes == 0) s->cfg.hbm_budget_bytes = (size_t)80 << 30;
     if (s->cfg.max_active <= 0) s->cfg.max_active = 4096;
+    if (s->cfg.max_active_cells <= 0) s->cfg.max_active_cells = 32.0e6;
     WS_CUDA(cudaGetDevice(&s->dev));
     WS_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     // keep freed request memory in the pool instead of returning it to the OS
@@ -406,6 +423,7 @@ int ws_server_get_stats(ws_server* s, ws_server_stats* out) {
         return a / l.size();
     }();
     out->served_cell_rhs = s->served_cell_rhs;
+    out->executed_cell_rhs = s->executed_cell_rhs;
     out->busy_s = s->busy_s;
     out->elapsed_s = now_s() - s->t_start;
     return WS_OK;
