@@ -1,0 +1,90 @@
+"""Properties of the inviscid operator, checked on the oracle (CPU).
+
+The reference has no test suite or golden data (its only evidence is a
+10,000-step energy/temperature comparison in its README), so the oracle is
+pinned by the reference's own scalar kernels (test_oracle_pin.py) and by
+these properties of the discretisation.
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle import LAP, make_grid
+from windstencil_b200 import workloads as wl
+
+
+def _rhs(oracle, g, f):
+    return oracle.rhs_conserved(g, f)
+
+
+def test_free_stream_preservation(oracle):
+    g = make_grid(20, 12, 10)
+    d = np.ones((10, 12, 20)) * 1.3
+    u, v, w = np.full_like(d, 0.7), np.full_like(d, -0.2), np.full_like(d, 0.1)
+    T = np.full_like(d, 0.9)
+    f = wl.prim_to_cons(d, u, v, w, T)
+    du = _rhs(oracle, g, f)
+    assert np.max(np.abs(du)) <= 1e-12
+
+
+def test_discrete_conservation_periodic(oracle):
+    """Telescoping face differences: sum of du over a periodic grid is 0."""
+    g = make_grid(24, 16, 12)
+    f = wl.fourier_state(24, 16, 12, seed=3)
+    du = _rhs(oracle, g, f)
+    for v in range(5):
+        scale = np.sum(np.abs(du[v]))
+        assert abs(np.sum(du[v])) <= 1e-12 * scale
+
+
+def test_axis_permutation(oracle):
+    """Swapping x and y of the state (and of u, v) swaps the RHS."""
+    nx, ny, nz = 16, 16, 8
+    g = make_grid(nx, ny, nz)
+    f = wl.fourier_state(nx, ny, nz, seed=4)
+    ft = np.ascontiguousarray(np.swapaxes(f, 2, 3)[[0, 2, 1, 3, 4]])
+    a = _rhs(oracle, g, f)
+    b = _rhs(oracle, g, ft)
+    bt = np.swapaxes(b, 2, 3)[[0, 2, 1, 3, 4]]
+    assert np.max(np.abs(a - bt)) <= 1e-11 * np.max(np.abs(a))
+
+
+def test_smooth_convergence_order(oracle):
+    """Entropy wave rho = 1 + 0.1 sin(2 pi x), u = 0.5 (subsonic everywhere,
+    so the split fluxes are smooth), p = 1/gamma, periodic in x: the mass RHS
+    error against the exact -d(rho u)/dx falls at fourth order: the
+    bandwidth-optimised linear weights of WENO-SYMBO (OCFD_Schemes.cpp:344-348)
+    trade formal order for resolution, and the observed order is ~4.0-4.5."""
+    errs = []
+    for n in (16, 32, 64):
+        L = 1.0
+        h = L / n
+        g = make_grid(n, 4, 4, hx=h, hy=h, hz=h)
+        x = np.arange(n) * h
+        d = (1 + 0.1 * np.sin(2 * np.pi * x))[None, None, :] * np.ones((4, 4, n))
+        u = np.full_like(d, 0.5)
+        T = 1.0 / d            # p = rho T / gamma = 1/gamma
+        f = wl.prim_to_cons(d, u, np.zeros_like(d), np.zeros_like(d), T)
+        du = _rhs(oracle, g, f)
+        exact = -(0.5 * 0.1 * 2 * np.pi * np.cos(2 * np.pi * x))[None, None, :]
+        errs.append(np.max(np.abs(du[0] - exact)))
+    orders = np.log2(np.array(errs[:-1]) / np.array(errs[1:]))
+    assert orders.min() >= 3.8, (errs, orders)
+
+
+@pytest.mark.timeout(120)
+def test_high_mach_noisy_state_goes_nonphysical_in_reference_arithmetic(oracle):
+    """A synthetic request state (Mach 2.17 Sod-type jump with 1% cell noise)
+    loses positivity within 100 steps at CFL 0.5 in the oracle, whose scalar
+    kernels are the reference's own: such requests fail with
+    WS_ERR_NONFINITE on the GPU for the same reason, not a GPU defect."""
+    nx, ny, nz = 90, 25, 32
+    g = make_grid(nx, ny, nz)
+    f = wl.synth_state(nx, ny, nz, 1615840711, 2.173, 0.608)
+    dt = oracle.compute_dt(g, f, 0.5)
+    f = oracle.rk3_steps(g, f, dt, 60)
+    assert np.all(np.isfinite(f)) and f[0].min() > 0
+    f = oracle.rk3_steps(g, f, dt, 40)
+    d, u, v, w, T, _ = oracle.cons_to_prim(g, f) if np.all(np.isfinite(f)) else [None] * 6
+    bad = (not np.all(np.isfinite(f))) or f[0].min() <= 0 or \
+        np.min(T[LAP:-LAP, LAP:-LAP, LAP:-LAP]) <= 0
+    assert bad

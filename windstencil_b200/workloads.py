@@ -123,6 +123,36 @@ def batch_state(spec: GridSpec, gamma=1.4, ama=1.0):
     return prim_to_cons(d, u, v, w, T, gamma, ama)
 
 
+_M64 = np.uint64(0xFFFFFFFFFFFFFFFF)
+
+
+def _splitmix_uniform(seed, n):
+    """[-1, 1) from the splitmix64 finaliser of seed + golden*(n+1) (Steele,
+    Lea and Flood 2014); the same counter-based hash as the server's device
+    generator, so host and device build identical synthetic states."""
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed) + np.uint64(0x9E3779B97F4A7C15) * (n.astype(np.uint64) + np.uint64(1))
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0) * 2.0 - 1.0
+
+
+def synth_state(nx, ny, nz, seed, mach, x_jump, gamma=1.4, ama=1.0):
+    """Host copy of the server's seeded synthetic request state (ws_request
+    with f0_host == NULL): periodic Sod-type jump moving at `mach`, 1% noise."""
+    t = np.arange(nx * ny * nz, dtype=np.int64).reshape(nz, ny, nx)
+    left = (np.arange(nx) + 0.5) < x_jump * nx
+    d = np.where(left, 1.0, 0.125)[None, None, :] * np.ones((nz, ny, nx))
+    p = np.where(left, 1.0, 0.1)[None, None, :] / gamma * np.ones((nz, ny, nx))
+    d = d * (1.0 + 0.01 * _splitmix_uniform(seed, 3 * t))
+    u = np.full_like(d, mach * ama)
+    v = 0.01 * _splitmix_uniform(seed, 3 * t + 1)
+    w = 0.01 * _splitmix_uniform(seed, 3 * t + 2)
+    T = gamma * ama * ama * p / d
+    return prim_to_cons(d, u, v, w, T, gamma, ama)
+
+
 def lap_from_interior(a, lap=4, pitch=None):
     """Dense LAP array (nz+8, ny+8, pitch or nx+8) with `a` in the interior."""
     nz, ny, nx = a.shape
