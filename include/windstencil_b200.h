@@ -180,6 +180,27 @@ WS_API int ws_prim_to_cons(const ws_grid* g, ws_field d, ws_field u, ws_field v,
 WS_API int ws_time_advance(const ws_grid* g, int krk, double dt, ws_soa f, ws_soa fn, ws_soa du,
                     ws_stream_t stream);
 
+/* CFL time step of n caller-owned grids, allocating nothing.
+ * No counterpart in the reference (it takes DT as an input).
+ * For callers that must not allocate device memory after start-up: a host
+ * code that owns every device buffer in its own arena (as the reference's
+ * time loop does) or runs under a hard device-memory cap, and any loop that
+ * cannot afford the device-wide wait that cudaMalloc/cudaFree imply.  The
+ * other dt entry points use allocated scratch; this one reduces into a fixed
+ * array of WS_DT_STATIC_MAX_GRIDS entries compiled into the library, present
+ * on every GPU that loads it until the process exits.
+ * prims: 4 LAP fields per grid, in the order u, v, w, cc.
+ * dt_out[i] = cfl / max over grid i's interior of
+ *             |u|/hx + |v|/hy + |w|/hz + cc*sqrt(hx^-2 + hy^-2 + hz^-2).
+ * n above WS_DT_STATIC_MAX_GRIDS is rejected with WS_ERR_INVALID.  The first
+ * call with a given device current looks up the array's device address;
+ * make that first call before any stream capture.  All calls share the
+ * array (each clears the entries it uses first), so calls whose work
+ * overlaps on the GPU race: serialise them.  Synchronises `stream`. */
+#define WS_DT_STATIC_MAX_GRIDS 4096
+WS_API int ws_compute_dt_static(const ws_grid* grids, const ws_field* prims, int n, double cfl,
+                                double* dt_out, ws_stream_t stream);
+
 /* ------------------------------------------------------------------------ */
 /* One grid, device-resident, SSP-RK3 step as one CUDA graph                 */
 /* Replaces the time loop NS_solver_real (OCFD_NS_Solver.cpp:64-90) with all  */

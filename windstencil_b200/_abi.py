@@ -122,6 +122,8 @@ SIGNATURES = {
     "ws_batch_step": (_I, [_P, _I, _P]),
     "ws_batch_status": (_I, [_P, C.POINTER(_I), _P]),
     "ws_batch_autotune": (_I, [_P, C.POINTER(WsTile), _P]),
+    "ws_compute_dt_static": (_I, [C.POINTER(WsGrid), C.POINTER(WsField), _I, C.c_double,
+                                  C.POINTER(C.c_double), _P]),
     "ws_server_create": (_I, [C.POINTER(WsServerConfig), C.POINTER(_P)]),
     "ws_server_destroy": (None, [_P]),
     "ws_server_submit": (_I, [_P, C.POINTER(WsRequest), C.POINTER(C.c_uint64)]),
