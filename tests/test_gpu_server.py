@@ -110,3 +110,21 @@ def test_server_failure_isolated(cuda):
     srv.close()
     assert st["failed"] == 1 and st["completed"] == 1
     assert st["p50_latency_s"] > 0
+
+
+def test_server_synthetic_state_matches_host_generator(cuda):
+    """The server's seeded device-side initial state equals the host
+    generator workloads.synth_state (same counter-based hash)."""
+    nx, ny, nz = 30, 12, 10
+    g = ws.Grid(nx, ny, nz)
+    srv = ws.Server()
+    rid = srv.submit(g, 1, dt=1e-4, seed=77, mach=1.5, x_jump=0.45)
+    out = srv.wait(rid, timeout=60)
+    srv.close()
+    f0 = wl.synth_state(nx, ny, nz, 77, 1.5, 0.45)
+    s = ws.Solver(g)
+    s.set_state(f0)
+    s.step(1e-4, 1)
+    ref = s.get_state()
+    s.close()
+    assert rel_linf(out, ref).max() <= 1e-13
