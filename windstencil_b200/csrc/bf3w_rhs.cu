@@ -60,6 +60,9 @@ struct RhsLayout {
     static constexpr size_t smem_bytes =
         (size_t)(N_STG + N_FX + N_FY + N_FZ) * sizeof(double) +
         (size_t)(N_RING + N_SX + N_SY) * sizeof(CT);
+    // two CTAs per SM when both fit (228 KB per SM, 1 KB reserved per CTA):
+    // one CTA's barrier waits then overlap the other's arithmetic
+    static constexpr int MINB = (2 * (smem_bytes + 1024) <= 228 * 1024) ? 2 : 1;
 };
 
 __device__ __forceinline__ size_t lap_index(int X, int Y, int Z, uint32_t pitch, int ny) {
@@ -301,7 +304,7 @@ __device__ __forceinline__ void sweep(const RhsArgs& a, const SplitK<CT>& k, uns
 }
 
 template <int BX, int BY, int NT, bool UNI, typename CT>
-__global__ void __launch_bounds__(NT, 1) bf3w_rhs_kernel(const __grid_constant__ RhsArgs a) {
+__global__ void __launch_bounds__(NT, RhsLayout<BX, BY, CT>::MINB) bf3w_rhs_kernel(const __grid_constant__ RhsArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const SplitK<CT> k = {CT(a.eps2), CT(a.hrg), CT(a.c1), CT(a.c3), CT(a.gm1)};
     const int G = gridDim.x, b = blockIdx.x;
@@ -337,7 +340,7 @@ __global__ void __launch_bounds__(NT, 1) bf3w_rhs_kernel(const __grid_constant__
 // contiguous range, so a CTA sweeps neighbouring columns of one grid in turn
 // and every CTA ends with the same number of planes.
 template <int BX, int BY, int NT, bool UNI, typename CT>
-__global__ void __launch_bounds__(NT, 1)
+__global__ void __launch_bounds__(NT, RhsLayout<BX, BY, CT>::MINB)
     bf3w_rhs_batch_kernel(const RhsArgs* __restrict__ grids, const long* __restrict__ cum,
                           int ngrids, int zc) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -370,7 +373,7 @@ __global__ void __launch_bounds__(NT, 1)
 // Compiled tile shapes and host launch
 // ---------------------------------------------------------------------------
 namespace {
-constexpr TileCfg kCfgs[] = {{16, 8, 512}, {16, 8, 256}, {16, 8, 448}};
+constexpr TileCfg kCfgs[] = {{16, 8, 512}, {16, 8, 256}, {16, 8, 448}, {8, 8, 256}};
 constexpr int kNumCfgs = sizeof(kCfgs) / sizeof(kCfgs[0]);
 
 template <int BX, int BY, int NT, bool UNI, typename CT>
@@ -460,6 +463,7 @@ int launch_rhs(const RhsArgs& a, int precision, bool uniform, int cfg, int ctas,
         case 0: return dispatch_launch<16, 8, 512>(a, precision, uniform, ctas, st);
         case 1: return dispatch_launch<16, 8, 256>(a, precision, uniform, ctas, st);
         case 2: return dispatch_launch<16, 8, 448>(a, precision, uniform, ctas, st);
+        case 3: return dispatch_launch<8, 8, 256>(a, precision, uniform, ctas, st);
         default: return fail(WS_ERR_INVALID, "unknown tile configuration");
     }
 }
@@ -470,6 +474,7 @@ int launch_rhs_batch(const RhsArgs* grids, const long* cum, int n, int zc, int p
         case 0: return dispatch_batch<16, 8, 512>(grids, cum, n, zc, precision, uniform, ctas, st);
         case 1: return dispatch_batch<16, 8, 256>(grids, cum, n, zc, precision, uniform, ctas, st);
         case 2: return dispatch_batch<16, 8, 448>(grids, cum, n, zc, precision, uniform, ctas, st);
+        case 3: return dispatch_batch<8, 8, 256>(grids, cum, n, zc, precision, uniform, ctas, st);
         default: return fail(WS_ERR_INVALID, "unknown tile configuration");
     }
 }
@@ -479,6 +484,7 @@ int rhs_max_ctas(int precision, bool uniform, int cfg) {
         case 0: return dispatch_max<16, 8, 512>(precision, uniform);
         case 1: return dispatch_max<16, 8, 256>(precision, uniform);
         case 2: return dispatch_max<16, 8, 448>(precision, uniform);
+        case 3: return dispatch_max<8, 8, 256>(precision, uniform);
         default: return 0;
     }
 }

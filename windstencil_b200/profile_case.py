@@ -1,0 +1,47 @@
+"""Small profiling case for the fused RHS kernels.
+
+Runs one fused-RHS evaluation per requested precision on a Sod state
+(x extrapolation, y/z periodic) through the one-grid solver, so that a
+profiler can capture exactly those launches, e.g.
+
+    ncu --set full --clock-control none -k regex:bf3w_rhs -c 2 -o prof \
+        python -m windstencil_b200.profile_case --nx 600 --ny 128 --nz 64
+
+The default 600x128x64 case holds ~1 GB on the device and its inputs exceed
+the 126 MB L2, so DRAM counters stay meaningful.
+"""
+from __future__ import annotations
+
+import argparse
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--nx", type=int, default=600)
+    ap.add_argument("--ny", type=int, default=128)
+    ap.add_argument("--nz", type=int, default=64)
+    ap.add_argument("--precision", default="fp64,mixed")
+    ap.add_argument("--tile", default="", help="tile_x,tile_y,scan_z,threads")
+    a = ap.parse_args()
+
+    import torch
+
+    import windstencil_b200 as ws
+    from windstencil_b200 import workloads as wl
+
+    f0 = wl.sod_state(a.nx, a.ny, a.nz, seed=2)
+    for name in a.precision.split(","):
+        prec = ws.MIXED if name == "mixed" else ws.FP64
+        g = ws.Grid(a.nx, a.ny, a.nz, faces=(1, 1, 0, 0, 0, 0), precision=prec)
+        s = ws.Solver(g)
+        if a.tile:
+            s.set_tile(tuple(int(v) for v in a.tile.split(",")))
+        s.set_state(f0)
+        s.rhs()
+        torch.cuda.synchronize()
+        s.close()
+    print("ok")
+
+
+if __name__ == "__main__":
+    main()
