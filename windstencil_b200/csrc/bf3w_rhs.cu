@@ -105,11 +105,11 @@ __device__ __forceinline__ double face_flux<double>(const double* bp, int pmoff,
     double t[8], np, dp, nm, dm;
 #pragma unroll
     for (int k = 0; k < 8; ++k) t[k] = bp[k * stride - (k >= kw ? wrap : 0)];
-    weno7_symbo_nd<double>(t, np, dp);
+    weno7_symbo_nd(t, np, dp);
     const double p3 = t[3];
 #pragma unroll
     for (int k = 0; k < 8; ++k) t[k] = bp[pmoff + (7 - k) * stride - ((7 - k) >= kw ? wrap : 0)];
-    weno7_symbo_nd<double>(t, nm, dm);
+    weno7_symbo_nd(t, nm, dm);
     const double m3 = t[3];
     return (p3 + m3) + (np * dm + nm * dp) / (dp * dm);
 }

@@ -118,85 +118,82 @@ __device__ __forceinline__ void sw_split_gen(T d, T u, T v, T w, T c, T a1, T a2
 // evaluated on the first, second and third differences of the stencil:
 //   D_j = t_{j+1}-t_j,  S_j = D_{j+1}-D_j,  T_j = S_{j+1}-S_j.
 // In these variables the reference's three derivative rounds of candidate k
-// are a 3-term first-difference form r_k, 6 x a 1-2 term second-difference
-// form s_k, and 6 x T_k, so (all indicators divided by 720, eps likewise)
-//   beta_k/720 = r_k^2 + 39 s_k^2 + 39.05 T_k^2
-// and, because each candidate's coefficients sum to 12,
-//   q_k = 12 t_3 + l_k(D),   face = t_3 + sum w_k l_k / (12 sum w_k).
-// Both are exact algebraic rewrites of OCFD_Schemes.cpp:306-368; they remove
-// about a fifth of the FP64 operations and agree with the reference form to
-// ~1e-15 relative.  The result is returned as t_3 + num/den so that the P and
-// M faces of one flux can share a single division.
-// FP64: the reference's product weights w_k = d_k * prod_{j != k}(eps + beta_j)
-// from shared partial products.  FP32 (mixed form): the equivalent normalised
-// weights d_k / (eps + beta_k), which cannot overflow the FP32 range the way a
-// product of four indicators can.
+// (OCFD_Schemes.cpp:306-368) are a 3-term first-difference form r_k, 6 x a
+// 1-2 term second-difference form s_k and 6 x T_k, so
+//   beta_k / (720 * 39) = (r_k/sqrt 39)^2 + s_k^2 + (39.05/39) T_k^2.
+// The common factor 720*39 is taken out of every indicator and of eps, which
+// leaves the normalised weights unchanged; 1/sqrt(39) is folded into the
+// r_k coefficients and eps into the sum, so e_k = eps' + beta'_k costs three
+// FMAs.  Each candidate's coefficients sum to 12, so q_k = 12 t_3 + l_k(D)
+// and face = t_3 + sum d_k P_k l_k / (12 sum d_k P_k), P_k the product of the
+// other four e_j (the reference's product weights); d_k is folded into the
+// l_k coefficients.  All of this is an exact algebraic rewrite (agreement
+// with the reference form ~1e-15 relative) that removes about a third of the
+// FP64 operations.  The result is t_3 + num/den so that the P and M faces of
+// one flux can share a single division.
 // ---------------------------------------------------------------------------
+namespace wk {
+constexpr double R = 0.16012815380508713;     // 1/sqrt(39)
+constexpr double C = 39.05 / 39.0;            // third-derivative weight / second's
+constexpr double EPS = 2.592e-6 / (720.0 * 39.0);
+constexpr double D0 = 0.0401954833730, D1 = 0.2493800006710, D2 = 0.4802686256260,
+                 D3 = 0.2009775476730, D4 = 0.0291783426580;
+}  // namespace wk
+
 template <typename T>
 struct WenoDiffs {
     T D0, D1, D2, D3, D4, D5, D6;
-    T b0, b1, b2, b3, b4;
+    T e0, e1, e2, e3, e4;     // eps' + beta'_k (e4 before the SYMBO max)
 };
 
 template <typename T>
-__device__ __forceinline__ void weno7_indicators(const T t[8], WenoDiffs<T>& o) {
-    o.D0 = t[1] - t[0]; o.D1 = t[2] - t[1]; o.D2 = t[3] - t[2]; o.D3 = t[4] - t[3];
-    o.D4 = t[5] - t[4]; o.D5 = t[6] - t[5]; o.D6 = t[7] - t[6];
-    const T S0 = o.D1 - o.D0, S1 = o.D2 - o.D1, S2 = o.D3 - o.D2, S3 = o.D4 - o.D3;
-    const T S4 = o.D5 - o.D4, S5 = o.D6 - o.D5;
-    const T T0 = S1 - S0, T1 = S2 - S1, T2 = S3 - S2, T3 = S4 - S3, T4 = S5 - S4;
-    const T c2 = T(39.0), c3 = T(39.05);
-    T r, s;
-    r = T(2) * o.D0 - T(7) * o.D1 + T(11) * o.D2;    s = T(2) * S1 - S0;
-    o.b0 = (c3 * T0) * T0 + ((c2 * s) * s + r * r);
-    r = T(5) * o.D2 - o.D1 + T(2) * o.D3;            s = S2;
-    o.b1 = (c3 * T1) * T1 + ((c2 * s) * s + r * r);
-    r = T(2) * o.D2 + T(5) * o.D3 - o.D4;            s = S3;
-    o.b2 = (c3 * T2) * T2 + ((c2 * s) * s + r * r);
-    r = T(11) * o.D3 - T(7) * o.D4 + T(2) * o.D5;    s = T(2) * S3 - S4;
-    o.b3 = (c3 * T3) * T3 + ((c2 * s) * s + r * r);
-    r = T(26) * o.D4 - T(31) * o.D5 + T(11) * o.D6;  s = T(3) * S4 - T(2) * S5;
-    o.b4 = (c3 * T4) * T4 + ((c2 * s) * s + r * r);
+__device__ __forceinline__ T weno_e(T r, T s, T t3) {
+    return fma(r, r, fma(s, s, fma(T(wk::C) * t3, t3, T(wk::EPS))));
 }
 
-template <typename T>
-__device__ __forceinline__ void weno7_candidates(const WenoDiffs<T>& o, T w0, T w1, T w2, T w3,
-                                                 T w4, T& num, T& den) {
-    const T l0 = T(3) * o.D0 - T(10) * o.D1 + T(13) * o.D2;
-    const T l1 = T(4) * o.D2 - o.D1 + T(3) * o.D3;
-    const T l2 = o.D2 + T(6) * o.D3 - o.D4;
-    const T l3 = T(9) * o.D3 - T(4) * o.D4 + o.D5;
-    const T l4 = T(12) * o.D3 - T(13) * o.D4 + T(10) * o.D5 - T(3) * o.D6;
-    num = w0 * l0 + w1 * l1 + w2 * l2 + w3 * l3 + w4 * l4;
-    den = T(12) * (w0 + w1 + w2 + w3 + w4);
+__device__ __forceinline__ void weno7_indicators(const double t[8], WenoDiffs<double>& o) {
+    using namespace wk;
+    o.D0 = t[1] - t[0]; o.D1 = t[2] - t[1]; o.D2 = t[3] - t[2]; o.D3 = t[4] - t[3];
+    o.D4 = t[5] - t[4]; o.D5 = t[6] - t[5]; o.D6 = t[7] - t[6];
+    const double S0 = o.D1 - o.D0, S1 = o.D2 - o.D1, S2 = o.D3 - o.D2, S3 = o.D4 - o.D3;
+    const double S4 = o.D5 - o.D4, S5 = o.D6 - o.D5;
+    const double T0 = S1 - S0, T1 = S2 - S1, T2 = S3 - S2, T3 = S4 - S3, T4 = S5 - S4;
+    o.e0 = weno_e(fma(11 * R, o.D2, fma(-7 * R, o.D1, (2 * R) * o.D0)), fma(2.0, S1, -S0), T0);
+    o.e1 = weno_e(fma(2 * R, o.D3, fma(5 * R, o.D2, -R * o.D1)), S2, T1);
+    o.e2 = weno_e(fma(-R, o.D4, fma(5 * R, o.D3, (2 * R) * o.D2)), S3, T2);
+    o.e3 = weno_e(fma(2 * R, o.D5, fma(-7 * R, o.D4, (11 * R) * o.D3)), fma(2.0, S3, -S4), T3);
+    o.e4 = weno_e(fma(11 * R, o.D6, fma(-31 * R, o.D5, (26 * R) * o.D4)),
+                  fma(-2.0, S5, 3.0 * S4), T4);
 }
 
 // face value = t[3] + num/den
-template <typename T>
-__device__ __forceinline__ void weno7_symbo_nd(const T t[8], T& num, T& den);
-
-template <>
-__device__ __forceinline__ void weno7_symbo_nd<double>(const double t[8], double& num,
-                                                       double& den) {
+__device__ __forceinline__ void weno7_symbo_nd(const double t[8], double& num, double& den) {
+    using namespace wk;
     WenoDiffs<double> o;
-    weno7_indicators<double>(t, o);
-    const double b4 = fmax(fmax(fmax(o.b0, o.b1), fmax(o.b2, o.b3)), o.b4);
-    const double e = 2.592e-6 / 720.0;
-    const double e0 = e + o.b0, e1 = e + o.b1, e2 = e + o.b2, e3 = e + o.b3, e4 = e + b4;
+    weno7_indicators(t, o);
+    const double e0 = o.e0, e1 = o.e1, e2 = o.e2, e3 = o.e3;
+    const double e4 = fmax(fmax(fmax(e0, e1), fmax(e2, e3)), o.e4);   // SYMBO
+    // leave-one-out products from prefix / suffix partial products
     const double p01 = e0 * e1, p34 = e3 * e4;
     const double p012 = p01 * e2, p234 = e2 * p34;
-    weno7_candidates<double>(o, 0.0401954833730 * (e1 * p234), 0.2493800006710 * (e0 * p234),
-                             0.4802686256260 * (p01 * p34), 0.2009775476730 * (p012 * e4),
-                             0.0291783426580 * (p012 * e3), num, den);
+    const double P0 = e1 * p234, P1 = e0 * p234, P2 = p01 * p34, P3 = p012 * e4, P4 = p012 * e3;
+    const double l0 = fma(13 * D0, o.D2, fma(-10 * D0, o.D1, (3 * D0) * o.D0));
+    const double l1 = fma(3 * D1, o.D3, fma(4 * D1, o.D2, -D1 * o.D1));
+    const double l2 = fma(-D2, o.D4, fma(6 * D2, o.D3, D2 * o.D2));
+    const double l3 = fma(D3, o.D5, fma(-4 * D3, o.D4, (9 * D3) * o.D3));
+    const double l4 = fma(-3 * D4, o.D6, fma(10 * D4, o.D5, fma(-13 * D4, o.D4, (12 * D4) * o.D3)));
+    num = fma(P4, l4, fma(P3, l3, fma(P2, l2, fma(P1, l1, P0 * l0))));
+    den = fma(12 * D4, P4, fma(12 * D3, P3, fma(12 * D2, P2, fma(12 * D1, P1, (12 * D0) * P0))));
 }
 
 // ---------------------------------------------------------------------------
 // Mixed form: the P and M reconstructions of one face are the same arithmetic
 // on two stencils, so they run as the two lanes of Blackwell's packed FP32x2
-// instructions (FFMA2/FADD2/FMUL2): t[k] = (P stencil k, M stencil k).  The
-// normalised weights d_k/(eps+beta_k) take their reciprocals in pairs,
-// 1/a = b/(ab) and 1/b = a/(ab), from the approximate hardware reciprocal;
-// ab stays inside the FP32 range for any indicator below ~1e19.
+// instructions (FFMA2/FADD2/FMUL2): t[k] = (P stencil k, M stencil k).  Same
+// rescaled indicators; the normalised weights d_k/e_k take their reciprocals
+// in pairs, 1/a = b/(ab) and 1/b = a/(ab), from the approximate hardware
+// reciprocal (ab stays inside the FP32 range for any indicator below ~1e17);
+// d_k is folded into the l_k coefficients.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float2 f2(float c) { return make_float2(c, c); }
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
@@ -211,10 +208,14 @@ __device__ __forceinline__ float rcp_approx(float x) {
 __device__ __forceinline__ float2 rcp2(float2 x) {
     return make_float2(rcp_approx(x.x), rcp_approx(x.y));
 }
+__device__ __forceinline__ float2 weno_e2(float2 r, float2 s, float2 t3) {
+    return fma2(r, r, fma2(s, s, fma2(mul2(f2((float)wk::C), t3), t3, f2((float)wk::EPS))));
+}
 
 // face value of lane L = t[3].L + num.L / den.L
 __device__ __forceinline__ void weno7_symbo_pm_f32x2(const float2 t[8], float2& num,
                                                      float2& den) {
+    constexpr float R = (float)wk::R;
     const float2 D0 = sub2(t[1], t[0]), D1 = sub2(t[2], t[1]), D2 = sub2(t[3], t[2]);
     const float2 D3 = sub2(t[4], t[3]), D4 = sub2(t[5], t[4]), D5 = sub2(t[6], t[5]);
     const float2 D6 = sub2(t[7], t[6]);
@@ -222,45 +223,30 @@ __device__ __forceinline__ void weno7_symbo_pm_f32x2(const float2 t[8], float2& 
     const float2 S4 = sub2(D5, D4), S5 = sub2(D6, D5);
     const float2 T0 = sub2(S1, S0), T1 = sub2(S2, S1), T2 = sub2(S3, S2), T3 = sub2(S4, S3);
     const float2 T4 = sub2(S5, S4);
-    const float2 c2 = f2(39.0f), c3 = f2(39.05f);
-    auto beta = [&](float2 r, float2 s, float2 T) {
-        return fma2(mul2(c3, T), T, fma2(mul2(c2, s), s, mul2(r, r)));
-    };
-    float2 r, s;
-    r = fma2(f2(11.f), D2, fma2(f2(-7.f), D1, mul2(f2(2.f), D0)));
-    s = fma2(f2(2.f), S1, mul2(f2(-1.f), S0));
-    const float2 b0 = beta(r, s, T0);
-    r = fma2(f2(2.f), D3, fma2(f2(5.f), D2, mul2(f2(-1.f), D1)));
-    const float2 b1 = beta(r, S2, T1);
-    r = fma2(f2(-1.f), D4, fma2(f2(5.f), D3, mul2(f2(2.f), D2)));
-    const float2 b2 = beta(r, S3, T2);
-    r = fma2(f2(2.f), D5, fma2(f2(-7.f), D4, mul2(f2(11.f), D3)));
-    s = fma2(f2(2.f), S3, mul2(f2(-1.f), S4));
-    const float2 b3 = beta(r, s, T3);
-    r = fma2(f2(11.f), D6, fma2(f2(-31.f), D5, mul2(f2(26.f), D4)));
-    s = fma2(f2(3.f), S4, mul2(f2(-2.f), S5));
-    float2 b4 = beta(r, s, T4);
-    b4.x = fmaxf(fmaxf(fmaxf(b0.x, b1.x), fmaxf(b2.x, b3.x)), b4.x);
-    b4.y = fmaxf(fmaxf(fmaxf(b0.y, b1.y), fmaxf(b2.y, b3.y)), b4.y);
-    const float2 e = f2(2.592e-6f / 720.0f);
-    const float2 e0 = add2(e, b0), e1 = add2(e, b1), e2 = add2(e, b2), e3 = add2(e, b3);
-    const float2 e4 = add2(e, b4);
+    const float2 e0 = weno_e2(fma2(f2(11 * R), D2, fma2(f2(-7 * R), D1, mul2(f2(2 * R), D0))),
+                              fma2(f2(2.f), S1, mul2(f2(-1.f), S0)), T0);
+    const float2 e1 = weno_e2(fma2(f2(2 * R), D3, fma2(f2(5 * R), D2, mul2(f2(-R), D1))), S2, T1);
+    const float2 e2 = weno_e2(fma2(f2(-R), D4, fma2(f2(5 * R), D3, mul2(f2(2 * R), D2))), S3, T2);
+    const float2 e3 = weno_e2(fma2(f2(2 * R), D5, fma2(f2(-7 * R), D4, mul2(f2(11 * R), D3))),
+                              fma2(f2(2.f), S3, mul2(f2(-1.f), S4)), T3);
+    float2 e4 = weno_e2(fma2(f2(11 * R), D6, fma2(f2(-31 * R), D5, mul2(f2(26 * R), D4))),
+                        fma2(f2(3.f), S4, mul2(f2(-2.f), S5)), T4);
+    e4.x = fmaxf(fmaxf(fmaxf(e0.x, e1.x), fmaxf(e2.x, e3.x)), e4.x);
+    e4.y = fmaxf(fmaxf(fmaxf(e0.y, e1.y), fmaxf(e2.y, e3.y)), e4.y);
     const float2 r01 = rcp2(mul2(e0, e1)), r23 = rcp2(mul2(e2, e3)), r4 = rcp2(e4);
-    const float2 w0 = mul2(mul2(f2(0.0401954833730f), e1), r01);
-    const float2 w1 = mul2(mul2(f2(0.2493800006710f), e0), r01);
-    const float2 w2 = mul2(mul2(f2(0.4802686256260f), e3), r23);
-    const float2 w3 = mul2(mul2(f2(0.2009775476730f), e2), r23);
-    const float2 w4 = mul2(f2(0.0291783426580f), r4);
-    const float2 l0 = fma2(f2(13.f), D2, fma2(f2(-10.f), D1, mul2(f2(3.f), D0)));
-    const float2 l1 = fma2(f2(3.f), D3, fma2(f2(4.f), D2, mul2(f2(-1.f), D1)));
-    const float2 l2 = fma2(f2(-1.f), D4, fma2(f2(6.f), D3, D2));
-    const float2 l3 = fma2(f2(-4.f), D4, fma2(f2(9.f), D3, D5));
+    const float2 i0 = mul2(e1, r01), i1 = mul2(e0, r01), i2 = mul2(e3, r23), i3 = mul2(e2, r23);
+    constexpr float d0 = (float)wk::D0, d1 = (float)wk::D1, d2 = (float)wk::D2,
+                    d3 = (float)wk::D3, d4 = (float)wk::D4;
+    const float2 l0 = fma2(f2(13 * d0), D2, fma2(f2(-10 * d0), D1, mul2(f2(3 * d0), D0)));
+    const float2 l1 = fma2(f2(3 * d1), D3, fma2(f2(4 * d1), D2, mul2(f2(-d1), D1)));
+    const float2 l2 = fma2(f2(-d2), D4, fma2(f2(6 * d2), D3, mul2(f2(d2), D2)));
+    const float2 l3 = fma2(f2(d3), D5, fma2(f2(-4 * d3), D4, mul2(f2(9 * d3), D3)));
     const float2 l4 =
-        fma2(f2(-3.f), D6, fma2(f2(10.f), D5, fma2(f2(-13.f), D4, mul2(f2(12.f), D3))));
-    num = fma2(w4, l4, fma2(w3, l3, fma2(w2, l2, fma2(w1, l1, mul2(w0, l0)))));
-    den = mul2(f2(12.f), add2(add2(add2(w0, w1), add2(w2, w3)), w4));
+        fma2(f2(-3 * d4), D6, fma2(f2(10 * d4), D5, fma2(f2(-13 * d4), D4, mul2(f2(12 * d4), D3))));
+    num = fma2(r4, l4, fma2(i3, l3, fma2(i2, l2, fma2(i1, l1, mul2(i0, l0)))));
+    den = fma2(f2(12 * d4), r4, fma2(f2(12 * d3), i3,
+               fma2(f2(12 * d2), i2, fma2(f2(12 * d1), i1, mul2(f2(12 * d0), i0)))));
 }
-
 // ---------------------------------------------------------------------------
 // Small PTX helpers: 8-byte asynchronous global->shared copies (cp.async).
 // ---------------------------------------------------------------------------

@@ -42,6 +42,7 @@ struct TileCfg {
 int num_tile_cfgs();
 TileCfg tile_cfg(int i);
 int find_tile_cfg(int bx, int by, int threads);   // index or -1
+int default_cfg(int precision);                   // tuned default shape
 
 // Launch the fused RHS for one grid; cfg indexes the compiled tile shapes.
 int launch_rhs(const RhsArgs& a, int precision, bool uniform, int cfg, int ctas,
