@@ -6,7 +6,8 @@ benchmark configuration "Plain FP64 fused RHS at 600x128x128 and 480x512x64":
 4 ghost cells, periodic in y and z, zero-gradient extrapolation in x, seeded
 Sod state (left rho=1, p=1; right rho=0.125, p=0.1; 1% noise), SSP-RK3 at
 CFL 0.5.  One bench step = one SSP-RK3 time step = 3 RHS evaluations
-(ghost fill -> fused RHS -> stage update, x3), replayed from a CUDA graph.
+(ghost fill -> fused RHS with the stage update in its epilogue, x3), replayed
+from a CUDA graph.
 
   value          Gcell-RHS/s = cells x 3 x K / device time of K steps
                  (CUDA events, max over ranks; the state is 1.2 GB > L2, so
@@ -25,7 +26,9 @@ CFL 0.5.  One bench step = one SSP-RK3 time step = 3 RHS evaluations
   mixed          the mixed-precision form on the 600x128x128 Fourier
                  workload: kernel speed-up over FP64 and state error after
                  100 steps (rel. L2 / L-inf per conserved field)
-  batched        256 uneven periodic grids, 50 SSP-RK3 steps, FP64 and mixed,
+  grid_480x512x64  the second size of the FP64 workload: RHS kernel alone
+                 (both forms) and whole SSP-RK3 steps
+  batched       256 uneven periodic grids, 50 SSP-RK3 steps, FP64 and mixed,
                  against one-grid-at-a-time FP64 solves of the same grids
   served         Poisson arrivals of solve requests into the continuous-
                  batching server; p50/p99 latency and served throughput
@@ -67,6 +70,7 @@ def parse():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-second", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--batch-grids", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=50)
@@ -281,6 +285,38 @@ def bench_mixed(a, torch, ws, wl, stream):
     return res
 
 
+def bench_second_grid(a, torch, ws, wl, stream, peak64):
+    """The second size of the FP64 workload, 480x512x64 (same faces and state
+    recipe): the RHS kernel alone in both forms and whole SSP-RK3 steps."""
+    nx, ny, nz = 480, 512, 64
+    cells = nx * ny * nz
+    f0 = wl.sod_state(nx, ny, nz, seed=3)
+    faces = (ws.FACE_EXTRAP, ws.FACE_EXTRAP, 0, 0, 0, 0)
+    res = {"workload": f"{nx}x{ny}x{nz} Sod state, periodic y/z, extrapolation in x"}
+    for name, prec in (("fp64", ws.FP64), ("mixed", ws.MIXED)):
+        g = ws.Grid(nx, ny, nz, faces=faces, precision=prec)
+        s = ws.Solver(g)
+        s.set_state(f0, stream=stream)
+        dt = s.compute_dt(0.5, stream=stream)
+        kms = time_rhs_kernel(torch, ws, g, s, stream, 10)
+        s.step(dt, 3, stream=stream)
+        e0, e1 = _events(torch)
+        e0.record(stream)
+        s.step(dt, 20, stream=stream)
+        e1.record(stream)
+        e1.synchronize()
+        sms = e0.elapsed_time(e1) / 20
+        s.close()
+        tf = FLOP_PER_CELL * cells / (kms * 1e-3) / 1e12
+        res[name] = {"kernel_ms": kms, "rhs_gcell_s": cells / (kms * 1e-3) / 1e9,
+                     "step_ms": sms, "value": cells * 3 / (sms * 1e-3) / 1e9,
+                     "unit": "Gcell-RHS/s", "achieved_tflops": tf}
+        if name == "fp64":
+            res[name]["frac_of_fp64_peak"] = tf / peak64 if peak64 else None
+    res["kernel_speedup_mixed_vs_fp64"] = res["fp64"]["kernel_ms"] / res["mixed"]["kernel_ms"]
+    return res
+
+
 def bench_batch(a, torch, ws, wl, stream):
     specs = wl.batch_specs(a.batch_grids, seed=4)
     cells = sum(s.cells for s in specs)
@@ -313,7 +349,7 @@ def bench_batch(a, torch, ws, wl, stream):
         res[name] = {"value": cells * 3 * a.batch_steps / (ms * 1e-3) / 1e9,
                      "unit": "Gcell-RHS/s", "ms_per_step": ms / a.batch_steps,
                      "tile": list(tile), "nonfinite_grids": int(sum(1 for x in st if x)),
-                     "launches_per_step": 9}
+                     "launches_per_step": 6}
     # one grid at a time, FP64, same grids (a sample of them), same steps
     nser = min(a.serial_grids, len(specs))
     tot_ms, ser_cells = 0.0, 0
@@ -498,6 +534,8 @@ def run_ours(a, rank, world, dist):
     if rank == 0 and world == 1:
         if not a.no_mixed:
             extra["mixed"] = bench_mixed(a, torch, ws, wl, stream)
+        if not a.no_second:
+            extra["grid_480x512x64"] = bench_second_grid(a, torch, ws, wl, stream, peak)
         serial = None
         if not a.no_batch:
             extra["batched"], serial = bench_batch(a, torch, ws, wl, stream)
@@ -521,7 +559,7 @@ def run_ours(a, rank, world, dist):
                            "rhs_per_step": 3, "cfl": 0.5, "dt": dt,
                            "inputs_exceed_l2": True, "parallelism": f"replicas{world}"},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": 9 * a.steps, "clocks": clk.summary(),
+                "gpu_launches": 6 * a.steps, "clocks": clk.summary(),
                 "device_status": status}
         line.update(extra)
         print(json.dumps(line), flush=True)

@@ -122,26 +122,80 @@ RhsArgs make_rhs_args(const ws_grid* g, ws_job job, const ws_field prims[5],
     return a;
 }
 
+int set_rhs_stage(RhsArgs& a, const ws_grid* g, ws_soa f_in, ws_soa fn, ws_soa f_out,
+                  const ws_field p_out[6], double dt, int* status) {
+    auto same = [](const ws_soa& x, const ws_soa& y) {
+        return x.pitch == y.pitch && x.length_Y == y.length_Y && x.length_Z == y.length_Z;
+    };
+    if (!same(f_in, fn) || !same(fn, f_out))
+        return fail(WS_ERR_INVALID, "stage epilogue: f_in, fn, f_out need one SoA shape");
+    a.f_in = f_in;
+    a.fn = fn;
+    a.f_out = f_out;
+    for (int i = 0; i < 6; ++i) {
+        if (p_out[i].pitch != p_out[0].pitch)
+            return fail(WS_ERR_INVALID, "stage epilogue: output fields need one pitch");
+        a.p_out[i] = p_out[i].ptr;
+    }
+    a.p_pitch = p_out[0].pitch;
+    a.dt = dt;
+    a.rcv = g->gamma * (g->gamma - 1.0) * g->ama * g->ama;   // 1/cv, OCFD_init.cpp:380
+    a.rama = 1.0 / g->ama;
+    a.status = status;
+    return WS_OK;
+}
+
+// persistent grid: one CTA per resident slot, but no more than keeps every
+// CTA at >= 16 planes of work once the tile columns run out
+int rhs_ctas(const ws_grid* g, const RhsArgs& a, int cfg, bool stage) {
+    const long ntile = (long)a.ntx * a.nty;
+    const long planes = ntile * (a.ez - a.sz);
+    int ctas = rhs_max_ctas(g->precision, g->metrics_uniform != 0, cfg, stage);
+    if (ctas <= 0) return 0;
+    const long want = ntile >= ctas ? ctas : std::max(ntile, planes / 16);
+    if (want < ctas) ctas = (int)std::max(1L, want);
+    return ctas;
+}
+
+int tile_index(const ws_grid* g, ws_tile tile, int* cfg) {
+    *cfg = default_cfg(g->precision);
+    if (tile.tile_x || tile.tile_y || tile.threads) {
+        *cfg = find_tile_cfg(tile.tile_x, tile.tile_y, tile.threads);
+        if (*cfg < 0) return fail(WS_ERR_UNSUPPORTED, "tile shape not compiled in this build");
+    }
+    return WS_OK;
+}
+
 // Fill RhsArgs and launch; shared by the drop-in entry and the solver.
 int rhs_enqueue(const ws_grid* g, ws_job job, const ws_field prims[5], const ws_metrics* m,
                 ws_soa du, ws_tile tile, cudaStream_t st) {
-    int cfg = default_cfg(g->precision);
-    if (tile.tile_x || tile.tile_y || tile.threads) {
-        cfg = find_tile_cfg(tile.tile_x, tile.tile_y, tile.threads);
-        if (cfg < 0) return fail(WS_ERR_UNSUPPORTED, "tile shape not compiled in this build");
-    }
+    int cfg = 0;
+    int rc = tile_index(g, tile, &cfg);
+    if (rc) return rc;
     const int scan = tile.scan_z > 0 ? tile.scan_z : default_scan(g);
-    const bool uni = g->metrics_uniform != 0;
     const RhsArgs a = make_rhs_args(g, job, prims, m, du, cfg, scan);
-    // persistent grid: one CTA per resident slot, but no more than keeps
-    // every CTA at >= 16 planes of work once the tile columns run out
-    const long ntile = (long)a.ntx * a.nty;
-    const long planes = ntile * (a.ez - a.sz);
-    int ctas = rhs_max_ctas(g->precision, uni, cfg);
+    const int ctas = rhs_ctas(g, a, cfg, false);
     if (ctas <= 0) return fail(WS_ERR_CUDA, "cannot size the persistent grid");
-    const long want = ntile >= ctas ? ctas : std::max(ntile, planes / 16);
-    if (want < ctas) ctas = (int)std::max(1L, want);
-    return launch_rhs(a, g->precision, uni, cfg, ctas, st);
+    return launch_rhs(a, g->precision, g->metrics_uniform != 0, cfg, ctas, 0, st);
+}
+
+// One fused RHS + SSP-RK3 stage over the whole interior (Cartesian grids):
+// reads primitives p_in (ghosts filled), f_in and fn; writes f_out and the
+// new primitives p_out.
+int rhs_stage_enqueue(const ws_grid* g, const ws_field p_in[6], ws_soa f_in, ws_soa fn,
+                      ws_soa f_out, const ws_field p_out[6], double dt, int krk, int* status,
+                      ws_tile tile, cudaStream_t st) {
+    int cfg = 0;
+    int rc = tile_index(g, tile, &cfg);
+    if (rc) return rc;
+    const int scan = tile.scan_z > 0 ? tile.scan_z : default_scan(g);
+    ws_job job{{4, 4, 4}, {g->nx + 4, g->ny + 4, g->nz + 4}};
+    const ws_field p5[5] = {p_in[0], p_in[1], p_in[2], p_in[3], p_in[5]};
+    RhsArgs a = make_rhs_args(g, job, p5, nullptr, ws_soa{}, cfg, scan);
+    if ((rc = set_rhs_stage(a, g, f_in, fn, f_out, p_out, dt, status))) return rc;
+    const int ctas = rhs_ctas(g, a, cfg, true);
+    if (ctas <= 0) return fail(WS_ERR_CUDA, "cannot size the persistent grid");
+    return launch_rhs(a, g->precision, true, cfg, ctas, krk, st);
 }
 
 }  // namespace ws

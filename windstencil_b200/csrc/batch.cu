@@ -2,8 +2,8 @@
 //
 // The reference solves one grid per MPI rank (src/solver/OCFD_NS_Solver.cpp);
 // this file adds what it does not have: device-resident states of many
-// uneven grids, advanced by SSP-RK3 with one batched launch per kernel per
-// stage (ghost fill, fused RHS, stage update), the step replayed from a CUDA
+// uneven grids, advanced by SSP-RK3 with two batched launches per stage
+// (ghost fill; fused RHS with the stage update), the step replayed from a CUDA
 // graph, and an autotuner that times the compiled tile shapes on the batch.
 #include <algorithm>
 #include <cstring>
@@ -57,7 +57,7 @@ int launch_max_speed(const ws_grid* g, const ws_field prims[6], unsigned long lo
 size_t grid_state_bytes(const ws_grid& g) {
     const size_t ncell = (size_t)g.nx * g.ny * g.nz;
     const size_t nlap = (size_t)lap_pitch(g.nx) * (g.ny + 8) * (g.nz + 8);
-    return 3 * align256(5 * ncell * sizeof(double)) + 6 * align256(nlap * sizeof(double)) + 256;
+    return 3 * align256(5 * ncell * sizeof(double)) + 12 * align256(nlap * sizeof(double)) + 256;
 }
 
 int grid_state_alloc(GridState& s, const ws_grid& g, cudaStream_t st) {
@@ -74,10 +74,11 @@ int grid_state_alloc(GridState& s, const ws_grid& g, cudaStream_t st) {
         if (b < 2) s.f[b] = q; else s.du = q;
         p += align256(5 * ncell * sizeof(double));
     }
-    for (int i = 0; i < 6; ++i) {
-        s.prims[i] = ws_field{reinterpret_cast<double*>(p), lp, 0};
-        p += align256(nlap * sizeof(double));
-    }
+    for (int b = 0; b < 2; ++b)
+        for (int i = 0; i < 6; ++i) {
+            s.pr[b][i] = ws_field{reinterpret_cast<double*>(p), lp, 0};
+            p += align256(nlap * sizeof(double));
+        }
     s.status = reinterpret_cast<int*>(p);
     s.cur = 0;
     return WS_OK;
@@ -92,11 +93,12 @@ int grid_state_upload(GridState& s, const double* f_host, cudaStream_t st) {
     const size_t n = (size_t)5 * s.g.nx * s.g.ny * s.g.nz;
     WS_CUDA(cudaMemcpyAsync(s.f[s.cur].ptr, f_host, n * sizeof(double), cudaMemcpyHostToDevice,
                             st));
-    int rc = launch_cons_to_prim(&s.g, s.f[s.cur], s.prims[0], s.prims[1], s.prims[2],
-                                 s.prims[3], s.prims[4], ws_field{nullptr, 0, 0}, s.status, st);
+    const ws_field* p = s.pr[s.cur];
+    int rc = launch_cons_to_prim(&s.g, s.f[s.cur], p[0], p[1], p[2], p[3], p[4],
+                                 ws_field{nullptr, 0, 0}, s.status, st);
     if (rc) return rc;
     ws_job job{{4, 4, 4}, {s.g.nx + 4, s.g.ny + 4, s.g.nz + 4}};
-    return launch_sound_speed(&s.g, job, s.prims[4], s.prims[5], st);
+    return launch_sound_speed(&s.g, job, p[4], p[5], st);
 }
 
 int grid_state_download(GridState& s, double* f_host, cudaStream_t st) {
@@ -141,41 +143,52 @@ int BatchRunner::build(const std::vector<GridState*>& grids, int cfg, int zc, cu
     for (auto* s : grids)
         if (s->g.precision != precision_ || !s->g.metrics_uniform)
             return fail(WS_ERR_INVALID, "a batch holds Cartesian grids of one precision");
-    const size_t gsz = ghost_args_size(), ssz = stage_args_size();
-    long n_gtab = 0, n_stab = 0;
-    for (auto* s : grids) {
-        n_gtab += ghost_chunks(&s->g);
-        n_stab += cell_chunks(&s->g);
-    }
-    if (n_gtab > (1L << 30) || n_stab > (1L << 30)) return fail(WS_ERR_INVALID, "batch too large");
+    long n_gtab = 0;
+    for (auto* s : grids) n_gtab += ghost_chunks(&s->g);
+    if (n_gtab > (1L << 30)) return fail(WS_ERR_INVALID, "batch too large");
     n_gtab_ = (int)n_gtab;
-    n_stab_ = (int)n_stab;
-    // layout of the device tables
-    const size_t o_rhs = 0;
-    const size_t o_cum = align256(o_rhs + n * sizeof(RhsArgs));
-    const size_t o_gh = align256(o_cum + (n + 1) * sizeof(long));
-    const size_t o_gt = align256(o_gh + n * gsz);
-    const size_t o_s0 = align256(o_gt + n_gtab * sizeof(int2));
-    const size_t o_s1 = align256(o_s0 + n * ssz);
-    const size_t o_st = align256(o_s1 + n * ssz);
-    const size_t bytes = align256(o_st + n_stab * sizeof(int2));
+    // layout of the device tables: 4 RhsArgs sets, cum, 2 ghost sets, block table
+    const size_t gsz = ghost_args_size();
+    size_t o = 0, o_rhs[4], o_gh[2];
+    for (int k = 0; k < 4; ++k) {
+        o_rhs[k] = o;
+        o = align256(o + n * sizeof(RhsArgs));
+    }
+    const size_t o_cum = o;
+    o = align256(o + (n + 1) * sizeof(long));
+    for (int k = 0; k < 2; ++k) {
+        o_gh[k] = o;
+        o = align256(o + n * gsz);
+    }
+    const size_t o_gt = o;
+    const size_t bytes = align256(o_gt + n_gtab * sizeof(int2));
     host_.assign(bytes, 0);
     unsigned char* h = host_.data();
-    RhsArgs* hr = reinterpret_cast<RhsArgs*>(h + o_rhs);
     long* hc = reinterpret_cast<long*>(h + o_cum);
     int2* hgt = reinterpret_cast<int2*>(h + o_gt);
-    int2* hst = reinterpret_cast<int2*>(h + o_st);
     hc[0] = 0;
-    long gi = 0, si = 0;
+    long gi = 0;
     for (int i = 0; i < n; ++i) {
         GridState* s = grids[i];
         ws_job job{{4, 4, 4}, {s->g.nx + 4, s->g.ny + 4, s->g.nz + 4}};
-        const ws_field p5[5] = {s->prims[0], s->prims[1], s->prims[2], s->prims[3], s->prims[5]};
-        hr[i] = make_rhs_args(&s->g, job, p5, nullptr, s->du, cfg, zc_);
-        hc[i + 1] = hc[i] + (long)hr[i].ntx * hr[i].nty * s->g.nz;
-        fill_ghost_args(h + o_gh + i * gsz, &s->g, s->prims);
+        for (int p = 0; p < 2; ++p) {
+            const int c = s->cur ^ p;
+            for (int two = 0; two < 2; ++two) {
+                // stage 2 reads pr[1-c] and writes pr[c]; stages 1 and 3 the reverse
+                const ws_field* pin = s->pr[two ? 1 - c : c];
+                const ws_field* pout = s->pr[two ? c : 1 - c];
+                const ws_field p5[5] = {pin[0], pin[1], pin[2], pin[3], pin[5]};
+                RhsArgs a = make_rhs_args(&s->g, job, p5, nullptr, s->du, cfg, zc_);
+                int rc = set_rhs_stage(a, &s->g, s->f[1 - c], s->f[c], s->f[1 - c], pout,
+                                       s->dt, s->status);
+                if (rc) return rc;
+                reinterpret_cast<RhsArgs*>(h + o_rhs[2 * p + two])[i] = a;
+            }
+            fill_ghost_args(h + o_gh[p] + i * gsz, &s->g, s->pr[c]);
+        }
+        const RhsArgs& a0 = reinterpret_cast<RhsArgs*>(h + o_rhs[0])[i];
+        hc[i + 1] = hc[i] + (long)a0.ntx * a0.nty * s->g.nz;
         for (long c = 0; c < ghost_chunks(&s->g); ++c) hgt[gi++] = make_int2(i, (int)c);
-        for (long c = 0; c < cell_chunks(&s->g); ++c) hst[si++] = make_int2(i, (int)c);
     }
     if (bytes > dev_bytes_) {
         if (dev_) cudaFreeAsync(dev_, st);
@@ -184,55 +197,53 @@ int BatchRunner::build(const std::vector<GridState*>& grids, int cfg, int zc, cu
         dev_bytes_ = bytes;
     }
     unsigned char* d = static_cast<unsigned char*>(dev_);
-    d_rhs_ = reinterpret_cast<RhsArgs*>(d + o_rhs);
+    for (int k = 0; k < 4; ++k) d_rhs_[k] = reinterpret_cast<RhsArgs*>(d + o_rhs[k]);
     d_cum_ = reinterpret_cast<long*>(d + o_cum);
-    d_ghost_ = d + o_gh;
+    for (int k = 0; k < 2; ++k) d_ghost_[k] = d + o_gh[k];
     d_gtab_ = reinterpret_cast<int2*>(d + o_gt);
-    d_stage_[0] = d + o_s0;
-    d_stage_[1] = d + o_s1;
-    d_stab_ = reinterpret_cast<int2*>(d + o_st);
-    int rc = upload_stage_tables(st);   // fills the stage blocks of host_ and uploads all
+    int rc = upload_tables(st);
     if (rc) return rc;
-    const int maxc = rhs_max_ctas(precision_, true, cfg_);
+    const int maxc = rhs_max_ctas(precision_, true, cfg_, true);
     if (maxc <= 0) return fail(WS_ERR_CUDA, "cannot size the persistent grid");
     const long planes = hc[n];
     ctas_ = (int)std::max(1L, std::min<long>(maxc, std::max<long>(1, planes / 16)));
     return WS_OK;
 }
 
-int BatchRunner::upload_stage_tables(cudaStream_t st) {
-    const int n = (int)grids_.size();
-    if (n == 0) return WS_OK;
-    const size_t ssz = stage_args_size();
-    unsigned char* h = host_.data();
-    const size_t o0 = static_cast<unsigned char*>(d_stage_[0]) - static_cast<unsigned char*>(dev_);
-    const size_t o1 = static_cast<unsigned char*>(d_stage_[1]) - static_cast<unsigned char*>(dev_);
-    for (int p = 0; p < 2; ++p)
-        for (int i = 0; i < n; ++i) {
-            GridState* s = grids_[i];
-            const int src = s->cur ^ p;
-            fill_stage_args(h + (p ? o1 : o0) + i * ssz, &s->g, s->dt, s->f[1 - src], s->f[src],
-                            s->du, s->prims, s->status);
-        }
+int BatchRunner::upload_tables(cudaStream_t st) {
     WS_CUDA(cudaMemcpyAsync(dev_, host_.data(), host_.size(), cudaMemcpyHostToDevice, st));
     // host_ must stay unchanged until the copy has read it
     WS_CUDA(cudaStreamSynchronize(st));
     return WS_OK;
 }
 
+// du of every grid's current state; d_rhs_[2 * parity_] reads pr[cur]
 int BatchRunner::enqueue_rhs(cudaStream_t st) {
     if (grids_.empty()) return WS_OK;
-    int rc = launch_ghost_fill_batch(d_ghost_, d_gtab_, n_gtab_, st);
+    int rc = launch_ghost_fill_batch(d_ghost_[parity_], d_gtab_, n_gtab_, st);
     if (rc) return rc;
-    return launch_rhs_batch(d_rhs_, d_cum_, (int)grids_.size(), zc_, precision_, true, cfg_,
-                            ctas_, st);
+    return launch_rhs_batch(d_rhs_[2 * parity_], d_cum_, (int)grids_.size(), zc_, precision_,
+                            true, cfg_, ctas_, 0, st);
+}
+
+// stage 1 alone: reads f[cur], pr[cur] and writes only the other buffers,
+// so it can be repeated without changing the current state
+int BatchRunner::enqueue_stage1(cudaStream_t st) {
+    if (grids_.empty()) return WS_OK;
+    int rc = launch_ghost_fill_batch(d_ghost_[parity_], d_gtab_, n_gtab_, st);
+    if (rc) return rc;
+    return launch_rhs_batch(d_rhs_[2 * parity_], d_cum_, (int)grids_.size(), zc_, precision_,
+                            true, cfg_, ctas_, 1, st);
 }
 
 int BatchRunner::enqueue_step(cudaStream_t st) {
+    if (grids_.empty()) return WS_OK;
     for (int krk = 1; krk <= 3; ++krk) {
-        int rc = enqueue_rhs(st);
+        const int two = krk == 2;
+        int rc = launch_ghost_fill_batch(d_ghost_[parity_ ^ two], d_gtab_, n_gtab_, st);
         if (rc) return rc;
-        rc = launch_stage_update_batch(d_stage_[parity_], d_stab_, n_stab_, krk, st);
+        rc = launch_rhs_batch(d_rhs_[2 * parity_ + two], d_cum_, (int)grids_.size(), zc_,
+                              precision_, true, cfg_, ctas_, krk, st);
         if (rc) return rc;
     }
     return WS_OK;
@@ -372,7 +383,7 @@ int ws_batch_compute_dt(ws_batch* b, double cfl, double* dt_out, ws_stream_t str
     WS_CUDA(cudaMallocAsync(&d, n * sizeof(unsigned long long), st));
     WS_CUDA(cudaMemsetAsync(d, 0, n * sizeof(unsigned long long), st));
     for (int i = 0; i < n; ++i) {
-        int rc = launch_max_speed(&b->states[i].g, b->states[i].prims, d + i, st);
+        int rc = launch_max_speed(&b->states[i].g, b->states[i].prims(), d + i, st);
         if (rc) return rc;
     }
     std::vector<unsigned long long> h(n);
@@ -442,8 +453,9 @@ int ws_batch_status(ws_batch* b, int* status, ws_stream_t stream) {
     return WS_OK;
 }
 
-// Times every compiled tile shape (and two sweep caps) on one batched RHS of
-// this batch and keeps the fastest; returns it in *chosen.
+// Times every compiled tile shape (and two sweep caps) on the first RK stage
+// of this batch (ghost fill + fused RHS and stage update; the current state
+// is left as it was) and keeps the fastest; returns it in *chosen.
 int ws_batch_autotune(ws_batch* b, ws_tile* chosen, ws_stream_t stream) {
     if (!b) return fail(WS_ERR_INVALID, "batch is NULL");
     cudaStream_t st = (cudaStream_t)stream;
@@ -459,14 +471,14 @@ int ws_batch_autotune(ws_batch* b, ws_tile* chosen, ws_stream_t stream) {
             b->tile = ws_tile{tc.bx, tc.by, cap, tc.threads};
             b->dirty = true;
             int rc = batch_ready(b, st);
-            if (rc == WS_OK) rc = b->runner.enqueue_rhs(st);    // warm-up
+            if (rc == WS_OK) rc = b->runner.enqueue_stage1(st);    // warm-up
             if (rc) {
                 cudaEventDestroy(e0);
                 cudaEventDestroy(e1);
                 return rc;
             }
             cudaEventRecord(e0, st);
-            for (int r = 0; r < 2; ++r) b->runner.enqueue_rhs(st);
+            for (int r = 0; r < 2; ++r) b->runner.enqueue_stage1(st);
             cudaEventRecord(e1, st);
             WS_CUDA(cudaEventSynchronize(e1));
             float ms = 0;

@@ -25,6 +25,14 @@
 //   * Primitive planes are staged with cp.async, double-buffered one plane
 //     ahead: the buffer of plane z holds its (BX+8) x (BY+8) box and the
 //     BX x BY centre of plane z+5.
+//   * Stage mode (EPI, used by the solver and batches): instead of writing
+//     du, the difference phase applies the SSP-RK3 stage to the conserved
+//     state and writes the primitives of the new state to a second set of
+//     LAP fields -- the separate stage kernel and the du round trip through
+//     HBM disappear.  One thread per cell (the last BX*BY threads, which have
+//     the least split work in the next interval) does all five variables,
+//     so it owns its cell's f/fn staging (cp.async one plane ahead) and no
+//     barrier guards it; the other threads go on to the next plane.
 //   * Persistent grid, one CTA per SM.  Whole tile columns are swept round
 //     robin (CTA b takes tiles b, b+G, ...), so the CTAs resident together
 //     sweep neighbouring columns at the same z and their halo re-reads hit
@@ -41,7 +49,7 @@
 
 namespace ws {
 
-template <int BX, int BY, typename CT>
+template <int BX, int BY, typename CT, bool EPI = false>
 struct RhsLayout {
     static constexpr int BXY = BX * BY;
     static constexpr int SXW = BX + 8;        // x-split row width
@@ -54,11 +62,12 @@ struct RhsLayout {
     static constexpr int N_FX = 5 * BY * (BX + 1);
     static constexpr int N_FY = 5 * (BY + 1) * BX;
     static constexpr int N_FZ = 2 * 5 * BXY;
+    static constexpr int N_FB = EPI ? 2 * 10 * BXY : 0;   // fn, f of a plane, x2
     static constexpr int N_RING = RING * RS;      // CT
     static constexpr int N_SX = 10 * BY * SXW;    // CT
     static constexpr int N_SY = 10 * SYH * BX;    // CT
     static constexpr size_t smem_bytes =
-        (size_t)(N_STG + N_FX + N_FY + N_FZ) * sizeof(double) +
+        (size_t)(N_STG + N_FX + N_FY + N_FZ + N_FB) * sizeof(double) +
         (size_t)(N_RING + N_SX + N_SY) * sizeof(CT);
     // two CTAs per SM when both fit (228 KB per SM, 1 KB reserved per CTA):
     // one CTA's barrier waits then overlap the other's arithmetic
@@ -67,6 +76,10 @@ struct RhsLayout {
 
 __device__ __forceinline__ size_t lap_index(int X, int Y, int Z, uint32_t pitch, int ny) {
     return (size_t)X + (size_t)pitch * ((size_t)Y + (size_t)(ny + 8) * (size_t)Z);
+}
+__device__ __forceinline__ size_t soa_index(const ws_soa& s, int i, int j, int k, int var) {
+    return (size_t)i + (size_t)s.pitch * ((size_t)j + (size_t)s.length_Y *
+                                          ((size_t)k + (size_t)s.length_Z * (size_t)var));
 }
 __device__ __forceinline__ double ldg_prim(const RhsArgs& a, int f, int X, int Y, int Z) {
     return __ldg(a.prim[f] + lap_index(X, Y, Z, a.ppitch[f], a.ny));
@@ -159,22 +172,63 @@ __device__ __forceinline__ void issue_stage(const RhsArgs& a, double* s, int x0,
     }
 }
 
-template <int BX, int BY, int NT, bool UNI, typename CT>
+// stage mode: cp.async fn (and, after stage 1, f) of one cell into
+// fb[v][col]; `cell` is the SoA offset of the cell's variable 0 and vs the
+// variable stride (f_in and fn share one SoA shape)
+__device__ __forceinline__ void issue_fcell(const RhsArgs& a, double* fb, int bxy, int col,
+                                            size_t cell, size_t vs, int krk) {
+#pragma unroll
+    for (int v = 0; v < 5; ++v) cp_async8(fb + v * bxy + col, a.fn.ptr + cell + v * vs);
+    if (krk > 1) {
+#pragma unroll
+        for (int v = 0; v < 5; ++v)
+            cp_async8(fb + (5 + v) * bxy + col, a.f_in.ptr + cell + v * vs);
+    }
+}
+
+// stage mode: primitives of the new state q of one cell into p_out
+// (commen_kernel.cpp:78-110; the divisions by rho, cv and Ama are taken as
+// one reciprocal and products)
+__device__ __forceinline__ void store_prims(const RhsArgs& a, const double q[5], int X, int Y,
+                                            int z) {
+    const double d1 = q[0], r = 1.0 / d1;
+    const double u1 = q[1] * r, v1 = q[2] * r, w1 = q[3] * r;
+    const double t1 = q[4] - 0.5 * d1 * (u1 * u1 + v1 * v1 + w1 * w1);
+    const double T1 = t1 * r * a.rcv;
+    const double vals[6] = {d1, u1, v1, w1, T1, sqrt(T1) * a.rama};
+    const size_t idx = lap_index(X, Y, z, a.p_pitch, a.ny);
+#pragma unroll
+    for (int f = 0; f < 6; ++f) a.p_out[f][idx] = vals[f];
+    if (!(d1 > 0.0 && T1 > 0.0 && T1 < INFINITY)) atomicOr(a.status, 1);
+}
+
+template <int BX, int BY, int NT, bool UNI, typename CT, bool EPI>
 __device__ __forceinline__ void sweep(const RhsArgs& a, const SplitK<CT>& k, unsigned char* smem,
-                                      int x0, int y0, int z0, int z1) {
-    using L = RhsLayout<BX, BY, CT>;
+                                      int x0, int y0, int z0, int z1, int krk) {
+    using L = RhsLayout<BX, BY, CT, EPI>;
     constexpr int BXY = L::BXY, SXW = L::SXW, SYH = L::SYH, BOXW = L::BOXW, BOX = L::BOX;
     constexpr int RS = L::RS;
     double* stg = reinterpret_cast<double*>(smem);       // [2][STG]
     double* fx = stg + L::N_STG;                         // [5][BY][BX+1]
     double* fy = fx + L::N_FX;                           // [5][BY+1][BX]
     double* fz = fy + L::N_FY;                           // [2][5][BXY]
-    CT* ring = reinterpret_cast<CT*>(fz + L::N_FZ);      // [9][10][BXY]
+    double* fb = fz + L::N_FZ;                           // [2][10][BXY]   (stage mode)
+    CT* ring = reinterpret_cast<CT*>(fb + L::N_FB);      // [9][10][BXY]
     CT* sxs = ring + L::N_RING;                          // [10][BY][SXW]
     CT* sys = sxs + L::N_SX;                             // [10][SYH][BX]
     const int tid = threadIdx.x;
+    static_assert(NT >= BXY, "one thread per cell in the stage epilogue");
+    static_assert(!EPI || UNI, "the stage epilogue is compiled for Cartesian grids");
+    // stage mode: this thread's cell (dcol < 0: none) and its SoA offsets
+    const int dcol = tid - (NT - BXY);
+    const int dX = x0 + (dcol >= 0 ? dcol % BX : 0), dY = y0 + (dcol >= 0 ? dcol / BX : 0);
+    const bool dcell = EPI && dcol >= 0 && dX < a.ex && dY < a.ey;
+    const size_t fps = (size_t)a.fn.pitch * a.fn.length_Y;      // plane stride
+    const size_t fvs = fps * a.fn.length_Z;                     // variable stride
+    const size_t fc0 = dcell ? soa_index(a.fn, dX - 4, dY - 4, 0, 0) - 4 * fps : 0;
 
     issue_stage<BX, BY, NT>(a, stg, x0, y0, z0);
+    if (dcell) issue_fcell(a, fb, BXY, dcol, fc0 + (size_t)z0 * fps, fvs, krk);
     cp_async_commit();
 
     // prologue: z split of planes z0-4 .. z0+4 into the ring
@@ -244,7 +298,8 @@ __device__ __forceinline__ void sweep(const RhsArgs& a, const SplitK<CT>& k, uns
         const int cur = prev ^ 1;
         const int s0 = (z - 3) % 9;
         constexpr int NXF = (BX + 1) * BY * 5, NYF = BX * (BY + 1) * 5, NZF = BXY * 5;
-        const int nitems = NXF + NYF + NZF + (more ? BXY : 0);
+        const int nsplit = more ? BXY : 0;
+        const int nitems = NXF + NYF + NZF + nsplit;
         for (int t = tid; t < nitems; t += NT) {
             if (t < NXF) {
                 const int var = t / ((BX + 1) * BY);
@@ -262,7 +317,7 @@ __device__ __forceinline__ void sweep(const RhsArgs& a, const SplitK<CT>& k, uns
                 const int var = t3 / BXY, col = t3 - var * BXY;
                 fz[cur * 5 * BXY + t3] = face_flux<CT>(ring + s0 * RS + var * BXY + col, 5 * BXY,
                                                        RS, 9 - s0, 9 * RS);
-            } else {
+            } else if (t < NXF + NYF + NZF + nsplit) {
                 const int col = t - NXF - NYF - NZF;
                 const double* cb = sb + 5 * BOX + col;
                 const int Z = z + 5;
@@ -278,33 +333,61 @@ __device__ __forceinline__ void sweep(const RhsArgs& a, const SplitK<CT>& k, uns
         cp_async_wait<0>();
         __syncthreads();
 
-        // ---- face difference: du of plane z (FP64)
-        for (int t = tid; t < 5 * BXY; t += NT) {
-            const int var = t / BXY, col = t - var * BXY;
-            const int xx = col % BX, yy = col / BX;
-            const int X = x0 + xx, Y = y0 + yy;
-            if (X < a.ex && Y < a.ey) {
-                const double* px = fx + (var * BY + yy) * (BX + 1) + xx;
-                const double* py = fy + (var * (BY + 1) + yy) * BX + xx;
-                const double dfx = px[1] - px[0];
-                const double dfy = py[BX] - py[0];
-                const double dfz = fz[cur * 5 * BXY + t] - fz[prev * 5 * BXY + t];
-                double r = dfx * a.rhx;
-                r = fma(dfy, a.rhy, r);
-                r = fma(dfz, a.rhz, r);
-                const double J = UNI ? 1.0 : ldg_met(a, 9, X, Y, z);
-                a.du[(size_t)(X - a.sx) +
-                     (size_t)a.du_pitch *
-                         ((size_t)(Y - a.sy) +
-                          (size_t)a.du_ly * ((size_t)(z - a.sz) + (size_t)a.du_lz * var))] = -J * r;
+        // ---- face difference of plane z (FP64): du, or the RK stage
+        if (EPI) {
+            if (dcell) {
+                const double* fbz = fb + b * 10 * BXY;
+                const size_t cell = fc0 + (size_t)z * fps;
+                const int xx = dcol % BX, yy = dcol / BX;
+                double q[5];
+#pragma unroll
+                for (int var = 0; var < 5; ++var) {
+                    const double* px = fx + (var * BY + yy) * (BX + 1) + xx;
+                    const double* py = fy + (var * (BY + 1) + yy) * BX + xx;
+                    const int i = var * BXY + dcol;
+                    double r = (px[1] - px[0]) * a.rhx;
+                    r = fma(py[BX] - py[0], a.rhy, r);
+                    r = fma(fz[cur * 5 * BXY + i] - fz[prev * 5 * BXY + i], a.rhz, r);
+                    const double fo = krk == 1 ? 0.0 : fbz[5 * BXY + i];
+                    q[var] = ws_rk_stage(krk, fbz[i], fo, -r, a.dt);
+                    a.f_out.ptr[cell + var * fvs] = q[var];
+                }
+                store_prims(a, q, dX, dY, z);
+                if (more) {   // own cell of the next plane; fb[b^1] was last read by this thread
+                    issue_fcell(a, fb + (b ^ 1) * 10 * BXY, BXY, dcol, cell + fps, fvs, krk);
+                    cp_async_commit();
+                }
+            }
+        } else {
+            for (int t = tid; t < 5 * BXY; t += NT) {
+                const int var = t / BXY, col = t - var * BXY;
+                const int xx = col % BX, yy = col / BX;
+                const int X = x0 + xx, Y = y0 + yy;
+                if (X < a.ex && Y < a.ey) {
+                    const double* px = fx + (var * BY + yy) * (BX + 1) + xx;
+                    const double* py = fy + (var * (BY + 1) + yy) * BX + xx;
+                    const double dfx = px[1] - px[0];
+                    const double dfy = py[BX] - py[0];
+                    const double dfz = fz[cur * 5 * BXY + t] - fz[prev * 5 * BXY + t];
+                    double r = dfx * a.rhx;
+                    r = fma(dfy, a.rhy, r);
+                    r = fma(dfz, a.rhz, r);
+                    const double J = UNI ? 1.0 : ldg_met(a, 9, X, Y, z);
+                    a.du[(size_t)(X - a.sx) +
+                         (size_t)a.du_pitch *
+                             ((size_t)(Y - a.sy) +
+                              (size_t)a.du_ly * ((size_t)(z - a.sz) + (size_t)a.du_lz * var))] =
+                        -J * r;
+                }
             }
         }
         prev = cur;
     }
 }
 
-template <int BX, int BY, int NT, bool UNI, typename CT>
-__global__ void __launch_bounds__(NT, RhsLayout<BX, BY, CT>::MINB) bf3w_rhs_kernel(const __grid_constant__ RhsArgs a) {
+template <int BX, int BY, int NT, bool UNI, typename CT, bool EPI>
+__global__ void __launch_bounds__(NT, (RhsLayout<BX, BY, CT, EPI>::MINB))
+    bf3w_rhs_kernel(const __grid_constant__ RhsArgs a, int krk) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const SplitK<CT> k = {CT(a.eps2), CT(a.hrg), CT(a.c1), CT(a.c3), CT(a.gm1)};
     const int G = gridDim.x, b = blockIdx.x;
@@ -317,7 +400,7 @@ __global__ void __launch_bounds__(NT, RhsLayout<BX, BY, CT>::MINB) bf3w_rhs_kern
         const int tile = b + r * G;
         const int x0 = a.sx + (tile % a.ntx) * BX, y0 = a.sy + (tile / a.ntx) * BY;
         for (int z = a.sz; z < a.ez; z += a.zc)
-            sweep<BX, BY, NT, UNI, CT>(a, k, smem_raw, x0, y0, z, min(z + a.zc, a.ez));
+            sweep<BX, BY, NT, UNI, CT, EPI>(a, k, smem_raw, x0, y0, z, min(z + a.zc, a.ez), krk);
     }
     // 2) the remaining tiles' (tile, plane) space cut into equal ranges
     const long total = (long)(ntile - full * G) * nzj;
@@ -328,8 +411,9 @@ __global__ void __launch_bounds__(NT, RhsLayout<BX, BY, CT>::MINB) bf3w_rhs_kern
         const int zoff = (int)(pos - tr * nzj);
         const int len = (int)min(min(nzj - zoff, hi - pos), (long)a.zc);
         const int tile = full * G + (int)tr;
-        sweep<BX, BY, NT, UNI, CT>(a, k, smem_raw, a.sx + (tile % a.ntx) * BX,
-                                   a.sy + (tile / a.ntx) * BY, a.sz + zoff, a.sz + zoff + len);
+        sweep<BX, BY, NT, UNI, CT, EPI>(a, k, smem_raw, a.sx + (tile % a.ntx) * BX,
+                                        a.sy + (tile / a.ntx) * BY, a.sz + zoff,
+                                        a.sz + zoff + len, krk);
         pos += len;
     }
 }
@@ -339,10 +423,10 @@ __global__ void __launch_bounds__(NT, RhsLayout<BX, BY, CT>::MINB) bf3w_rhs_kern
 // cum[g] is the number of tile-planes before grid g.  Each CTA takes an equal
 // contiguous range, so a CTA sweeps neighbouring columns of one grid in turn
 // and every CTA ends with the same number of planes.
-template <int BX, int BY, int NT, bool UNI, typename CT>
-__global__ void __launch_bounds__(NT, RhsLayout<BX, BY, CT>::MINB)
+template <int BX, int BY, int NT, bool UNI, typename CT, bool EPI>
+__global__ void __launch_bounds__(NT, (RhsLayout<BX, BY, CT, EPI>::MINB))
     bf3w_rhs_batch_kernel(const RhsArgs* __restrict__ grids, const long* __restrict__ cum,
-                          int ngrids, int zc) {
+                          int ngrids, int zc, int krk) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const long total = cum[ngrids];
     const long lo = total * blockIdx.x / gridDim.x, hi = total * (blockIdx.x + 1) / gridDim.x;
@@ -362,9 +446,9 @@ __global__ void __launch_bounds__(NT, RhsLayout<BX, BY, CT>::MINB)
         const long tile = local / nzj;
         const int zoff = (int)(local - tile * nzj);
         const int len = (int)min(min(nzj - zoff, hi - pos), (long)zc);
-        sweep<BX, BY, NT, UNI, CT>(a, k, smem_raw, a.sx + (int)(tile % a.ntx) * BX,
-                                   a.sy + (int)(tile / a.ntx) * BY, a.sz + zoff,
-                                   a.sz + zoff + len);
+        sweep<BX, BY, NT, UNI, CT, EPI>(a, k, smem_raw, a.sx + (int)(tile % a.ntx) * BX,
+                                        a.sy + (int)(tile / a.ntx) * BY, a.sz + zoff,
+                                        a.sz + zoff + len, krk);
         pos += len;
     }
 }
@@ -376,10 +460,10 @@ namespace {
 constexpr TileCfg kCfgs[] = {{16, 8, 512}, {16, 8, 256}, {16, 8, 448}, {8, 8, 256}};
 constexpr int kNumCfgs = sizeof(kCfgs) / sizeof(kCfgs[0]);
 
-template <int BX, int BY, int NT, bool UNI, typename CT>
+template <int BX, int BY, int NT, bool UNI, typename CT, bool EPI>
 struct Launcher {
-    static size_t smem() { return RhsLayout<BX, BY, CT>::smem_bytes; }
-    // per-device resident CTA count, computed once per device
+    static size_t smem() { return RhsLayout<BX, BY, CT, EPI>::smem_bytes; }
+    // attributes set and resident CTA count computed once per device
     static int max_ctas() {
         static int cached[64] = {0};
         int dev = 0;
@@ -388,64 +472,79 @@ struct Launcher {
         int sms = 0, per = 0;
         if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
             return 0;
-        if (cudaFuncSetAttribute(bf3w_rhs_kernel<BX, BY, NT, UNI, CT>,
+        if (cudaFuncSetAttribute(bf3w_rhs_kernel<BX, BY, NT, UNI, CT, EPI>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem()) != cudaSuccess ||
+            cudaFuncSetAttribute(bf3w_rhs_batch_kernel<BX, BY, NT, UNI, CT, EPI>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem()) != cudaSuccess)
             return 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                &per, bf3w_rhs_kernel<BX, BY, NT, UNI, CT>, NT, smem()) != cudaSuccess)
+                &per, bf3w_rhs_kernel<BX, BY, NT, UNI, CT, EPI>, NT, smem()) != cudaSuccess)
             return 0;
         cached[dev] = sms * per;
         return cached[dev];
     }
-    static int launch(const RhsArgs& a, int ctas, cudaStream_t st) {
-        bf3w_rhs_kernel<BX, BY, NT, UNI, CT><<<ctas, NT, smem(), st>>>(a);
+    static int launch(const RhsArgs& a, int ctas, int krk, cudaStream_t st) {
+        if (max_ctas() <= 0) return fail(WS_ERR_CUDA, "cannot prepare the RHS kernel");
+        bf3w_rhs_kernel<BX, BY, NT, UNI, CT, EPI><<<ctas, NT, smem(), st>>>(a, krk);
         WS_CUDA(cudaGetLastError());
         return WS_OK;
     }
     static int launch_batch(const RhsArgs* grids, const long* cum, int n, int zc, int ctas,
-                            cudaStream_t st) {
-        static int prepared[64] = {0};
-        int dev = 0;
-        WS_CUDA(cudaGetDevice(&dev));
-        if (dev >= 0 && dev < 64 && !prepared[dev]) {
-            WS_CUDA(cudaFuncSetAttribute(bf3w_rhs_batch_kernel<BX, BY, NT, UNI, CT>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem()));
-            prepared[dev] = 1;
-        }
-        bf3w_rhs_batch_kernel<BX, BY, NT, UNI, CT><<<ctas, NT, smem(), st>>>(grids, cum, n, zc);
+                            int krk, cudaStream_t st) {
+        if (max_ctas() <= 0) return fail(WS_ERR_CUDA, "cannot prepare the RHS kernel");
+        bf3w_rhs_batch_kernel<BX, BY, NT, UNI, CT, EPI><<<ctas, NT, smem(), st>>>(grids, cum, n,
+                                                                                  zc, krk);
         WS_CUDA(cudaGetLastError());
         return WS_OK;
     }
 };
 
-template <int BX, int BY, int NT>
-int dispatch_batch(const RhsArgs* grids, const long* cum, int n, int zc, int precision, bool uni,
-                   int ctas, cudaStream_t st) {
-    if (precision == WS_MIXED)
-        return uni ? Launcher<BX, BY, NT, true, float>::launch_batch(grids, cum, n, zc, ctas, st)
-                   : Launcher<BX, BY, NT, false, float>::launch_batch(grids, cum, n, zc, ctas, st);
-    return uni ? Launcher<BX, BY, NT, true, double>::launch_batch(grids, cum, n, zc, ctas, st)
-               : Launcher<BX, BY, NT, false, double>::launch_batch(grids, cum, n, zc, ctas, st);
+// the stage epilogue is compiled for Cartesian grids only (solver, batches)
+template <int BX, int BY, int NT, typename CT>
+int launch_t(const RhsArgs& a, bool uni, int ctas, int krk, cudaStream_t st) {
+    if (krk > 0) {
+        if (!uni) return fail(WS_ERR_UNSUPPORTED, "stage epilogue needs Cartesian metrics");
+        return Launcher<BX, BY, NT, true, CT, true>::launch(a, ctas, krk, st);
+    }
+    return uni ? Launcher<BX, BY, NT, true, CT, false>::launch(a, ctas, 0, st)
+               : Launcher<BX, BY, NT, false, CT, false>::launch(a, ctas, 0, st);
+}
+template <int BX, int BY, int NT, typename CT>
+int launch_batch_t(const RhsArgs* g, const long* cum, int n, int zc, bool uni, int ctas, int krk,
+                   cudaStream_t st) {
+    if (krk > 0) {
+        if (!uni) return fail(WS_ERR_UNSUPPORTED, "stage epilogue needs Cartesian metrics");
+        return Launcher<BX, BY, NT, true, CT, true>::launch_batch(g, cum, n, zc, ctas, krk, st);
+    }
+    return uni ? Launcher<BX, BY, NT, true, CT, false>::launch_batch(g, cum, n, zc, ctas, 0, st)
+               : Launcher<BX, BY, NT, false, CT, false>::launch_batch(g, cum, n, zc, ctas, 0, st);
+}
+template <int BX, int BY, int NT, typename CT>
+int max_t(bool uni, bool stage) {
+    if (stage) return Launcher<BX, BY, NT, true, CT, true>::max_ctas();
+    return uni ? Launcher<BX, BY, NT, true, CT, false>::max_ctas()
+               : Launcher<BX, BY, NT, false, CT, false>::max_ctas();
 }
 
 template <int BX, int BY, int NT>
-int dispatch_launch(const RhsArgs& a, int precision, bool uni, int ctas, cudaStream_t st) {
-    if (precision == WS_MIXED) {
-        return uni ? Launcher<BX, BY, NT, true, float>::launch(a, ctas, st)
-                   : Launcher<BX, BY, NT, false, float>::launch(a, ctas, st);
-    }
-    return uni ? Launcher<BX, BY, NT, true, double>::launch(a, ctas, st)
-               : Launcher<BX, BY, NT, false, double>::launch(a, ctas, st);
+int dispatch_launch(const RhsArgs& a, int precision, bool uni, int ctas, int krk,
+                    cudaStream_t st) {
+    return precision == WS_MIXED ? launch_t<BX, BY, NT, float>(a, uni, ctas, krk, st)
+                                 : launch_t<BX, BY, NT, double>(a, uni, ctas, krk, st);
 }
 template <int BX, int BY, int NT>
-int dispatch_max(int precision, bool uni) {
-    if (precision == WS_MIXED)
-        return uni ? Launcher<BX, BY, NT, true, float>::max_ctas()
-                   : Launcher<BX, BY, NT, false, float>::max_ctas();
-    return uni ? Launcher<BX, BY, NT, true, double>::max_ctas()
-               : Launcher<BX, BY, NT, false, double>::max_ctas();
+int dispatch_batch(const RhsArgs* g, const long* cum, int n, int zc, int precision, bool uni,
+                   int ctas, int krk, cudaStream_t st) {
+    return precision == WS_MIXED
+               ? launch_batch_t<BX, BY, NT, float>(g, cum, n, zc, uni, ctas, krk, st)
+               : launch_batch_t<BX, BY, NT, double>(g, cum, n, zc, uni, ctas, krk, st);
+}
+template <int BX, int BY, int NT>
+int dispatch_max(int precision, bool uni, bool stage) {
+    return precision == WS_MIXED ? max_t<BX, BY, NT, float>(uni, stage)
+                                 : max_t<BX, BY, NT, double>(uni, stage);
 }
 }  // namespace
 
@@ -457,34 +556,34 @@ int find_tile_cfg(int bx, int by, int threads) {
     return -1;
 }
 
-int launch_rhs(const RhsArgs& a, int precision, bool uniform, int cfg, int ctas,
+int launch_rhs(const RhsArgs& a, int precision, bool uniform, int cfg, int ctas, int krk,
                cudaStream_t st) {
     switch (cfg) {
-        case 0: return dispatch_launch<16, 8, 512>(a, precision, uniform, ctas, st);
-        case 1: return dispatch_launch<16, 8, 256>(a, precision, uniform, ctas, st);
-        case 2: return dispatch_launch<16, 8, 448>(a, precision, uniform, ctas, st);
-        case 3: return dispatch_launch<8, 8, 256>(a, precision, uniform, ctas, st);
+        case 0: return dispatch_launch<16, 8, 512>(a, precision, uniform, ctas, krk, st);
+        case 1: return dispatch_launch<16, 8, 256>(a, precision, uniform, ctas, krk, st);
+        case 2: return dispatch_launch<16, 8, 448>(a, precision, uniform, ctas, krk, st);
+        case 3: return dispatch_launch<8, 8, 256>(a, precision, uniform, ctas, krk, st);
         default: return fail(WS_ERR_INVALID, "unknown tile configuration");
     }
 }
 
 int launch_rhs_batch(const RhsArgs* grids, const long* cum, int n, int zc, int precision,
-                     bool uniform, int cfg, int ctas, cudaStream_t st) {
+                     bool uniform, int cfg, int ctas, int krk, cudaStream_t st) {
     switch (cfg) {
-        case 0: return dispatch_batch<16, 8, 512>(grids, cum, n, zc, precision, uniform, ctas, st);
-        case 1: return dispatch_batch<16, 8, 256>(grids, cum, n, zc, precision, uniform, ctas, st);
-        case 2: return dispatch_batch<16, 8, 448>(grids, cum, n, zc, precision, uniform, ctas, st);
-        case 3: return dispatch_batch<8, 8, 256>(grids, cum, n, zc, precision, uniform, ctas, st);
+        case 0: return dispatch_batch<16, 8, 512>(grids, cum, n, zc, precision, uniform, ctas, krk, st);
+        case 1: return dispatch_batch<16, 8, 256>(grids, cum, n, zc, precision, uniform, ctas, krk, st);
+        case 2: return dispatch_batch<16, 8, 448>(grids, cum, n, zc, precision, uniform, ctas, krk, st);
+        case 3: return dispatch_batch<8, 8, 256>(grids, cum, n, zc, precision, uniform, ctas, krk, st);
         default: return fail(WS_ERR_INVALID, "unknown tile configuration");
     }
 }
 
-int rhs_max_ctas(int precision, bool uniform, int cfg) {
+int rhs_max_ctas(int precision, bool uniform, int cfg, bool stage) {
     switch (cfg) {
-        case 0: return dispatch_max<16, 8, 512>(precision, uniform);
-        case 1: return dispatch_max<16, 8, 256>(precision, uniform);
-        case 2: return dispatch_max<16, 8, 448>(precision, uniform);
-        case 3: return dispatch_max<8, 8, 256>(precision, uniform);
+        case 0: return dispatch_max<16, 8, 512>(precision, uniform, stage);
+        case 1: return dispatch_max<16, 8, 256>(precision, uniform, stage);
+        case 2: return dispatch_max<16, 8, 448>(precision, uniform, stage);
+        case 3: return dispatch_max<8, 8, 256>(precision, uniform, stage);
         default: return 0;
     }
 }

@@ -191,57 +191,6 @@ __global__ void time_advance_kernel(const __grid_constant__ StageArgs a) {
     }
 }
 
-}  // namespace
-
-// Stage update fused with cons->prim and the interior sound speed.
-struct StagePrimArgs {
-    StageArgs s;
-    ws_field d, u, v, w, T, cc;
-    double cv, ama;
-    int* status;
-};
-
-namespace {
-
-// stage update of cell t (interior, x fastest) for stage krk
-template <int KRK>
-__device__ __forceinline__ void stage_cell(const StagePrimArgs& a, long t) {
-    const int nx = a.s.nx, ny = a.s.ny;
-    const int i = (int)(t % nx);
-    const long r = t / nx;
-    const int j = (int)(r % ny), k = (int)(r / ny);
-    double q[5];
-#pragma unroll
-    for (int var = 0; var < 5; ++var) {
-        const size_t p = soa_idx(i, j, k, var, a.s.f);
-        const double fo = KRK == 1 ? 0.0 : a.s.f.ptr[p];   // stage 1 does not read f
-        const double fnv = a.s.fn.ptr[soa_idx(i, j, k, var, a.s.fn)];
-        const double duv = a.s.du.ptr[soa_idx(i, j, k, var, a.s.du)];
-        q[var] = rk_stage(KRK, fnv, fo, duv, a.s.dt);
-        a.s.f.ptr[p] = q[var];
-    }
-    const double d1 = q[0];
-    const double u1 = q[1] / d1, v1 = q[2] / d1, w1 = q[3] / d1;
-    const double t1 = q[4] - 0.5 * d1 * (u1 * u1 + v1 * v1 + w1 * w1);
-    const double T1 = t1 / (d1 * a.cv);
-    const int I = i + 4, J = j + 4, K = k + 4;
-    a.d.ptr[lap_idx(I, J, K, a.d.pitch, ny)] = d1;
-    a.u.ptr[lap_idx(I, J, K, a.u.pitch, ny)] = u1;
-    a.v.ptr[lap_idx(I, J, K, a.v.pitch, ny)] = v1;
-    a.w.ptr[lap_idx(I, J, K, a.w.pitch, ny)] = w1;
-    a.T.ptr[lap_idx(I, J, K, a.T.pitch, ny)] = T1;
-    a.cc.ptr[lap_idx(I, J, K, a.cc.pitch, ny)] = sqrt(T1) / a.ama;
-    if (a.status && !(d1 > 0.0 && T1 > 0.0 && T1 < INFINITY)) atomicOr(a.status, 1);
-}
-
-template <int KRK>
-__global__ void stage_update_kernel(const __grid_constant__ StagePrimArgs a) {
-    const long n = (long)a.s.nx * a.s.ny * a.s.nz;
-    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n;
-         t += (long)gridDim.x * blockDim.x)
-        stage_cell<KRK>(a, t);
-}
-
 // ---- batched forms: block b works on grid tab[b].x, chunk tab[b].y of
 // kBatchChunk points (a host-built table; no search on the device)
 constexpr int kBatchThreads = 256;
@@ -255,17 +204,6 @@ __global__ void ghost_fill_batch_kernel(const GhostArgs* __restrict__ grids,
     const long t0 = (long)e.y * kBatchChunk;
     const long t1 = min(total, t0 + kBatchChunk);
     for (long t = t0 + threadIdx.x; t < t1; t += blockDim.x) ghost_fill_point(a, t);
-}
-
-template <int KRK>
-__global__ void stage_update_batch_kernel(const StagePrimArgs* __restrict__ grids,
-                                          const int2* __restrict__ tab) {
-    const int2 e = tab[blockIdx.x];
-    const StagePrimArgs& a = grids[e.x];
-    const long total = (long)a.s.nx * a.s.ny * a.s.nz;
-    const long t0 = (long)e.y * kBatchChunk;
-    const long t1 = min(total, t0 + kBatchChunk);
-    for (long t = t0 + threadIdx.x; t < t1; t += blockDim.x) stage_cell<KRK>(a, t);
 }
 
 int grid_for(long n, int threads) {
@@ -338,37 +276,12 @@ int launch_time_advance(const ws_grid* g, int krk, double dt, ws_soa f, ws_soa f
     return WS_OK;
 }
 
-StagePrimArgs make_stage_args(const ws_grid* g, int krk, double dt, ws_soa f, ws_soa fn,
-                              ws_soa du, const ws_field prims[6], int* status) {
-    StagePrimArgs a{};
-    a.s.f = f; a.s.fn = fn; a.s.du = du;
-    a.s.nx = g->nx; a.s.ny = g->ny; a.s.nz = g->nz; a.s.krk = krk; a.s.dt = dt;
-    a.d = prims[0]; a.u = prims[1]; a.v = prims[2]; a.w = prims[3]; a.T = prims[4];
-    a.cc = prims[5];
-    a.cv = 1.0 / (g->gamma * (g->gamma - 1.0) * g->ama * g->ama);
-    a.ama = g->ama;
-    a.status = status;
-    return a;
-}
-
-int launch_stage_update(const ws_grid* g, int krk, double dt, ws_soa f, ws_soa fn, ws_soa du,
-                        const ws_field prims[6], int* status, cudaStream_t st) {
-    const StagePrimArgs a = make_stage_args(g, krk, dt, f, fn, du, prims, status);
-    const int blocks = grid_for((long)g->nx * g->ny * g->nz, 256);
-    if (krk == 1) stage_update_kernel<1><<<blocks, 256, 0, st>>>(a);
-    else if (krk == 2) stage_update_kernel<2><<<blocks, 256, 0, st>>>(a);
-    else stage_update_kernel<3><<<blocks, 256, 0, st>>>(a);
-    WS_CUDA(cudaGetLastError());
-    return WS_OK;
-}
-
 int launch_ghost_fill_prims(const ws_grid* g, const ws_field prims[6], cudaStream_t st) {
     return launch_ghost_fill(g, prims, 6, st);
 }
 
 // ---- batched launches ----------------------------------------------------
 size_t ghost_args_size() { return sizeof(GhostArgs); }
-size_t stage_args_size() { return sizeof(StagePrimArgs); }
 
 void fill_ghost_args(void* out, const ws_grid* g, const ws_field prims[6]) {
     GhostArgs a{};
@@ -382,33 +295,13 @@ void fill_ghost_args(void* out, const ws_grid* g, const ws_field prims[6]) {
     *reinterpret_cast<GhostArgs*>(out) = a;
 }
 
-void fill_stage_args(void* out, const ws_grid* g, double dt, ws_soa f, ws_soa fn, ws_soa du,
-                     const ws_field prims[6], int* status) {
-    *reinterpret_cast<StagePrimArgs*>(out) = make_stage_args(g, 0, dt, f, fn, du, prims, status);
-}
-
 long ghost_chunks(const ws_grid* g) {
     return (ghost_count(g->nx, g->ny, g->nz) + kBatchChunk - 1) / kBatchChunk;
 }
-long cell_chunks(const ws_grid* g) {
-    return ((long)g->nx * g->ny * g->nz + kBatchChunk - 1) / kBatchChunk;
-}
-
 int launch_ghost_fill_batch(const void* grids, const int2* tab, int nblocks, cudaStream_t st) {
     if (nblocks <= 0) return WS_OK;
     ghost_fill_batch_kernel<<<nblocks, kBatchThreads, 0, st>>>(
         reinterpret_cast<const GhostArgs*>(grids), tab);
-    WS_CUDA(cudaGetLastError());
-    return WS_OK;
-}
-
-int launch_stage_update_batch(const void* grids, const int2* tab, int nblocks, int krk,
-                              cudaStream_t st) {
-    if (nblocks <= 0) return WS_OK;
-    const StagePrimArgs* g = reinterpret_cast<const StagePrimArgs*>(grids);
-    if (krk == 1) stage_update_batch_kernel<1><<<nblocks, kBatchThreads, 0, st>>>(g, tab);
-    else if (krk == 2) stage_update_batch_kernel<2><<<nblocks, kBatchThreads, 0, st>>>(g, tab);
-    else stage_update_batch_kernel<3><<<nblocks, kBatchThreads, 0, st>>>(g, tab);
     WS_CUDA(cudaGetLastError());
     return WS_OK;
 }

@@ -176,17 +176,17 @@ int start_requests(ws_server* s, std::vector<Req*>& fresh) {
                 q->st.f[q->st.cur], g.nx, g.ny, g.nz, g.gamma, g.ama, q->r.synth_mach,
                 q->r.synth_x_jump, q->r.synth_seed);
             WS_CUDA(cudaGetLastError());
-            rc = launch_cons_to_prim(&g, q->st.f[q->st.cur], q->st.prims[0], q->st.prims[1],
-                                     q->st.prims[2], q->st.prims[3], q->st.prims[4],
+            const ws_field* pr = q->st.prims();
+            rc = launch_cons_to_prim(&g, q->st.f[q->st.cur], pr[0], pr[1], pr[2], pr[3], pr[4],
                                      ws_field{nullptr, 0, 0}, q->st.status, st);
             if (!rc) {
                 ws_job job{{4, 4, 4}, {g.nx + 4, g.ny + 4, g.nz + 4}};
-                rc = launch_sound_speed(&g, job, q->st.prims[4], q->st.prims[5], st);
+                rc = launch_sound_speed(&g, job, pr[4], pr[5], st);
             }
         }
         if (rc) return rc;
         if (q->r.dt > 0) continue;
-        rc = launch_max_speed(&q->r.grid, q->st.prims, d + i, st);
+        rc = launch_max_speed(&q->r.grid, q->st.prims(), d + i, st);
         if (rc) return rc;
     }
     std::vector<unsigned long long> h(n);

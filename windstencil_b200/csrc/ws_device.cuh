@@ -42,6 +42,16 @@ __device__ __forceinline__ float ws_sqrt(float x) {
 __device__ __forceinline__ double ws_div(double a, double b) { return a / b; }
 __device__ __forceinline__ float ws_div(float a, float b) { return __fdividef(a, b); }
 
+// SSP-RK3 stage formulas, src/solver/OCFD_time.cpp:15-65 (ker1/ker2/ker3):
+// stage 1 f = fn + dt*du; stage 2 f = 3/4 fn + 1/4 (f + dt*du);
+// stage 3 f = 1/3 fn + 2/3 (f + dt*du).
+__device__ __forceinline__ double ws_rk_stage(int krk, double fn, double f, double du,
+                                              double dt) {
+    if (krk == 1) return fn + dt * du;
+    if (krk == 2) return (3.0 / 4.0) * fn + (1.0 / 4.0) * (f + dt * du);
+    return (1.0 / 3.0) * fn + (2.0 / 3.0) * (f + dt * du);
+}
+
 // ---------------------------------------------------------------------------
 // Steger-Warming split, Cartesian metrics (gradient = unit vector of DIR,
 // |grad| = 1): F+ in out[0..4], F- in out[5..9].

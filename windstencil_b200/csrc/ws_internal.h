@@ -33,7 +33,30 @@ struct RhsArgs {
     int ntx, nty, nzc, zc;     // tiles in x and y, z chunks and chunk length
     double rhx, rhy, rhz;      // 1/h
     double eps2, hrg, c1, c3, gm1;
+    // fused SSP-RK3 stage epilogue (solver and batches, whole interior):
+    // f_out <- stage(fn, f_in, dt*du); d,u,v,w,T,cc of the new state into the
+    // interiors of p_out (a second set of LAP fields: other CTAs still read
+    // the current primitives).  f_in may alias f_out (stages 2 and 3).
+    // f_in, fn and f_out share one SoA shape, the p_out fields one pitch.
+    ws_soa f_in, fn, f_out;
+    double* p_out[6];
+    uint32_t p_pitch;
+    double dt, rcv, rama;      // dt, 1/cv, 1/Ama
+    int* status;
 };
+
+// fill the epilogue fields of `a` for one stage (WS_ERR_INVALID when the
+// SoA shapes or the p_out pitches differ)
+int set_rhs_stage(RhsArgs& a, const ws_grid* g, ws_soa f_in, ws_soa fn, ws_soa f_out,
+                  const ws_field p_out[6], double dt, int* status);
+// resident-CTA count for one grid's launch (0 on failure)
+int rhs_ctas(const ws_grid* g, const RhsArgs& a, int cfg, bool stage);
+// One fused RHS + SSP-RK3 stage krk over the whole interior (Cartesian):
+// reads primitives p_in (ghosts filled), f_in and fn; writes f_out and the
+// new primitives p_out.
+int rhs_stage_enqueue(const ws_grid* g, const ws_field p_in[6], ws_soa f_in, ws_soa fn,
+                      ws_soa f_out, const ws_field p_out[6], double dt, int krk, int* status,
+                      ws_tile tile, cudaStream_t st);
 
 // Tile configurations compiled into the library.
 struct TileCfg {
@@ -45,13 +68,14 @@ int find_tile_cfg(int bx, int by, int threads);   // index or -1
 int default_cfg(int precision);                   // tuned default shape
 
 // Launch the fused RHS for one grid; cfg indexes the compiled tile shapes.
-int launch_rhs(const RhsArgs& a, int precision, bool uniform, int cfg, int ctas,
+// krk == 0: write du; krk in 1..3: fused SSP-RK3 stage epilogue (Cartesian).
+int launch_rhs(const RhsArgs& a, int precision, bool uniform, int cfg, int ctas, int krk,
                cudaStream_t st);
-int rhs_max_ctas(int precision, bool uniform, int cfg);   // resident CTAs on the device
+int rhs_max_ctas(int precision, bool uniform, int cfg, bool stage);   // resident CTAs
 // Batched RHS over n grids (device array of RhsArgs, cum[n+1] tile-plane
 // prefix sums); all grids share precision, metric kind and tile shape.
 int launch_rhs_batch(const RhsArgs* grids, const long* cum, int n, int zc, int precision,
-                     bool uniform, int cfg, int ctas, cudaStream_t st);
+                     bool uniform, int cfg, int ctas, int krk, cudaStream_t st);
 // Host-side RhsArgs of one grid and job (tile shape cfg, sweep cap scan).
 RhsArgs make_rhs_args(const ws_grid* g, ws_job job, const ws_field prims[5],
                       const ws_metrics* m, ws_soa du, int cfg, int scan);
@@ -68,40 +92,32 @@ int launch_prim_to_cons(const ws_grid* g, ws_field d, ws_field u, ws_field v, ws
                         ws_field T, ws_soa f, cudaStream_t st);
 int launch_time_advance(const ws_grid* g, int krk, double dt, ws_soa f, ws_soa fn, ws_soa du,
                         cudaStream_t st);
-// Fused stage: f <- stage(krk), then cons->prim (d,u,v,w,T interiors) and
-// cc on the interior; status word set on non-finite/rho<=0/p<=0.
-int launch_stage_update(const ws_grid* g, int krk, double dt, ws_soa f, ws_soa fn, ws_soa du,
-                        const ws_field prims[6], int* status, cudaStream_t st);
 // Fill ghosts of d,u,v,w,T and recompute cc on ghost layers only.
 int launch_ghost_fill_prims(const ws_grid* g, const ws_field prims[6], cudaStream_t st);
 
 uint32_t lap_pitch(uint32_t nx);
 
-// Batched field kernels: per-grid argument blocks (opaque, sizes below) in
+// Batched ghost fill: per-grid argument blocks (opaque, size below) in
 // device memory and a block table int2{grid, chunk}.
 size_t ghost_args_size();
-size_t stage_args_size();
 void fill_ghost_args(void* out, const ws_grid* g, const ws_field prims[6]);
-void fill_stage_args(void* out, const ws_grid* g, double dt, ws_soa f, ws_soa fn, ws_soa du,
-                     const ws_field prims[6], int* status);
 long ghost_chunks(const ws_grid* g);
-long cell_chunks(const ws_grid* g);
 int launch_ghost_fill_batch(const void* grids, const int2* tab, int nblocks, cudaStream_t st);
-int launch_stage_update_batch(const void* grids, const int2* tab, int nblocks, int krk,
-                              cudaStream_t st);
 
 // Device-resident state of one grid (used by the solver, batches and the
-// server): f[2] and du SoA, d,u,v,w,T,cc LAP fields and a status word, in
-// one allocation.
+// server): f[2] and du SoA, two sets of d,u,v,w,T,cc LAP fields and a
+// status word, in one allocation.  f[cur] is the current state and pr[cur]
+// its primitives; a step writes the other buffer of each.
 struct GridState {
     ws_grid g{};
     void* mem = nullptr;
     size_t bytes = 0;
     ws_soa f[2]{}, du{};
-    ws_field prims[6]{};
+    ws_field pr[2][6]{};
     int* status = nullptr;
-    int cur = 0;            // buffer holding the current state
+    int cur = 0;
     double dt = 0.0;
+    const ws_field* prims() const { return pr[cur]; }
 };
 size_t grid_state_bytes(const ws_grid& g);
 // stream-ordered allocation from the device's default memory pool
@@ -122,6 +138,8 @@ class BatchRunner {
     // invalidates captured graphs
     int build(const std::vector<GridState*>& grids, int cfg, int zc, cudaStream_t st);
     int enqueue_rhs(cudaStream_t st);
+    // the first RK stage only (leaves the current state unchanged; tuning)
+    int enqueue_stage1(cudaStream_t st);
     // one SSP-RK3 step of every grid from its current buffer into the other
     int enqueue_step(cudaStream_t st);
     // nsteps steps (graph replay); flips every grid's current buffer
@@ -132,18 +150,21 @@ class BatchRunner {
     void release(cudaStream_t st);
 
   private:
-    int upload_stage_tables(cudaStream_t st);
+    int upload_tables(cudaStream_t st);
     std::vector<GridState*> grids_;
     int precision_ = 0, cfg_ = 0, zc_ = 1 << 30, ctas_ = 0;
     void* dev_ = nullptr;           // device tables
     size_t dev_bytes_ = 0;
-    RhsArgs* d_rhs_ = nullptr;
+    // With c = cur ^ p (p = step parity since build), a step reads f[c] and
+    // writes f[1-c]; stages 1 and 3 read primitives pr[c] and write pr[1-c],
+    // stage 2 the reverse.  d_rhs_[2*p + (stage == 2)] holds the RHS
+    // arguments (with the stage epilogue) of every grid for that case, and
+    // d_ghost_[s] the ghost-fill arguments of primitive set pr[cur ^ s].
+    RhsArgs* d_rhs_[4] = {nullptr, nullptr, nullptr, nullptr};
+    void* d_ghost_[2] = {nullptr, nullptr};
     long* d_cum_ = nullptr;
-    void* d_ghost_ = nullptr;
     int2* d_gtab_ = nullptr;
-    void* d_stage_[2] = {nullptr, nullptr};   // parity 0: cur -> other; 1: swapped
-    int2* d_stab_ = nullptr;
-    int n_gtab_ = 0, n_stab_ = 0;
+    int n_gtab_ = 0;
     int parity_ = 0;
     cudaStream_t cap_ = nullptr;
     cudaGraphExec_t exec_[2] = {nullptr, nullptr};

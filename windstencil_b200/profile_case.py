@@ -1,8 +1,9 @@
 """Small profiling case for the fused RHS kernels.
 
 Runs one fused-RHS evaluation per requested precision on a Sod state
-(x extrapolation, y/z periodic) through the one-grid solver, so that a
-profiler can capture exactly those launches, e.g.
+(x extrapolation, y/z periodic) through the one-grid solver and, with
+--step, one SSP-RK3 step after it (three launches of the RHS with the stage
+epilogue), so that a profiler can capture exactly those launches, e.g.
 
     ncu --set full --clock-control none -k regex:bf3w_rhs -c 2 -o prof \
         python -m windstencil_b200.profile_case --nx 600 --ny 128 --nz 64
@@ -22,6 +23,7 @@ def main() -> None:
     ap.add_argument("--nz", type=int, default=64)
     ap.add_argument("--precision", default="fp64,mixed")
     ap.add_argument("--tile", default="", help="tile_x,tile_y,scan_z,threads")
+    ap.add_argument("--step", action="store_true", help="also one SSP-RK3 step")
     a = ap.parse_args()
 
     import torch
@@ -38,6 +40,8 @@ def main() -> None:
             s.set_tile(tuple(int(v) for v in a.tile.split(",")))
         s.set_state(f0)
         s.rhs()
+        if a.step:
+            s.step(s.compute_dt(0.5), 1)
         torch.cuda.synchronize()
         s.close()
     print("ok")
