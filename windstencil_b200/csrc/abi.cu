@@ -75,10 +75,12 @@ bool job_empty(ws_job j) {
 
 }  // namespace
 
-// default tile shape per precision (measured on B200 at 600x128x128): FP64
-// 16x8 columns / 512 threads (one 188 KB CTA per SM); mixed 8x8 / 256 threads
-// (two CTAs per SM hide each other's barrier waits)
-int default_cfg(int precision) { return precision == WS_MIXED ? 3 : 0; }
+// default tile shape (measured on B200 at 600x128x128, both precisions):
+// 16x8 columns / 768 threads, one CTA per SM.  24 warps hide the FP64 and
+// barrier latencies better than 16 (FP64 RHS 3.86 -> 3.55 ms) although the
+// 85-register budget spills a little; 896 and 1024 threads spill more and
+// are slower again.
+int default_cfg(int) { return 0; }
 
 namespace {
 // sweep length cap: unlimited (each persistent CTA sweeps its whole share)

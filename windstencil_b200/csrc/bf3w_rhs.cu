@@ -457,7 +457,7 @@ __global__ void __launch_bounds__(NT, (RhsLayout<BX, BY, CT, EPI>::MINB))
 // Compiled tile shapes and host launch
 // ---------------------------------------------------------------------------
 namespace {
-constexpr TileCfg kCfgs[] = {{16, 8, 512}, {16, 8, 256}, {16, 8, 448}, {8, 8, 256}};
+constexpr TileCfg kCfgs[] = {{16, 8, 768}, {16, 8, 512}, {8, 8, 256}, {8, 8, 384}};
 constexpr int kNumCfgs = sizeof(kCfgs) / sizeof(kCfgs[0]);
 
 template <int BX, int BY, int NT, bool UNI, typename CT, bool EPI>
@@ -559,10 +559,10 @@ int find_tile_cfg(int bx, int by, int threads) {
 int launch_rhs(const RhsArgs& a, int precision, bool uniform, int cfg, int ctas, int krk,
                cudaStream_t st) {
     switch (cfg) {
-        case 0: return dispatch_launch<16, 8, 512>(a, precision, uniform, ctas, krk, st);
-        case 1: return dispatch_launch<16, 8, 256>(a, precision, uniform, ctas, krk, st);
-        case 2: return dispatch_launch<16, 8, 448>(a, precision, uniform, ctas, krk, st);
-        case 3: return dispatch_launch<8, 8, 256>(a, precision, uniform, ctas, krk, st);
+        case 0: return dispatch_launch<16, 8, 768>(a, precision, uniform, ctas, krk, st);
+        case 1: return dispatch_launch<16, 8, 512>(a, precision, uniform, ctas, krk, st);
+        case 2: return dispatch_launch<8, 8, 256>(a, precision, uniform, ctas, krk, st);
+        case 3: return dispatch_launch<8, 8, 384>(a, precision, uniform, ctas, krk, st);
         default: return fail(WS_ERR_INVALID, "unknown tile configuration");
     }
 }
@@ -570,20 +570,20 @@ int launch_rhs(const RhsArgs& a, int precision, bool uniform, int cfg, int ctas,
 int launch_rhs_batch(const RhsArgs* grids, const long* cum, int n, int zc, int precision,
                      bool uniform, int cfg, int ctas, int krk, cudaStream_t st) {
     switch (cfg) {
-        case 0: return dispatch_batch<16, 8, 512>(grids, cum, n, zc, precision, uniform, ctas, krk, st);
-        case 1: return dispatch_batch<16, 8, 256>(grids, cum, n, zc, precision, uniform, ctas, krk, st);
-        case 2: return dispatch_batch<16, 8, 448>(grids, cum, n, zc, precision, uniform, ctas, krk, st);
-        case 3: return dispatch_batch<8, 8, 256>(grids, cum, n, zc, precision, uniform, ctas, krk, st);
+        case 0: return dispatch_batch<16, 8, 768>(grids, cum, n, zc, precision, uniform, ctas, krk, st);
+        case 1: return dispatch_batch<16, 8, 512>(grids, cum, n, zc, precision, uniform, ctas, krk, st);
+        case 2: return dispatch_batch<8, 8, 256>(grids, cum, n, zc, precision, uniform, ctas, krk, st);
+        case 3: return dispatch_batch<8, 8, 384>(grids, cum, n, zc, precision, uniform, ctas, krk, st);
         default: return fail(WS_ERR_INVALID, "unknown tile configuration");
     }
 }
 
 int rhs_max_ctas(int precision, bool uniform, int cfg, bool stage) {
     switch (cfg) {
-        case 0: return dispatch_max<16, 8, 512>(precision, uniform, stage);
-        case 1: return dispatch_max<16, 8, 256>(precision, uniform, stage);
-        case 2: return dispatch_max<16, 8, 448>(precision, uniform, stage);
-        case 3: return dispatch_max<8, 8, 256>(precision, uniform, stage);
+        case 0: return dispatch_max<16, 8, 768>(precision, uniform, stage);
+        case 1: return dispatch_max<16, 8, 512>(precision, uniform, stage);
+        case 2: return dispatch_max<8, 8, 256>(precision, uniform, stage);
+        case 3: return dispatch_max<8, 8, 384>(precision, uniform, stage);
         default: return 0;
     }
 }
