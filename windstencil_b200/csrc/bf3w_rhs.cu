@@ -297,28 +297,39 @@ __device__ __forceinline__ void sweep(const RhsArgs& a, const SplitK<CT>& k, uns
         // ---- interval B: faces of plane z, z face z+1/2, z-split of plane z+5
         const int cur = prev ^ 1;
         const int s0 = (z - 3) % 9;
-        constexpr int NXF = (BX + 1) * BY * 5, NYF = BX * (BY + 1) * 5, NZF = BXY * 5;
-        const int nsplit = more ? BXY : 0;
-        const int nitems = NXF + NYF + NZF + nsplit;
-        for (int t = tid; t < nitems; t += NT) {
-            if (t < NXF) {
-                const int var = t / ((BX + 1) * BY);
-                const int r = t - var * (BX + 1) * BY;
-                const int yy = r / (BX + 1), f = r - yy * (BX + 1);
-                fx[t] = face_flux<CT>(sxs + (var * BY + yy) * SXW + f, 5 * BY * SXW, 1, 8, 0);
-            } else if (t < NXF + NYF) {
-                const int t2 = t - NXF;
-                const int var = t2 / ((BY + 1) * BX);
-                const int r = t2 - var * (BY + 1) * BX;
-                const int g = r / BX, xx = r - g * BX;
-                fy[t2] = face_flux<CT>(sys + (var * SYH + g) * BX + xx, 5 * SYH * BX, BX, 8, 0);
-            } else if (t < NXF + NYF + NZF) {
-                const int t3 = t - NXF - NYF;
-                const int var = t3 / BXY, col = t3 - var * BXY;
-                fz[cur * 5 * BXY + t3] = face_flux<CT>(ring + s0 * RS + var * BXY + col, 5 * BXY,
-                                                       RS, 9 - s0, 9 * RS);
-            } else if (t < NXF + NYF + NZF + nsplit) {
-                const int col = t - NXF - NYF - NZF;
+        // One round robin over the plane's items, split into loops by item
+        // kind (no per-item branch chain): the x face right of each column
+        // and the y face above each row (power-of-two index math), the z
+        // faces, the left/bottom faces of the tile, then the z split.
+        constexpr unsigned NXR = 5 * BXY, NYR = 5 * BXY, NZF = 5 * BXY;
+        constexpr unsigned NE = 5 * (BY + BX);
+        unsigned t = tid;
+        for (; t < NXR; t += NT) {
+            const unsigned var = t / BXY, r = t % BXY, yy = r / BX, xx = r % BX;
+            fx[(var * BY + yy) * (BX + 1) + xx + 1] =
+                face_flux<CT>(sxs + (var * BY + yy) * SXW + xx + 1, 5 * BY * SXW, 1, 8, 0);
+        }
+        for (t -= NXR; t < NYR; t += NT) {
+            const unsigned var = t / BXY, r = t % BXY, g = r / BX + 1, xx = r % BX;
+            fy[(var * (BY + 1) + g) * BX + xx] =
+                face_flux<CT>(sys + (var * SYH + g) * BX + xx, 5 * SYH * BX, BX, 8, 0);
+        }
+        for (t -= NYR; t < NZF; t += NT)
+            fz[cur * 5 * BXY + t] = face_flux<CT>(ring + s0 * RS + t, 5 * BXY, RS, 9 - s0, 9 * RS);
+        for (t -= NZF; t < NE; t += NT) {
+            if (t < 5 * BY) {
+                const unsigned var = t / BY, yy = t % BY;
+                fx[(var * BY + yy) * (BX + 1)] =
+                    face_flux<CT>(sxs + (var * BY + yy) * SXW, 5 * BY * SXW, 1, 8, 0);
+            } else {
+                const unsigned var = (t - 5 * BY) / BX, xx = (t - 5 * BY) % BX;
+                fy[var * (BY + 1) * BX + xx] =
+                    face_flux<CT>(sys + var * SYH * BX + xx, 5 * SYH * BX, BX, 8, 0);
+            }
+        }
+        if (more) {
+            for (t -= NE; t < BXY; t += NT) {
+                const int col = t;
                 const double* cb = sb + 5 * BOX + col;
                 const int Z = z + 5;
                 CT out[10];

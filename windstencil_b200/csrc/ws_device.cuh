@@ -156,9 +156,29 @@ struct WenoDiffs {
     T e0, e1, e2, e3, e4;     // eps' + beta'_k (e4 before the SYMBO max)
 };
 
-template <typename T>
-__device__ __forceinline__ T weno_e(T r, T s, T t3) {
-    return fma(r, r, fma(s, s, fma(T(wk::C) * t3, t3, T(wk::EPS))));
+// The FP64 coefficients live in constant memory: a DFMA/DMUL takes a
+// constant-bank operand directly, whereas a 64-bit literal that does not fit
+// the instruction's immediate field is rebuilt in uniform registers (two
+// moves) at every use -- about 30 extra issue slots per reconstruction.
+// The array is never written; its values are the constexpr ones above.
+namespace wk {
+enum Coef {
+    R11, RM7, R2, R5, RM1, RM31, R26, CC, EPSC,                // indicators
+    L0A, L0B, L0C, L1A, L1B, L1C, L2A, L2B, L2C, L3A, L3B, L3C,   // d_k l_k
+    L4A, L4B, L4C, L4D,
+    Q0, Q1, Q2, Q3, Q4,                                       // 12 d_k
+    NCOEF
+};
+}  // namespace wk
+static __constant__ double wkc[wk::NCOEF] = {
+    11 * wk::R, -7 * wk::R, 2 * wk::R, 5 * wk::R, -wk::R, -31 * wk::R, 26 * wk::R, wk::C, wk::EPS,
+    13 * wk::D0, -10 * wk::D0, 3 * wk::D0, 3 * wk::D1, 4 * wk::D1, -wk::D1,
+    -wk::D2, 6 * wk::D2, wk::D2, wk::D3, -4 * wk::D3, 9 * wk::D3,
+    -3 * wk::D4, 10 * wk::D4, -13 * wk::D4, 12 * wk::D4,
+    12 * wk::D0, 12 * wk::D1, 12 * wk::D2, 12 * wk::D3, 12 * wk::D4};
+
+__device__ __forceinline__ double weno_e(double r, double s, double t3) {
+    return fma(r, r, fma(s, s, fma(wkc[wk::CC] * t3, t3, wkc[wk::EPSC])));
 }
 
 __device__ __forceinline__ void weno7_indicators(const double t[8], WenoDiffs<double>& o) {
@@ -168,11 +188,12 @@ __device__ __forceinline__ void weno7_indicators(const double t[8], WenoDiffs<do
     const double S0 = o.D1 - o.D0, S1 = o.D2 - o.D1, S2 = o.D3 - o.D2, S3 = o.D4 - o.D3;
     const double S4 = o.D5 - o.D4, S5 = o.D6 - o.D5;
     const double T0 = S1 - S0, T1 = S2 - S1, T2 = S3 - S2, T3 = S4 - S3, T4 = S5 - S4;
-    o.e0 = weno_e(fma(11 * R, o.D2, fma(-7 * R, o.D1, (2 * R) * o.D0)), fma(2.0, S1, -S0), T0);
-    o.e1 = weno_e(fma(2 * R, o.D3, fma(5 * R, o.D2, -R * o.D1)), S2, T1);
-    o.e2 = weno_e(fma(-R, o.D4, fma(5 * R, o.D3, (2 * R) * o.D2)), S3, T2);
-    o.e3 = weno_e(fma(2 * R, o.D5, fma(-7 * R, o.D4, (11 * R) * o.D3)), fma(2.0, S3, -S4), T3);
-    o.e4 = weno_e(fma(11 * R, o.D6, fma(-31 * R, o.D5, (26 * R) * o.D4)),
+    const double* k = wkc;
+    o.e0 = weno_e(fma(k[R11], o.D2, fma(k[RM7], o.D1, k[R2] * o.D0)), fma(2.0, S1, -S0), T0);
+    o.e1 = weno_e(fma(k[R2], o.D3, fma(k[R5], o.D2, k[RM1] * o.D1)), S2, T1);
+    o.e2 = weno_e(fma(k[RM1], o.D4, fma(k[R5], o.D3, k[R2] * o.D2)), S3, T2);
+    o.e3 = weno_e(fma(k[R2], o.D5, fma(k[RM7], o.D4, k[R11] * o.D3)), fma(2.0, S3, -S4), T3);
+    o.e4 = weno_e(fma(k[R11], o.D6, fma(k[RM31], o.D5, k[R26] * o.D4)),
                   fma(-2.0, S5, 3.0 * S4), T4);
 }
 
@@ -187,13 +208,14 @@ __device__ __forceinline__ void weno7_symbo_nd(const double t[8], double& num, d
     const double p01 = e0 * e1, p34 = e3 * e4;
     const double p012 = p01 * e2, p234 = e2 * p34;
     const double P0 = e1 * p234, P1 = e0 * p234, P2 = p01 * p34, P3 = p012 * e4, P4 = p012 * e3;
-    const double l0 = fma(13 * D0, o.D2, fma(-10 * D0, o.D1, (3 * D0) * o.D0));
-    const double l1 = fma(3 * D1, o.D3, fma(4 * D1, o.D2, -D1 * o.D1));
-    const double l2 = fma(-D2, o.D4, fma(6 * D2, o.D3, D2 * o.D2));
-    const double l3 = fma(D3, o.D5, fma(-4 * D3, o.D4, (9 * D3) * o.D3));
-    const double l4 = fma(-3 * D4, o.D6, fma(10 * D4, o.D5, fma(-13 * D4, o.D4, (12 * D4) * o.D3)));
+    const double* k = wkc;
+    const double l0 = fma(k[L0A], o.D2, fma(k[L0B], o.D1, k[L0C] * o.D0));
+    const double l1 = fma(k[L1A], o.D3, fma(k[L1B], o.D2, k[L1C] * o.D1));
+    const double l2 = fma(k[L2A], o.D4, fma(k[L2B], o.D3, k[L2C] * o.D2));
+    const double l3 = fma(k[L3A], o.D5, fma(k[L3B], o.D4, k[L3C] * o.D3));
+    const double l4 = fma(k[L4A], o.D6, fma(k[L4B], o.D5, fma(k[L4C], o.D4, k[L4D] * o.D3)));
     num = fma(P4, l4, fma(P3, l3, fma(P2, l2, fma(P1, l1, P0 * l0))));
-    den = fma(12 * D4, P4, fma(12 * D3, P3, fma(12 * D2, P2, fma(12 * D1, P1, (12 * D0) * P0))));
+    den = fma(k[Q4], P4, fma(k[Q3], P3, fma(k[Q2], P2, fma(k[Q1], P1, k[Q0] * P0))));
 }
 
 // ---------------------------------------------------------------------------
