@@ -197,13 +197,22 @@ __device__ __forceinline__ void weno7_indicators(const double t[8], WenoDiffs<do
                   fma(-2.0, S5, 3.0 * S4), T4);
 }
 
+// max of two indicators (both > 0): positive doubles order like their bit
+// patterns read as signed integers, so the comparison runs on the integer
+// pipe instead of the FP64 one (a NaN operand is selected and propagates to
+// the face value, as it would through the products anyway)
+__device__ __forceinline__ double pos_max(double a, double b) {
+    const long long x = __double_as_longlong(a), y = __double_as_longlong(b);
+    return __longlong_as_double(x > y ? x : y);
+}
+
 // face value = t[3] + num/den
 __device__ __forceinline__ void weno7_symbo_nd(const double t[8], double& num, double& den) {
     using namespace wk;
     WenoDiffs<double> o;
     weno7_indicators(t, o);
     const double e0 = o.e0, e1 = o.e1, e2 = o.e2, e3 = o.e3;
-    const double e4 = fmax(fmax(fmax(e0, e1), fmax(e2, e3)), o.e4);   // SYMBO
+    const double e4 = pos_max(pos_max(pos_max(e0, e1), pos_max(e2, e3)), o.e4);   // SYMBO
     // leave-one-out products from prefix / suffix partial products
     const double p01 = e0 * e1, p34 = e3 * e4;
     const double p012 = p01 * e2, p234 = e2 * p34;
