@@ -31,11 +31,11 @@ def oracle_prims(oracle, og, f):
     return d, u, v, w, T, cc
 
 
-def _case(oracle, torch, g, f, metrics=None, ajac=None, tile=None, job=None):
+def _case(oracle, torch, g, f, metrics=None, ajac=None, tile=None, job=None, lap=None):
     og = or_grid(g.nx, g.ny, g.nz, g.hx, g.hy, g.hz, g.gamma, g.ama, g.epsl_sw, g.faces)
     d, u, v, w, T, cc = oracle_prims(oracle, og, f)
     ref = oracle.du_invis(og, d, u, v, w, cc, metrics, ajac)
-    dev = [to_lap(torch, g, a) for a in (d, u, v, w, cc)]
+    dev = [(lap or to_lap)(torch, g, a) for a in (d, u, v, w, cc)]
     mdev = None
     if metrics is not None:
         mdev = [to_lap(torch, g, a) for a in list(metrics) + [ajac]]
@@ -183,4 +183,30 @@ def test_solver_rhs_matches_oracle(oracle, cuda):
     s.rhs()
     out = s.get_rhs()
     ref = oracle.rhs_conserved(og, f0)
+    assert rel_linf(out, ref).max() <= TOL
+
+
+def test_rhs_subjob_even_start(oracle, cuda):
+    # even job start in x: the primitive planes are staged with TMA tiles
+    g = ws.Grid(30, 20, 18)
+    job = ws.WsJob(ws.WsDim3(6, 5, 9), ws.WsDim3(29, 21, 20))
+    out, ref = _case(oracle, cuda, g, wl.fourier_state(30, 20, 18, seed=11), job=job)
+    assert rel_linf(out, ref).max() <= TOL
+
+
+@pytest.mark.parametrize("layout", ["odd_pitch", "offset_8_bytes"])
+def test_rhs_fields_tma_cannot_stage(oracle, cuda, layout):
+    # fields whose rows or base break the 16-byte rule of TMA tiles: the
+    # kernel stages them with cp.async instead, with the same results
+    g = ws.Grid(30, 14, 12)
+
+    def lap(torch, g, a):
+        if layout == "odd_pitch":      # rows of 39 doubles
+            t = torch.zeros((g.nz + 8, g.ny + 8, g.nx + 9), dtype=torch.float64, device="cuda")
+        else:                          # rows of 40 doubles, base 8 bytes past 16-byte alignment
+            t = torch.zeros((g.nz + 8, g.ny + 8, g.nx + 10), dtype=torch.float64,
+                            device="cuda")[:, :, 1:g.nx + 9]
+        t[:, :, :g.nx + 8] = torch.from_numpy(np.ascontiguousarray(a)).cuda()
+        return t
+    out, ref = _case(oracle, cuda, g, wl.fourier_state(30, 14, 12, seed=12), lap=lap)
     assert rel_linf(out, ref).max() <= TOL

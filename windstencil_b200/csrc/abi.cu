@@ -75,17 +75,57 @@ bool job_empty(ws_job j) {
 
 }  // namespace
 
-// default tile shape (measured on B200 at 600x128x128, both precisions):
-// 16x8 columns / 768 threads, one CTA per SM.  24 warps hide the FP64 and
-// barrier latencies better than 16 (FP64 RHS 3.86 -> 3.55 ms) although the
-// 85-register budget spills a little; 896 and 1024 threads spill more and
-// are slower again.
-int default_cfg(int) { return 0; }
+// default tile shape (measured on B200 at 600x128x128): FP64 16x8 columns /
+// 768 threads, one CTA per SM -- 24 warps hide the FP64 and barrier
+// latencies better than 16 within an 80-register budget; mixed 8x8 / 384
+// threads, two CTAs per SM (one CTA's barrier waits overlap the other's
+// arithmetic).
+int default_cfg(int precision) { return precision == WS_MIXED ? 3 : 0; }
 
 namespace {
 // sweep length cap: unlimited (each persistent CTA sweeps its whole share)
 int default_scan(const ws_grid*) { return 1 << 30; }
 
+}  // namespace
+
+namespace {
+// cuTensorMapEncodeTiled from the driver, looked up once (nullptr when the
+// driver does not provide it: staging then stays on cp.async)
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+    static const EncodeTiledFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return static_cast<EncodeTiledFn>(nullptr);
+        return reinterpret_cast<EncodeTiledFn>(p);
+    }();
+    return fn;
+}
+
+// 3D map of one LAP field (x: nx+8, y: ny+8, z: nz+8 elements) with a
+// bw x bh x 1 box; false when the field breaks TMA's alignment rules
+bool encode_lap_map(CUtensorMap* map, const ws_grid* g, const ws_field& f, int bw, int bh) {
+    const EncodeTiledFn fn = encode_tiled();
+    if (!fn || !f.ptr || (reinterpret_cast<uintptr_t>(f.ptr) & 15) || (f.pitch & 1) ||
+        f.pitch < (uint32_t)g->nx + 8)
+        return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)g->nx + 8, (cuuint64_t)g->ny + 8,
+                                (cuuint64_t)g->nz + 8};
+    const cuuint64_t strides[2] = {(cuuint64_t)f.pitch * 8,
+                                   (cuuint64_t)f.pitch * (g->ny + 8) * 8};
+    const cuuint32_t box[3] = {(cuuint32_t)bw, (cuuint32_t)bh, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, f.ptr, dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 }  // namespace
 
 RhsArgs make_rhs_args(const ws_grid* g, ws_job job, const ws_field prims[5],
@@ -121,6 +161,13 @@ RhsArgs make_rhs_args(const ws_grid* g, ws_job job, const ws_field prims[5],
     a.c1 = 2.0 * (g->gamma - 1.0);
     a.c3 = (3.0 - g->gamma) / (2.0 * (g->gamma - 1.0));
     a.gm1 = g->gamma - 1.0;
+    // TMA staging: box starts at x = sx - 4 + k*bx and centres at sx + k*bx
+    // are even (16-byte aligned for doubles) when sx is even
+    bool tma = (job.start.x % 2) == 0;
+    for (int i = 0; i < 5 && tma; ++i)
+        tma = encode_lap_map(&a.tm_box[i], g, prims[i], c.bx + 8, c.by + 8) &&
+              encode_lap_map(&a.tm_ctr[i], g, prims[i], c.bx, c.by);
+    a.tma = tma ? 1 : 0;
     return a;
 }
 

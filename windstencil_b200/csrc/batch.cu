@@ -182,11 +182,12 @@ int BatchRunner::build(const std::vector<GridState*>& grids, int cfg, int zc, cu
                 int rc = set_rhs_stage(a, &s->g, s->f[1 - c], s->f[c], s->f[1 - c], pout,
                                        s->dt, s->status);
                 if (rc) return rc;
-                reinterpret_cast<RhsArgs*>(h + o_rhs[2 * p + two])[i] = a;
+                std::memcpy(h + o_rhs[2 * p + two] + i * sizeof(RhsArgs), &a, sizeof a);
             }
             fill_ghost_args(h + o_gh[p] + i * gsz, &s->g, s->pr[c]);
         }
-        const RhsArgs& a0 = reinterpret_cast<RhsArgs*>(h + o_rhs[0])[i];
+        RhsArgs a0;
+        std::memcpy(&a0, h + o_rhs[0] + i * sizeof(RhsArgs), sizeof a0);
         hc[i + 1] = hc[i] + (long)a0.ntx * a0.nty * s->g.nz;
         for (long c = 0; c < ghost_chunks(&s->g); ++c) hgt[gi++] = make_int2(i, (int)c);
     }

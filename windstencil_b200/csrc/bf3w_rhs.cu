@@ -71,7 +71,7 @@ struct RhsLayout {
         (size_t)(N_RING + N_SX + N_SY) * sizeof(CT);
     // two CTAs per SM when both fit (228 KB per SM, 1 KB reserved per CTA):
     // one CTA's barrier waits then overlap the other's arithmetic
-    static constexpr int MINB = (2 * (smem_bytes + 1024) <= 228 * 1024) ? 2 : 1;
+    static constexpr int MINB = (2 * (smem_bytes + 128 + 1024) <= 228 * 1024) ? 2 : 1;
 };
 
 __device__ __forceinline__ size_t lap_index(int X, int Y, int Z, uint32_t pitch, int ny) {
@@ -172,6 +172,42 @@ __device__ __forceinline__ void issue_stage(const RhsArgs& a, double* s, int x0,
     }
 }
 
+// TMA form of issue_stage, issued by one thread: the 5 boxes and 5 centres
+// as 3D tiles completing on `bar`.  Box starts outside the array read zeros
+// (partial tiles; never used).  GMAP: the maps live in global memory (the
+// batched kernel's argument table) and are fenced for the tensor-map proxy
+// before their first use in a sweep.
+template <int BX, int BY, bool GMAP>
+__device__ __forceinline__ void issue_stage_tma(const RhsArgs& a, double* s, int x0, int y0,
+                                                int z, uint64_t* bar, bool first) {
+    using L = RhsLayout<BX, BY, double>;
+    if (GMAP && first) {
+        for (int f = 0; f < 5; ++f) {
+            asm volatile("fence.proxy.tensormap::generic.acquire.sys [%0], 128;\n" ::"l"(
+                             &a.tm_box[f])
+                         : "memory");
+            asm volatile("fence.proxy.tensormap::generic.acquire.sys [%0], 128;\n" ::"l"(
+                             &a.tm_ctr[f])
+                         : "memory");
+        }
+    }
+    mbar_expect_tx(bar, (uint32_t)(L::STG * sizeof(double)));
+    const int zc = min(z + 5, a.nz + 7);
+#pragma unroll
+    for (int f = 0; f < 5; ++f) {
+        tma_load_3d(s + f * L::BOX, &a.tm_box[f], x0 - 4, y0 - 4, z, bar);
+        tma_load_3d(s + 5 * L::BOX + f * L::BXY, &a.tm_ctr[f], x0, y0, zc, bar);
+    }
+}
+
+// a staging wait that gave up: recorded in the grid's status word (bit 1)
+// or, for the drop-in path that has none, in this flag
+__device__ int g_rhs_stage_timeout;
+__device__ __forceinline__ void report_stage_timeout(const RhsArgs& a) {
+    if (a.status) atomicOr(a.status, 2);
+    else atomicOr(&g_rhs_stage_timeout, 1);
+}
+
 // stage mode: cp.async fn (and, after stage 1, f) of one cell into
 // fb[v][col]; `cell` is the SoA offset of the cell's variable 0 and vs the
 // variable stride (f_in and fn share one SoA shape)
@@ -202,9 +238,11 @@ __device__ __forceinline__ void store_prims(const RhsArgs& a, const double q[5],
     if (!(d1 > 0.0 && T1 > 0.0 && T1 < INFINITY)) atomicOr(a.status, 1);
 }
 
-template <int BX, int BY, int NT, bool UNI, typename CT, bool EPI>
-__device__ __forceinline__ void sweep(const RhsArgs& a, const SplitK<CT>& k, unsigned char* smem,
-                                      int x0, int y0, int z0, int z1, int krk) {
+// Returns false when a TMA staging wait gave up (the caller then stops).
+template <int BX, int BY, int NT, bool UNI, typename CT, bool EPI, bool GMAP>
+__device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, unsigned char* smem,
+                                      int x0, int y0, int z0, int z1, int krk, uint64_t* bar,
+                                      uint32_t& ph, bool& first) {
     using L = RhsLayout<BX, BY, CT, EPI>;
     constexpr int BXY = L::BXY, SXW = L::SXW, SYH = L::SYH, BOXW = L::BOXW, BOX = L::BOX;
     constexpr int RS = L::RS;
@@ -227,7 +265,10 @@ __device__ __forceinline__ void sweep(const RhsArgs& a, const SplitK<CT>& k, uns
     const size_t fvs = fps * a.fn.length_Z;                     // variable stride
     const size_t fc0 = dcell ? soa_index(a.fn, dX - 4, dY - 4, 0, 0) - 4 * fps : 0;
 
-    issue_stage<BX, BY, NT>(a, stg, x0, y0, z0);
+    const bool tma = a.tma != 0;
+    if (!tma) issue_stage<BX, BY, NT>(a, stg, x0, y0, z0);
+    else if (tid == 0) issue_stage_tma<BX, BY, GMAP>(a, stg, x0, y0, z0, &bar[0], first);
+    first = false;
     if (dcell) issue_fcell(a, fb, BXY, dcol, fc0 + (size_t)z0 * fps, fvs, krk);
     cp_async_commit();
 
@@ -253,7 +294,17 @@ __device__ __forceinline__ void sweep(const RhsArgs& a, const SplitK<CT>& k, uns
         }
     }
     cp_async_wait<0>();
-    __syncthreads();
+    {
+        const bool bad = tma && !mbar_wait_bounded(&bar[0], ph & 1u);
+        if (tma) ph ^= 1u;
+        if (__syncthreads_or(bad)) {
+            if (tid == 0) {
+                report_stage_timeout(a);
+                mbar_wait_bounded(&bar[0], ph & 1u);   // copies in flight
+            }
+            return false;
+        }
+    }
 
     int prev = 0;
     for (int z = z0; z < z1; ++z) {
@@ -289,8 +340,13 @@ __device__ __forceinline__ void sweep(const RhsArgs& a, const SplitK<CT>& k, uns
         }
         const bool more = z + 1 < z1;
         if (more) {
-            issue_stage<BX, BY, NT>(a, stg + (b ^ 1) * L::STG, x0, y0, z + 1);
-            cp_async_commit();
+            if (!tma) {
+                issue_stage<BX, BY, NT>(a, stg + (b ^ 1) * L::STG, x0, y0, z + 1);
+                cp_async_commit();
+            } else if (tid == 0) {
+                issue_stage_tma<BX, BY, GMAP>(a, stg + (b ^ 1) * L::STG, x0, y0, z + 1,
+                                              &bar[b ^ 1], false);
+            }
         }
         __syncthreads();
 
@@ -342,7 +398,18 @@ __device__ __forceinline__ void sweep(const RhsArgs& a, const SplitK<CT>& k, uns
             }
         }
         cp_async_wait<0>();
-        __syncthreads();
+        {   // the next plane's staging has landed (TMA: its barrier phase)
+            const bool wt = tma && more;
+            const bool bad = wt && !mbar_wait_bounded(&bar[b ^ 1], (ph >> (b ^ 1)) & 1u);
+            if (wt) ph ^= 1u << (b ^ 1);
+            if (__syncthreads_or(bad)) {
+                if (tid == 0) {
+                    report_stage_timeout(a);
+                    mbar_wait_bounded(&bar[b ^ 1], (ph >> (b ^ 1)) & 1u);   // copies in flight
+                }
+                return false;
+            }
+        }
 
         // ---- face difference of plane z (FP64): du, or the RK stage
         if (EPI) {
@@ -394,12 +461,30 @@ __device__ __forceinline__ void sweep(const RhsArgs& a, const SplitK<CT>& k, uns
         }
         prev = cur;
     }
+    return true;
+}
+
+// mbarriers of the two staging buffers (TMA path), set up once per CTA
+__device__ __forceinline__ void init_stage_barriers(uint64_t* bar) {
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
 }
 
 template <int BX, int BY, int NT, bool UNI, typename CT, bool EPI>
 __global__ void __launch_bounds__(NT, (RhsLayout<BX, BY, CT, EPI>::MINB))
     bf3w_rhs_kernel(const __grid_constant__ RhsArgs a, int krk) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_dyn[];
+    // TMA tile destinations must be 128-byte aligned: align explicitly (the
+    // launch adds 128 bytes of slack)
+    unsigned char* smem_raw = smem_dyn + ((128 - (smem_addr(smem_dyn) & 127)) & 127);
+    __shared__ uint64_t bar[2];
+    init_stage_barriers(bar);
+    uint32_t ph = 0;
+    bool first = true;
     const SplitK<CT> k = {CT(a.eps2), CT(a.hrg), CT(a.c1), CT(a.c3), CT(a.gm1)};
     const int G = gridDim.x, b = blockIdx.x;
     const long nzj = a.ez - a.sz;
@@ -411,7 +496,10 @@ __global__ void __launch_bounds__(NT, (RhsLayout<BX, BY, CT, EPI>::MINB))
         const int tile = b + r * G;
         const int x0 = a.sx + (tile % a.ntx) * BX, y0 = a.sy + (tile / a.ntx) * BY;
         for (int z = a.sz; z < a.ez; z += a.zc)
-            sweep<BX, BY, NT, UNI, CT, EPI>(a, k, smem_raw, x0, y0, z, min(z + a.zc, a.ez), krk);
+            if (!sweep<BX, BY, NT, UNI, CT, EPI, false>(a, k, smem_raw, x0, y0, z,
+                                                        min(z + a.zc, a.ez), krk, bar, ph,
+                                                        first))
+                return;
     }
     // 2) the remaining tiles' (tile, plane) space cut into equal ranges
     const long total = (long)(ntile - full * G) * nzj;
@@ -422,9 +510,10 @@ __global__ void __launch_bounds__(NT, (RhsLayout<BX, BY, CT, EPI>::MINB))
         const int zoff = (int)(pos - tr * nzj);
         const int len = (int)min(min(nzj - zoff, hi - pos), (long)a.zc);
         const int tile = full * G + (int)tr;
-        sweep<BX, BY, NT, UNI, CT, EPI>(a, k, smem_raw, a.sx + (tile % a.ntx) * BX,
-                                        a.sy + (tile / a.ntx) * BY, a.sz + zoff,
-                                        a.sz + zoff + len, krk);
+        if (!sweep<BX, BY, NT, UNI, CT, EPI, false>(a, k, smem_raw, a.sx + (tile % a.ntx) * BX,
+                                                    a.sy + (tile / a.ntx) * BY, a.sz + zoff,
+                                                    a.sz + zoff + len, krk, bar, ph, first))
+            return;
         pos += len;
     }
 }
@@ -438,7 +527,13 @@ template <int BX, int BY, int NT, bool UNI, typename CT, bool EPI>
 __global__ void __launch_bounds__(NT, (RhsLayout<BX, BY, CT, EPI>::MINB))
     bf3w_rhs_batch_kernel(const RhsArgs* __restrict__ grids, const long* __restrict__ cum,
                           int ngrids, int zc, int krk) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_dyn[];
+    // TMA tile destinations must be 128-byte aligned: align explicitly (the
+    // launch adds 128 bytes of slack)
+    unsigned char* smem_raw = smem_dyn + ((128 - (smem_addr(smem_dyn) & 127)) & 127);
+    __shared__ uint64_t bar[2];
+    init_stage_barriers(bar);
+    uint32_t ph = 0;
     const long total = cum[ngrids];
     const long lo = total * blockIdx.x / gridDim.x, hi = total * (blockIdx.x + 1) / gridDim.x;
     if (lo >= hi) return;
@@ -448,6 +543,7 @@ __global__ void __launch_bounds__(NT, (RhsLayout<BX, BY, CT, EPI>::MINB))
         if (cum[mid] <= lo) g = mid; else top = mid;
     }
     long pos = lo;
+    int fenced = -1;                  // grid whose tensor maps this CTA has fenced
     while (pos < hi) {
         while (cum[g + 1] <= pos) ++g;
         const RhsArgs& a = grids[g];
@@ -457,9 +553,12 @@ __global__ void __launch_bounds__(NT, (RhsLayout<BX, BY, CT, EPI>::MINB))
         const long tile = local / nzj;
         const int zoff = (int)(local - tile * nzj);
         const int len = (int)min(min(nzj - zoff, hi - pos), (long)zc);
-        sweep<BX, BY, NT, UNI, CT, EPI>(a, k, smem_raw, a.sx + (int)(tile % a.ntx) * BX,
-                                        a.sy + (int)(tile / a.ntx) * BY, a.sz + zoff,
-                                        a.sz + zoff + len, krk);
+        bool first = fenced != g;
+        fenced = g;
+        if (!sweep<BX, BY, NT, UNI, CT, EPI, true>(a, k, smem_raw, a.sx + (int)(tile % a.ntx) * BX,
+                                                   a.sy + (int)(tile / a.ntx) * BY, a.sz + zoff,
+                                                   a.sz + zoff + len, krk, bar, ph, first))
+            return;
         pos += len;
     }
 }
@@ -473,7 +572,7 @@ constexpr int kNumCfgs = sizeof(kCfgs) / sizeof(kCfgs[0]);
 
 template <int BX, int BY, int NT, bool UNI, typename CT, bool EPI>
 struct Launcher {
-    static size_t smem() { return RhsLayout<BX, BY, CT, EPI>::smem_bytes; }
+    static size_t smem() { return RhsLayout<BX, BY, CT, EPI>::smem_bytes + 128; }
     // attributes set and resident CTA count computed once per device
     static int max_ctas() {
         static int cached[64] = {0};

@@ -1,5 +1,6 @@
 // ws_internal.h -- host-side declarations shared by the library's .cu/.cpp files.
 #pragma once
+#include <cuda.h>             // CUtensorMap (types only; the encoder is fetched at run time)
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -43,6 +44,12 @@ struct RhsArgs {
     uint32_t p_pitch;
     double dt, rcv, rama;      // dt, 1/cv, 1/Ama
     int* status;
+    // TMA staging (tma != 0): per primitive, a map of its LAP array with the
+    // (BX+8) x (BY+8) box of a plane and one with the BX x BY centre box.
+    // Set only when every box start is 16-byte aligned (even job start x,
+    // even pitches, 16-byte aligned fields); otherwise staging uses cp.async.
+    int tma;
+    CUtensorMap tm_box[5], tm_ctr[5];
 };
 
 // fill the epilogue fields of `a` for one stage (WS_ERR_INVALID when the
