@@ -62,6 +62,8 @@ size_t grid_state_bytes(const ws_grid& g) {
 
 int grid_state_alloc(GridState& s, const ws_grid& g, cudaStream_t st) {
     s.g = g;
+    s.args.clear();
+    s.args_cfg = -1;
     s.bytes = grid_state_bytes(g);
     WS_CUDA(cudaMallocAsync(&s.mem, s.bytes, st));
     WS_CUDA(cudaMemsetAsync(s.mem, 0, s.bytes, st));
@@ -170,25 +172,34 @@ int BatchRunner::build(const std::vector<GridState*>& grids, int cfg, int zc, cu
     long gi = 0;
     for (int i = 0; i < n; ++i) {
         GridState* s = grids[i];
-        ws_job job{{4, 4, 4}, {s->g.nx + 4, s->g.ny + 4, s->g.nz + 4}};
+        if (s->args.size() != 4 || s->args_cfg != cfg || s->args_zc != zc_ ||
+            s->args_dt != s->dt) {
+            ws_job job{{4, 4, 4}, {s->g.nx + 4, s->g.ny + 4, s->g.nz + 4}};
+            s->args.resize(4);
+            for (int c = 0; c < 2; ++c)
+                for (int two = 0; two < 2; ++two) {
+                    // stage 2 reads pr[1-c] and writes pr[c]; stages 1 and 3 the reverse
+                    const ws_field* pin = s->pr[two ? 1 - c : c];
+                    const ws_field* pout = s->pr[two ? c : 1 - c];
+                    const ws_field p5[5] = {pin[0], pin[1], pin[2], pin[3], pin[5]};
+                    RhsArgs& a = s->args[2 * c + two];
+                    a = make_rhs_args(&s->g, job, p5, nullptr, s->du, cfg, zc_);
+                    int rc = set_rhs_stage(a, &s->g, s->f[1 - c], s->f[c], s->f[1 - c], pout,
+                                           s->dt, s->status);
+                    if (rc) return rc;
+                }
+            s->args_cfg = cfg;
+            s->args_zc = zc_;
+            s->args_dt = s->dt;
+        }
         for (int p = 0; p < 2; ++p) {
             const int c = s->cur ^ p;
-            for (int two = 0; two < 2; ++two) {
-                // stage 2 reads pr[1-c] and writes pr[c]; stages 1 and 3 the reverse
-                const ws_field* pin = s->pr[two ? 1 - c : c];
-                const ws_field* pout = s->pr[two ? c : 1 - c];
-                const ws_field p5[5] = {pin[0], pin[1], pin[2], pin[3], pin[5]};
-                RhsArgs a = make_rhs_args(&s->g, job, p5, nullptr, s->du, cfg, zc_);
-                int rc = set_rhs_stage(a, &s->g, s->f[1 - c], s->f[c], s->f[1 - c], pout,
-                                       s->dt, s->status);
-                if (rc) return rc;
-                std::memcpy(h + o_rhs[2 * p + two] + i * sizeof(RhsArgs), &a, sizeof a);
-            }
+            for (int two = 0; two < 2; ++two)
+                std::memcpy(h + o_rhs[2 * p + two] + i * sizeof(RhsArgs), &s->args[2 * c + two],
+                            sizeof(RhsArgs));
             fill_ghost_args(h + o_gh[p] + i * gsz, &s->g, s->pr[c]);
         }
-        RhsArgs a0;
-        std::memcpy(&a0, h + o_rhs[0] + i * sizeof(RhsArgs), sizeof a0);
-        hc[i + 1] = hc[i] + (long)a0.ntx * a0.nty * s->g.nz;
+        hc[i + 1] = hc[i] + (long)s->args[0].ntx * s->args[0].nty * s->g.nz;
         for (long c = 0; c < ghost_chunks(&s->g); ++c) hgt[gi++] = make_int2(i, (int)c);
     }
     if (bytes > dev_bytes_) {
@@ -246,6 +257,17 @@ int BatchRunner::enqueue_step(cudaStream_t st) {
         rc = launch_rhs_batch(d_rhs_[2 * parity_ + two], d_cum_, (int)grids_.size(), zc_,
                               precision_, true, cfg_, ctas_, krk, st);
         if (rc) return rc;
+    }
+    return WS_OK;
+}
+
+int BatchRunner::step_eager(int nsteps, cudaStream_t st) {
+    if (grids_.empty()) return WS_OK;
+    for (int i = 0; i < nsteps; ++i) {
+        int rc = enqueue_step(st);
+        if (rc) return rc;
+        parity_ ^= 1;
+        for (auto* s : grids_) s->cur ^= 1;
     }
     return WS_OK;
 }

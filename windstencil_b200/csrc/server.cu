@@ -6,8 +6,9 @@
 //   admit  : move queued requests to active slots while the HBM state budget
 //            and the slot limit allow; upload (or generate) the initial state
 //            and compute its time step on the device;
-//   tick   : one SSP-RK3 step of every active grid -- one batched launch per
-//            kernel per stage and precision (BatchRunner, graph replay);
+//   tick   : SSP-RK3 steps of every active grid -- two batched launches per
+//            stage and precision (BatchRunner) -- up to the next completion
+//            (at most 4 steps while the queue is empty);
 //   retire : grids that reached their step count copy their state back, free
 //            their slot and record their latency.
 // Requests arriving while others run are admitted at the next tick, so their
@@ -119,6 +120,8 @@ struct ws_server {
 };
 
 namespace {
+
+constexpr int kTickSteps = 4;
 
 double cells_of(const Req* q) {
     return (double)q->r.grid.nx * q->r.grid.ny * q->r.grid.nz;
@@ -267,13 +270,25 @@ void loop(ws_server* s) {
             }
             s->rebuild = false;
         }
-        for (int p = 0; p < 2; ++p) s->runner[p].step(1, st);
+        // steps this tick: up to the first completion; at most kTickSteps
+        // while nothing waits in the queue (a request arriving now is then
+        // admitted within that many steps)
+        int k = 1 << 30;
+        for (Req* q : s->active) k = std::min(k, q->r.nsteps - q->steps_done);
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            if (s->queue.empty()) k = std::min(k, kTickSteps);
+        }
+        k = std::max(k, 1);
+        // the batch changes every few ticks: launch the steps directly
+        // rather than capture a graph for each new batch
+        for (int p = 0; p < 2; ++p) s->runner[p].step_eager(k, st);
         cudaStreamSynchronize(st);
         s->ticks++;
-        s->executed_cell_rhs += 3.0 * s->active_cells;
+        s->executed_cell_rhs += 3.0 * k * s->active_cells;
         std::vector<Req*> done;
         for (Req* q : s->active)
-            if (++q->steps_done >= q->r.nsteps) done.push_back(q);
+            if ((q->steps_done += k) >= q->r.nsteps) done.push_back(q);
         if (!done.empty()) {
             int err = WS_OK;
             for (Req* q : done) {

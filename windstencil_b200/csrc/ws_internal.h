@@ -125,6 +125,12 @@ struct GridState {
     int cur = 0;
     double dt = 0.0;
     const ws_field* prims() const { return pr[cur]; }
+    // fused-stage arguments [2 * c + (stage == 2)] for state buffer c (with
+    // their tensor maps), kept while the tile shape, sweep cap and dt stay
+    // the same, so re-forming a batch does not re-encode them
+    std::vector<RhsArgs> args;
+    int args_cfg = -1, args_zc = 0;
+    double args_dt = 0.0;
 };
 size_t grid_state_bytes(const ws_grid& g);
 // stream-ordered allocation from the device's default memory pool
@@ -151,6 +157,8 @@ class BatchRunner {
     int enqueue_step(cudaStream_t st);
     // nsteps steps (graph replay); flips every grid's current buffer
     int step(int nsteps, cudaStream_t st);
+    // the same without graphs (a batch that changes every few steps)
+    int step_eager(int nsteps, cudaStream_t st);
     int size() const { return (int)grids_.size(); }
     int cfg() const { return cfg_; }
     int zc() const { return zc_; }
