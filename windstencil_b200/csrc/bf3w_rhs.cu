@@ -16,15 +16,17 @@
 //     round-trips fpY/fmY/fpZ/fmZ through global scratch).
 //   * Per plane, two barrier intervals:
 //       A: x-split over (BX+8) x BY points and y-split over BX x (BY+8)
-//          points into shared memory;
+//          points into shared memory, and the z-split of the plane 5 ahead
+//          into the ring;
 //       B: every x, y face of the plane and the z face above it as one work
-//          item (face, variable) evaluating its P and M WENO once, plus the
-//          z-split of the plane 5 ahead into the ring;
+//          item (face, variable) evaluating its P and M WENO once;
 //     then the FP64 face difference writes du (no barrier needed before the
 //     next plane's split interval: the arrays are disjoint).
-//   * Primitive planes are staged with cp.async, double-buffered one plane
+//   * Primitive planes are staged with TMA tile loads (one thread issues
+//     them, an mbarrier tracks their bytes), double-buffered one plane
 //     ahead: the buffer of plane z holds its (BX+8) x (BY+8) box and the
-//     BX x BY centre of plane z+5.
+//     BX x BY centre of plane z+5.  Fields whose box starts would not be
+//     16-byte aligned are staged with per-thread cp.async instead.
 //   * Stage mode (EPI, used by the solver and batches): instead of writing
 //     du, the difference phase applies the SSP-RK3 stage to the conserved
 //     state and writes the primitives of the new state to a second set of
@@ -311,9 +313,11 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
         const int b = (z - z0) & 1;
         const double* sb = stg + b * L::STG;
 
-        // ---- interval A: x- and y-split of plane z
-        constexpr int NXS = SXW * BY, NYS = BX * SYH;
-        for (int t = tid; t < NXS + NYS; t += NT) {
+        // ---- interval A: x- and y-split of plane z, z-split of plane z+5
+        constexpr unsigned NXS = SXW * BY, NYS = BX * SYH;
+        unsigned ta = tid;
+        for (; ta < NXS + NYS; ta += NT) {
+            const int t = ta;
             CT out[10];
             if (t < NXS) {
                 const int yy = t / SXW, xi = t - yy * SXW;
@@ -339,6 +343,20 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
             }
         }
         const bool more = z + 1 < z1;
+        if (more) {   // plane z+5 enters the ring (slot of plane z-4, last read by face z-1/2)
+            for (ta -= NXS + NYS; ta < BXY; ta += NT) {
+                const int col = ta;
+                const double* cb = sb + 5 * BOX + col;
+                const int Z = z + 5;
+                CT out[10];
+                split_point<2, UNI, CT>(a, k, cb[0], cb[BXY], cb[2 * BXY], cb[3 * BXY],
+                                        cb[4 * BXY], min(x0 + col % BX, a.nx + 7),
+                                        min(y0 + col / BX, a.ny + 7), min(Z, a.nz + 7), out);
+                CT* dst = ring + (Z % 9) * RS + col;
+#pragma unroll
+                for (int c = 0; c < 10; ++c) dst[c * BXY] = out[c];
+            }
+        }
         if (more) {
             if (!tma) {
                 issue_stage<BX, BY, NT>(a, stg + (b ^ 1) * L::STG, x0, y0, z + 1);
@@ -350,13 +368,13 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
         }
         __syncthreads();
 
-        // ---- interval B: faces of plane z, z face z+1/2, z-split of plane z+5
+        // ---- interval B: faces of plane z and the z face z+1/2
         const int cur = prev ^ 1;
         const int s0 = (z - 3) % 9;
         // One round robin over the plane's items, split into loops by item
         // kind (no per-item branch chain): the x face right of each column
         // and the y face above each row (power-of-two index math), the z
-        // faces, the left/bottom faces of the tile, then the z split.
+        // faces, then the left/bottom faces of the tile.
         constexpr unsigned NXR = 5 * BXY, NYR = 5 * BXY, NZF = 5 * BXY;
         constexpr unsigned NE = 5 * (BY + BX);
         unsigned t = tid;
@@ -381,20 +399,6 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
                 const unsigned var = (t - 5 * BY) / BX, xx = (t - 5 * BY) % BX;
                 fy[var * (BY + 1) * BX + xx] =
                     face_flux<CT>(sys + var * SYH * BX + xx, 5 * SYH * BX, BX, 8, 0);
-            }
-        }
-        if (more) {
-            for (t -= NE; t < BXY; t += NT) {
-                const int col = t;
-                const double* cb = sb + 5 * BOX + col;
-                const int Z = z + 5;
-                CT out[10];
-                split_point<2, UNI, CT>(a, k, cb[0], cb[BXY], cb[2 * BXY], cb[3 * BXY],
-                                        cb[4 * BXY], min(x0 + col % BX, a.nx + 7),
-                                        min(y0 + col / BX, a.ny + 7), min(Z, a.nz + 7), out);
-                CT* dst = ring + (Z % 9) * RS + col;
-#pragma unroll
-                for (int c = 0; c < 10; ++c) dst[c * BXY] = out[c];
             }
         }
         cp_async_wait<0>();
