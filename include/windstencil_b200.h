@@ -64,7 +64,14 @@ typedef struct ws_job { ws_dim3 start, end; } ws_job;
 
 enum ws_face_kind {
     WS_FACE_PERIODIC = 0,   /* ghosts wrap (the reference's periodic self-exchange) */
-    WS_FACE_EXTRAP = 1      /* zero-gradient ghosts (copy of the boundary cell)     */
+    WS_FACE_EXTRAP = 1,     /* zero-gradient ghosts (copy of the boundary cell)     */
+    /* x and y faces only: zero-gradient ghosts, and the faces next to it take
+     * the boundary closures of the reference's fused path (its ring kernel
+     * split_Jac3d_Stager_Warming_ker_boundary, OCFD_NS_Jacobian3d.cpp:
+     * 1063-1085 for x and :1515-1584 for y): WENO5 one-sided forms, linear
+     * extrapolation / averages (x) or minmod2 forms (y) at the high end, and
+     * the reference's dropped M term of the last y cell.  >= 8 cells.       */
+    WS_FACE_CLOSURE = 2
 };
 
 enum ws_precision {

@@ -11,7 +11,11 @@ and the index macros to host C++, compiles them with g++ into
 reference source is kept (``oracle/_ref/`` is git-ignored).
 
 Functions taken from the reference (path within the WindStencil tree):
-  src/kernels/OCFD_Schemes.cpp        OCFD_weno7_SYMBO_kernel_P_opt, _M_opt
+  src/kernels/OCFD_Schemes.cpp        OCFD_weno7_SYMBO_kernel_P_opt, _M_opt,
+                                      OCFD_weno5_kernel_P, _M, sign, minmod2
+  src/boundary/OCFD_bound_Scheme.cpp  OCFD_weno5_kernel_P_lift, _P_lift_plus,
+                                      _P_right_plus, _M_lift, _M_lift_plus,
+                                      _M_right_plus
   src/solver/OCFD_NS_Jacobian3d.cpp   split_Jac3d_Stager_Warming_ker_origin
   src/kernels/commen_kernel.cpp       cons_to_pri_kernel, pri_to_cons_kernel,
                                       sound_speed_kernel
@@ -22,7 +26,10 @@ Functions taken from the reference (path within the WindStencil tree):
 The host drivers below (``ref_*``) are this project's code: they set the
 HIP thread coordinates for every point and call the reference function, and
 ``ref_du_invis`` assembles the decomposed RHS from the reference's split and
-WENO functions with the loop of oracle/oracle.cpp (or_du_invis).
+WENO functions with the loop of oracle/oracle.cpp (or_du_invis); for CLOSURE
+faces it takes the face values near them from the reference's WENO5 closure
+functions, by the per-face rules this project reads out of the fused path's
+ring kernel (OCFD_NS_Jacobian3d.cpp:1063-1085 x, :1515-1584 y).
 
 Only tests/ and bench.py's CPU-baseline legs use the result, as the checker.
 Usage:  python oracle/build_ref.py [--ref /path/to/reference] [--native]
@@ -43,6 +50,16 @@ DEFAULT_REF = "/root/reference"
 FUNCS = [
     ("src/kernels/OCFD_Schemes.cpp", "OCFD_weno7_SYMBO_kernel_P_opt"),
     ("src/kernels/OCFD_Schemes.cpp", "OCFD_weno7_SYMBO_kernel_M_opt"),
+    ("src/kernels/OCFD_Schemes.cpp", "sign"),
+    ("src/kernels/OCFD_Schemes.cpp", "minmod2"),
+    ("src/kernels/OCFD_Schemes.cpp", "OCFD_weno5_kernel_P"),
+    ("src/kernels/OCFD_Schemes.cpp", "OCFD_weno5_kernel_M"),
+    ("src/boundary/OCFD_bound_Scheme.cpp", "OCFD_weno5_kernel_P_lift"),
+    ("src/boundary/OCFD_bound_Scheme.cpp", "OCFD_weno5_kernel_P_lift_plus"),
+    ("src/boundary/OCFD_bound_Scheme.cpp", "OCFD_weno5_kernel_P_right_plus"),
+    ("src/boundary/OCFD_bound_Scheme.cpp", "OCFD_weno5_kernel_M_lift"),
+    ("src/boundary/OCFD_bound_Scheme.cpp", "OCFD_weno5_kernel_M_lift_plus"),
+    ("src/boundary/OCFD_bound_Scheme.cpp", "OCFD_weno5_kernel_M_right_plus"),
     ("src/solver/OCFD_NS_Jacobian3d.cpp", "split_Jac3d_Stager_Warming_ker_origin"),
     ("src/kernels/commen_kernel.cpp", "pri_to_cons_kernel"),
     ("src/kernels/commen_kernel.cpp", "cons_to_pri_kernel"),
@@ -59,7 +76,7 @@ SHIM_HEAD = r"""
 #include <cmath>
 #include <cstring>
 #include <vector>
-using std::sqrt; using std::fmax; using std::fmin;
+using std::sqrt; using std::fmax; using std::fmin; using std::abs;
 typedef double REAL;
 #define LAP 4
 #define __device__
@@ -107,6 +124,25 @@ void ref_weno_p_batch(const double* s, long n, double* out) {
 void ref_weno_m_batch(const double* s, long n, double* out) {
   #pragma omp parallel for schedule(static)
   for (long i = 0; i < n; ++i) out[i] = ref_weno_m(s + 8 * i); }
+
+// WENO5 closure family, same order as the oracle's or_weno5_batch
+void ref_weno5_batch(int which, const double* s, long n, double* out) {
+  #pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; ++i) {
+    REAL t[5]; std::memcpy(t, s + 5 * i, sizeof t);
+    switch (which) {
+      case 0: out[i] = OCFD_weno5_kernel_P_lift(t); break;
+      case 1: out[i] = OCFD_weno5_kernel_P_lift_plus(t); break;
+      case 2: out[i] = OCFD_weno5_kernel_P(t); break;
+      case 3: out[i] = OCFD_weno5_kernel_P_right_plus(t); break;
+      case 4: out[i] = OCFD_weno5_kernel_M_lift(t); break;
+      case 5: out[i] = OCFD_weno5_kernel_M_lift_plus(t); break;
+      case 6: out[i] = OCFD_weno5_kernel_M(t); break;
+      case 7: out[i] = OCFD_weno5_kernel_M_right_plus(t); break;
+      default: out[i] = minmod2(t[0], t[1]); break;
+    }
+  }
+}
 
 // one-point fields: pitch 1 and unit padded extents make every index 0 (+var)
 void ref_split_batch(const double* in, long n, double gamma, double eps,
@@ -194,14 +230,45 @@ void ref_time_advance(int krk, double dt, int nx, int ny, int nz, double* f, dou
   }
 }
 
+// Face value of the ring kernel's closures for face f (between cells f-1
+// and f) of a line of n cells (F[c] = split flux of cell c); false: WENO7.
+// The rules read out of OCFD_NS_Jacobian3d.cpp:1063-1085 (x) and :1515-1584
+// (y), as one value per face.
+bool ref_closure_face(int pm, int dir, long f, long n, bool lo, bool hi, REAL* F, double* out) {
+  if (pm == 0) {
+    if (lo && f == 0) { *out = F[0]; return true; }
+    if (lo && f == 1) { *out = OCFD_weno5_kernel_P_lift(F + f - 3); return true; }
+    if (lo && f == 2) { *out = OCFD_weno5_kernel_P_lift_plus(F + f - 3); return true; }
+    if ((lo && f == 3) || (hi && f == n - 2)) { *out = OCFD_weno5_kernel_P(F + f - 3); return true; }
+    if (hi && f == n - 1) { *out = OCFD_weno5_kernel_P_right_plus(F + f - 3); return true; }
+    if (hi && f == n) {
+      *out = dir == 0 ? 1.5*F[n - 1] - 0.5*F[n - 2]
+                      : F[n - 1]+0.5*minmod2(F[n - 1] -F[n - 2], F[n - 1] -F[n - 2]);
+      return true;
+    }
+    return false;
+  }
+  if (lo && f == 0) { *out = OCFD_weno5_kernel_M_lift(F + f - 2); return true; }
+  if (lo && f == 1) { *out = OCFD_weno5_kernel_M_lift_plus(F + f - 2); return true; }
+  if ((lo && (f == 2 || f == 3)) || (hi && f == n - 3)) { *out = OCFD_weno5_kernel_M(F + f - 2); return true; }
+  if (hi && f == n - 2) { *out = OCFD_weno5_kernel_M_right_plus(F + f - 2); return true; }
+  if (hi && f == n - 1) {
+    *out = dir == 0 ? 0.5 *F[n - 1] + 0.5 *F[n - 2]
+                    : F[n - 1]-0.5*minmod2(F[n - 1] - F[n - 2], F[n - 1] - F[n - 2]);
+    return true;
+  }
+  if (hi && f == n) { *out = dir == 0 ? 0.5 *F[n - 1] + 0.5 *F[n - 2] : F[n - 1]; return true; }
+  return false;
+}
+
 // Decomposed inviscid RHS from the reference's split and WENO functions; the
 // loop structure is or_du_invis() of oracle/oracle.cpp.  Cartesian metrics
-// when metrics == NULL, J = 1 when ajac == NULL.  face_kind is not needed:
-// ghosts must be filled by the caller.
+// when metrics == NULL, J = 1 when ajac == NULL.  Ghosts must be filled by
+// the caller; face_kind (may be NULL) marks CLOSURE faces (value 2).
 void ref_du_invis(int nx, int ny, int nz, double hx, double hy, double hz, double gamma,
                   double eps, const double* d, const double* u, const double* v,
                   const double* w, const double* cc, const double* const* metrics,
-                  const double* ajac, double* du) {
+                  const double* ajac, double* du, const int* face_kind) {
   const long px = nx + 2 * LAP, py = ny + 2 * LAP;
   auto lap = [&](long i, long j, long k) { return (i + LAP) + px * ((j + LAP) + py * (k + LAP)); };
   const double h[3] = {hx, hy, hz};
@@ -239,13 +306,19 @@ void ref_du_invis(int nx, int ny, int nz, double hx, double hy, double hz, doubl
             fm[var * (n + 2 * LAP) + s + LAP] = mm[var];
           }
         }
+        const bool lo = face_kind && dir < 2 && face_kind[2 * dir] == 2;
+        const bool hi = face_kind && dir < 2 && face_kind[2 * dir + 1] == 2;
         for (int pm = 0; pm < 2; ++pm) for (int var = 0; var < 5; ++var) {
           double* line = (pm == 0 ? fp.data() : fm.data()) + var * (n + 2 * LAP);
           for (long i = -1; i < n; ++i) {
             REAL* st = line + (i - 3 + LAP);
+            if ((lo || hi) && ref_closure_face(pm, dir, i + 1, n, lo, hi, line + LAP, &face[i + 1]))
+              continue;
             face[i + 1] = pm == 0 ? OCFD_weno7_SYMBO_kernel_P_opt(st) : OCFD_weno7_SYMBO_kernel_M_opt(st);
           }
-          for (long i = 0; i < n; ++i) {
+          // the ring kernel never adds the y M term of the last cell
+          const long iend = (dir == 1 && pm == 1 && hi) ? n - 1 : n;
+          for (long i = 0; i < iend; ++i) {
             const double J = ajac ? ajac[at(i)] : 1.0;
             du[cell(i, var)] += -J * (face[i + 1] - face[i]) / h[dir];
           }

@@ -160,6 +160,166 @@ void sw_split(R d, R u, R v, R w, R cc, R a1, R a2, R a3, double gamma,
 }
 
 // ----------------------------------------------------------------------------
+// CLOSURE face mode: the boundary closures of the fused path's ring kernel
+// (split_Jac3d_Stager_Warming_ker_boundary, OCFD_NS_Jacobian3d.cpp:828-2530),
+// which that kernel applies near the x and y faces of the domain.
+//
+// WENO5 family (s[0..4] a 5-point stencil): the one- and two-candidate forms
+// of OCFD_bound_Scheme.cpp:540-720 (eps = 1e-6, unit linear weights, weights
+// 1/(12 eps + S)^2) and the three-candidate forms OCFD_Schemes.cpp:1110-1140
+// (P) and :1170-1200 (M).  The P form builds its weights a0 and a1 from S1
+// and S2 before they are accumulated (so from zero); that is reproduced.
+// Operation order as in the reference.
+// ----------------------------------------------------------------------------
+constexpr double kEp5 = 1e-6;
+
+double w5_p_lift(const double* s) {            // OCFD_bound_Scheme.cpp:560-576
+    double S0 = 0.0, t;
+    t = s[2] - 2.0 * s[3] + s[4];       S0 += 13 * t * t;
+    t = 3.0 * s[2] - 4.0 * s[3] + s[4]; S0 += 3 * t * t;
+    const double a0 = 1.0 / ((12.0 * kEp5 + S0) * (12.0 * kEp5 + S0));
+    const double q03 = (2.0 * s[2] + 5.0 * s[3] - s[4]);
+    return a0 * q03 / (6.0 * a0);
+}
+double w5_m_lift(const double* s) {            // OCFD_bound_Scheme.cpp:598-615
+    double S2 = 0.0, t;
+    t = s[4] - 2.0 * s[3] + s[2];       S2 += 13 * t * t;
+    t = s[4] - 4.0 * s[3] + 3.0 * s[2]; S2 += 3 * t * t;
+    const double a2 = 1.0 / ((12.0 * kEp5 + S2) * (12.0 * kEp5 + S2));
+    const double q23 = (2.0 * s[4] - 7.0 * s[3] + 11.0 * s[2]);
+    return a2 * q23 / (6.0 * a2);
+}
+double w5_p_right_plus(const double* s) {      // OCFD_bound_Scheme.cpp:617-641
+    double S1 = 0.0, S2 = 0.0, t;
+    t = s[1] - 2.0 * s[2] + s[3]; S1 += 13 * t * t;
+    t = s[1] - s[3];              S1 += 3 * t * t;
+    const double a1 = 1.0 / ((12.0 * kEp5 + S1) * (12.0 * kEp5 + S1));
+    const double q13 = (-s[1] + 5.0 * s[2] + 2.0 * s[3]);
+    t = s[0] - 2.0 * s[1] + s[2];       S2 += 13 * t * t;
+    t = s[0] - 4.0 * s[1] + 3.0 * s[2]; S2 += 3 * t * t;
+    const double a2 = 1.0 / ((12.0 * kEp5 + S2) * (12.0 * kEp5 + S2));
+    const double q23 = (2.0 * s[0] - 7.0 * s[1] + 11.0 * s[2]);
+    return (a1 * q13 + a2 * q23) / (6.0 * (a1 + a2));
+}
+double w5_p_lift_plus(const double* s) {       // OCFD_bound_Scheme.cpp:643-667
+    double S0 = 0.0, S1 = 0.0, t;
+    t = s[2] - 2.0 * s[3] + s[4];       S0 += 13 * t * t;
+    t = 3.0 * s[2] - 4.0 * s[3] + s[4]; S0 += 3 * t * t;
+    const double a0 = 1.0 / ((12.0 * kEp5 + S0) * (12.0 * kEp5 + S0));
+    const double q03 = (2.0 * s[2] + 5.0 * s[3] - s[4]);
+    t = s[1] - 2.0 * s[2] + s[3]; S1 += 13 * t * t;
+    t = s[1] - s[3];              S1 += 3 * t * t;
+    const double a1 = 1.0 / ((12.0 * kEp5 + S1) * (12.0 * kEp5 + S1));
+    const double q13 = (-s[1] + 5.0 * s[2] + 2.0 * s[3]);
+    return (a0 * q03 + a1 * q13) / (6.0 * (a0 + a1));
+}
+double w5_m_right_plus(const double* s) {      // OCFD_bound_Scheme.cpp:669-693
+    double S0 = 0.0, S1 = 0.0, t;
+    t = s[2] - 2.0 * s[1] + s[0];       S0 += 13 * t * t;
+    t = 3.0 * s[2] - 4.0 * s[1] + s[0]; S0 += 3 * t * t;
+    const double a0 = 1.0 / ((12.0 * kEp5 + S0) * (12.0 * kEp5 + S0));
+    const double q03 = (2.0 * s[2] + 5.0 * s[1] - s[0]);
+    t = s[3] - 2.0 * s[2] + s[1]; S1 += 13 * t * t;
+    t = s[3] - s[1];              S1 += 3 * t * t;
+    const double a1 = 1.0 / ((12.0 * kEp5 + S1) * (12.0 * kEp5 + S1));
+    const double q13 = (-s[3] + 5.0 * s[2] + 2.0 * s[1]);
+    return (a0 * q03 + a1 * q13) / (6.0 * (a0 + a1));
+}
+double w5_m_lift_plus(const double* s) {       // OCFD_bound_Scheme.cpp:695-719
+    double S1 = 0.0, S2 = 0.0, t;
+    t = s[3] - 2.0 * s[2] + s[1]; S1 += 13 * t * t;
+    t = s[3] - s[1];              S1 += 3 * t * t;
+    const double a1 = 1.0 / ((12.0 * kEp5 + S1) * (12.0 * kEp5 + S1));
+    const double q13 = (-s[3] + 5.0 * s[2] + 2.0 * s[1]);
+    t = s[4] - 2.0 * s[3] + s[2];       S2 += 13 * t * t;
+    t = s[4] - 4.0 * s[3] + 3.0 * s[2]; S2 += 3 * t * t;
+    const double a2 = 1.0 / ((12.0 * kEp5 + S2) * (12.0 * kEp5 + S2));
+    const double q23 = (2.0 * s[4] - 7.0 * s[3] + 11.0 * s[2]);
+    return (a1 * q13 + a2 * q23) / (6.0 * (a1 + a2));
+}
+double w5_p(const double* s) {                 // OCFD_Schemes.cpp:1110-1140
+    double S0 = 0.0, S1 = 0.0, S2 = 0.0, t;
+    t = s[2] - 2.0 * s[3] + s[4];       S0 += 13 * t * t;
+    t = 3.0 * s[2] - 4.0 * s[3] + s[4]; S0 += 3 * t * t;
+    // a0 from S1, S2 while they are still 0.0 (the reference's order)
+    const double a0 = ((12.0 * kEp5 + S1) * (12.0 * kEp5 + S1)) *
+                      ((12.0 * kEp5 + S2) * (12.0 * kEp5 + S2));
+    const double q03 = (2.0 * s[2] + 5.0 * s[3] - s[4]);
+    t = s[1] - 2.0 * s[2] + s[3]; S1 += 13 * t * t;
+    t = s[1] - s[3];              S1 += 3 * t * t;
+    const double a1 = ((12.0 * kEp5 + S0) * (12.0 * kEp5 + S0)) *
+                      ((12.0 * kEp5 + S2) * (12.0 * kEp5 + S2));
+    const double q13 = (-s[1] + 5.0 * s[2] + 2.0 * s[3]);
+    t = s[0] - 2.0 * s[1] + s[2];       S2 += 13 * t * t;
+    t = s[0] - 4.0 * s[1] + 3.0 * s[2]; S2 += 3 * t * t;
+    const double a2 = ((12.0 * kEp5 + S0) * (12.0 * kEp5 + S0)) *
+                      ((12.0 * kEp5 + S1) * (12.0 * kEp5 + S1));
+    const double q23 = (2.0 * s[0] - 7.0 * s[1] + 11.0 * s[2]);
+    return (a0 * q03 + a1 * q13 + a2 * q23) / (6.0 * (a0 + a1 + a2));
+}
+double w5_m(const double* s) {                 // OCFD_Schemes.cpp:1170-1200
+    double S0 = 0.0, S1 = 0.0, S2 = 0.0, t;
+    t = s[2] - 2.0 * s[1] + s[0];       S0 += 13 * t * t;
+    t = 3.0 * s[2] - 4.0 * s[1] + s[0]; S0 += 3 * t * t;
+    const double a0 = 1.0 / ((12.0 * kEp5 + S0) * (12.0 * kEp5 + S0));
+    const double q03 = (2.0 * s[2] + 5.0 * s[1] - s[0]);
+    t = s[3] - 2.0 * s[2] + s[1]; S1 += 13 * t * t;
+    t = s[3] - s[1];              S1 += 3 * t * t;
+    const double a1 = 1.0 / ((12.0 * kEp5 + S1) * (12.0 * kEp5 + S1));
+    const double q13 = (-s[3] + 5.0 * s[2] + 2.0 * s[1]);
+    t = s[4] - 2.0 * s[3] + s[2];       S2 += 13 * t * t;
+    t = s[4] - 4.0 * s[3] + 3.0 * s[2]; S2 += 3 * t * t;
+    const double a2 = 1.0 / ((12.0 * kEp5 + S2) * (12.0 * kEp5 + S2));
+    const double q23 = (2.0 * s[4] - 7.0 * s[3] + 11.0 * s[2]);
+    return (a0 * q03 + a1 * q13 + a2 * q23) / (6.0 * (a0 + a1 + a2));
+}
+// OCFD_Schemes.cpp:822-835
+double sign_of(double x1, double x2) { return x2 >= 0 ? std::fabs(x1) : -std::fabs(x1); }
+double minmod2(double x1, double x2) {
+    return 0.5 * (sign_of(1.0, x1) + sign_of(1.0, x2)) * std::fmin(std::fabs(x1), std::fabs(x2));
+}
+
+// Closure value of face f (between cells f-1 and f, f = 0..n) of a line of n
+// cells in the x (dir 0) or y (dir 1) direction; F[c] is the split flux of
+// cell c (F[-4..n+3] valid), pm 0 for F+ (P faces), 1 for F- (M faces).  lo /
+// hi: the low / high face of the direction is a CLOSURE face.  Returns false
+// when face f keeps its WENO7-SYMBO value.  The per-face rules restate the
+// ring kernel's x rules (OCFD_NS_Jacobian3d.cpp:1063-1069 P, :1079-1085 M) and
+// y rules (:1515-1584), read as one value per face: every face value is the
+// same from both cells that share it.  x and y differ at the high end: x
+// extrapolates linearly and averages, y uses minmod2 forms and a copy.
+bool closure_face(int pm, int dir, long f, long n, bool lo, bool hi, const double* F,
+                  double* out) {
+    if (pm == 0) {
+        if (lo && f == 0) { *out = F[0]; return true; }
+        if (lo && f == 1) { *out = w5_p_lift(F + f - 3); return true; }
+        if (lo && f == 2) { *out = w5_p_lift_plus(F + f - 3); return true; }
+        if ((lo && f == 3) || (hi && f == n - 2)) { *out = w5_p(F + f - 3); return true; }
+        if (hi && f == n - 1) { *out = w5_p_right_plus(F + f - 3); return true; }
+        if (hi && f == n) {
+            *out = dir == 0 ? 1.5 * F[n - 1] - 0.5 * F[n - 2]
+                            : F[n - 1] + 0.5 * minmod2(F[n - 1] - F[n - 2], F[n - 1] - F[n - 2]);
+            return true;
+        }
+        return false;
+    }
+    if (lo && f == 0) { *out = w5_m_lift(F + f - 2); return true; }
+    if (lo && f == 1) { *out = w5_m_lift_plus(F + f - 2); return true; }
+    if ((lo && (f == 2 || f == 3)) || (hi && f == n - 3)) { *out = w5_m(F + f - 2); return true; }
+    if (hi && f == n - 2) { *out = w5_m_right_plus(F + f - 2); return true; }
+    if (hi && f == n - 1) {
+        *out = dir == 0 ? 0.5 * F[n - 1] + 0.5 * F[n - 2]
+                        : F[n - 1] - 0.5 * minmod2(F[n - 1] - F[n - 2], F[n - 1] - F[n - 2]);
+        return true;
+    }
+    if (hi && f == n) {
+        *out = dir == 0 ? 0.5 * F[n - 1] + 0.5 * F[n - 2] : F[n - 1];
+        return true;
+    }
+    return false;
+}
+
+// ----------------------------------------------------------------------------
 // Indexing helpers (reference: cuda_utility.h:16-27).
 // ----------------------------------------------------------------------------
 struct Dims {
@@ -193,6 +353,27 @@ void or_weno7_p_batch(const double* s, long n, double* out) {
 void or_weno7_m_batch(const double* s, long n, double* out) {
 #pragma omp parallel for schedule(static)
     for (long i = 0; i < n; ++i) out[i] = weno_m<double>(s + 8 * i);
+}
+
+// WENO5 closure family over n 5-point stencils; which: 0 P_lift, 1 P_lift_plus,
+// 2 P, 3 P_right_plus, 4 M_lift, 5 M_lift_plus, 6 M, 7 M_right_plus, 8 minmod2
+// of (s[0], s[1])
+void or_weno5_batch(int which, const double* s, long n, double* out) {
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < n; ++i) {
+        const double* p = s + 5 * i;
+        switch (which) {
+            case 0: out[i] = w5_p_lift(p); break;
+            case 1: out[i] = w5_p_lift_plus(p); break;
+            case 2: out[i] = w5_p(p); break;
+            case 3: out[i] = w5_p_right_plus(p); break;
+            case 4: out[i] = w5_m_lift(p); break;
+            case 5: out[i] = w5_m_lift_plus(p); break;
+            case 6: out[i] = w5_m(p); break;
+            case 7: out[i] = w5_m_right_plus(p); break;
+            default: out[i] = minmod2(p[0], p[1]); break;
+        }
+    }
 }
 
 void or_split(double d, double u, double v, double w, double cc, double a1,
@@ -312,7 +493,14 @@ void or_du_invis(const or_grid* g, const double* d, const double* u,
                             fm[var * (n + 2 * L) + (s + L)] = mm[var];
                         }
                     }
-                    // faces i+1/2 for i = -1..n-1 use points i-3..i+4
+                    // faces i+1/2 for i = -1..n-1 use points i-3..i+4; in
+                    // CLOSURE mode the faces near a CLOSURE x or y face take
+                    // the ring kernel's closure values, and the y direction
+                    // drops the M term of the last cell (the ring kernel
+                    // computes it but never adds it, OCFD_NS_Jacobian3d.cpp:
+                    // 1580-1583)
+                    const bool lo = dir < 2 && g->face_kind[2 * dir] == OR_FACE_CLOSURE;
+                    const bool hi = dir < 2 && g->face_kind[2 * dir + 1] == OR_FACE_CLOSURE;
                     std::vector<double> face(n + 1);
                     for (int pm = 0; pm < 2; ++pm)
                         for (int var = 0; var < 5; ++var) {
@@ -320,10 +508,14 @@ void or_du_invis(const or_grid* g, const double* d, const double* u,
                                 (pm == 0 ? fp.data() : fm.data()) + var * (n + 2 * L);
                             for (long i = -1; i < n; ++i) {
                                 const double* st = line + (i - 3 + L);
+                                if ((lo || hi) &&
+                                    closure_face(pm, dir, i + 1, n, lo, hi, line + L, &face[i + 1]))
+                                    continue;
                                 face[i + 1] = pm == 0 ? weno_p<double>(st)
                                                       : weno_m<double>(st);
                             }
-                            for (long i = 0; i < n; ++i) {
+                            const long iend = (dir == 1 && pm == 1 && hi) ? n - 1 : n;
+                            for (long i = 0; i < iend; ++i) {
                                 const double J = ajac ? ajac[at(i)] : 1.0;
                                 du[cell(i, var)] += -J * (face[i + 1] - face[i]) / h[dir];
                             }

@@ -32,7 +32,9 @@ extern "C" {
 
 #define OR_LAP 4
 
-enum { OR_FACE_PERIODIC = 0, OR_FACE_EXTRAP = 1 };
+/* CLOSURE (x and y faces only): zero-gradient ghosts, and the faces next to
+ * it take the boundary closures of the fused path's ring kernel */
+enum { OR_FACE_PERIODIC = 0, OR_FACE_EXTRAP = 1, OR_FACE_CLOSURE = 2 };
 
 typedef struct or_grid {
     int nx, ny, nz;            /* interior extents                                  */
@@ -48,6 +50,8 @@ double or_weno7_p(const double* s8);
 double or_weno7_m(const double* s8);
 void   or_weno7_p_batch(const double* s8n, long n, double* out);
 void   or_weno7_m_batch(const double* s8n, long n, double* out);
+/* WENO5 closure family on n 5-point stencils (which: see oracle.cpp) */
+void   or_weno5_batch(int which, const double* s5n, long n, double* out);
 void   or_split(double d, double u, double v, double w, double cc,
                 double a1, double a2, double a3, double gamma, double epsl_sw,
                 double* fp5, double* fm5);

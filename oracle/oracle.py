@@ -19,7 +19,10 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LAP = 4
-FACE_PERIODIC, FACE_EXTRAP = 0, 1
+FACE_PERIODIC, FACE_EXTRAP, FACE_CLOSURE = 0, 1, 2
+# WENO5 closure family, in the order of or_weno5_batch / ref_weno5_batch
+WENO5_FORMS = ("p_lift", "p_lift_plus", "p", "p_right_plus", "m_lift", "m_lift_plus",
+               "m", "m_right_plus", "minmod2")
 
 _dp = C.POINTER(C.c_double)
 
@@ -83,6 +86,7 @@ class Oracle:
         L.or_split_batch.argtypes = [_dp, C.c_long, C.c_double, C.c_double, _dp, _dp]
         L.or_weno7_p_batch.argtypes = [_dp, C.c_long, _dp]
         L.or_weno7_m_batch.argtypes = [_dp, C.c_long, _dp]
+        L.or_weno5_batch.argtypes = [C.c_int, _dp, C.c_long, _dp]
         L.or_time_advance.argtypes = [C.c_int, C.c_double, C.c_long, _dp, _dp, _dp]
 
     # -- scalar kernels ----------------------------------------------------
@@ -96,6 +100,13 @@ class Oracle:
         s = np.ascontiguousarray(s, dtype=np.float64).reshape(-1, 8)
         out = np.empty(len(s))
         self.lib.or_weno7_m_batch(_p(s), len(s), _p(out))
+        return out
+
+    def weno5(self, form: str, s: np.ndarray) -> np.ndarray:
+        """WENO5 closure form (WENO5_FORMS) on rows of 5 points."""
+        s = np.ascontiguousarray(s, dtype=np.float64).reshape(-1, 5)
+        out = np.empty(len(s))
+        self.lib.or_weno5_batch(WENO5_FORMS.index(form), _p(s), len(s), _p(out))
         return out
 
     def split(self, pts: np.ndarray, gamma=1.4, epsl_sw=1e-6):
@@ -184,12 +195,13 @@ class RefFunctions:
         L.ref_split_batch.argtypes = [_dp, C.c_long, C.c_double, C.c_double, _dp, _dp]
         L.ref_weno_p_batch.argtypes = [_dp, C.c_long, _dp]
         L.ref_weno_m_batch.argtypes = [_dp, C.c_long, _dp]
+        L.ref_weno5_batch.argtypes = [C.c_int, _dp, C.c_long, _dp]
         L.ref_cons_to_prim.argtypes = [C.c_int] * 3 + [C.c_double] * 2 + [_dp] * 7
         L.ref_prim_to_cons.argtypes = [C.c_int] * 3 + [C.c_double] * 2 + [_dp] * 6
         L.ref_sound_speed.argtypes = [C.c_int] * 3 + [C.c_double, _dp, _dp]
         L.ref_time_advance.argtypes = [C.c_int, C.c_double] + [C.c_int] * 3 + [_dp] * 3
         L.ref_du_invis.argtypes = ([C.c_int] * 3 + [C.c_double] * 5 + [_dp] * 5 +
-                                   [C.POINTER(_dp), _dp, _dp])
+                                   [C.POINTER(_dp), _dp, _dp, C.POINTER(C.c_int)])
 
     def weno_p(self, s):
         s = np.ascontiguousarray(s, dtype=np.float64).reshape(-1, 8)
@@ -201,6 +213,12 @@ class RefFunctions:
         s = np.ascontiguousarray(s, dtype=np.float64).reshape(-1, 8)
         out = np.empty(len(s))
         self.lib.ref_weno_m_batch(_p(s), len(s), _p(out))
+        return out
+
+    def weno5(self, form, s):
+        s = np.ascontiguousarray(s, dtype=np.float64).reshape(-1, 5)
+        out = np.empty(len(s))
+        self.lib.ref_weno5_batch(WENO5_FORMS.index(form), _p(s), len(s), _p(out))
         return out
 
     def split(self, pts, gamma=1.4, epsl_sw=1e-6):
@@ -232,7 +250,8 @@ class RefFunctions:
 
     def du_invis(self, g: OrGrid, d, u, v, w, cc, metrics=None, ajac=None):
         du = np.empty((5, g.nz, g.ny, g.nx))
+        kinds = (C.c_int * 6)(*[g.face_kind[i] for i in range(6)])
         self.lib.ref_du_invis(g.nx, g.ny, g.nz, g.hx, g.hy, g.hz, g.gamma, g.epsl_sw,
                               _p(d), _p(u), _p(v), _p(w), _p(cc), _ptr_array(metrics),
-                              _p(ajac), _p(du))
+                              _p(ajac), _p(du), kinds)
         return du

@@ -97,3 +97,31 @@ def test_du_invis_bitexact(oracle, reffn, general):
     a = oracle.du_invis(g, d, u, v, w, cc, metrics, ajac)
     b = reffn.du_invis(g, d, u, v, w, cc, metrics, ajac)
     assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("form", ["p_lift", "p_lift_plus", "p", "p_right_plus", "m_lift",
+                                  "m_lift_plus", "m", "m_right_plus", "minmod2"])
+def test_weno5_closures_bitexact(oracle, reffn, form):
+    # the CLOSURE mode's WENO5 family and minmod2, including the reference's
+    # weight order of OCFD_weno5_kernel_P
+    rng = np.random.default_rng(18)
+    s = rng.standard_normal((200_000, 5)) * rng.uniform(1e-3, 30.0, (200_000, 1))
+    s[:1000] = rng.uniform(-2, 2, (1000, 1))                      # constant
+    s[1000:2000] = np.where(np.arange(5) > 2, 1.0, 0.125)         # step
+    s[2000:2100, :2] = 0.0                                        # minmod2 zeros
+    s[2100:2200, 1] = -s[2100:2200, 0]                            # opposite signs
+    assert np.array_equal(oracle.weno5(form, s), reffn.weno5(form, s))
+
+
+@pytest.mark.parametrize("faces", [(2, 2, 0, 0, 0, 0), (0, 0, 2, 2, 0, 0), (2, 2, 2, 2, 1, 1),
+                                   (2, 1, 1, 2, 0, 0), (1, 2, 2, 0, 0, 0)])
+def test_du_invis_closure_bitexact(oracle, reffn, faces):
+    # CLOSURE faces: the ring kernel's boundary closures near the x / y faces
+    g = make_grid(17, 13, 9, face_kind=faces)
+    d, u, v, w, T = _prims(g, 19)
+    for a in (d, u, v, w, T):
+        oracle.ghost_fill(g, a)
+    cc = oracle.sound_speed(g, T)
+    a = oracle.du_invis(g, d, u, v, w, cc)
+    b = reffn.du_invis(g, d, u, v, w, cc)
+    assert np.array_equal(a, b)

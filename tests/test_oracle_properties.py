@@ -88,3 +88,15 @@ def test_high_mach_noisy_state_goes_nonphysical_in_reference_arithmetic(oracle):
     bad = (not np.all(np.isfinite(f))) or f[0].min() <= 0 or \
         np.min(T[LAP:-LAP, LAP:-LAP, LAP:-LAP]) <= 0
     assert bad
+
+
+def test_closure_faces_preserve_free_stream(oracle):
+    # a uniform state stays uniform next to CLOSURE faces (every closure form
+    # reproduces a constant stencil up to rounding)
+    from oracle.oracle import make_grid as mg
+    g = mg(20, 12, 8, face_kind=(2, 2, 2, 2, 0, 0))
+    shp = (8 + 8, 12 + 8, 20 + 8)
+    d, u, v, w, T = (np.full(shp, x) for x in (1.3, 0.4, -0.2, 0.1, 0.9))
+    cc = oracle.sound_speed(g, T)
+    du = oracle.du_invis(g, d, u, v, w, cc)
+    assert np.abs(du).max() <= 1e-11

@@ -19,12 +19,12 @@ from __future__ import annotations
 import ctypes as C
 from dataclasses import dataclass, field
 
-from ._abi import (FACE_EXTRAP, FACE_PERIODIC, FP64, LAP, MIXED, WsDim3, WsError, WsField,
+from ._abi import (FACE_CLOSURE, FACE_EXTRAP, FACE_PERIODIC, FP64, LAP, MIXED, WsDim3, WsError, WsField,
                    WsGrid, WsJob, WsMetrics, WsSoa, WsTile, check, header_symbols, last_error,
                    load)
 
 __all__ = [
-    "FACE_EXTRAP", "FACE_PERIODIC", "FP64", "MIXED", "LAP", "WsError", "Grid", "make_grid",
+    "FACE_CLOSURE", "FACE_EXTRAP", "FACE_PERIODIC", "FP64", "MIXED", "LAP", "WsError", "Grid", "make_grid",
     "lap_tensor", "soa_tensor", "field_desc", "soa_desc", "interior_job", "du_invis_jacobian3d",
     "du_invis_jacobian3d_init", "ghost_fill", "cons_to_prim", "prim_to_cons", "time_advance",
     "Solver", "load", "header_symbols", "last_error",

@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(HERE, "libwindstencil_b200.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "windstencil_b200.h")
 
 LAP = 4
-FACE_PERIODIC, FACE_EXTRAP = 0, 1
+FACE_PERIODIC, FACE_EXTRAP, FACE_CLOSURE = 0, 1, 2
 FP64, MIXED = 0, 1
 
 WS_OK = 0

@@ -37,9 +37,16 @@ int check_grid(const ws_grid* g) {
     if (!(g->hx > 0 && g->hy > 0 && g->hz > 0)) return fail(WS_ERR_INVALID, "h must be > 0");
     if (!(g->gamma > 1.0) || !(g->ama > 0) || !(g->epsl_sw >= 0))
         return fail(WS_ERR_INVALID, "need gamma > 1, ama > 0, epsl_sw >= 0");
-    for (int i = 0; i < 6; ++i)
-        if (g->face_kind[i] != WS_FACE_PERIODIC && g->face_kind[i] != WS_FACE_EXTRAP)
-            return fail(WS_ERR_INVALID, "face_kind must be WS_FACE_PERIODIC or WS_FACE_EXTRAP");
+    for (int i = 0; i < 6; ++i) {
+        const int k = g->face_kind[i];
+        if (k != WS_FACE_PERIODIC && k != WS_FACE_EXTRAP && k != WS_FACE_CLOSURE)
+            return fail(WS_ERR_INVALID, "face_kind must be a ws_face_kind value");
+        if (k == WS_FACE_CLOSURE && i >= 4)
+            return fail(WS_ERR_UNSUPPORTED, "CLOSURE faces are x and y faces only "
+                                            "(the reference closes z through its ghosts)");
+        if (k == WS_FACE_CLOSURE && (i < 2 ? g->nx : g->ny) < 8)
+            return fail(WS_ERR_INVALID, "a CLOSURE direction needs >= 8 cells");
+    }
     if (g->precision != WS_FP64 && g->precision != WS_MIXED)
         return fail(WS_ERR_INVALID, "precision must be WS_FP64 or WS_MIXED");
     return WS_OK;
@@ -161,6 +168,7 @@ RhsArgs make_rhs_args(const ws_grid* g, ws_job job, const ws_field prims[5],
     a.c1 = 2.0 * (g->gamma - 1.0);
     a.c3 = (3.0 - g->gamma) / (2.0 * (g->gamma - 1.0));
     a.gm1 = g->gamma - 1.0;
+    for (int i = 0; i < 4; ++i) a.clo[i] = g->face_kind[i] == WS_FACE_CLOSURE ? 1 : 0;
     // TMA staging: box starts at x = sx - 4 + k*bx and centres at sx + k*bx
     // are even (16-byte aligned for doubles) when sx is even
     bool tma = (job.start.x % 2) == 0;
@@ -199,7 +207,8 @@ int set_rhs_stage(RhsArgs& a, const ws_grid* g, ws_soa f_in, ws_soa fn, ws_soa f
 int rhs_ctas(const ws_grid* g, const RhsArgs& a, int cfg, bool stage) {
     const long ntile = (long)a.ntx * a.nty;
     const long planes = ntile * (a.ez - a.sz);
-    int ctas = rhs_max_ctas(g->precision, g->metrics_uniform != 0, cfg, stage);
+    const bool clo = a.clo[0] | a.clo[1] | a.clo[2] | a.clo[3];
+    int ctas = rhs_max_ctas(g->precision, g->metrics_uniform != 0, clo, cfg, stage);
     if (ctas <= 0) return 0;
     const long want = ntile >= ctas ? ctas : std::max(ntile, planes / 16);
     if (want < ctas) ctas = (int)std::max(1L, want);
@@ -246,6 +255,8 @@ int rhs_stage_enqueue(const ws_grid* g, const ws_field p_in[6], ws_soa f_in, ws_
     if (ctas <= 0) return fail(WS_ERR_CUDA, "cannot size the persistent grid");
     return launch_rhs(a, g->precision, true, cfg, ctas, krk, st);
 }
+
+int validate_grid(const ws_grid* g) { return check_grid(g); }
 
 }  // namespace ws
 

@@ -215,7 +215,10 @@ int BatchRunner::build(const std::vector<GridState*>& grids, int cfg, int zc, cu
     d_gtab_ = reinterpret_cast<int2*>(d + o_gt);
     int rc = upload_tables(st);
     if (rc) return rc;
-    const int maxc = rhs_max_ctas(precision_, true, cfg_, true);
+    closure_ = false;
+    for (auto* s : grids)
+        for (int i = 0; i < 4; ++i) closure_ |= s->g.face_kind[i] == WS_FACE_CLOSURE;
+    const int maxc = rhs_max_ctas(precision_, true, closure_, cfg_, true);
     if (maxc <= 0) return fail(WS_ERR_CUDA, "cannot size the persistent grid");
     const long planes = hc[n];
     ctas_ = (int)std::max(1L, std::min<long>(maxc, std::max<long>(1, planes / 16)));
@@ -235,7 +238,7 @@ int BatchRunner::enqueue_rhs(cudaStream_t st) {
     int rc = launch_ghost_fill_batch(d_ghost_[parity_], d_gtab_, n_gtab_, st);
     if (rc) return rc;
     return launch_rhs_batch(d_rhs_[2 * parity_], d_cum_, (int)grids_.size(), zc_, precision_,
-                            true, cfg_, ctas_, 0, st);
+                            true, closure_, cfg_, ctas_, 0, st);
 }
 
 // stage 1 alone: reads f[cur], pr[cur] and writes only the other buffers,
@@ -245,7 +248,7 @@ int BatchRunner::enqueue_stage1(cudaStream_t st) {
     int rc = launch_ghost_fill_batch(d_ghost_[parity_], d_gtab_, n_gtab_, st);
     if (rc) return rc;
     return launch_rhs_batch(d_rhs_[2 * parity_], d_cum_, (int)grids_.size(), zc_, precision_,
-                            true, cfg_, ctas_, 1, st);
+                            true, closure_, cfg_, ctas_, 1, st);
 }
 
 int BatchRunner::enqueue_step(cudaStream_t st) {
@@ -255,7 +258,7 @@ int BatchRunner::enqueue_step(cudaStream_t st) {
         int rc = launch_ghost_fill_batch(d_ghost_[parity_ ^ two], d_gtab_, n_gtab_, st);
         if (rc) return rc;
         rc = launch_rhs_batch(d_rhs_[2 * parity_ + two], d_cum_, (int)grids_.size(), zc_,
-                              precision_, true, cfg_, ctas_, krk, st);
+                              precision_, true, closure_, cfg_, ctas_, krk, st);
         if (rc) return rc;
     }
     return WS_OK;
@@ -341,6 +344,7 @@ int ws_batch_create(const ws_grid* grids, int n, ws_batch** out) {
     if (!grids || n <= 0) return fail(WS_ERR_INVALID, "need at least one grid");
     for (int i = 0; i < n; ++i) {
         const ws_grid& g = grids[i];
+        if (int rc = validate_grid(&g)) return rc;
         if (g.lap != WS_LAP || g.nx < 4 || g.ny < 4 || g.nz < 4 || !g.metrics_uniform ||
             (g.precision != WS_FP64 && g.precision != WS_MIXED) ||
             g.precision != grids[0].precision)

@@ -93,8 +93,7 @@ int ws_solver_create(const ws_grid* g, ws_solver** out) {
     if (!out) return fail(WS_ERR_INVALID, "out is NULL");
     *out = nullptr;
     if (!g) return fail(WS_ERR_INVALID, "grid is NULL");
-    if (g->lap != WS_LAP || g->nx < 4 || g->ny < 4 || g->nz < 4)
-        return fail(WS_ERR_INVALID, "invalid grid");
+    if (int rc = validate_grid(g)) return rc;
     if (g->precision != WS_FP64 && g->precision != WS_MIXED)
         return fail(WS_ERR_INVALID, "precision must be WS_FP64 or WS_MIXED");
     if (!g->metrics_uniform)

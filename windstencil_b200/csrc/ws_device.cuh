@@ -228,6 +228,89 @@ __device__ __forceinline__ void weno7_symbo_nd(const double t[8], double& num, d
 }
 
 // ---------------------------------------------------------------------------
+// CLOSURE face mode: the boundary closures of the reference's ring kernel
+// (split_Jac3d_Stager_Warming_ker_boundary, OCFD_NS_Jacobian3d.cpp:1063-1085
+// for x, :1515-1584 for y).  WENO5 family on a 5-point stencil s[0..4]
+// (OCFD_bound_Scheme.cpp:560-719; three-candidate forms OCFD_Schemes.cpp:
+// 1110-1140 and :1170-1200, whose P form takes a0 and a1 from S1 and S2
+// before they are accumulated -- kept), eps = 1e-6, no linear weights.
+// These run only on the faces next to a CLOSURE face, in FP64.
+// ---------------------------------------------------------------------------
+namespace w5 {
+constexpr double E12 = 12.0 * 1e-6;
+__device__ __forceinline__ double s_lo(const double* s) {   // candidate on s[2..4]
+    const double t0 = s[2] - 2.0 * s[3] + s[4], t1 = 3.0 * s[2] - 4.0 * s[3] + s[4];
+    return 13 * t0 * t0 + 3 * t1 * t1;
+}
+__device__ __forceinline__ double s_mid(const double* s) {  // candidate on s[1..3]
+    const double t0 = s[1] - 2.0 * s[2] + s[3], t1 = s[1] - s[3];
+    return 13 * t0 * t0 + 3 * t1 * t1;
+}
+__device__ __forceinline__ double s_hi(const double* s) {   // candidate on s[0..2]
+    const double t0 = s[0] - 2.0 * s[1] + s[2], t1 = s[0] - 4.0 * s[1] + 3.0 * s[2];
+    return 13 * t0 * t0 + 3 * t1 * t1;
+}
+__device__ __forceinline__ double s_lo_m(const double* s) { // mirror of s_hi on s[2..4]
+    const double t0 = s[4] - 2.0 * s[3] + s[2], t1 = s[4] - 4.0 * s[3] + 3.0 * s[2];
+    return 13 * t0 * t0 + 3 * t1 * t1;
+}
+__device__ __forceinline__ double s_hi_m(const double* s) { // mirror of s_lo on s[0..2]
+    const double t0 = s[2] - 2.0 * s[1] + s[0], t1 = 3.0 * s[2] - 4.0 * s[1] + s[0];
+    return 13 * t0 * t0 + 3 * t1 * t1;
+}
+__device__ __forceinline__ double w(double S) { return 1.0 / ((E12 + S) * (E12 + S)); }
+__device__ __forceinline__ double sq(double S) { return (E12 + S) * (E12 + S); }
+// candidate values (times 6)
+__device__ __forceinline__ double q_lo(const double* s) { return 2.0 * s[2] + 5.0 * s[3] - s[4]; }
+__device__ __forceinline__ double q_mid(const double* s) { return -s[1] + 5.0 * s[2] + 2.0 * s[3]; }
+__device__ __forceinline__ double q_hi(const double* s) { return 2.0 * s[0] - 7.0 * s[1] + 11.0 * s[2]; }
+__device__ __forceinline__ double qm_lo(const double* s) { return 2.0 * s[4] - 7.0 * s[3] + 11.0 * s[2]; }
+__device__ __forceinline__ double qm_mid(const double* s) { return -s[3] + 5.0 * s[2] + 2.0 * s[1]; }
+__device__ __forceinline__ double qm_hi(const double* s) { return 2.0 * s[2] + 5.0 * s[1] - s[0]; }
+
+__device__ __forceinline__ double p_lift(const double* s) {
+    const double a0 = w(s_lo(s));
+    return a0 * q_lo(s) / (6.0 * a0);
+}
+__device__ __forceinline__ double p_lift_plus(const double* s) {
+    const double a0 = w(s_lo(s)), a1 = w(s_mid(s));
+    return (a0 * q_lo(s) + a1 * q_mid(s)) / (6.0 * (a0 + a1));
+}
+__device__ __forceinline__ double p_right_plus(const double* s) {
+    const double a1 = w(s_mid(s)), a2 = w(s_hi(s));
+    return (a1 * q_mid(s) + a2 * q_hi(s)) / (6.0 * (a1 + a2));
+}
+__device__ __forceinline__ double p3(const double* s) {
+    const double S0 = s_lo(s), S1 = s_mid(s);
+    const double a0 = sq(0.0) * sq(0.0);     // from S1, S2 before they are accumulated
+    const double a1 = sq(S0) * sq(0.0);
+    const double a2 = sq(S0) * sq(S1);
+    return (a0 * q_lo(s) + a1 * q_mid(s) + a2 * q_hi(s)) / (6.0 * (a0 + a1 + a2));
+}
+__device__ __forceinline__ double m_lift(const double* s) {
+    const double a2 = w(s_lo_m(s));
+    return a2 * qm_lo(s) / (6.0 * a2);
+}
+__device__ __forceinline__ double m_lift_plus(const double* s) {
+    const double a1 = w(s_mid(s)), a2 = w(s_lo_m(s));
+    return (a1 * qm_mid(s) + a2 * qm_lo(s)) / (6.0 * (a1 + a2));
+}
+__device__ __forceinline__ double m_right_plus(const double* s) {
+    const double a0 = w(s_hi_m(s)), a1 = w(s_mid(s));
+    return (a0 * qm_hi(s) + a1 * qm_mid(s)) / (6.0 * (a0 + a1));
+}
+__device__ __forceinline__ double m3(const double* s) {
+    const double a0 = w(s_hi_m(s)), a1 = w(s_mid(s)), a2 = w(s_lo_m(s));
+    return (a0 * qm_hi(s) + a1 * qm_mid(s) + a2 * qm_lo(s)) / (6.0 * (a0 + a1 + a2));
+}
+// OCFD_Schemes.cpp:822-835
+__device__ __forceinline__ double minmod2(double x1, double x2) {
+    const double s1 = x1 >= 0 ? 1.0 : -1.0, s2 = x2 >= 0 ? 1.0 : -1.0;
+    return 0.5 * (s1 + s2) * fmin(fabs(x1), fabs(x2));
+}
+}  // namespace w5
+
+// ---------------------------------------------------------------------------
 // Mixed form: the P and M reconstructions of one face are the same arithmetic
 // on two stencils, so they run as the two lanes of Blackwell's packed FP32x2
 // instructions (FFMA2/FADD2/FMUL2): t[k] = (P stencil k, M stencil k).  Same

@@ -11,6 +11,10 @@
 
 namespace ws {
 
+// Grid checks shared by every entry point (extents, constants, face kinds,
+// precision); WS_OK or the error code with its message set.
+int validate_grid(const ws_grid* g);
+
 // Error reporting: the message of the last failure, per host thread.
 void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);
@@ -34,6 +38,7 @@ struct RhsArgs {
     int ntx, nty, nzc, zc;     // tiles in x and y, z chunks and chunk length
     double rhx, rhy, rhz;      // 1/h
     double eps2, hrg, c1, c3, gm1;
+    int clo[4];                // CLOSURE faces: x-, x+, y-, y+ (0/1)
     // fused SSP-RK3 stage epilogue (solver and batches, whole interior):
     // f_out <- stage(fn, f_in, dt*du); d,u,v,w,T,cc of the new state into the
     // interiors of p_out (a second set of LAP fields: other CTAs still read
@@ -78,11 +83,14 @@ int default_cfg(int precision);                   // tuned default shape
 // krk == 0: write du; krk in 1..3: fused SSP-RK3 stage epilogue (Cartesian).
 int launch_rhs(const RhsArgs& a, int precision, bool uniform, int cfg, int ctas, int krk,
                cudaStream_t st);
-int rhs_max_ctas(int precision, bool uniform, int cfg, bool stage);   // resident CTAs
+// resident CTAs of the kernel for (precision, metric kind, CLOSURE faces
+// present, tile shape, stage epilogue)
+int rhs_max_ctas(int precision, bool uniform, bool closure, int cfg, bool stage);
 // Batched RHS over n grids (device array of RhsArgs, cum[n+1] tile-plane
-// prefix sums); all grids share precision, metric kind and tile shape.
+// prefix sums); all grids share precision, metric kind and tile shape;
+// closure: some grid has CLOSURE faces.
 int launch_rhs_batch(const RhsArgs* grids, const long* cum, int n, int zc, int precision,
-                     bool uniform, int cfg, int ctas, int krk, cudaStream_t st);
+                     bool uniform, bool closure, int cfg, int ctas, int krk, cudaStream_t st);
 // Host-side RhsArgs of one grid and job (tile shape cfg, sweep cap scan).
 RhsArgs make_rhs_args(const ws_grid* g, ws_job job, const ws_field prims[5],
                       const ws_metrics* m, ws_soa du, int cfg, int scan);
@@ -168,6 +176,7 @@ class BatchRunner {
     int upload_tables(cudaStream_t st);
     std::vector<GridState*> grids_;
     int precision_ = 0, cfg_ = 0, zc_ = 1 << 30, ctas_ = 0;
+    bool closure_ = false;          // some grid has CLOSURE faces
     void* dev_ = nullptr;           // device tables
     size_t dev_bytes_ = 0;
     // With c = cur ^ p (p = step parity since build), a step reads f[c] and
