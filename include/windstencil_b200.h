@@ -167,6 +167,31 @@ WS_API int ws_du_invis_jacobian3d_tiled(const ws_grid* g, ws_job job, ws_field d
                                  const ws_metrics* metrics, ws_soa du, ws_tile tile,
                                  ws_stream_t stream);
 
+/* Viscous constants of the Navier-Stokes RHS: Reynolds number, Prandtl
+ * number, Sutherland reference temperature Ref_T (Sutherland constant
+ * 110.4 K, viscosity 1/Re at T = 1) and the central-difference order of the
+ * derivatives, 6 or 8 (the reference's Scheme_vis_ID 203 / 204). */
+typedef struct ws_viscous {
+    double re, pr, ref_t;
+    int32_t scheme;
+    int32_t dummy0;
+} ws_viscous;
+
+/* Device workspace that ws_du_vis_jacobian3d needs for grid g (bytes). */
+WS_API size_t ws_du_vis_workspace_bytes(const ws_grid* g);
+
+/* du[1..4] (SoA, whole interior) += viscous terms of momentum and energy from
+ * the LAP fields u, v, w, T (ghosts filled); du[0] is left as it is.
+ * Replaces du_vis_Jacobian3d (OCFD_Stream.cpp:229-345: gradient kernels
+ * OCFD_NS_Jacobian3d.cpp:455-475, vis_flux_ker :477-624 per direction,
+ * halo exchange of the fluxes, derivative and YF_Pe_XF accumulation), with
+ * the fluxes' ghosts filled by g->face_kind.  workspace: caller-owned device
+ * memory of ws_du_vis_workspace_bytes(g) (the reference keeps the same
+ * fields as globals); the call allocates nothing. */
+WS_API int ws_du_vis_jacobian3d(const ws_grid* g, const ws_viscous* vis, ws_field u, ws_field v,
+                                ws_field w, ws_field T, const ws_metrics* metrics, ws_soa du,
+                                void* workspace, size_t workspace_bytes, ws_stream_t stream);
+
 /* In-place ghost fill (4 layers) of nfields LAP fields by g->face_kind.
  * Replaces exchange_boundary_xyz_packed_dev (OCFD_mpi_dev.cpp:123-290) on one
  * GPU: no host staging, no MPI. */
@@ -235,6 +260,9 @@ WS_API int  ws_solver_step(ws_solver* s, double dt, int nsteps, ws_stream_t stre
 /* Device status word (0 or WS_ERR_NONFINITE); synchronises `stream`. */
 WS_API int  ws_solver_status(ws_solver* s, int* status, ws_stream_t stream);
 WS_API int  ws_solver_set_tile(ws_solver* s, ws_tile tile);
+/* Navier-Stokes: every RHS adds the viscous terms (NULL: Euler again).  The
+ * solver keeps their workspace; the RK stage adds them before its update. */
+WS_API int  ws_solver_set_viscous(ws_solver* s, const ws_viscous* vis);
 
 /* ------------------------------------------------------------------------ */
 /* Many independent grids, device-resident, stepped together: per RK stage   */

@@ -16,6 +16,9 @@ Functions taken from the reference (path within the WindStencil tree):
   src/boundary/OCFD_bound_Scheme.cpp  OCFD_weno5_kernel_P_lift, _P_lift_plus,
                                       _P_right_plus, _M_lift, _M_lift_plus,
                                       _M_right_plus
+  src/kernels/OCFD_Schemes.cpp        OCFD_kernel_CD6, OCFD_kernel_CD8
+  src/solver/OCFD_NS_Jacobian3d.cpp   vis_flux_ker
+  src/kernels/commen_kernel.cpp       get_Amu_kernal, YF_Pe_XF
   src/solver/OCFD_NS_Jacobian3d.cpp   split_Jac3d_Stager_Warming_ker_origin
   src/kernels/commen_kernel.cpp       cons_to_pri_kernel, pri_to_cons_kernel,
                                       sound_speed_kernel
@@ -60,6 +63,11 @@ FUNCS = [
     ("src/boundary/OCFD_bound_Scheme.cpp", "OCFD_weno5_kernel_M_lift"),
     ("src/boundary/OCFD_bound_Scheme.cpp", "OCFD_weno5_kernel_M_lift_plus"),
     ("src/boundary/OCFD_bound_Scheme.cpp", "OCFD_weno5_kernel_M_right_plus"),
+    ("src/kernels/OCFD_Schemes.cpp", "OCFD_kernel_CD6"),
+    ("src/kernels/OCFD_Schemes.cpp", "OCFD_kernel_CD8"),
+    ("src/solver/OCFD_NS_Jacobian3d.cpp", "vis_flux_ker"),
+    ("src/kernels/commen_kernel.cpp", "get_Amu_kernal"),
+    ("src/kernels/commen_kernel.cpp", "YF_Pe_XF"),
     ("src/solver/OCFD_NS_Jacobian3d.cpp", "split_Jac3d_Stager_Warming_ker_origin"),
     ("src/kernels/commen_kernel.cpp", "pri_to_cons_kernel"),
     ("src/kernels/commen_kernel.cpp", "cons_to_pri_kernel"),
@@ -93,6 +101,7 @@ struct cudaJobPackage { dim3 start, end;
   cudaJobPackage(const dim3& s, const dim3& e) : start(s), end(e) {} };
 static thread_local REAL epsl_sw_d, Gamma_d, split_C1_d, split_C3_d, Cv_d, Ama_d, dt_d;
 static thread_local unsigned ny_d, nz_d, ny_2lap_d, nz_2lap_d;
+static thread_local REAL vis_flux_init_c_d, amu_C0_d, Tsb_d;
 """
 
 DRIVERS = r"""
@@ -322,6 +331,114 @@ void ref_du_invis(int nx, int ny, int nz, double hx, double hy, double hz, doubl
             const double J = ajac ? ajac[at(i)] : 1.0;
             du[cell(i, var)] += -J * (face[i + 1] - face[i]) / h[dir];
           }
+        }
+      }
+    }
+  }
+}
+// Viscous terms (du_vis_Jacobian3d) from the reference's vis_flux_ker,
+// get_Amu_kernal, OCFD_kernel_CD6/CD8 and YF_Pe_XF, with the loop structure
+// of or_du_vis() in oracle/oracle.cpp: derivatives of u, v, w, T through
+// the ghosts (value / h, as put_d0_kernel), viscosity, then per direction
+// the flux on the interior, its ghosts filled by face_kind, its derivative
+// and du[1..4] += J * derivative.  metrics / ajac may be NULL (Cartesian).
+void ref_du_vis(int nx, int ny, int nz, double hx, double hy, double hz, double gamma,
+                double ama, double re, double pr, double ref_t, int scheme, double* u,
+                double* v, double* w, double* T, const double* const* metrics,
+                const double* ajac, double* du, const int* face_kind) {
+  const long px = nx + 2 * LAP, py = ny + 2 * LAP, pz = nz + 2 * LAP, L = px * py * pz;
+  const long N = (long)nx * ny * nz;
+  auto lap = [&](long i, long j, long k) { return (i + LAP) + px * ((j + LAP) + py * (k + LAP)); };
+  const double h[3] = {hx, hy, hz};
+  const long r = scheme == 6 ? 3 : 4;
+  // Cartesian metrics as fields when none are given
+  std::vector<double> unit(L, 1.0), zero(L, 0.0);
+  const double* M[9];
+  for (int m = 0; m < 9; ++m)
+    M[m] = metrics ? metrics[m] : (m == 0 || m == 4 || m == 8 ? unit.data() : zero.data());
+  const double* J = ajac ? ajac : unit.data();
+  auto cf = [&](const double* p, long pitch) { cudaField f; f.ptr = const_cast<double*>(p);
+    f.pitch = (unsigned)pitch; f.dummy0 = 0; return f; };
+  auto d0 = [&](const double* f, int dir, double* out) {
+    #pragma omp parallel for collapse(2) schedule(static)
+    for (long k = 0; k < nz; ++k) for (long j = 0; j < ny; ++j) for (long i = 0; i < nx; ++i) {
+      REAL st[9];
+      for (long q = -r; q <= r; ++q)
+        st[q + r] = f[dir == 0 ? lap(i + q, j, k) : dir == 1 ? lap(i, j + q, k) : lap(i, j, k + q)];
+      const REAL tmp = scheme == 6 ? OCFD_kernel_CD6(st) : OCFD_kernel_CD8(st);
+      out[i + nx * (j + ny * k)] = tmp / h[dir];
+    }
+  };
+  auto ghost = [&](double* f) {      // periodic wrap / zero gradient, x then y then z
+    for (long k = -LAP; k < nz + LAP; ++k) for (long j = -LAP; j < ny + LAP; ++j)
+      for (long l = 1; l <= LAP; ++l) {
+        f[lap(-l, j, k)] = f[lap(face_kind[0] == 0 ? nx - l : 0, j, k)];
+        f[lap(nx - 1 + l, j, k)] = f[lap(face_kind[1] == 0 ? l - 1 : nx - 1, j, k)];
+      }
+    for (long k = -LAP; k < nz + LAP; ++k) for (long l = 1; l <= LAP; ++l)
+      for (long i = -LAP; i < nx + LAP; ++i) {
+        f[lap(i, -l, k)] = f[lap(i, face_kind[2] == 0 ? ny - l : 0, k)];
+        f[lap(i, ny - 1 + l, k)] = f[lap(i, face_kind[3] == 0 ? l - 1 : ny - 1, k)];
+      }
+    for (long l = 1; l <= LAP; ++l) for (long j = -LAP; j < ny + LAP; ++j)
+      for (long i = -LAP; i < nx + LAP; ++i) {
+        f[lap(i, j, -l)] = f[lap(i, j, face_kind[4] == 0 ? nz - l : 0)];
+        f[lap(i, j, nz - 1 + l)] = f[lap(i, j, face_kind[5] == 0 ? l - 1 : nz - 1)];
+      }
+  };
+  std::vector<double> grad(12 * N), amu(N), Ev(4 * L), dv(N);
+  double* prim[4] = {u, v, w, T};
+  for (int dir = 0; dir < 3; ++dir) for (int q = 0; q < 4; ++q)
+    d0(prim[q], dir, grad.data() + (4 * dir + q) * N);
+  #pragma omp parallel
+  {
+    set_consts(gamma, ama, 0.0); set_dims(nx, ny, nz);
+    // OCFD_init.cpp:380-396
+    const double Cp = 1.0 / ((gamma - 1.0) * ama * ama);
+    Tsb_d = 110.4 / ref_t;
+    amu_C0_d = 1.0 / re * (1.0 + 110.4 / ref_t);
+    vis_flux_init_c_d = Cp / pr;
+    cudaJobPackage job0(dim3(0, 0, 0), dim3(nx, ny, nz));
+    #pragma omp for collapse(2) schedule(static)
+    for (int k = 0; k < nz; ++k) for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i) {
+      threadIdx = dim3(i, j, k); blockIdx = dim3(0, 0, 0); blockDim = dim3(1, 1, 1);
+      get_Amu_kernal(cf(amu.data(), nx), cf(T, px), job0);
+    }
+  }
+  auto G = [&](int dir, int q) { return cf(grad.data() + (4 * dir + q) * N, nx); };
+  for (int dir = 0; dir < 3; ++dir) {
+    std::fill(Ev.begin(), Ev.end(), 0.0);
+    #pragma omp parallel
+    {
+      set_consts(gamma, ama, 0.0); set_dims(nx, ny, nz);
+      const double Cp = 1.0 / ((gamma - 1.0) * ama * ama);
+      vis_flux_init_c_d = Cp / pr;
+      cudaJobPackage job(dim3(LAP, LAP, LAP), dim3(nx + LAP, ny + LAP, nz + LAP));
+      #pragma omp for collapse(2) schedule(static)
+      for (int k = 0; k < nz; ++k) for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i) {
+        threadIdx = dim3(i, j, k); blockIdx = dim3(0, 0, 0); blockDim = dim3(1, 1, 1);
+        vis_flux_ker(G(0, 0), G(0, 1), G(0, 2), G(1, 0), G(1, 1), G(1, 2), G(2, 0), G(2, 1),
+                     G(2, 2), G(0, 3), G(1, 3), G(2, 3), cf(amu.data(), nx),
+                     cf(u, px), cf(v, px), cf(w, px),
+                     cf(M[3 * dir], px), cf(M[3 * dir + 1], px), cf(M[3 * dir + 2], px),
+                     cf(J, px), cf(M[0], px), cf(M[1], px), cf(M[2], px), cf(M[3], px),
+                     cf(M[4], px), cf(M[5], px), cf(M[6], px), cf(M[7], px), cf(M[8], px),
+                     cf(Ev.data(), px), cf(Ev.data() + L, px), cf(Ev.data() + 2 * L, px),
+                     cf(Ev.data() + 3 * L, px), job);
+      }
+    }
+    for (int q = 0; q < 4; ++q) {
+      double* e = Ev.data() + q * L;
+      ghost(e);
+      d0(e, dir, dv.data());
+      #pragma omp parallel
+      {
+        set_dims(nx, ny, nz);
+        cudaJobPackage job0(dim3(0, 0, 0), dim3(nx, ny, nz));
+        #pragma omp for collapse(2) schedule(static)
+        for (int k = 0; k < nz; ++k) for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i) {
+          threadIdx = dim3(i, j, k); blockIdx = dim3(0, 0, 0); blockDim = dim3(1, 1, 1);
+          YF_Pe_XF(cf(du + (q + 1) * N, nx), cf(dv.data(), nx), cf(J, px), job0);
         }
       }
     }

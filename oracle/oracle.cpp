@@ -18,6 +18,7 @@
 
 #include <cmath>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <vector>
 #ifdef _OPENMP
@@ -441,6 +442,138 @@ void or_sound_speed(const or_grid* g, const double* T, double* cc) {
     for (long i = 0; i < n; ++i) cc[i] = std::sqrt(T[i]) / g->ama;
 }
 
+// ----------------------------------------------------------------------------
+// Viscous terms: du_vis_Jacobian3d (OCFD_Stream.cpp:229-345).
+//   1. first derivatives of u, v, w, T along the three computational
+//      directions on the interior: central CD6 / CD8 through the ghosts
+//      (OCFD_Schemes.cpp:97-104, :134-142; value / h, put_d0_kernel :74-95);
+//   2. Sutherland viscosity (get_Amu_kernal, commen_kernel.cpp:123-132);
+//   3. per direction: the viscous flux Ev1..4 on the interior
+//      (vis_flux_ker, OCFD_NS_Jacobian3d.cpp:477-624), its ghosts filled by
+//      the face kinds, its derivative along that direction, and
+//      du[1..4] += J * derivative (YF_Pe_XF, commen_kernel.cpp:159-170).
+// Constants as OCFD_init.cpp:380-396: Cp = 1/((g-1) Ama^2), Tsb = 110.4/Ref_T,
+// amu_C0 = 1/Re*(1 + 110.4/Ref_T), heat-flux factor Cp/Pr.
+// ----------------------------------------------------------------------------
+namespace {
+double cd6(const double* s) {
+    return (45.0 * (s[4] - s[2]) - 9.0 * (s[5] - s[1]) + (s[6] - s[0])) / 60.0;
+}
+double cd8(const double* s) {
+    return (672.0 * (s[5] - s[3]) - 168.0 * (s[6] - s[2]) + 32.0 * (s[7] - s[1]) -
+            3.0 * (s[8] - s[0])) / 840.0;
+}
+// derivative along dir of LAP field f on the interior (dense out)
+void d0_field(const or_grid* g, int scheme, int dir, const double* f, double* out) {
+    Dims D(g);
+    const long r = scheme == 6 ? 3 : 4;
+    const double h = dir == 0 ? g->hx : dir == 1 ? g->hy : g->hz;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (long k = 0; k < D.nz; ++k)
+        for (long j = 0; j < D.ny; ++j)
+            for (long i = 0; i < D.nx; ++i) {
+                double st[9];
+                for (long q = -r; q <= r; ++q)
+                    st[q + r] = f[dir == 0 ? D.lap(i + q, j, k)
+                                           : dir == 1 ? D.lap(i, j + q, k) : D.lap(i, j, k + q)];
+                const double tmp = scheme == 6 ? cd6(st) : cd8(st);
+                out[i + D.nx * (j + D.ny * k)] = tmp / h;
+            }
+}
+}  // namespace
+
+void or_amu(const or_grid* g, const or_vis* vis, const double* T, double* amu) {
+    Dims D(g);
+    const double Tsb = 110.4 / vis->ref_t;
+    const double amu_C0 = 1.0 / vis->re * (1.0 + 110.4 / vis->ref_t);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (long k = 0; k < D.nz; ++k)
+        for (long j = 0; j < D.ny; ++j)
+            for (long i = 0; i < D.nx; ++i) {
+                const double tmp = T[D.lap(i, j, k)];
+                amu[i + D.nx * (j + D.ny * k)] = amu_C0 * std::sqrt(tmp * tmp * tmp) / (Tsb + tmp);
+            }
+}
+
+void or_du_vis(const or_grid* g, const or_vis* vis, const double* u, const double* v,
+               const double* w, const double* T, const double* const* metrics,
+               const double* ajac, double* du) {
+    Dims D(g);
+    const long N = D.cells();
+    const double Cp = 1.0 / ((g->gamma - 1.0) * g->ama * g->ama);
+    const double vfc = Cp / vis->pr;
+    // grad[4*dir + q]: derivative along dir of (u, v, w, T)[q]
+    std::vector<double> grad(12 * N), amu(N);
+    const double* prim[4] = {u, v, w, T};
+    for (int dir = 0; dir < 3; ++dir)
+        for (int q = 0; q < 4; ++q)
+            d0_field(g, vis->scheme, dir, prim[q], grad.data() + (4 * dir + q) * N);
+    or_amu(g, vis, T, amu.data());
+    auto met = [&](int m, long p) {       // akx..asz, Cartesian when metrics == NULL
+        return metrics ? metrics[m][p] : (m == 0 || m == 4 || m == 8 ? 1.0 : 0.0);
+    };
+    std::vector<double> Ev(4 * D.lap_size()), dv(N);
+    for (int dir = 0; dir < 3; ++dir) {
+        std::fill(Ev.begin(), Ev.end(), 0.0);
+#pragma omp parallel for collapse(2) schedule(static)
+        for (long k = 0; k < D.nz; ++k)
+            for (long j = 0; j < D.ny; ++j)
+                for (long i = 0; i < D.nx; ++i) {
+                    const long c = i + D.nx * (j + D.ny * k), p = D.lap(i, j, k);
+                    auto G = [&](int d, int q) { return grad[(4 * d + q) * N + c]; };
+                    const double Akx = met(0, p), Aky = met(1, p), Akz = met(2, p);
+                    const double Aix = met(3, p), Aiy = met(4, p), Aiz = met(5, p);
+                    const double Asx = met(6, p), Asy = met(7, p), Asz = met(8, p);
+                    const double ux = G(0, 0) * Akx + G(1, 0) * Aix + G(2, 0) * Asx;
+                    const double vx = G(0, 1) * Akx + G(1, 1) * Aix + G(2, 1) * Asx;
+                    const double wx = G(0, 2) * Akx + G(1, 2) * Aix + G(2, 2) * Asx;
+                    const double uy = G(0, 0) * Aky + G(1, 0) * Aiy + G(2, 0) * Asy;
+                    const double vy = G(0, 1) * Aky + G(1, 1) * Aiy + G(2, 1) * Asy;
+                    const double wy = G(0, 2) * Aky + G(1, 2) * Aiy + G(2, 2) * Asy;
+                    const double uz = G(0, 0) * Akz + G(1, 0) * Aiz + G(2, 0) * Asz;
+                    const double vz = G(0, 1) * Akz + G(1, 1) * Aiz + G(2, 1) * Asz;
+                    const double wz = G(0, 2) * Akz + G(1, 2) * Aiz + G(2, 2) * Asz;
+                    const double div = ux + vy + wz;
+                    const double Amu1 = amu[c];
+                    const double s11 = (2.0 * ux - 2.0 / 3.0 * div) * Amu1;
+                    const double s22 = (2.0 * vy - 2.0 / 3.0 * div) * Amu1;
+                    const double s33 = (2.0 * wz - 2.0 / 3.0 * div) * Amu1;
+                    const double s12 = (uy + vx) * Amu1;
+                    const double s13 = (uz + wx) * Amu1;
+                    const double s23 = (vz + wy) * Amu1;
+                    const double Amuk = amu[c] * vfc;
+                    const double Tx = G(0, 3) * Akx + G(1, 3) * Aix + G(2, 3) * Asx;
+                    const double Ty = G(0, 3) * Aky + G(1, 3) * Aiy + G(2, 3) * Asy;
+                    const double Tz = G(0, 3) * Akz + G(1, 3) * Aiz + G(2, 3) * Asz;
+                    const double E1 = u[p] * s11 + v[p] * s12 + w[p] * s13 + Amuk * Tx;
+                    const double E2 = u[p] * s12 + v[p] * s22 + w[p] * s23 + Amuk * Ty;
+                    const double E3 = u[p] * s13 + v[p] * s23 + w[p] * s33 + Amuk * Tz;
+                    const double Aj1 = ajac ? ajac[p] : 1.0;
+                    const double akx = met(3 * dir, p) * Aj1;
+                    const double aky = met(3 * dir + 1, p) * Aj1;
+                    const double akz = met(3 * dir + 2, p) * Aj1;
+                    const long L = D.lap_size();
+                    Ev[p] = (akx * s11 + aky * s12 + akz * s13);
+                    Ev[L + p] = (akx * s12 + aky * s22 + akz * s23);
+                    Ev[2 * L + p] = (akx * s13 + aky * s23 + akz * s33);
+                    Ev[3 * L + p] = (akx * E1 + aky * E2 + akz * E3);
+                }
+        for (int q = 0; q < 4; ++q) {
+            double* e = Ev.data() + q * D.lap_size();
+            or_ghost_fill(g, e);
+            d0_field(g, vis->scheme, dir, e, dv.data());
+#pragma omp parallel for collapse(2) schedule(static)
+            for (long k = 0; k < D.nz; ++k)
+                for (long j = 0; j < D.ny; ++j)
+                    for (long i = 0; i < D.nx; ++i) {
+                        const long c = i + D.nx * (j + D.ny * k);
+                        const double aj = ajac ? ajac[D.lap(i, j, k)] : 1.0;
+                        du[D.soa(i, j, k, q + 1)] += aj * dv[c];
+                    }
+        }
+    }
+}
+
 // Inviscid RHS (decomposed form of the BF3W operator), du overwritten.
 void or_du_invis(const or_grid* g, const double* d, const double* u,
                  const double* v, const double* w, const double* cc,
@@ -617,7 +750,8 @@ struct Work {
 };
 
 void rhs_from_cons(const or_grid* g, const double* f, Work& W,
-                   const double* const* metrics, const double* ajac) {
+                   const double* const* metrics, const double* ajac,
+                   const or_vis* vis = nullptr) {
     or_cons_to_prim(g, f, W.d.data(), W.u.data(), W.v.data(), W.w.data(),
                     W.T.data(), W.P.data());
     or_ghost_fill(g, W.d.data());
@@ -628,6 +762,9 @@ void rhs_from_cons(const or_grid* g, const double* f, Work& W,
     or_sound_speed(g, W.T.data(), W.cc.data());
     or_du_invis(g, W.d.data(), W.u.data(), W.v.data(), W.w.data(), W.cc.data(),
                 metrics, ajac, W.du.data());
+    if (vis)   // du_comput: inviscid, then viscous (OCFD_Stream.cpp:27-45)
+        or_du_vis(g, vis, W.u.data(), W.v.data(), W.w.data(), W.T.data(), metrics, ajac,
+                  W.du.data());
 }
 }  // namespace
 
@@ -640,21 +777,35 @@ int or_rhs_conserved(const or_grid* g, const double* f, double* du,
     return 0;
 }
 
+int or_rhs_conserved_ns(const or_grid* g, const or_vis* vis, const double* f, double* du,
+                        const double* const* metrics, const double* ajac) {
+    Dims D(g);
+    Work W(D);
+    rhs_from_cons(g, f, W, metrics, ajac, vis);
+    std::memcpy(du, W.du.data(), sizeof(double) * 5 * D.cells());
+    return 0;
+}
+
 // Solver loop OCFD_NS_Solver.cpp:64-90 with all three SSP-RK3 stages: the
 // state at the start of the step is kept in fn (the reference's pf/pfn swap).
-int or_rk3_steps(const or_grid* g, double* f, double dt, int nsteps,
-                 const double* const* metrics, const double* ajac) {
+int or_rk3_steps_ns(const or_grid* g, const or_vis* vis, double* f, double dt, int nsteps,
+                    const double* const* metrics, const double* ajac) {
     Dims D(g);
     Work W(D);
     const long n = 5 * D.cells();
     for (int s = 0; s < nsteps; ++s) {
         std::memcpy(W.fn.data(), f, sizeof(double) * n);
         for (int krk = 1; krk <= 3; ++krk) {
-            rhs_from_cons(g, f, W, metrics, ajac);
+            rhs_from_cons(g, f, W, metrics, ajac, vis);
             or_time_advance(krk, dt, n, f, W.fn.data(), W.du.data());
         }
     }
     return 0;
+}
+
+int or_rk3_steps(const or_grid* g, double* f, double dt, int nsteps,
+                 const double* const* metrics, const double* ajac) {
+    return or_rk3_steps_ns(g, nullptr, f, dt, nsteps, metrics, ajac);
 }
 
 // Algorithmic operation counts of one cell-RHS, from the same templates the

@@ -45,6 +45,15 @@ typedef struct or_grid {
     int face_kind[6];          /* x-, x+, y-, y+, z-, z+ : OR_FACE_*               */
 } or_grid;
 
+/* Viscous terms (du_vis_Jacobian3d, OCFD_Stream.cpp:229-345): Reynolds and
+ * Prandtl numbers, the Sutherland reference temperature Ref_T (Sutherland
+ * constant 110.4 K) and the central difference order (6: Scheme_vis_ID 203,
+ * 8: 204). */
+typedef struct or_vis {
+    double re, pr, ref_t;
+    int scheme;
+} or_vis;
+
 /* scalar kernels ------------------------------------------------------------ */
 double or_weno7_p(const double* s8);
 double or_weno7_m(const double* s8);
@@ -79,6 +88,18 @@ void   or_time_advance(int krk, double dt, long n, double* f, const double* fn,
 double or_compute_dt(const or_grid* g, const double* f, double cfl);
 /* nsteps SSP-RK3 steps of the Euler system, f (SoA) updated in place.
  * Returns 0, or -1 on allocation failure. */
+/* viscosity mu(T) on the interior (dense nx*ny*nz) */
+void   or_amu(const or_grid* g, const or_vis* vis, const double* T, double* amu);
+/* du (SoA) += viscous terms of momentum and energy (vars 1..4) from LAP
+ * u, v, w, T with filled ghosts; metrics as or_du_invis */
+void   or_du_vis(const or_grid* g, const or_vis* vis, const double* u, const double* v,
+                 const double* w, const double* T, const double* const* metrics,
+                 const double* ajac, double* du);
+/* Navier-Stokes forms of or_rhs_conserved / or_rk3_steps (vis may be NULL) */
+int    or_rhs_conserved_ns(const or_grid* g, const or_vis* vis, const double* f, double* du,
+                           const double* const* metrics, const double* ajac);
+int    or_rk3_steps_ns(const or_grid* g, const or_vis* vis, double* f, double dt, int nsteps,
+                       const double* const* metrics, const double* ajac);
 int    or_rk3_steps(const or_grid* g, double* f, double dt, int nsteps,
                     const double* const* metrics, const double* ajac);
 /* du from conserved state f: cons->prim, ghost fill, sound speed, RHS. */

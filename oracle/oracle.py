@@ -34,6 +34,18 @@ class OrGrid(C.Structure):
                 ("face_kind", C.c_int * 6)]
 
 
+class OrVis(C.Structure):
+    """Viscous constants: Re, Pr, Sutherland Ref_T, central-difference order 6 or 8."""
+    _fields_ = [("re", C.c_double), ("pr", C.c_double), ("ref_t", C.c_double),
+                ("scheme", C.c_int)]
+
+
+def make_vis(re=500.0, pr=0.72, ref_t=288.15, scheme=8) -> OrVis:
+    v = OrVis()
+    v.re, v.pr, v.ref_t, v.scheme = re, pr, ref_t, scheme
+    return v
+
+
 def make_grid(nx, ny, nz, hx=None, hy=None, hz=None, gamma=1.4, ama=1.0,
               epsl_sw=1e-6, face_kind=(0, 0, 0, 0, 0, 0)) -> OrGrid:
     """Grid spacing defaults to the reference's h = 1/(N-1) (OCFD_init.cpp:29-31)."""
@@ -159,6 +171,30 @@ class Oracle:
             raise MemoryError("oracle rk3 allocation failed")
         return out
 
+    def du_vis(self, g: OrGrid, vis: OrVis, u, v, w, T, metrics=None, ajac=None,
+               du=None) -> np.ndarray:
+        """du[1..4] += viscous terms (du zero when not given)."""
+        du = np.zeros((5, g.nz, g.ny, g.nx)) if du is None else du
+        self.lib.or_du_vis(C.byref(g), C.byref(vis), _p(u), _p(v), _p(w), _p(T),
+                           _ptr_array(metrics), _p(ajac), _p(du))
+        return du
+
+    def rhs_conserved_ns(self, g: OrGrid, vis: OrVis, f: np.ndarray, metrics=None,
+                         ajac=None) -> np.ndarray:
+        du = np.empty_like(f)
+        self.lib.or_rhs_conserved_ns(C.byref(g), C.byref(vis), _p(f), _p(du),
+                                     _ptr_array(metrics), _p(ajac))
+        return du
+
+    def rk3_steps_ns(self, g: OrGrid, vis: OrVis, f: np.ndarray, dt: float, nsteps: int,
+                     metrics=None, ajac=None) -> np.ndarray:
+        out = np.array(f, dtype=np.float64, order="C", copy=True)
+        rc = self.lib.or_rk3_steps_ns(C.byref(g), C.byref(vis), _p(out), C.c_double(dt),
+                                      nsteps, _ptr_array(metrics), _p(ajac))
+        if rc != 0:
+            raise MemoryError("oracle rk3 allocation failed")
+        return out
+
     def rhs_conserved(self, g: OrGrid, f: np.ndarray, metrics=None, ajac=None) -> np.ndarray:
         du = np.empty_like(f)
         self.lib.or_rhs_conserved(C.byref(g), _p(f), _p(du), _ptr_array(metrics), _p(ajac))
@@ -202,6 +238,8 @@ class RefFunctions:
         L.ref_time_advance.argtypes = [C.c_int, C.c_double] + [C.c_int] * 3 + [_dp] * 3
         L.ref_du_invis.argtypes = ([C.c_int] * 3 + [C.c_double] * 5 + [_dp] * 5 +
                                    [C.POINTER(_dp), _dp, _dp, C.POINTER(C.c_int)])
+        L.ref_du_vis.argtypes = ([C.c_int] * 3 + [C.c_double] * 8 + [C.c_int] + [_dp] * 4 +
+                                 [C.POINTER(_dp), _dp, _dp, C.POINTER(C.c_int)])
 
     def weno_p(self, s):
         s = np.ascontiguousarray(s, dtype=np.float64).reshape(-1, 8)
@@ -254,4 +292,12 @@ class RefFunctions:
         self.lib.ref_du_invis(g.nx, g.ny, g.nz, g.hx, g.hy, g.hz, g.gamma, g.epsl_sw,
                               _p(d), _p(u), _p(v), _p(w), _p(cc), _ptr_array(metrics),
                               _p(ajac), _p(du), kinds)
+        return du
+
+    def du_vis(self, g: OrGrid, vis: OrVis, u, v, w, T, metrics=None, ajac=None, du=None):
+        du = np.zeros((5, g.nz, g.ny, g.nx)) if du is None else du
+        kinds = (C.c_int * 6)(*[g.face_kind[i] for i in range(6)])
+        self.lib.ref_du_vis(g.nx, g.ny, g.nz, g.hx, g.hy, g.hz, g.gamma, g.ama, vis.re,
+                            vis.pr, vis.ref_t, vis.scheme, _p(u), _p(v), _p(w), _p(T),
+                            _ptr_array(metrics), _p(ajac), _p(du), kinds)
         return du

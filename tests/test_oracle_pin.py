@@ -125,3 +125,29 @@ def test_du_invis_closure_bitexact(oracle, reffn, faces):
     a = oracle.du_invis(g, d, u, v, w, cc)
     b = reffn.du_invis(g, d, u, v, w, cc)
     assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("scheme", [6, 8])
+@pytest.mark.parametrize("general", [False, True])
+@pytest.mark.parametrize("faces", [(0, 0, 0, 0, 0, 0), (1, 1, 0, 0, 1, 1)])
+def test_du_vis_bitexact(oracle, reffn, scheme, general, faces):
+    # viscous terms: CD6/CD8 gradients, Sutherland viscosity, viscous fluxes
+    # per direction and their divergence, added to du[1..4]
+    from oracle.oracle import make_vis
+    g = make_grid(14, 10, 9, face_kind=faces, ama=0.7)
+    vis = make_vis(re=300.0, pr=0.72, ref_t=250.0, scheme=scheme)
+    d, u, v, w, T = _prims(g, 20)
+    for a in (u, v, w, T):
+        oracle.ghost_fill(g, a)
+    metrics = ajac = None
+    if general:
+        rng = np.random.default_rng(21)
+        shp = d.shape
+        metrics = [np.ascontiguousarray(rng.uniform(0.5, 1.5, shp) if i % 4 == 0 else
+                                        rng.uniform(-0.3, 0.3, shp)) for i in range(9)]
+        ajac = rng.uniform(0.7, 1.3, shp)
+    base = np.random.default_rng(22).normal(size=(5, g.nz, g.ny, g.nx))
+    a = oracle.du_vis(g, vis, u, v, w, T, metrics, ajac, base.copy())
+    b = reffn.du_vis(g, vis, u, v, w, T, metrics, ajac, base.copy())
+    assert np.array_equal(a, b)
+    assert np.array_equal(a[0], base[0])        # no viscous mass term

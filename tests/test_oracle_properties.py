@@ -100,3 +100,34 @@ def test_closure_faces_preserve_free_stream(oracle):
     cc = oracle.sound_speed(g, T)
     du = oracle.du_invis(g, d, u, v, w, cc)
     assert np.abs(du).max() <= 1e-11
+
+
+def test_viscous_shear_wave_matches_analytic(oracle):
+    # u = U sin(2 pi y), T = 1 (mu = 1/Re), periodic: the viscous x-momentum
+    # term is mu u'' and the energy term d/dy(mu u u') (constant-density shear
+    # wave); CD8 applied twice is accurate to ~1e-5 here
+    from oracle.oracle import make_grid as mg, make_vis
+    nx, ny, nz = 8, 48, 8
+    g = mg(nx, ny, nz, hx=1.0 / nx, hy=1.0 / ny, hz=1.0 / nz)
+    vis = make_vis(re=100.0, pr=0.72, ref_t=288.15, scheme=8)
+    shp = (nz + 8, ny + 8, nx + 8)
+    y = (np.arange(ny + 8) - 4) / ny
+    U = 0.3
+    u = np.broadcast_to((U * np.sin(2 * np.pi * y))[None, :, None], shp).copy()
+    v, w, T = np.zeros(shp), np.zeros(shp), np.ones(shp)
+    du = oracle.du_vis(g, vis, u, v, w, T)
+    yi = np.arange(ny) / ny
+    k = 2 * np.pi
+    mx = -(1 / vis.re) * U * k * k * np.sin(k * yi)
+    en = (1 / vis.re) * U * U * k * k * (np.cos(k * yi) ** 2 - np.sin(k * yi) ** 2)
+    assert np.abs(du[1] - mx[None, :, None]).max() <= 1e-4 * np.abs(mx).max()
+    assert np.abs(du[4] - en[None, :, None]).max() <= 1e-4 * np.abs(en).max()
+    assert np.abs(du[0]).max() == 0 and np.abs(du[2]).max() == 0 and np.abs(du[3]).max() == 0
+
+
+def test_viscous_uniform_flow_is_free(oracle):
+    from oracle.oracle import make_grid as mg, make_vis
+    g = mg(10, 9, 8, face_kind=(1, 1, 0, 0, 1, 1))
+    shp = (16, 17, 18)
+    du = oracle.du_vis(g, make_vis(scheme=6), *(np.full(shp, x) for x in (0.4, -0.2, 0.1, 1.3)))
+    assert np.abs(du).max() == 0

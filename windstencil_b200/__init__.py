@@ -19,13 +19,14 @@ from __future__ import annotations
 import ctypes as C
 from dataclasses import dataclass, field
 
-from ._abi import (FACE_CLOSURE, FACE_EXTRAP, FACE_PERIODIC, FP64, LAP, MIXED, WsDim3, WsError, WsField,
-                   WsGrid, WsJob, WsMetrics, WsSoa, WsTile, check, header_symbols, last_error,
-                   load)
+from ._abi import (FACE_CLOSURE, FACE_EXTRAP, FACE_PERIODIC, FP64, LAP, MIXED, WsDim3, WsError,
+                   WsField, WsGrid, WsJob, WsMetrics, WsSoa, WsTile, WsViscous, check,
+                   header_symbols, last_error, load)
 
 __all__ = [
     "FACE_CLOSURE", "FACE_EXTRAP", "FACE_PERIODIC", "FP64", "MIXED", "LAP", "WsError", "Grid", "make_grid",
     "lap_tensor", "soa_tensor", "field_desc", "soa_desc", "interior_job", "du_invis_jacobian3d",
+    "du_vis_jacobian3d", "viscous",
     "du_invis_jacobian3d_init", "ghost_fill", "cons_to_prim", "prim_to_cons", "time_advance",
     "Solver", "load", "header_symbols", "last_error",
 ]
@@ -128,6 +129,35 @@ def _metrics(m):
         return C.byref(m)
     mm = WsMetrics(*[field_desc(t) for t in m])   # 10 tensors: akx..asz, ajac
     return C.byref(mm)
+
+
+def viscous(re=500.0, pr=0.72, ref_t=288.15, scheme=8) -> WsViscous:
+    """ws_viscous: Reynolds and Prandtl numbers, Sutherland Ref_T, CD order 6 or 8."""
+    return WsViscous(re, pr, ref_t, scheme, 0)
+
+
+def du_vis_jacobian3d(g: Grid, vis, u, v, w, T, du, metrics=None, workspace=None,
+                      stream=None) -> None:
+    """du[1..4] += viscous terms (ws_du_vis_jacobian3d); the workspace is a
+    device tensor of at least ws_du_vis_workspace_bytes(g) bytes (allocated
+    here when not given)."""
+    torch = _torch()
+    gc = g.c()
+    lib = load()
+    need = int(lib.ws_du_vis_workspace_bytes(C.byref(gc)))
+    if workspace is None:
+        workspace = torch.empty(need // 8 + 2, dtype=torch.float64, device=du.device)
+    vp = vis if isinstance(vis, WsViscous) else viscous(**vis)
+    mp = None
+    if metrics is not None:
+        mm = metrics if isinstance(metrics, WsMetrics) else WsMetrics(
+            *[field_desc(t) for t in metrics])
+        mp = C.byref(mm)
+    fs = [field_desc(t) for t in (u, v, w, T)]
+    check(lib.ws_du_vis_jacobian3d(C.byref(gc), C.byref(vp), *fs, mp, soa_desc(du),
+                                   C.c_void_p(workspace.data_ptr()),
+                                   workspace.numel() * workspace.element_size(),
+                                   _stream(stream)))
 
 
 def du_invis_jacobian3d_init(g: Grid, job: WsJob, T, cc, stream=None) -> None:
@@ -246,6 +276,15 @@ class Solver:
 
     def set_tile(self, tile):
         check(load().ws_solver_set_tile(self.h, WsTile(*tile)))
+
+    def set_viscous(self, vis):
+        """Navier-Stokes with ws_viscous constants (a WsViscous, a dict with
+        re, pr, ref_t, scheme, or None for Euler)."""
+        if vis is None:
+            check(load().ws_solver_set_viscous(self.h, None))
+            return
+        v = vis if isinstance(vis, WsViscous) else viscous(**vis)
+        check(load().ws_solver_set_viscous(self.h, C.byref(v)))
 
 
 class Batch:

@@ -54,6 +54,11 @@ class WsMetrics(C.Structure):
                 ("akx", "aky", "akz", "aix", "aiy", "aiz", "asx", "asy", "asz", "ajac")]
 
 
+class WsViscous(C.Structure):
+    _fields_ = [("re", C.c_double), ("pr", C.c_double), ("ref_t", C.c_double),
+                ("scheme", C.c_int32), ("dummy0", C.c_int32)]
+
+
 class WsTile(C.Structure):
     _fields_ = [("tile_x", C.c_int32), ("tile_y", C.c_int32), ("scan_z", C.c_int32),
                 ("threads", C.c_int32)]
@@ -108,6 +113,10 @@ SIGNATURES = {
     "ws_solver_step": (_I, [_P, C.c_double, _I, _P]),
     "ws_solver_status": (_I, [_P, C.POINTER(_I), _P]),
     "ws_solver_set_tile": (_I, [_P, WsTile]),
+    "ws_solver_set_viscous": (_I, [_P, C.POINTER(WsViscous)]),
+    "ws_du_vis_workspace_bytes": (C.c_size_t, [C.POINTER(WsGrid)]),
+    "ws_du_vis_jacobian3d": (_I, [C.POINTER(WsGrid), C.POINTER(WsViscous)] + [WsField] * 4 +
+                             [C.POINTER(WsMetrics), WsSoa, _P, C.c_size_t, _P]),
     "ws_batch_create": (_I, [C.POINTER(WsGrid), _I, C.POINTER(_P)]),
     "ws_batch_destroy": (None, [_P]),
     "ws_batch_size": (_I, [_P]),

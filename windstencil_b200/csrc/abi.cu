@@ -242,7 +242,7 @@ int rhs_enqueue(const ws_grid* g, ws_job job, const ws_field prims[5], const ws_
 // new primitives p_out.
 int rhs_stage_enqueue(const ws_grid* g, const ws_field p_in[6], ws_soa f_in, ws_soa fn,
                       ws_soa f_out, const ws_field p_out[6], double dt, int krk, int* status,
-                      ws_tile tile, cudaStream_t st) {
+                      ws_soa dvis, ws_tile tile, cudaStream_t st) {
     int cfg = 0;
     int rc = tile_index(g, tile, &cfg);
     if (rc) return rc;
@@ -251,6 +251,12 @@ int rhs_stage_enqueue(const ws_grid* g, const ws_field p_in[6], ws_soa f_in, ws_
     const ws_field p5[5] = {p_in[0], p_in[1], p_in[2], p_in[3], p_in[5]};
     RhsArgs a = make_rhs_args(g, job, p5, nullptr, ws_soa{}, cfg, scan);
     if ((rc = set_rhs_stage(a, g, f_in, fn, f_out, p_out, dt, status))) return rc;
+    if (dvis.ptr) {
+        if (dvis.pitch != fn.pitch || dvis.length_Y != fn.length_Y ||
+            dvis.length_Z != fn.length_Z)
+            return fail(WS_ERR_INVALID, "stage epilogue: viscous terms need the state's shape");
+        a.dvis = dvis;
+    }
     const int ctas = rhs_ctas(g, a, cfg, true);
     if (ctas <= 0) return fail(WS_ERR_CUDA, "cannot size the persistent grid");
     return launch_rhs(a, g->precision, true, cfg, ctas, krk, st);
@@ -283,6 +289,34 @@ int ws_du_invis_jacobian3d_init(const ws_grid* g, ws_job job, ws_field T, ws_fie
     if ((rc = check_field(g, T, "T")) || (rc = check_field(g, cc, "cc"))) return rc;
     if (job_empty(job)) return WS_OK;
     return launch_sound_speed(g, job, T, cc, (cudaStream_t)stream);
+}
+
+size_t ws_du_vis_workspace_bytes(const ws_grid* g) {
+    return g ? vis_workspace_bytes(g) : 0;
+}
+
+int ws_du_vis_jacobian3d(const ws_grid* g, const ws_viscous* vis, ws_field u, ws_field v,
+                         ws_field w, ws_field T, const ws_metrics* metrics, ws_soa du,
+                         void* workspace, size_t workspace_bytes, ws_stream_t stream) {
+    int rc;
+    if ((rc = check_grid(g)) || (rc = check_viscous(vis))) return rc;
+    if ((rc = check_field(g, u, "u")) || (rc = check_field(g, v, "v")) ||
+        (rc = check_field(g, w, "w")) || (rc = check_field(g, T, "T")))
+        return rc;
+    if (!g->metrics_uniform) {
+        if (!metrics) return fail(WS_ERR_INVALID, "metrics are NULL for a non-uniform grid");
+        const ws_field* mf = &metrics->akx;
+        for (int i = 0; i < 10; ++i)
+            if ((rc = check_field(g, mf[i], "metric"))) return rc;
+    }
+    if ((rc = check_soa(du, g->nx, g->ny, g->nz, "du"))) return rc;
+    if (!workspace || workspace_bytes < vis_workspace_bytes(g))
+        return fail(WS_ERR_INVALID, "viscous workspace missing or smaller than "
+                                    "ws_du_vis_workspace_bytes()");
+    if (reinterpret_cast<uintptr_t>(workspace) & 15)
+        return fail(WS_ERR_INVALID, "viscous workspace must be 16-byte aligned");
+    const ws_field p4[4] = {u, v, w, T};
+    return launch_du_vis(g, vis, p4, metrics, du, workspace, true, (cudaStream_t)stream);
 }
 
 int ws_du_invis_jacobian3d_tiled(const ws_grid* g, ws_job job, ws_field d, ws_field u,

@@ -517,7 +517,9 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
                     r = fma(py[BX] - py[0], a.rhy, r);
                     r = fma(fz[cur * 5 * BXY + i] - fz[prev * 5 * BXY + i], a.rhz, r);
                     const double fo = krk == 1 ? 0.0 : fbz[5 * BXY + i];
-                    q[var] = ws_rk_stage(krk, fbz[i], fo, -r, a.dt);
+                    // Navier-Stokes: the viscous terms of this cell (same SoA shape)
+                    const double dv = a.dvis.ptr ? __ldg(a.dvis.ptr + cell + var * fvs) : 0.0;
+                    q[var] = ws_rk_stage(krk, fbz[i], fo, dv - r, a.dt);
                     a.f_out.ptr[cell + var * fvs] = q[var];
                 }
                 store_prims(a, q, dX, dY, z);

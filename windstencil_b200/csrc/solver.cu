@@ -1,4 +1,5 @@
-// solver.cu -- one grid, device-resident state, SSP-RK3 steps from CUDA graphs.
+// solver.cu -- one grid, device-resident state, SSP-RK3 steps from CUDA graphs
+// (Euler, or Navier-Stokes with ws_solver_set_viscous).
 //
 // Replaces the reference's time loop (src/solver/OCFD_NS_Solver.cpp:64-90)
 // for the Euler system.  The reference's pf/pfn pointer swap becomes two
@@ -28,6 +29,10 @@ struct ws_solver {
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     double graph_dt = 0.0;
     ws_tile tile{0, 0, 0, 0};
+    // Navier-Stokes: viscous constants and the workspace of their fluxes
+    bool viscous = false;
+    ws_viscous vis{};
+    void* vis_ws = nullptr;
 };
 
 namespace {
@@ -39,7 +44,7 @@ void drop_graphs(ws_solver* s) {
         }
 }
 
-// du of the current state (ghost fill + RHS)
+// du of the current state (ghost fill + RHS, + viscous terms)
 int enqueue_rhs(ws_solver* s, cudaStream_t st) {
     GridState& g = s->s;
     int rc = launch_ghost_fill_prims(&g.g, g.prims(), st);
@@ -47,7 +52,10 @@ int enqueue_rhs(ws_solver* s, cudaStream_t st) {
     ws_job job{{4, 4, 4}, {g.g.nx + 4, g.g.ny + 4, g.g.nz + 4}};
     const ws_field* p = g.prims();
     const ws_field p5[5] = {p[0], p[1], p[2], p[3], p[5]};
-    return rhs_enqueue(&g.g, job, p5, nullptr, g.du, s->tile, st);
+    rc = rhs_enqueue(&g.g, job, p5, nullptr, g.du, s->tile, st);
+    if (rc || !s->viscous) return rc;
+    const ws_field p4[4] = {p[1], p[2], p[3], p[4]};
+    return launch_du_vis(&g.g, &s->vis, p4, nullptr, g.du, s->vis_ws, true, st);
 }
 
 // one SSP-RK3 step from state buffer c into 1-c; primitives pr[c] -> pr[1-c]
@@ -59,8 +67,15 @@ int enqueue_step(ws_solver* s, int c, double dt, cudaStream_t st) {
         const ws_field* pout = g.pr[krk == 2 ? c : 1 - c];
         int rc = launch_ghost_fill_prims(&g.g, pin, st);
         if (rc) return rc;
+        ws_soa dvis{};
+        if (s->viscous) {   // viscous terms of the stage's input into du
+            const ws_field p4[4] = {pin[1], pin[2], pin[3], pin[4]};
+            rc = launch_du_vis(&g.g, &s->vis, p4, nullptr, g.du, s->vis_ws, false, st);
+            if (rc) return rc;
+            dvis = g.du;
+        }
         rc = rhs_stage_enqueue(&g.g, pin, g.f[1 - c], g.f[c], g.f[1 - c], pout, dt, krk,
-                               g.status, s->tile, st);
+                               g.status, dvis, s->tile, st);
         if (rc) return rc;
     }
     return WS_OK;
@@ -119,6 +134,7 @@ void ws_solver_destroy(ws_solver* s) {
     drop_graphs(s);
     if (s->cap) cudaStreamDestroy(s->cap);
     cudaFree(s->scratch);
+    cudaFree(s->vis_ws);
     grid_state_free(s->s, nullptr);
     cudaStreamSynchronize(nullptr);
     delete s;
@@ -130,6 +146,24 @@ int ws_solver_set_tile(ws_solver* s, ws_tile tile) {
         find_tile_cfg(tile.tile_x, tile.tile_y, tile.threads) < 0)
         return fail(WS_ERR_UNSUPPORTED, "tile shape not compiled in this build");
     s->tile = tile;
+    drop_graphs(s);
+    return WS_OK;
+}
+
+int ws_solver_set_viscous(ws_solver* s, const ws_viscous* vis) {
+    if (!s) return fail(WS_ERR_INVALID, "solver is NULL");
+    if (!vis) {
+        s->viscous = false;
+        drop_graphs(s);
+        return WS_OK;
+    }
+    if (int rc = check_viscous(vis)) return rc;
+    if (!s->vis_ws) {
+        WS_CUDA(cudaMalloc(&s->vis_ws, vis_workspace_bytes(&s->s.g)));
+        WS_CUDA(cudaMemset(s->vis_ws, 0, vis_workspace_bytes(&s->s.g)));
+    }
+    s->vis = *vis;
+    s->viscous = true;
     drop_graphs(s);
     return WS_OK;
 }

@@ -49,6 +49,9 @@ struct RhsArgs {
     uint32_t p_pitch;
     double dt, rcv, rama;      // dt, 1/cv, 1/Ama
     int* status;
+    // viscous terms of the stage (ptr NULL: none): du[0..4] added to the
+    // inviscid RHS before the update; same SoA shape as fn
+    ws_soa dvis;
     // TMA staging (tma != 0): per primitive, a map of its LAP array with the
     // (BX+8) x (BY+8) box of a plane and one with the BX x BY centre box.
     // Set only when every box start is 16-byte aligned (even job start x,
@@ -66,9 +69,18 @@ int rhs_ctas(const ws_grid* g, const RhsArgs& a, int cfg, bool stage);
 // One fused RHS + SSP-RK3 stage krk over the whole interior (Cartesian):
 // reads primitives p_in (ghosts filled), f_in and fn; writes f_out and the
 // new primitives p_out.
+// dvis.ptr may be NULL (no viscous terms).
 int rhs_stage_enqueue(const ws_grid* g, const ws_field p_in[6], ws_soa f_in, ws_soa fn,
                       ws_soa f_out, const ws_field p_out[6], double dt, int krk, int* status,
-                      ws_tile tile, cudaStream_t st);
+                      ws_soa dvis, ws_tile tile, cudaStream_t st);
+
+// Viscous terms (viscous.cu): workspace size, parameter check, and du[1..4]
+// += (accumulate) or = the viscous terms (du[0] = 0 when storing) from the
+// LAP fields u, v, w, T (ghosts filled).
+size_t vis_workspace_bytes(const ws_grid* g);
+int check_viscous(const ws_viscous* vis);
+int launch_du_vis(const ws_grid* g, const ws_viscous* vis, const ws_field prims[4],
+                  const ws_metrics* m, ws_soa du, void* ws, bool accumulate, cudaStream_t st);
 
 // Tile configurations compiled into the library.
 struct TileCfg {
