@@ -28,6 +28,8 @@ from a CUDA graph.
                  100 steps (rel. L2 / L-inf per conserved field)
   grid_480x512x64  the second size of the FP64 workload: RHS kernel alone
                  (both forms) and whole SSP-RK3 steps
+  navier_stokes  the headline grid with the viscous terms added (CD8,
+                 Re 1000): whole SSP-RK3 steps and the viscous terms alone
   batched        256 uneven periodic grids, 50 SSP-RK3 steps, FP64 and mixed,
                  against one-grid-at-a-time FP64 solves of the same grids
   served         Poisson arrivals of solve requests into the continuous-
@@ -71,6 +73,7 @@ def parse():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-second", action="store_true")
+    ap.add_argument("--no-ns", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--batch-grids", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=50)
@@ -317,6 +320,58 @@ def bench_second_grid(a, torch, ws, wl, stream, peak64):
     return res
 
 
+def bench_navier_stokes(a, torch, ws, wl, stream):
+    """Navier-Stokes (inviscid + viscous terms, CD8, Re 1000) on the headline
+    grid: whole SSP-RK3 steps, and the viscous terms alone through the
+    drop-in entry point."""
+    nx, ny, nz = a.nx, a.ny, a.nz
+    cells = nx * ny * nz
+    vis = dict(re=1000.0, pr=0.72, ref_t=288.15, scheme=8)
+    faces = (ws.FACE_EXTRAP, ws.FACE_EXTRAP, 0, 0, 0, 0)
+    g = ws.Grid(nx, ny, nz, faces=faces)
+    f0 = wl.sod_state(nx, ny, nz, seed=2)
+    s = ws.Solver(g)
+    s.set_viscous(vis)
+    s.set_state(f0, stream=stream)
+    dt = s.compute_dt(0.5, stream=stream)
+    s.step(dt, 3, stream=stream)
+    e0, e1 = _events(torch)
+    e0.record(stream)
+    s.step(dt, 20, stream=stream)
+    e1.record(stream)
+    e1.synchronize()
+    sms = e0.elapsed_time(e1) / 20
+    status = s.status(stream=stream)
+    # viscous terms alone (drop-in, caller workspace) on the current state
+    _, du, prims = s.fields()
+    import ctypes as C
+    lib = ws.load()
+    gc = g.c()
+    need = int(lib.ws_du_vis_workspace_bytes(C.byref(gc)))
+    work = torch.empty(need // 8 + 2, dtype=torch.float64, device="cuda")
+    vp = ws.viscous(**vis)
+    call = lambda: ws._abi.check(lib.ws_du_vis_jacobian3d(   # noqa: E731
+        C.byref(gc), C.byref(vp), prims[1], prims[2], prims[3], prims[4], None, du,
+        C.c_void_p(work.data_ptr()), need + 16, stream.cuda_stream))
+    call()
+    e0.record(stream)
+    for _ in range(10):
+        call()
+    e1.record(stream)
+    e1.synchronize()
+    vms = e0.elapsed_time(e1) / 10
+    s.close()
+    return {"workload": f"{nx}x{ny}x{nz} Sod, Navier-Stokes (Re 1000, Pr 0.72, Sutherland "
+                        "Ref_T 288.15, CD8 viscous derivatives), SSP-RK3 CFL 0.5",
+            "value": cells * 3 / (sms * 1e-3) / 1e9, "unit": "Gcell-RHS/s", "step_ms": sms,
+            "viscous_terms_ms": vms,
+            "viscous_hbm_gbs_lower_bound": 224.0 * cells / (vms * 1e-3) / 1e9,
+            "note": "viscous_terms_ms: gradients + fluxes pass, flux ghost fill, divergence "
+                    "pass through ws_du_vis_jacobian3d; ~224 B/cell of compulsory traffic "
+                    "(4 primitives in, 12 fluxes out and in, du[1..4] read and written)",
+            "device_status": status}
+
+
 def bench_batch(a, torch, ws, wl, stream):
     specs = wl.batch_specs(a.batch_grids, seed=4)
     cells = sum(s.cells for s in specs)
@@ -536,6 +591,8 @@ def run_ours(a, rank, world, dist):
             extra["mixed"] = bench_mixed(a, torch, ws, wl, stream)
         if not a.no_second:
             extra["grid_480x512x64"] = bench_second_grid(a, torch, ws, wl, stream, peak)
+        if not a.no_ns:
+            extra["navier_stokes"] = bench_navier_stokes(a, torch, ws, wl, stream)
         serial = None
         if not a.no_batch:
             extra["batched"], serial = bench_batch(a, torch, ws, wl, stream)
