@@ -69,7 +69,7 @@ struct RhsLayout {
     static constexpr int N_FX = 5 * BY * (BX + 1);
     static constexpr int N_FY = 5 * (BY + 1) * BX;
     static constexpr int N_FZ = 2 * 5 * BXY;
-    static constexpr int N_FB = EPI ? 2 * 10 * BXY : 0;   // fn, f of a plane, x2
+    static constexpr int N_FB = EPI ? 2 * 15 * BXY : 0;   // fn, f, viscous terms, x2
     static constexpr int N_RING = RING * RS;      // CT
     static constexpr int N_SX = 10 * BY * SXW;    // CT
     static constexpr int N_SY = 10 * SYH * BX;    // CT
@@ -275,9 +275,10 @@ __device__ __forceinline__ void report_stage_timeout(const RhsArgs& a) {
     else atomicOr(&g_rhs_stage_timeout, 1);
 }
 
-// stage mode: cp.async fn (and, after stage 1, f) of one cell into
-// fb[v][col]; `cell` is the SoA offset of the cell's variable 0 and vs the
-// variable stride (f_in and fn share one SoA shape)
+// stage mode: cp.async fn (and, after stage 1, f; with viscous terms,
+// those) of one cell into fb[v][col] (fn 0..4, f 5..9, viscous 10..14);
+// `cell` is the SoA offset of the cell's variable 0 and vs the variable
+// stride (f_in, fn and the viscous terms share one SoA shape)
 __device__ __forceinline__ void issue_fcell(const RhsArgs& a, double* fb, int bxy, int col,
                                             size_t cell, size_t vs, int krk) {
 #pragma unroll
@@ -286,6 +287,11 @@ __device__ __forceinline__ void issue_fcell(const RhsArgs& a, double* fb, int bx
 #pragma unroll
         for (int v = 0; v < 5; ++v)
             cp_async8(fb + (5 + v) * bxy + col, a.f_in.ptr + cell + v * vs);
+    }
+    if (a.dvis.ptr) {
+#pragma unroll
+        for (int v = 0; v < 5; ++v)
+            cp_async8(fb + (10 + v) * bxy + col, a.dvis.ptr + cell + v * vs);
     }
 }
 
@@ -317,7 +323,7 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
     double* fx = stg + L::N_STG;                         // [5][BY][BX+1]
     double* fy = fx + L::N_FX;                           // [5][BY+1][BX]
     double* fz = fy + L::N_FY;                           // [2][5][BXY]
-    double* fb = fz + L::N_FZ;                           // [2][10][BXY]   (stage mode)
+    double* fb = fz + L::N_FZ;                           // [2][15][BXY]   (stage mode)
     CT* ring = reinterpret_cast<CT*>(fb + L::N_FB);      // [9][10][BXY]
     CT* sxs = ring + L::N_RING;                          // [10][BY][SXW]
     CT* sys = sxs + L::N_SX;                             // [10][SYH][BX]
@@ -504,7 +510,7 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
         // ---- face difference of plane z (FP64): du, or the RK stage
         if (EPI) {
             if (dcell) {
-                const double* fbz = fb + b * 10 * BXY;
+                const double* fbz = fb + b * 15 * BXY;
                 const size_t cell = fc0 + (size_t)z * fps;
                 const int xx = dcol % BX, yy = dcol / BX;
                 double q[5];
@@ -517,14 +523,14 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
                     r = fma(py[BX] - py[0], a.rhy, r);
                     r = fma(fz[cur * 5 * BXY + i] - fz[prev * 5 * BXY + i], a.rhz, r);
                     const double fo = krk == 1 ? 0.0 : fbz[5 * BXY + i];
-                    // Navier-Stokes: the viscous terms of this cell (same SoA shape)
-                    const double dv = a.dvis.ptr ? __ldg(a.dvis.ptr + cell + var * fvs) : 0.0;
+                    // Navier-Stokes: the viscous terms of this cell (staged with f, fn)
+                    const double dv = a.dvis.ptr ? fbz[10 * BXY + i] : 0.0;
                     q[var] = ws_rk_stage(krk, fbz[i], fo, dv - r, a.dt);
                     a.f_out.ptr[cell + var * fvs] = q[var];
                 }
                 store_prims(a, q, dX, dY, z);
                 if (more) {   // own cell of the next plane; fb[b^1] was last read by this thread
-                    issue_fcell(a, fb + (b ^ 1) * 10 * BXY, BXY, dcol, cell + fps, fvs, krk);
+                    issue_fcell(a, fb + (b ^ 1) * 15 * BXY, BXY, dcol, cell + fps, fvs, krk);
                     cp_async_commit();
                 }
             }

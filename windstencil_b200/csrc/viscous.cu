@@ -55,14 +55,18 @@ __device__ __forceinline__ double cdiff(const double* f, uint32_t pitch, int ny,
             3.0 * (__ldg(c + 4 * s) - __ldg(c - 4 * s))) / 840.0;
 }
 
+// Blocks of 32 x 8 threads cover 32 x 8 cells of one plane, so the x and y
+// neighbours of a stencil are mostly read by the same block (L1); the grid
+// strides over the (x tile, y tile, plane) space.
 template <int R>
 __global__ void __launch_bounds__(256) vis_flux_kernel(const __grid_constant__ VisArgs a) {
-    const long n = (long)a.nx * a.ny * a.nz;
-    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n;
-         t += (long)gridDim.x * blockDim.x) {
-        const int i = (int)(t % a.nx);
-        const long r = t / a.nx;
-        const int j = (int)(r % a.ny), k = (int)(r / a.ny);
+    const int tx = (a.nx + 31) / 32, ty = (a.ny + 7) / 8;
+    const long ntile = (long)tx * ty * a.nz;
+    for (long b = blockIdx.x; b < ntile; b += gridDim.x) {
+        const int i = (int)(b % tx) * 32 + threadIdx.x % 32;
+        const long r = b / tx;
+        const int j = (int)(r % ty) * 8 + threadIdx.x / 32, k = (int)(r / ty);
+        if (i >= a.nx || j >= a.ny) continue;
         const int X = i + 4, Y = j + 4, Z = k + 4;
         // derivatives along the computational directions: g[q][dir]
         double g[4][3];
@@ -119,12 +123,13 @@ __global__ void __launch_bounds__(256) vis_flux_kernel(const __grid_constant__ V
 
 template <int R>
 __global__ void __launch_bounds__(256) vis_div_kernel(const __grid_constant__ VisArgs a) {
-    const long n = (long)a.nx * a.ny * a.nz;
-    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n;
-         t += (long)gridDim.x * blockDim.x) {
-        const int i = (int)(t % a.nx);
-        const long r = t / a.nx;
-        const int j = (int)(r % a.ny), k = (int)(r / a.ny);
+    const int tx = (a.nx + 31) / 32, ty = (a.ny + 7) / 8;
+    const long ntile = (long)tx * ty * a.nz;
+    for (long b = blockIdx.x; b < ntile; b += gridDim.x) {
+        const int i = (int)(b % tx) * 32 + threadIdx.x % 32;
+        const long r = b / tx;
+        const int j = (int)(r % ty) * 8 + threadIdx.x / 32, k = (int)(r / ty);
+        if (i >= a.nx || j >= a.ny) continue;
         const int X = i + 4, Y = j + 4, Z = k + 4;
         const double aj = a.uniform ? 1.0 : __ldg(a.met[9] + lapi(X, Y, Z, a.mpitch[9], a.ny));
 #pragma unroll
@@ -143,10 +148,9 @@ __global__ void __launch_bounds__(256) vis_div_kernel(const __grid_constant__ Vi
     }
 }
 
-int grid_for(long n) {
-    long b = (n + 255) / 256;
-    const long cap = 148L * 8;
-    return (int)std::max(1L, std::min(b, cap));
+int grid_for(const ws_grid* g) {
+    const long tiles = (long)((g->nx + 31) / 32) * ((g->ny + 7) / 8) * g->nz;
+    return (int)std::max(1L, std::min(tiles, 148L * 8));
 }
 
 }  // namespace
@@ -189,7 +193,7 @@ int launch_du_vis(const ws_grid* g, const ws_viscous* vis, const ws_field prims[
     a.amu_c0 = 1.0 / vis->re * (1.0 + 110.4 / vis->ref_t);
     a.vfc = Cp / vis->pr;
     a.accumulate = accumulate ? 1 : 0;
-    const int blocks = grid_for((long)g->nx * g->ny * g->nz);
+    const int blocks = grid_for(g);
     if (vis->scheme == 6) vis_flux_kernel<3><<<blocks, 256, 0, st>>>(a);
     else vis_flux_kernel<4><<<blocks, 256, 0, st>>>(a);
     WS_CUDA(cudaGetLastError());
