@@ -90,7 +90,8 @@ enum ws_status {
     WS_ERR_TIMEOUT = 6,     /* a bounded device wait gave up                 */
     WS_ERR_BUDGET = 7,      /* admission would exceed the HBM budget         */
     WS_ERR_BUSY = 8,        /* object in use / queue full                    */
-    WS_ERR_NOT_FOUND = 9    /* unknown request id                            */
+    WS_ERR_NOT_FOUND = 9,   /* unknown request id                            */
+    WS_ERR_IO = 10          /* file missing, short or not in the expected format */
 };
 
 /* Grid and physics constants.  Replaces the reference's __constant__ set
@@ -192,6 +193,25 @@ WS_API int ws_du_vis_jacobian3d(const ws_grid* g, const ws_viscous* vis, ws_fiel
                                 ws_field w, ws_field T, const ws_metrics* metrics, ws_soa du,
                                 void* workspace, size_t workspace_bytes, ws_stream_t stream);
 
+/* ------------------------------------------------------------------------ */
+/* The reference's on-disk formats (one domain, little-endian, Fortran-style  */
+/* records: int32 length | data | int32 length; each 3D field is nz plane     */
+/* records of nx*ny float64, x fastest).                                     */
+/* ------------------------------------------------------------------------ */
+/* Restart file OCFD%08d.dat (OCFD_save / read_file, src/io/OCFD_IO.c:24-226):
+ * header record (int32 Istep, float64 tt), then d, u, v, w, T.
+ * prims: host [5][nz][ny][nx] in that order. */
+WS_API int ws_restart_write(const char* path, int nx, int ny, int nz, int32_t istep, double tt,
+                            const double* prims);
+WS_API int ws_restart_read(const char* path, int nx, int ny, int nz, int32_t* istep, double* tt,
+                           double* prims);
+/* Metrics file OCFD3d-Jacobi.dat (OCFD_Comput_Jacobian3d.cpp:120-211): no
+ * header; x, y, z, akx, aky, akz, aix, aiy, aiz, asx, asy, asz, ajac.
+ * fields: host [13][nz][ny][nx] in that order (interiors; ghosts are filled
+ * afterwards, e.g. with ws_ghost_fill). */
+WS_API int ws_metrics_write(const char* path, int nx, int ny, int nz, const double* fields);
+WS_API int ws_metrics_read(const char* path, int nx, int ny, int nz, double* fields);
+
 /* In-place ghost fill (4 layers) of nfields LAP fields by g->face_kind.
  * Replaces exchange_boundary_xyz_packed_dev (OCFD_mpi_dev.cpp:123-290) on one
  * GPU: no host staging, no MPI. */
@@ -260,6 +280,13 @@ WS_API int  ws_solver_step(ws_solver* s, double dt, int nsteps, ws_stream_t stre
 /* Device status word (0 or WS_ERR_NONFINITE); synchronises `stream`. */
 WS_API int  ws_solver_status(ws_solver* s, int* status, ws_stream_t stream);
 WS_API int  ws_solver_set_tile(ws_solver* s, ws_tile tile);
+/* Current state to / from a restart file (d, u, v, w, T from / to the
+ * conserved state with the formulas of cons_to_pri_kernel / pri_to_cons_kernel,
+ * commen_kernel.cpp:33-110); synchronise `stream`. */
+WS_API int  ws_solver_save(ws_solver* s, const char* path, int32_t istep, double tt,
+                           ws_stream_t stream);
+WS_API int  ws_solver_load(ws_solver* s, const char* path, int32_t* istep, double* tt,
+                           ws_stream_t stream);
 /* Navier-Stokes: every RHS adds the viscous terms (NULL: Euler again).  The
  * solver keeps their workspace; the RK stage adds them before its update. */
 WS_API int  ws_solver_set_viscous(ws_solver* s, const ws_viscous* vis);

@@ -19,6 +19,8 @@ from __future__ import annotations
 import ctypes as C
 from dataclasses import dataclass, field
 
+import numpy as np
+
 from ._abi import (FACE_CLOSURE, FACE_EXTRAP, FACE_PERIODIC, FP64, LAP, MIXED, WsDim3, WsError,
                    WsField, WsGrid, WsJob, WsMetrics, WsSoa, WsTile, WsViscous, check,
                    header_symbols, last_error, load)
@@ -26,7 +28,8 @@ from ._abi import (FACE_CLOSURE, FACE_EXTRAP, FACE_PERIODIC, FP64, LAP, MIXED, W
 __all__ = [
     "FACE_CLOSURE", "FACE_EXTRAP", "FACE_PERIODIC", "FP64", "MIXED", "LAP", "WsError", "Grid", "make_grid",
     "lap_tensor", "soa_tensor", "field_desc", "soa_desc", "interior_job", "du_invis_jacobian3d",
-    "du_vis_jacobian3d", "viscous",
+    "du_vis_jacobian3d", "viscous", "restart_write", "restart_read", "metrics_write",
+    "metrics_read",
     "du_invis_jacobian3d_init", "ghost_fill", "cons_to_prim", "prim_to_cons", "time_advance",
     "Solver", "load", "header_symbols", "last_error",
 ]
@@ -134,6 +137,38 @@ def _metrics(m):
 def viscous(re=500.0, pr=0.72, ref_t=288.15, scheme=8) -> WsViscous:
     """ws_viscous: Reynolds and Prandtl numbers, Sutherland Ref_T, CD order 6 or 8."""
     return WsViscous(re, pr, ref_t, scheme, 0)
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def restart_write(path: str, prims, istep: int = 0, tt: float = 0.0) -> None:
+    """prims: float64 [5, nz, ny, nx] (d, u, v, w, T) to an OCFD%08d.dat file."""
+    a = np.ascontiguousarray(prims, dtype=np.float64)
+    _, nz, ny, nx = a.shape
+    check(load().ws_restart_write(path.encode(), nx, ny, nz, istep, tt, _dp(a)))
+
+
+def restart_read(path: str, nx: int, ny: int, nz: int):
+    """(Istep, tt, prims [5, nz, ny, nx]) from an OCFD%08d.dat file."""
+    a = np.empty((5, nz, ny, nx))
+    i, t = C.c_int32(), C.c_double()
+    check(load().ws_restart_read(path.encode(), nx, ny, nz, C.byref(i), C.byref(t), _dp(a)))
+    return i.value, t.value, a
+
+
+def metrics_write(path: str, fields) -> None:
+    """fields: float64 [13, nz, ny, nx] (x, y, z, akx..asz, ajac)."""
+    a = np.ascontiguousarray(fields, dtype=np.float64)
+    _, nz, ny, nx = a.shape
+    check(load().ws_metrics_write(path.encode(), nx, ny, nz, _dp(a)))
+
+
+def metrics_read(path: str, nx: int, ny: int, nz: int):
+    a = np.empty((13, nz, ny, nx))
+    check(load().ws_metrics_read(path.encode(), nx, ny, nz, _dp(a)))
+    return a
 
 
 def du_vis_jacobian3d(g: Grid, vis, u, v, w, T, du, metrics=None, workspace=None,
@@ -276,6 +311,17 @@ class Solver:
 
     def set_tile(self, tile):
         check(load().ws_solver_set_tile(self.h, WsTile(*tile)))
+
+    def save(self, path: str, istep: int = 0, tt: float = 0.0, stream=None) -> None:
+        """Current state to a restart file (OCFD%08d.dat format)."""
+        check(load().ws_solver_save(self.h, path.encode(), istep, tt, _stream(stream)))
+
+    def load_restart(self, path: str, stream=None):
+        """State from a restart file; returns (Istep, tt)."""
+        i, t = C.c_int32(), C.c_double()
+        check(load().ws_solver_load(self.h, path.encode(), C.byref(i), C.byref(t),
+                                    _stream(stream)))
+        return i.value, t.value
 
     def set_viscous(self, vis):
         """Navier-Stokes with ws_viscous constants (a WsViscous, a dict with

@@ -21,7 +21,7 @@ FP64, MIXED = 0, 1
 WS_OK = 0
 ERRORS = {1: "WS_ERR_INVALID", 2: "WS_ERR_CUDA", 3: "WS_ERR_ALLOC", 4: "WS_ERR_UNSUPPORTED",
           5: "WS_ERR_NONFINITE", 6: "WS_ERR_TIMEOUT", 7: "WS_ERR_BUDGET", 8: "WS_ERR_BUSY",
-          9: "WS_ERR_NOT_FOUND"}
+          9: "WS_ERR_NOT_FOUND", 10: "WS_ERR_IO"}
 
 
 class WsField(C.Structure):
@@ -87,6 +87,7 @@ class WsServerStats(C.Structure):
 
 _P = C.c_void_p
 _I = C.c_int
+_DP = C.POINTER(C.c_double)
 SIGNATURES = {
     "ws_abi_version": (_I, []),
     "ws_last_error": (_I, [C.c_char_p, C.c_size_t]),
@@ -114,6 +115,14 @@ SIGNATURES = {
     "ws_solver_status": (_I, [_P, C.POINTER(_I), _P]),
     "ws_solver_set_tile": (_I, [_P, WsTile]),
     "ws_solver_set_viscous": (_I, [_P, C.POINTER(WsViscous)]),
+    "ws_solver_save": (_I, [_P, C.c_char_p, C.c_int32, C.c_double, _P]),
+    "ws_solver_load": (_I, [_P, C.c_char_p, C.POINTER(C.c_int32), C.POINTER(C.c_double), _P]),
+    "ws_restart_write": (_I, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int32, C.c_double,
+                              _DP]),
+    "ws_restart_read": (_I, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int32),
+                             C.POINTER(C.c_double), _DP]),
+    "ws_metrics_write": (_I, [C.c_char_p, C.c_int, C.c_int, C.c_int, _DP]),
+    "ws_metrics_read": (_I, [C.c_char_p, C.c_int, C.c_int, C.c_int, _DP]),
     "ws_du_vis_workspace_bytes": (C.c_size_t, [C.POINTER(WsGrid)]),
     "ws_du_vis_jacobian3d": (_I, [C.POINTER(WsGrid), C.POINTER(WsViscous)] + [WsField] * 4 +
                              [C.POINTER(WsMetrics), WsSoa, _P, C.c_size_t, _P]),

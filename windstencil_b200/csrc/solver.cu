@@ -10,6 +10,7 @@
 // primitive buffer.  The reference's shipped loop runs stage 1 only
 // (`KRK <= 1`, :77); all three stage formulas of OCFD_time.cpp:15-65 are used.
 #include <cstring>
+#include <vector>
 
 #include "ws_internal.h"
 
@@ -165,6 +166,45 @@ int ws_solver_set_viscous(ws_solver* s, const ws_viscous* vis) {
     s->vis = *vis;
     s->viscous = true;
     drop_graphs(s);
+    return WS_OK;
+}
+
+int ws_solver_save(ws_solver* s, const char* path, int32_t istep, double tt,
+                   ws_stream_t stream) {
+    if (!s || !path) return fail(WS_ERR_INVALID, "NULL argument");
+    const ws_grid& g = s->s.g;
+    const size_t n = (size_t)g.nx * g.ny * g.nz;
+    std::vector<double> f(5 * n), p(5 * n);
+    int rc = ws_solver_get_state(s, f.data(), stream);
+    if (rc) return rc;
+    const double cv = 1.0 / (g.gamma * (g.gamma - 1.0) * g.ama * g.ama);
+    for (size_t c = 0; c < n; ++c) {    // cons_to_pri_kernel, commen_kernel.cpp:78-110
+        const double d1 = f[c];
+        const double u1 = f[n + c] / d1, v1 = f[2 * n + c] / d1, w1 = f[3 * n + c] / d1;
+        double T1 = f[4 * n + c] - 0.5 * d1 * (u1 * u1 + v1 * v1 + w1 * w1);
+        T1 = T1 / (d1 * cv);
+        p[c] = d1; p[n + c] = u1; p[2 * n + c] = v1; p[3 * n + c] = w1; p[4 * n + c] = T1;
+    }
+    return ws_restart_write(path, g.nx, g.ny, g.nz, istep, tt, p.data());
+}
+
+int ws_solver_load(ws_solver* s, const char* path, int32_t* istep, double* tt,
+                   ws_stream_t stream) {
+    if (!s || !path || !istep || !tt) return fail(WS_ERR_INVALID, "NULL argument");
+    const ws_grid& g = s->s.g;
+    const size_t n = (size_t)g.nx * g.ny * g.nz;
+    std::vector<double> p(5 * n), f(5 * n);
+    int rc = ws_restart_read(path, g.nx, g.ny, g.nz, istep, tt, p.data());
+    if (rc) return rc;
+    const double cv = 1.0 / (g.gamma * (g.gamma - 1.0) * g.ama * g.ama);
+    for (size_t c = 0; c < n; ++c) {    // pri_to_cons_kernel, commen_kernel.cpp:33-70
+        const double d = p[c], u = p[n + c], v = p[2 * n + c], w = p[3 * n + c];
+        f[c] = d; f[n + c] = u * d; f[2 * n + c] = v * d; f[3 * n + c] = w * d;
+        f[4 * n + c] = d * ((u * u + v * v + w * w) * 0.5 + cv * p[4 * n + c]);
+    }
+    rc = grid_state_upload(s->s, f.data(), (cudaStream_t)stream);
+    if (rc) return rc;
+    WS_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
     return WS_OK;
 }
 
