@@ -36,9 +36,10 @@ from a CUDA graph.
                  batching server; p50/p99 latency and served throughput
 
 --impl reference runs only the CPU reference arm (rank 0) on the headline
-workload and metric.  --gpus N > 1 runs N independent replicas (one grid per
-rank, weak scaling: the single-grid path has no exchange step at one grid
-per GPU).
+workload and metric.  --gpus N > 1 (one rank per GPU under torchrun) steps one
+grid of (N*nx) x ny x nz split into N x slabs of nx x ny x nz, one per GPU,
+with the x halos exchanged over NCCL before every RK stage (weak scaling: each
+GPU keeps the single-GPU workload's cells).
 """
 from __future__ import annotations
 
@@ -74,6 +75,7 @@ def parse():
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-second", action="store_true")
     ap.add_argument("--no-ns", action="store_true")
+    ap.add_argument("--no-slabs", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--batch-grids", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=50)
@@ -85,9 +87,23 @@ def parse():
     return ap.parse_args()
 
 
-def workload_name(a):
-    return (f"fp64 fused RHS {a.nx}x{a.ny}x{a.nz}, Sod (rho 1/0.125, p 1/0.1, 1% noise), "
-            "x extrapolation, y/z periodic, SSP-RK3 CFL 0.5")
+def workload_name(a, world=1):
+    if world == 1:
+        return (f"fp64 fused RHS {a.nx}x{a.ny}x{a.nz}, Sod (rho 1/0.125, p 1/0.1, 1% noise), "
+                "x extrapolation, y/z periodic, SSP-RK3 CFL 0.5")
+    return (f"fp64 fused RHS {a.nx * world}x{a.ny}x{a.nz} split into {world} x slabs of "
+            f"{a.nx}x{a.ny}x{a.nz} (one per GPU, x halo exchanged over NCCL every RK stage), "
+            "Sod per slab (rho 1/0.125, p 1/0.1, 1% noise), x extrapolation, y/z periodic, "
+            "SSP-RK3 CFL 0.5")
+
+
+def config_of(a, world, **kw):
+    c = {"workload": workload_name(a, world), "grid": [a.nx * world, a.ny, a.nz],
+         "grid_per_gpu": [a.nx, a.ny, a.nz], "rhs_per_step": 3, "cfl": 0.5,
+         "inputs_exceed_l2": True,
+         "parallelism": "single" if world == 1 else f"xslab{world}"}
+    c.update(kw)
+    return c
 
 
 class ClockSampler:
@@ -200,8 +216,7 @@ def run_reference(a, rank, world):
             "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": el / a.steps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": workload_name(a), "grid": [a.nx, a.ny, a.nz],
-                       "inputs_exceed_l2": True},
+            "config": config_of(a, world),
             "cpu_baseline": {"value": value, "unit": "Gcell-RHS/s", "cores": o.threads(),
                              "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": "Gcell-RHS/s", "h2d_bytes_per_step": 0,
@@ -318,6 +333,49 @@ def bench_second_grid(a, torch, ws, wl, stream, peak64):
             res[name]["frac_of_fp64_peak"] = tf / peak64 if peak64 else None
     res["kernel_speedup_mixed_vs_fp64"] = res["fp64"]["kernel_ms"] / res["mixed"]["kernel_ms"]
     return res
+
+
+def bench_slabs_one_gpu(a, torch, ws, wl, stream, parts=2):
+    """The multi-GPU path's per-stage work on one GPU: a (parts*nx) x ny x nz
+    grid split into `parts` x slabs, all on this GPU (halo pack, hand-over
+    in process, unpack, ghost fill, fused stage per slab and stage, launched
+    eagerly), against the same grid stepped whole from its graphs."""
+    from windstencil_b200 import halo
+    faces = (ws.FACE_EXTRAP, ws.FACE_EXTRAP, 0, 0, 0, 0)
+    g = ws.Grid(a.nx * parts, a.ny, a.nz, faces=faces)
+    f0 = wl.sod_state(g.nx, g.ny, g.nz, seed=12)
+    steps = max(3, min(a.steps, 20))
+    whole = ws.Solver(g)
+    whole.set_state(f0, stream=stream)
+    dt = whole.compute_dt(0.5, stream=stream)
+    whole.step(dt, 3, stream=stream)
+    e0, e1 = _events(torch)
+    e0.record(stream)
+    whole.step(dt, steps, stream=stream)
+    e1.record(stream)
+    e1.synchronize()
+    ms_whole = e0.elapsed_time(e1) / steps
+    whole.close()
+    with torch.cuda.stream(stream):
+        st = halo.in_process(g, parts)
+        st.set_state(f0)
+        st.step(dt, 3)
+        e0.record(stream)
+        st.step(dt, steps)
+        e1.record(stream)
+    e1.synchronize()
+    ms_slabs = e0.elapsed_time(e1) / steps
+    status = st.status()
+    st.close()
+    return {"workload": f"{g.nx}x{g.ny}x{g.nz} Sod, x extrapolation, split into {parts} x "
+                        f"slabs of {a.nx}x{a.ny}x{a.nz} on one GPU",
+            "steps": steps, "step_ms_whole_grid": ms_whole, "step_ms_slabs": ms_slabs,
+            "slab_overhead": ms_slabs / ms_whole - 1.0,
+            "halo_bytes_per_stage_per_face": ws.halo_x_bytes(g, halo.HALO_FIELDS),
+            "device_status": status,
+            "note": "slabs: per stage per slab a halo pack and unpack per shared face, "
+                    "ghost fill, fused RHS + stage; the exchange between GPUs (NCCL) is "
+                    "not in this number"}
 
 
 def bench_navier_stokes(a, torch, ws, wl, stream):
@@ -497,27 +555,50 @@ def run_ours(a, rank, world, dist):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     faces = (ws.FACE_EXTRAP, ws.FACE_EXTRAP, 0, 0, 0, 0)
-    g = ws.Grid(a.nx, a.ny, a.nz, faces=faces)
-    cells = g.cells
     f0 = wl.sod_state(a.nx, a.ny, a.nz, seed=2 + rank)
-    s = ws.Solver(g)
     stream = torch.cuda.Stream()
-    s.set_state(f0, stream=stream)
-    dt = s.compute_dt(0.5, stream=stream)
+    if world == 1:
+        # one grid: the step's two graphs (ghost fill + fused RHS/stage, x3)
+        g = ws.Grid(a.nx, a.ny, a.nz, faces=faces)
+        s = ws.Solver(g)
+        s.set_state(f0, stream=stream)
+        dt = s.compute_dt(0.5, stream=stream)
+        launches_per_step = 6
+
+        def run_steps(n):
+            s.step(dt, n, stream=stream)
+    else:
+        # this rank's x slab of one (world*nx) x ny x nz grid; per stage: halo
+        # pack, NCCL send/recv with the x neighbours, unpack, fused stage
+        from windstencil_b200 import halo
+        gg = ws.Grid(a.nx * world, a.ny, a.nz, faces=faces)
+        with torch.cuda.stream(stream):
+            stepper = halo.distributed(gg)
+            runner = stepper.runners[0]
+            runner.set_state(f0)
+            dt = stepper.compute_dt(0.5)
+        g, s = runner.grid, runner.solver
+        sides = (runner.slab.left is not None) + (runner.slab.right is not None)
+        launches_per_step = 3 * (2 + 2 * sides)
+
+        def run_steps(n):
+            with torch.cuda.stream(stream):
+                stepper.step(dt, n)
+    cells = g.cells
 
     def barrier():
         if dist is not None:
             dist.barrier()
 
-    # ---- whole-job value: K SSP-RK3 steps from the captured graphs
-    s.step(dt, a.warmup, stream=stream)
+    # ---- whole-job value: K SSP-RK3 steps
+    run_steps(a.warmup)
     stream.synchronize()
     barrier()
     torch.cuda.synchronize()
     e0, e1 = _events(torch)
     with ClockSampler(local) as clk:
         e0.record(stream)
-        s.step(dt, a.steps, stream=stream)
+        run_steps(a.steps)
         e1.record(stream)
         e1.synchronize()
     torch.cuda.synchronize()
@@ -561,7 +642,7 @@ def run_ours(a, rank, world, dist):
 
         def one():
             ws._abi.check(lib.ws_solver_set_state(s.h, ptr, stream.cuda_stream))
-            s.step(dt, 1, stream=stream)
+            run_steps(1)
             ws._abi.check(lib.ws_solver_get_state(s.h, ptr, stream.cuda_stream))
         one()
         barrier()
@@ -584,7 +665,10 @@ def run_ours(a, rank, world, dist):
                "steps": n_e2e, "wall_s": wall,
                "note": "every step: pinned host state -> device, one SSP-RK3 step, "
                        "state -> pinned host, through ws_solver_set_state/step/get_state"}
-    s.close()
+    if world == 1:
+        s.close()
+    else:
+        stepper.close()
 
     extra = {}
     if rank == 0 and world == 1:
@@ -592,6 +676,8 @@ def run_ours(a, rank, world, dist):
             extra["mixed"] = bench_mixed(a, torch, ws, wl, stream)
         if not a.no_second:
             extra["grid_480x512x64"] = bench_second_grid(a, torch, ws, wl, stream, peak)
+        if not a.no_slabs:
+            extra["x_slabs_one_gpu"] = bench_slabs_one_gpu(a, torch, ws, wl, stream)
         if not a.no_ns:
             extra["navier_stokes"] = bench_navier_stokes(a, torch, ws, wl, stream)
         serial = None
@@ -613,11 +699,9 @@ def run_ours(a, rank, world, dist):
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms / a.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64", "data": "synthetic",
-                "config": {"workload": workload_name(a), "grid": [a.nx, a.ny, a.nz],
-                           "rhs_per_step": 3, "cfl": 0.5, "dt": dt,
-                           "inputs_exceed_l2": True, "parallelism": f"replicas{world}"},
+                "config": config_of(a, world, dt=dt),
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": 6 * a.steps, "clocks": clk.summary(),
+                "gpu_launches": launches_per_step * a.steps, "clocks": clk.summary(),
                 "device_status": status}
         line.update(extra)
         print(json.dumps(line), flush=True)

@@ -71,7 +71,14 @@ enum ws_face_kind {
      * 1063-1085 for x and :1515-1584 for y): WENO5 one-sided forms, linear
      * extrapolation / averages (x) or minmod2 forms (y) at the high end, and
      * the reference's dropped M term of the last y cell.  >= 8 cells.       */
-    WS_FACE_CLOSURE = 2
+    WS_FACE_CLOSURE = 2,
+    /* x faces only: the face is shared with a neighbouring subdomain (a slab
+     * of a grid split along x); its 4 ghost planes at interior y, z are
+     * written by the caller (ws_halo_unpack_x), as the reference's
+     * exchange_boundary_x_packed_dev does (OCFD_mpi_dev.cpp:185-218); the
+     * ghost fill leaves them and copies them into the y/z ghost edges.
+     * Faces next to it are reconstructed with WENO7 through those ghosts. */
+    WS_FACE_EXTERNAL = 3
 };
 
 enum ws_precision {
@@ -188,7 +195,9 @@ WS_API size_t ws_du_vis_workspace_bytes(const ws_grid* g);
  * halo exchange of the fluxes, derivative and YF_Pe_XF accumulation), with
  * the fluxes' ghosts filled by g->face_kind.  workspace: caller-owned device
  * memory of ws_du_vis_workspace_bytes(g) (the reference keeps the same
- * fields as globals); the call allocates nothing. */
+ * fields as globals); the call allocates nothing.  WS_ERR_UNSUPPORTED for a
+ * grid with WS_FACE_EXTERNAL faces: the fluxes' x halos would need an
+ * exchange of their own between the two passes. */
 WS_API int ws_du_vis_jacobian3d(const ws_grid* g, const ws_viscous* vis, ws_field u, ws_field v,
                                 ws_field w, ws_field T, const ws_metrics* metrics, ws_soa du,
                                 void* workspace, size_t workspace_bytes, ws_stream_t stream);
@@ -216,6 +225,24 @@ WS_API int ws_metrics_read(const char* path, int nx, int ny, int nz, double* fie
  * Replaces exchange_boundary_xyz_packed_dev (OCFD_mpi_dev.cpp:123-290) on one
  * GPU: no host staging, no MPI. */
 WS_API int ws_ghost_fill(const ws_grid* g, const ws_field* fields, int nfields, ws_stream_t stream);
+
+/* Halo planes of a grid split into slabs along x (the reference's MPI_COMM_X
+ * decomposition, OCFD_mpi.c:124-145, with one subdomain per GPU).
+ * side 0 is the low-x face, side 1 the high-x face.  A halo buffer holds
+ * nfields x nz x ny x 4 doubles, [field][z][y][x], interior y and z only
+ * (the packed layout of cudaFieldBoundaryPack_kernel, OCFD_mpi_dev.cpp:137-152).
+ * Buffers are device memory, 8-byte aligned; 1 <= nfields <= 8. */
+WS_API size_t ws_halo_x_bytes(const ws_grid* g, int nfields);
+/* Interior planes next to face `side` (side 0: x = 4..7; side 1: x = nx..nx+3
+ * in LAP coordinates) -> buf.  The sends of exchange_boundary_x_packed_dev
+ * (OCFD_mpi_dev.cpp:185-218): side 0 goes to the low-x neighbour. */
+WS_API int ws_halo_pack_x(const ws_grid* g, const ws_field* fields, int nfields, int side,
+                          void* buf, ws_stream_t stream);
+/* buf -> the ghost planes beyond face `side` (side 0: x = 0..3; side 1:
+ * x = nx+4..nx+7): the receives of exchange_boundary_x_packed_dev.  The low
+ * ghosts take the low-x neighbour's side-1 planes, and the reverse. */
+WS_API int ws_halo_unpack_x(const ws_grid* g, const ws_field* fields, int nfields, int side,
+                            const void* buf, ws_stream_t stream);
 
 /* Conserved (SoA f) -> LAP interiors of d,u,v,w,T and P (P.ptr may be NULL).
  * Replaces get_duvwT / cons_to_pri_kernel (commen_kernel.cpp:78-119). */
@@ -275,8 +302,22 @@ WS_API int  ws_solver_fields(ws_solver* s, ws_soa* f, ws_soa* du, ws_field prims
 WS_API int  ws_solver_compute_dt(ws_solver* s, double cfl, double* dt, ws_stream_t stream);
 /* du of the current state (prims, ghost fill, cc, RHS). */
 WS_API int  ws_solver_rhs(ws_solver* s, ws_stream_t stream);
-/* nsteps SSP-RK3 steps with time step dt, replayed from one CUDA graph. */
+/* nsteps SSP-RK3 steps with time step dt, replayed from one CUDA graph.
+ * WS_ERR_UNSUPPORTED for a grid with WS_FACE_EXTERNAL faces (those step by
+ * stages, with a halo exchange before each). */
 WS_API int  ws_solver_step(ws_solver* s, double dt, int nsteps, ws_stream_t stream);
+/* One SSP-RK3 stage, krk = 1, 2, 3 in that order (stage 3 completes the step
+ * and makes its result the current state): ghost fill of the stage's input
+ * primitives on every face that is not WS_FACE_EXTERNAL, then the fused RHS
+ * with the stage update.  Before each stage the caller writes the EXTERNAL
+ * faces' ghost planes into ws_solver_stage_fields(s, krk).  The reference's
+ * loop body per stage: exchange_boundary_xyz_packed_dev, du_comput,
+ * OCFD_time_advance (OCFD_NS_Solver.cpp:64-90).  WS_ERR_INVALID when krk is
+ * not the next stage. */
+WS_API int  ws_solver_stage(ws_solver* s, int krk, double dt, ws_stream_t stream);
+/* The primitive fields d,u,v,w,T,cc that stage krk reads (stage 1: the
+ * current state's). */
+WS_API int  ws_solver_stage_fields(ws_solver* s, int krk, ws_field prims[6]);
 /* Device status word (0 or WS_ERR_NONFINITE); synchronises `stream`. */
 WS_API int  ws_solver_status(ws_solver* s, int* status, ws_stream_t stream);
 WS_API int  ws_solver_set_tile(ws_solver* s, ws_tile tile);
@@ -288,7 +329,8 @@ WS_API int  ws_solver_save(ws_solver* s, const char* path, int32_t istep, double
 WS_API int  ws_solver_load(ws_solver* s, const char* path, int32_t* istep, double* tt,
                            ws_stream_t stream);
 /* Navier-Stokes: every RHS adds the viscous terms (NULL: Euler again).  The
- * solver keeps their workspace; the RK stage adds them before its update. */
+ * solver keeps their workspace; the RK stage adds them before its update.
+ * WS_ERR_UNSUPPORTED for a grid with WS_FACE_EXTERNAL faces. */
 WS_API int  ws_solver_set_viscous(ws_solver* s, const ws_viscous* vis);
 
 /* ------------------------------------------------------------------------ */
@@ -296,7 +338,8 @@ WS_API int  ws_solver_set_viscous(ws_solver* s, const ws_viscous* vis);
 /* one batched ghost fill, one persistent fused-RHS launch over all grids,   */
 /* one batched stage update; the step is replayed from a CUDA graph.  No     */
 /* reference counterpart (the reference solves one grid per MPI rank).       */
-/* All grids: Cartesian (metrics_uniform = 1) and one precision.             */
+/* All grids: Cartesian (metrics_uniform = 1), one precision, no EXTERNAL   */
+/* faces.                                                                    */
 /* ------------------------------------------------------------------------ */
 typedef struct ws_batch ws_batch;
 

@@ -397,10 +397,15 @@ void or_split_batch(const double* in, long n, double gamma, double epsl_sw,
 // periodic self-exchange (OCFD_mpi_dev.cpp:123-290) with an in-place copy;
 // OR_FACE_EXTRAP copies the nearest interior value (zero gradient).  Axes are
 // filled x, then y, then z over the full padded extent of the other axes,
-// so edge and corner ghosts are defined (the RHS never reads them).
+// so edge and corner ghosts are defined (the RHS never reads them).  An
+// OR_FACE_EXTERNAL x face keeps its ghost planes (a neighbouring subdomain's
+// halo, unpacked by the caller as exchange_boundary_x_packed_dev does,
+// OCFD_mpi_dev.cpp:185-218); the y and z passes copy them into the edges.
 void or_ghost_fill(const or_grid* g, double* f) {
     Dims D(g);
     const long L = OR_LAP;
+    const bool ext_lo = g->face_kind[0] == OR_FACE_EXTERNAL;
+    const bool ext_hi = g->face_kind[1] == OR_FACE_EXTERNAL;
     // x
 #pragma omp parallel for collapse(2) schedule(static)
     for (long k = -L; k < D.nz + L; ++k)
@@ -408,8 +413,8 @@ void or_ghost_fill(const or_grid* g, double* f) {
             for (long l = 1; l <= L; ++l) {
                 long lo = g->face_kind[0] == OR_FACE_PERIODIC ? D.nx - l : 0;
                 long hi = g->face_kind[1] == OR_FACE_PERIODIC ? l - 1 : D.nx - 1;
-                f[D.lap(-l, j, k)] = f[D.lap(lo, j, k)];
-                f[D.lap(D.nx - 1 + l, j, k)] = f[D.lap(hi, j, k)];
+                if (!ext_lo) f[D.lap(-l, j, k)] = f[D.lap(lo, j, k)];
+                if (!ext_hi) f[D.lap(D.nx - 1 + l, j, k)] = f[D.lap(hi, j, k)];
             }
     // y
 #pragma omp parallel for collapse(2) schedule(static)

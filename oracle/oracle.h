@@ -33,8 +33,10 @@ extern "C" {
 #define OR_LAP 4
 
 /* CLOSURE (x and y faces only): zero-gradient ghosts, and the faces next to
- * it take the boundary closures of the fused path's ring kernel */
-enum { OR_FACE_PERIODIC = 0, OR_FACE_EXTRAP = 1, OR_FACE_CLOSURE = 2 };
+ * it take the boundary closures of the fused path's ring kernel.
+ * EXTERNAL (x faces only): ghost planes written by the caller (a halo from a
+ * neighbouring subdomain); the ghost fill keeps them. */
+enum { OR_FACE_PERIODIC = 0, OR_FACE_EXTRAP = 1, OR_FACE_CLOSURE = 2, OR_FACE_EXTERNAL = 3 };
 
 typedef struct or_grid {
     int nx, ny, nz;            /* interior extents                                  */

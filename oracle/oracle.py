@@ -19,7 +19,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LAP = 4
-FACE_PERIODIC, FACE_EXTRAP, FACE_CLOSURE = 0, 1, 2
+FACE_PERIODIC, FACE_EXTRAP, FACE_CLOSURE, FACE_EXTERNAL = 0, 1, 2, 3
 # WENO5 closure family, in the order of or_weno5_batch / ref_weno5_batch
 WENO5_FORMS = ("p_lift", "p_lift_plus", "p", "p_right_plus", "m_lift", "m_lift_plus",
                "m", "m_right_plus", "minmod2")

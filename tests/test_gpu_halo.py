@@ -1,0 +1,156 @@
+"""x slabs on the GPU: the halo pack / unpack kernels, the ghost fill of
+EXTERNAL faces, the per-stage solver entry points, and whole SSP-RK3 runs of
+a grid split into slabs (all slabs on this GPU, halos passed between them in
+process) against the same grid stepped whole.
+
+A slab's cells see exactly the values the whole grid's cells see (the halo
+carries the neighbour's d, u, v, w, T, cc), so the split run must agree with
+the whole-grid run bit for bit wherever both use the same compiled kernel;
+the oracle bounds both at rel. L-inf 1e-12 per field.
+"""
+import numpy as np
+import pytest
+
+import windstencil_b200 as ws
+from windstencil_b200 import halo
+from windstencil_b200 import workloads as wl
+from oracle.oracle import make_grid as or_grid
+from tests.conftest import rel_linf
+
+pytestmark = pytest.mark.gpu
+PE, EX, CL, XT = ws.FACE_PERIODIC, ws.FACE_EXTRAP, ws.FACE_CLOSURE, ws.FACE_EXTERNAL
+
+
+def _rand_fields(torch, g, n, seed):
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    t = ws.lap_tensor(g, n)
+    t.copy_(torch.rand(t.shape, generator=gen, device="cuda", dtype=torch.float64))
+    return [t[i] for i in range(n)]
+
+
+@pytest.mark.parametrize("nf", [1, 6])
+@pytest.mark.parametrize("shape", [(19, 13, 7), (40, 24, 10)])
+def test_halo_pack_unpack(cuda, nf, shape):
+    torch = cuda
+    g = ws.Grid(*shape, faces=(XT, XT, PE, PE, PE, PE))
+    nx, ny, nz = shape
+    fields = _rand_fields(torch, g, nf, 5)
+    nb = ws.halo_x_bytes(g, nf) // 8
+    assert nb == nf * nz * ny * 4
+    for side, x0 in ((0, 4), (1, nx)):
+        buf = torch.full((nb,), -1.0, dtype=torch.float64, device="cuda")
+        ws.halo_pack_x(g, fields, side, buf)
+        want = torch.stack([f[4:nz + 4, 4:ny + 4, x0:x0 + 4] for f in fields]).reshape(-1)
+        assert torch.equal(buf, want)
+    for side, x0 in ((0, 0), (1, nx + 4)):
+        before = [f.clone() for f in fields]
+        buf = torch.rand(nb, dtype=torch.float64, device="cuda")
+        ws.halo_unpack_x(g, fields, side, buf)
+        b = buf.reshape(nf, nz, ny, 4)
+        for q, f in enumerate(fields):
+            assert torch.equal(f[4:nz + 4, 4:ny + 4, x0:x0 + 4], b[q])
+            mask = torch.ones_like(f, dtype=torch.bool)
+            mask[4:nz + 4, 4:ny + 4, x0:x0 + 4] = False
+            assert torch.equal(f[mask], before[q][mask])      # nothing else written
+    torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("faces", [(XT, XT, PE, EX, PE, PE), (EX, XT, EX, EX, PE, EX),
+                                   (XT, CL, CL, CL, PE, PE)])
+def test_ghost_fill_external(oracle, cuda, faces):
+    """EXTERNAL x ghosts at interior y, z are kept; the y/z ghost edges take
+    them; every other ghost as the oracle's fill."""
+    torch = cuda
+    shape = (21, 11, 9)
+    nx, ny, nz = shape
+    g = ws.Grid(*shape, faces=faces)
+    (f,) = _rand_fields(torch, g, 1, 9)
+    host = f[:, :, :nx + 8].cpu().numpy().copy()
+    ws.ghost_fill(g, [f])
+    oracle.ghost_fill(or_grid(*shape, face_kind=faces), host)
+    got = f[:, :, :nx + 8].cpu().numpy()
+    assert np.array_equal(got, host)
+
+
+def _run_whole(g, f0, dt, nsteps):
+    s = ws.Solver(g)
+    s.set_state(f0)
+    s.step(dt, nsteps)
+    out = s.get_state()
+    assert s.status() == 0
+    s.close()
+    return out
+
+
+def test_stages_equal_step(cuda):
+    g = ws.Grid(33, 20, 12, faces=(EX, EX, PE, PE, PE, PE))
+    f0 = wl.sod_state(g.nx, g.ny, g.nz, seed=31)
+    s = ws.Solver(g)
+    s.set_state(f0)
+    dt = s.compute_dt(0.5)
+    assert [p.ptr for p in s.stage_fields(1)] == [p.ptr for p in s.fields()[2]]
+    for _ in range(2):
+        for krk in (1, 2, 3):
+            s.stage(krk, dt)
+    staged = s.get_state()
+    s.close()
+    assert np.array_equal(staged, _run_whole(g, f0, dt, 2))
+
+
+def test_stage_rules(cuda):
+    g = ws.Grid(16, 16, 16, faces=(XT, EX, PE, PE, PE, PE))
+    s = ws.Solver(g)
+    s.set_state(wl.fourier_state(16, 16, 16, seed=2))
+    with pytest.raises(ws.WsError, match="WS_ERR_INVALID"):
+        s.stage(2, 1e-4)                                   # stage 1 is due
+    with pytest.raises(ws.WsError, match="WS_ERR_UNSUPPORTED"):
+        s.step(1e-4, 1)                                    # EXTERNAL: staged only
+    with pytest.raises(ws.WsError, match="WS_ERR_UNSUPPORTED"):
+        s.set_viscous(ws.viscous())
+    s.stage(1, 1e-4)
+    s.set_state(wl.fourier_state(16, 16, 16, seed=2))      # a new state restarts at 1
+    s.stage(1, 1e-4)
+    s.close()
+    with pytest.raises(ws.WsError, match="WS_ERR_UNSUPPORTED"):
+        ws.Batch([g])
+
+
+CASES = [
+    ("periodic_2", (64, 24, 12), (PE,) * 6, 2, ws.FP64),
+    ("periodic_3_ragged", (70, 20, 10), (PE,) * 6, 3, ws.FP64),
+    ("extrap_4", (96, 16, 12), (EX, EX, PE, PE, PE, PE), 4, ws.FP64),
+    ("closure_2", (64, 24, 10), (CL, CL, CL, CL, PE, PE), 2, ws.FP64),
+    ("mixed_periodic_2", (64, 24, 12), (PE,) * 6, 2, ws.MIXED),
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_slabs_match_whole_grid(oracle, cuda, case):
+    _, shape, faces, parts, prec = case
+    g = ws.Grid(*shape, faces=faces, precision=prec)
+    f0 = wl.sod_state(*shape, seed=17)
+    nsteps = 3
+    st = halo.in_process(g, parts)
+    try:
+        st.set_state(f0)
+        whole = ws.Solver(g)
+        whole.set_state(f0)
+        dt = whole.compute_dt(0.5)
+        whole.close()
+        assert st.compute_dt(0.5) == dt
+        st.step(dt, nsteps)
+        got = halo.join_state(st.get_state())
+        assert st.status() == 0
+    finally:
+        st.close()
+    want = _run_whole(g, f0, dt, nsteps)
+    diff = rel_linf(got, want).max()
+    if CL in faces:
+        # the end slabs run the closure kernel, the middle ones the plain one;
+        # the whole grid runs the closure kernel everywhere
+        assert diff <= 1e-13, diff
+    else:
+        assert np.array_equal(got, want), diff
+    if prec == ws.FP64:
+        ref = oracle.rk3_steps(or_grid(*shape, face_kind=faces), f0, dt, nsteps)
+        assert rel_linf(got, ref).max() <= 1e-12

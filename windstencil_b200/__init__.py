@@ -8,7 +8,8 @@ points fails loudly when the library has not been built.
 Reference interface this mirrors (WindStencil, src/):
   du_invis_Jacobian3d_init  solver/OCFD_NS_Jacobian3d.cpp:24-33   -> du_invis_jacobian3d_init
   du_invis_Jacobian3d_x     solver/OCFD_NS_Jacobian3d.cpp:133-414 -> du_invis_jacobian3d
-  exchange_boundary_xyz_packed_dev  mpi/OCFD_mpi_dev.cpp:123-290 -> ghost_fill
+  exchange_boundary_xyz_packed_dev  mpi/OCFD_mpi_dev.cpp:123-290 -> ghost_fill (one domain),
+                                     halo_pack_x / halo_unpack_x + halo.SlabStepper (x slabs)
   get_duvwT / cons_to_pri_kernel     kernels/commen_kernel.cpp:78-119 -> cons_to_prim
   pri_to_cons_kernel_warp            kernels/commen_kernel.cpp:33-73  -> prim_to_cons
   OCFD_time_advance                  solver/OCFD_time.cpp:15-91        -> time_advance
@@ -21,12 +22,14 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from ._abi import (FACE_CLOSURE, FACE_EXTRAP, FACE_PERIODIC, FP64, LAP, MIXED, WsDim3, WsError,
+from ._abi import (FACE_CLOSURE, FACE_EXTERNAL, FACE_EXTRAP, FACE_PERIODIC, FP64, LAP, MIXED,
+                   WsDim3, WsError,
                    WsField, WsGrid, WsJob, WsMetrics, WsSoa, WsTile, WsViscous, check,
                    header_symbols, last_error, load)
 
 __all__ = [
-    "FACE_CLOSURE", "FACE_EXTRAP", "FACE_PERIODIC", "FP64", "MIXED", "LAP", "WsError", "Grid", "make_grid",
+    "FACE_CLOSURE", "FACE_EXTERNAL", "FACE_EXTRAP", "FACE_PERIODIC", "FP64", "MIXED", "LAP",
+    "WsError", "Grid", "make_grid", "halo_x_bytes", "halo_pack_x", "halo_unpack_x",
     "lap_tensor", "soa_tensor", "field_desc", "soa_desc", "interior_job", "du_invis_jacobian3d",
     "du_vis_jacobian3d", "viscous", "restart_write", "restart_read", "metrics_write",
     "metrics_read",
@@ -227,6 +230,32 @@ def ghost_fill(g: Grid, fields, stream=None) -> None:
     check(load().ws_ghost_fill(C.byref(gc), arr, len(fields), _stream(stream)))
 
 
+def halo_x_bytes(g: Grid, nfields: int) -> int:
+    """Bytes of one side's x halo: nfields x nz x ny x 4 doubles."""
+    gc = g.c()
+    return int(load().ws_halo_x_bytes(C.byref(gc), nfields))
+
+
+def _halo(fn, g: Grid, fields, side: int, buf, stream):
+    gc = g.c()
+    arr = (WsField * len(fields))(*[f if isinstance(f, WsField) else field_desc(f)
+                                    for f in fields])
+    assert buf.dtype.itemsize == 8 and buf.is_contiguous()
+    assert buf.numel() * 8 >= halo_x_bytes(g, len(fields)), "halo buffer too small"
+    check(fn(C.byref(gc), arr, len(fields), side, buf.data_ptr(), _stream(stream)))
+
+
+def halo_pack_x(g: Grid, fields, side: int, buf, stream=None) -> None:
+    """Interior x planes next to face `side` (0 low, 1 high) of LAP fields
+    (tensors or WsField) -> buf (contiguous float64 device tensor)."""
+    _halo(load().ws_halo_pack_x, g, fields, side, buf, stream)
+
+
+def halo_unpack_x(g: Grid, fields, side: int, buf, stream=None) -> None:
+    """buf -> the ghost x planes beyond face `side` of the fields."""
+    _halo(load().ws_halo_unpack_x, g, fields, side, buf, stream)
+
+
 def cons_to_prim(g: Grid, f, d, u, v, w, T, P=None, stream=None) -> None:
     gc = g.c()
     pd = field_desc(P) if P is not None else WsField(None, 0, 0)
@@ -303,6 +332,16 @@ class Solver:
 
     def step(self, dt: float, nsteps: int = 1, stream=None):
         check(load().ws_solver_step(self.h, dt, nsteps, _stream(stream)))
+
+    def stage(self, krk: int, dt: float, stream=None):
+        """One SSP-RK3 stage (1, 2, 3 in order); EXTERNAL ghosts come from the caller."""
+        check(load().ws_solver_stage(self.h, krk, dt, _stream(stream)))
+
+    def stage_fields(self, krk: int):
+        """WsField descriptors of d,u,v,w,T,cc that stage krk reads."""
+        prims = (WsField * 6)()
+        check(load().ws_solver_stage_fields(self.h, krk, prims))
+        return list(prims)
 
     def status(self, stream=None) -> int:
         s = C.c_int()

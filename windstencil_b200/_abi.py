@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(HERE, "libwindstencil_b200.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "windstencil_b200.h")
 
 LAP = 4
-FACE_PERIODIC, FACE_EXTRAP, FACE_CLOSURE = 0, 1, 2
+FACE_PERIODIC, FACE_EXTRAP, FACE_CLOSURE, FACE_EXTERNAL = 0, 1, 2, 3
 FP64, MIXED = 0, 1
 
 WS_OK = 0
@@ -100,6 +100,9 @@ SIGNATURES = {
     "ws_du_invis_jacobian3d_tiled": (_I, [C.POINTER(WsGrid), WsJob] + [WsField] * 5 +
                                      [C.POINTER(WsMetrics), WsSoa, WsTile, _P]),
     "ws_ghost_fill": (_I, [C.POINTER(WsGrid), C.POINTER(WsField), _I, _P]),
+    "ws_halo_x_bytes": (C.c_size_t, [C.POINTER(WsGrid), _I]),
+    "ws_halo_pack_x": (_I, [C.POINTER(WsGrid), C.POINTER(WsField), _I, _I, _P, _P]),
+    "ws_halo_unpack_x": (_I, [C.POINTER(WsGrid), C.POINTER(WsField), _I, _I, _P, _P]),
     "ws_cons_to_prim": (_I, [C.POINTER(WsGrid), WsSoa] + [WsField] * 6 + [_P]),
     "ws_prim_to_cons": (_I, [C.POINTER(WsGrid)] + [WsField] * 5 + [WsSoa, _P]),
     "ws_time_advance": (_I, [C.POINTER(WsGrid), _I, C.c_double, WsSoa, WsSoa, WsSoa, _P]),
@@ -112,6 +115,8 @@ SIGNATURES = {
     "ws_solver_compute_dt": (_I, [_P, C.c_double, C.POINTER(C.c_double), _P]),
     "ws_solver_rhs": (_I, [_P, _P]),
     "ws_solver_step": (_I, [_P, C.c_double, _I, _P]),
+    "ws_solver_stage": (_I, [_P, _I, C.c_double, _P]),
+    "ws_solver_stage_fields": (_I, [_P, _I, C.POINTER(WsField)]),
     "ws_solver_status": (_I, [_P, C.POINTER(_I), _P]),
     "ws_solver_set_tile": (_I, [_P, WsTile]),
     "ws_solver_set_viscous": (_I, [_P, C.POINTER(WsViscous)]),

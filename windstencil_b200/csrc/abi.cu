@@ -39,8 +39,12 @@ int check_grid(const ws_grid* g) {
         return fail(WS_ERR_INVALID, "need gamma > 1, ama > 0, epsl_sw >= 0");
     for (int i = 0; i < 6; ++i) {
         const int k = g->face_kind[i];
-        if (k != WS_FACE_PERIODIC && k != WS_FACE_EXTRAP && k != WS_FACE_CLOSURE)
+        if (k != WS_FACE_PERIODIC && k != WS_FACE_EXTRAP && k != WS_FACE_CLOSURE &&
+            k != WS_FACE_EXTERNAL)
             return fail(WS_ERR_INVALID, "face_kind must be a ws_face_kind value");
+        if (k == WS_FACE_EXTERNAL && i >= 2)
+            return fail(WS_ERR_UNSUPPORTED, "EXTERNAL faces are x faces only "
+                                            "(slabs split along x)");
         if (k == WS_FACE_CLOSURE && i >= 4)
             return fail(WS_ERR_UNSUPPORTED, "CLOSURE faces are x and y faces only "
                                             "(the reference closes z through its ghosts)");
@@ -264,6 +268,12 @@ int rhs_stage_enqueue(const ws_grid* g, const ws_field p_in[6], ws_soa f_in, ws_
 
 int validate_grid(const ws_grid* g) { return check_grid(g); }
 
+bool has_external(const ws_grid* g) {
+    for (int i = 0; i < 6; ++i)
+        if (g->face_kind[i] == WS_FACE_EXTERNAL) return true;
+    return false;
+}
+
 }  // namespace ws
 
 using namespace ws;
@@ -300,6 +310,8 @@ int ws_du_vis_jacobian3d(const ws_grid* g, const ws_viscous* vis, ws_field u, ws
                          void* workspace, size_t workspace_bytes, ws_stream_t stream) {
     int rc;
     if ((rc = check_grid(g)) || (rc = check_viscous(vis))) return rc;
+    if (has_external(g))
+        return fail(WS_ERR_UNSUPPORTED, "viscous terms on a grid with EXTERNAL faces");
     if ((rc = check_field(g, u, "u")) || (rc = check_field(g, v, "v")) ||
         (rc = check_field(g, w, "w")) || (rc = check_field(g, T, "T")))
         return rc;
@@ -358,6 +370,42 @@ int ws_ghost_fill(const ws_grid* g, const ws_field* fields, int nfields, ws_stre
     for (int i = 0; i < nfields; ++i)
         if ((rc = check_field(g, fields[i], "field"))) return rc;
     return launch_ghost_fill(g, fields, nfields, (cudaStream_t)stream);
+}
+
+size_t ws_halo_x_bytes(const ws_grid* g, int nfields) {
+    if (!g || nfields < 1 || nfields > 8) return 0;
+    return (size_t)nfields * g->nz * g->ny * 4 * sizeof(double);
+}
+
+int ws_halo_pack_x(const ws_grid* g, const ws_field* fields, int nfields, int side, void* buf,
+                   ws_stream_t stream) {
+    int rc;
+    if ((rc = check_grid(g))) return rc;
+    if (!fields || nfields < 1 || nfields > 8)
+        return fail(WS_ERR_INVALID, "halo pack takes 1..8 fields");
+    if (side != 0 && side != 1) return fail(WS_ERR_INVALID, "side must be 0 or 1");
+    if (!buf || (reinterpret_cast<uintptr_t>(buf) & 7))
+        return fail(WS_ERR_INVALID, "halo buffer NULL or not 8-byte aligned");
+    for (int i = 0; i < nfields; ++i)
+        if ((rc = check_field(g, fields[i], "field"))) return rc;
+    return launch_halo_x(g, fields, nfields, side, static_cast<double*>(buf), true,
+                         (cudaStream_t)stream);
+}
+
+int ws_halo_unpack_x(const ws_grid* g, const ws_field* fields, int nfields, int side,
+                     const void* buf, ws_stream_t stream) {
+    int rc;
+    if ((rc = check_grid(g))) return rc;
+    if (!fields || nfields < 1 || nfields > 8)
+        return fail(WS_ERR_INVALID, "halo unpack takes 1..8 fields");
+    if (side != 0 && side != 1) return fail(WS_ERR_INVALID, "side must be 0 or 1");
+    if (!buf || (reinterpret_cast<uintptr_t>(buf) & 7))
+        return fail(WS_ERR_INVALID, "halo buffer NULL or not 8-byte aligned");
+    for (int i = 0; i < nfields; ++i)
+        if ((rc = check_field(g, fields[i], "field"))) return rc;
+    return launch_halo_x(g, fields, nfields, side,
+                         const_cast<double*>(static_cast<const double*>(buf)), false,
+                         (cudaStream_t)stream);
 }
 
 int ws_cons_to_prim(const ws_grid* g, ws_soa f, ws_field d, ws_field u, ws_field v, ws_field w,

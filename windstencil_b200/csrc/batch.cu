@@ -345,6 +345,8 @@ int ws_batch_create(const ws_grid* grids, int n, ws_batch** out) {
     for (int i = 0; i < n; ++i) {
         const ws_grid& g = grids[i];
         if (int rc = validate_grid(&g)) return rc;
+        if (has_external(&g))
+            return fail(WS_ERR_UNSUPPORTED, "EXTERNAL faces need a halo exchange");
         if (g.lap != WS_LAP || g.nx < 4 || g.ny < 4 || g.nz < 4 || !g.metrics_uniform ||
             (g.precision != WS_FP64 && g.precision != WS_MIXED) ||
             g.precision != grids[0].precision)

@@ -6,6 +6,8 @@
 //                  LAP-extended job by OCFD_NS_Jacobian3d.cpp:24-33)
 //   ghost fill     src/mpi/OCFD_mpi_dev.cpp:123-290 (host-staged periodic
 //                  self-exchange; here an in-place device copy)
+//   x halo planes  cudaFieldBoundaryPack/Unpack_kernel with the jobs of
+//                  exchange_boundary_x_packed_dev, OCFD_mpi_dev.cpp:137-218
 //   cons->prim     src/kernels/commen_kernel.cpp:78-119
 //   prim->cons     src/kernels/commen_kernel.cpp:33-73
 //   RK3 stages     src/solver/OCFD_time.cpp:15-91
@@ -23,10 +25,14 @@ __device__ __forceinline__ size_t soa_idx(int i, int j, int k, int var, const ws
                                           ((size_t)k + (size_t)s.length_Z * (size_t)var));
 }
 
-// source interior index of a (possibly ghost) LAP index along one axis
+// source index of a (possibly ghost) LAP index along one axis: an interior
+// index, or the ghost index itself on an EXTERNAL face (its value comes from
+// the neighbour's halo and is kept)
 __device__ __forceinline__ int ghost_src(int i, int n, int lo_kind, int hi_kind) {
-    if (i < 4) return lo_kind == WS_FACE_PERIODIC ? i + n : 4;
-    if (i >= n + 4) return hi_kind == WS_FACE_PERIODIC ? i - n : n + 3;
+    if (i < 4)
+        return lo_kind == WS_FACE_PERIODIC ? i + n : lo_kind == WS_FACE_EXTERNAL ? i : 4;
+    if (i >= n + 4)
+        return hi_kind == WS_FACE_PERIODIC ? i - n : hi_kind == WS_FACE_EXTERNAL ? i : n + 3;
     return i;
 }
 
@@ -71,15 +77,18 @@ struct GhostArgs {
     int kind[6];
 };
 
-// value at a ghost point = interior value at the wrapped / clamped
-// coordinates; the source is always an interior point, so one pass fills
-// every face without ordering between them.
+// value at a ghost point = value at the wrapped / clamped coordinates.  The
+// source is an interior point, or an x ghost at interior y, z of an EXTERNAL
+// face (which this pass never writes), so one pass fills every face without
+// ordering between them; EXTERNAL ghosts at interior y, z map onto themselves
+// and are skipped.
 __device__ __forceinline__ void ghost_fill_point(const GhostArgs& a, long t) {
     int i, j, k;
     ghost_point(t, a.nx, a.ny, a.nz, i, j, k);
     const int si = ghost_src(i, a.nx, a.kind[0], a.kind[1]);
     const int sj = ghost_src(j, a.ny, a.kind[2], a.kind[3]);
     const int sk = ghost_src(k, a.nz, a.kind[4], a.kind[5]);
+    if (si == i && sj == j && sk == k) return;
     for (int f = 0; f < a.nf; ++f) {
         double* p = a.ptr[f];
         p[lap_idx(i, j, k, a.pitch[f], a.ny)] = p[lap_idx(si, sj, sk, a.pitch[f], a.ny)];
@@ -91,6 +100,34 @@ __global__ void ghost_fill_kernel(const __grid_constant__ GhostArgs a) {
     for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total;
          t += (long)gridDim.x * blockDim.x)
         ghost_fill_point(a, t);
+}
+
+struct HaloArgs {
+    double* ptr[8];
+    uint32_t pitch[8];
+    int nf, ny, nz;
+    int x0;          // first LAP x plane of the four
+    double* buf;     // [nf][nz][ny][4]
+    int pack;        // 1: planes -> buf, 0: buf -> planes
+};
+
+// one double per thread in buffer order: a warp covers 8 rows of 4 planes
+__global__ void halo_x_kernel(const __grid_constant__ HaloArgs a) {
+    const long total = (long)a.nf * a.nz * a.ny * 4;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total;
+         t += (long)gridDim.x * blockDim.x) {
+        const int m = (int)(t & 3);
+        const long r = t >> 2;
+        const int j = (int)(r % a.ny);
+        const long r2 = r / a.ny;
+        const int k = (int)(r2 % a.nz);
+        const int f = (int)(r2 / a.nz);
+        double* p = a.ptr[f] + lap_idx(a.x0 + m, j + 4, k + 4, a.pitch[f], a.ny);
+        if (a.pack)
+            a.buf[t] = *p;
+        else
+            *p = a.buf[t];
+    }
 }
 
 __global__ void sound_speed_kernel(ws_field T, ws_field cc, int i0, int j0, int k0, int ni,
@@ -226,6 +263,28 @@ int launch_ghost_fill(const ws_grid* g, const ws_field* f, int nf, cudaStream_t 
     a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
     for (int i = 0; i < 6; ++i) a.kind[i] = g->face_kind[i];
     ghost_fill_kernel<<<grid_for(ghost_count(g->nx, g->ny, g->nz), 256), 256, 0, st>>>(a);
+    WS_CUDA(cudaGetLastError());
+    return WS_OK;
+}
+
+int launch_halo_x(const ws_grid* g, const ws_field* f, int nf, int side, double* buf, bool pack,
+                  cudaStream_t st) {
+    if (nf < 1 || nf > 8) return fail(WS_ERR_INVALID, "halo: 1..8 fields");
+    HaloArgs a{};
+    for (int i = 0; i < nf; ++i) {
+        a.ptr[i] = f[i].ptr;
+        a.pitch[i] = f[i].pitch;
+    }
+    a.nf = nf;
+    a.ny = g->ny;
+    a.nz = g->nz;
+    // pack: interior planes 4..7 (low) / nx..nx+3 (high);
+    // unpack: ghost planes 0..3 (low) / nx+4..nx+7 (high)
+    a.x0 = pack ? (side == 0 ? 4 : (int)g->nx) : (side == 0 ? 0 : (int)g->nx + 4);
+    a.buf = buf;
+    a.pack = pack ? 1 : 0;
+    const long n = (long)nf * g->nz * g->ny * 4;
+    halo_x_kernel<<<grid_for(n, 256), 256, 0, st>>>(a);
     WS_CUDA(cudaGetLastError());
     return WS_OK;
 }

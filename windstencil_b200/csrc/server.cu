@@ -367,6 +367,8 @@ int ws_server_submit(ws_server* s, const ws_request* r, uint64_t* id) {
     if (!s || !r) return fail(WS_ERR_INVALID, "NULL argument");
     const ws_grid& g = r->grid;
     if (int rc = validate_grid(&g)) return rc;
+    if (has_external(&g))
+        return fail(WS_ERR_UNSUPPORTED, "EXTERNAL faces need a halo exchange");
     if (g.lap != WS_LAP || g.nx < 4 || g.ny < 4 || g.nz < 4 || !g.metrics_uniform ||
         (g.precision != WS_FP64 && g.precision != WS_MIXED))
         return fail(WS_ERR_INVALID, "request grid: Cartesian, n >= 4, FP64 or mixed");

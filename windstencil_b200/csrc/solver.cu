@@ -34,6 +34,7 @@ struct ws_solver {
     bool viscous = false;
     ws_viscous vis{};
     void* vis_ws = nullptr;
+    int next_stage = 1;                      // ws_solver_stage: the stage due next
 };
 
 namespace {
@@ -59,26 +60,35 @@ int enqueue_rhs(ws_solver* s, cudaStream_t st) {
     return launch_du_vis(&g.g, &s->vis, p4, nullptr, g.du, s->vis_ws, true, st);
 }
 
-// one SSP-RK3 step from state buffer c into 1-c; primitives pr[c] -> pr[1-c]
-// (stage 1), pr[1-c] -> pr[c] (stage 2), pr[c] -> pr[1-c] (stage 3)
-int enqueue_step(ws_solver* s, int c, double dt, cudaStream_t st) {
+// primitives that stage krk of a step from state buffer c reads
+const ws_field* stage_input(const GridState& g, int c, int krk) {
+    return g.pr[krk == 2 ? 1 - c : c];
+}
+
+// stage krk of the SSP-RK3 step from state buffer c into 1-c; primitives
+// pr[c] -> pr[1-c] (stage 1), pr[1-c] -> pr[c] (stage 2), pr[c] -> pr[1-c]
+// (stage 3)
+int enqueue_stage(ws_solver* s, int c, int krk, double dt, cudaStream_t st) {
     GridState& g = s->s;
-    for (int krk = 1; krk <= 3; ++krk) {
-        const ws_field* pin = g.pr[krk == 2 ? 1 - c : c];
-        const ws_field* pout = g.pr[krk == 2 ? c : 1 - c];
-        int rc = launch_ghost_fill_prims(&g.g, pin, st);
+    const ws_field* pin = stage_input(g, c, krk);
+    const ws_field* pout = g.pr[krk == 2 ? c : 1 - c];
+    int rc = launch_ghost_fill_prims(&g.g, pin, st);
+    if (rc) return rc;
+    ws_soa dvis{};
+    if (s->viscous) {   // viscous terms of the stage's input into du
+        const ws_field p4[4] = {pin[1], pin[2], pin[3], pin[4]};
+        rc = launch_du_vis(&g.g, &s->vis, p4, nullptr, g.du, s->vis_ws, false, st);
         if (rc) return rc;
-        ws_soa dvis{};
-        if (s->viscous) {   // viscous terms of the stage's input into du
-            const ws_field p4[4] = {pin[1], pin[2], pin[3], pin[4]};
-            rc = launch_du_vis(&g.g, &s->vis, p4, nullptr, g.du, s->vis_ws, false, st);
-            if (rc) return rc;
-            dvis = g.du;
-        }
-        rc = rhs_stage_enqueue(&g.g, pin, g.f[1 - c], g.f[c], g.f[1 - c], pout, dt, krk,
-                               g.status, dvis, s->tile, st);
-        if (rc) return rc;
+        dvis = g.du;
     }
+    return rhs_stage_enqueue(&g.g, pin, g.f[1 - c], g.f[c], g.f[1 - c], pout, dt, krk,
+                             g.status, dvis, s->tile, st);
+}
+
+// one SSP-RK3 step from state buffer c into 1-c
+int enqueue_step(ws_solver* s, int c, double dt, cudaStream_t st) {
+    for (int krk = 1; krk <= 3; ++krk)
+        if (int rc = enqueue_stage(s, c, krk, dt, st)) return rc;
     return WS_OK;
 }
 
@@ -159,6 +169,8 @@ int ws_solver_set_viscous(ws_solver* s, const ws_viscous* vis) {
         return WS_OK;
     }
     if (int rc = check_viscous(vis)) return rc;
+    if (has_external(&s->s.g))
+        return fail(WS_ERR_UNSUPPORTED, "viscous terms on a grid with EXTERNAL faces");
     if (!s->vis_ws) {
         WS_CUDA(cudaMalloc(&s->vis_ws, vis_workspace_bytes(&s->s.g)));
         WS_CUDA(cudaMemset(s->vis_ws, 0, vis_workspace_bytes(&s->s.g)));
@@ -202,6 +214,7 @@ int ws_solver_load(ws_solver* s, const char* path, int32_t* istep, double* tt,
         f[c] = d; f[n + c] = u * d; f[2 * n + c] = v * d; f[3 * n + c] = w * d;
         f[4 * n + c] = d * ((u * u + v * v + w * w) * 0.5 + cv * p[4 * n + c]);
     }
+    s->next_stage = 1;
     rc = grid_state_upload(s->s, f.data(), (cudaStream_t)stream);
     if (rc) return rc;
     WS_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
@@ -210,6 +223,7 @@ int ws_solver_load(ws_solver* s, const char* path, int32_t* istep, double* tt,
 
 int ws_solver_set_state(ws_solver* s, const double* f_host, ws_stream_t stream) {
     if (!s || !f_host) return fail(WS_ERR_INVALID, "NULL argument");
+    s->next_stage = 1;
     return grid_state_upload(s->s, f_host, (cudaStream_t)stream);
 }
 
@@ -264,6 +278,10 @@ int ws_solver_compute_dt(ws_solver* s, double cfl, double* dt, ws_stream_t strea
 int ws_solver_step(ws_solver* s, double dt, int nsteps, ws_stream_t stream) {
     if (!s) return fail(WS_ERR_INVALID, "solver is NULL");
     if (nsteps < 0 || !(dt > 0)) return fail(WS_ERR_INVALID, "need dt > 0 and nsteps >= 0");
+    if (has_external(&s->s.g))
+        return fail(WS_ERR_UNSUPPORTED, "a grid with EXTERNAL faces steps by stages "
+                                        "(ws_solver_stage) with a halo exchange before each");
+    if (s->next_stage != 1) return fail(WS_ERR_INVALID, "a staged step is in progress");
     if (!s->exec[0] || s->graph_dt != dt) {
         int rc = capture(s, dt);
         if (rc) return rc;
@@ -272,6 +290,31 @@ int ws_solver_step(ws_solver* s, double dt, int nsteps, ws_stream_t stream) {
     for (int i = 0; i < nsteps; ++i) {
         WS_CUDA(cudaGraphLaunch(s->exec[s->s.cur], st));
         s->s.cur ^= 1;
+    }
+    return WS_OK;
+}
+
+int ws_solver_stage_fields(ws_solver* s, int krk, ws_field prims[6]) {
+    if (!s || !prims) return fail(WS_ERR_INVALID, "NULL argument");
+    if (krk < 1 || krk > 3) return fail(WS_ERR_INVALID, "krk must be 1, 2 or 3");
+    const ws_field* p = stage_input(s->s, s->s.cur, krk);
+    for (int i = 0; i < 6; ++i) prims[i] = p[i];
+    return WS_OK;
+}
+
+int ws_solver_stage(ws_solver* s, int krk, double dt, ws_stream_t stream) {
+    if (!s) return fail(WS_ERR_INVALID, "solver is NULL");
+    if (!(dt > 0)) return fail(WS_ERR_INVALID, "need dt > 0");
+    if (krk != s->next_stage)
+        return fail(WS_ERR_INVALID, "stage " + std::to_string(krk) + " called when stage " +
+                                        std::to_string(s->next_stage) + " is due");
+    int rc = enqueue_stage(s, s->s.cur, krk, dt, (cudaStream_t)stream);
+    if (rc) return rc;
+    if (krk == 3) {
+        s->s.cur ^= 1;
+        s->next_stage = 1;
+    } else {
+        s->next_stage = krk + 1;
     }
     return WS_OK;
 }

@@ -14,6 +14,12 @@ namespace ws {
 // Grid checks shared by every entry point (extents, constants, face kinds,
 // precision); WS_OK or the error code with its message set.
 int validate_grid(const ws_grid* g);
+// any face of kind WS_FACE_EXTERNAL (ghosts written by the caller's halo exchange)
+bool has_external(const ws_grid* g);
+// 4 x planes of nf LAP fields <-> halo buffer [nf][nz][ny][4]: pack reads the
+// interior planes next to face `side`, unpack writes the ghost planes beyond it
+int launch_halo_x(const ws_grid* g, const ws_field* f, int nf, int side, double* buf, bool pack,
+                  cudaStream_t st);
 
 // Error reporting: the message of the last failure, per host thread.
 void set_error(const std::string& msg);
