@@ -14,8 +14,8 @@
 //   vis_div_kernel: one pass adds J * d(Ev_dir)/d(dir) of the three
 //     directions to du[1..4] (or stores it, for the fused RK stage), x then y
 //     then z as the reference accumulates.
-// Memory-bound: per cell ~32 B of primitives in (stencil re-reads hit L1/L2),
-// 96 B of fluxes out and in again, 32-64 B of du.
+// Memory-bound: per cell ~32 B of primitives in, 96 B of fluxes out and in
+// again, 32-64 B of du.
 #include "ws_internal.h"
 
 namespace ws {
@@ -31,7 +31,7 @@ struct VisArgs {
     double* du;                // SoA [5][nz][ny][du_pitch]
     uint32_t du_pitch, du_ly, du_lz;
     int nx, ny, nz;
-    double rh[3];              // 1/h
+    double rh[3];              // 1 / (h * the difference's divisor: 60 CD6, 840 CD8)
     double tsb, amu_c0, vfc;   // Sutherland constants, Cp/Pr
     int uniform, accumulate;
 };
@@ -40,118 +40,327 @@ __device__ __forceinline__ size_t lapi(int X, int Y, int Z, uint32_t pitch, int 
     return (size_t)X + (size_t)pitch * ((size_t)Y + (size_t)(ny + 8) * (size_t)Z);
 }
 
-// central first difference (times h) along DIR at LAP point (X, Y, Z):
-// OCFD_Schemes.cpp:97-104 (CD6) and :134-142 (CD8)
-template <int R, int DIR>
-__device__ __forceinline__ double cdiff(const double* f, uint32_t pitch, int ny, int X, int Y,
-                                        int Z) {
-    const long s = DIR == 0 ? 1 : DIR == 1 ? (long)pitch : (long)pitch * (ny + 8);
-    const double* c = f + lapi(X, Y, Z, pitch, ny);
-    if (R == 3)
-        return (45.0 * (__ldg(c + s) - __ldg(c - s)) - 9.0 * (__ldg(c + 2 * s) - __ldg(c - 2 * s)) +
-                (__ldg(c + 3 * s) - __ldg(c - 3 * s))) / 60.0;
-    return (672.0 * (__ldg(c + s) - __ldg(c - s)) - 168.0 * (__ldg(c + 2 * s) - __ldg(c - 2 * s)) +
-            32.0 * (__ldg(c + 3 * s) - __ldg(c - 3 * s)) -
-            3.0 * (__ldg(c + 4 * s) - __ldg(c - 4 * s))) / 840.0;
+// Both passes march in z over a tile of VBX x VBY columns, one thread per
+// column, as the fused RHS sweep does: a z derivative takes its nine values
+// from the thread's own window of planes (shared memory, private to the
+// thread, so no barrier guards it), x and y derivatives from a tile of the
+// current plane with an R-cell rim staged by the whole block.  Each plane is
+// read from HBM once (the rims and the window's lead plane come back through
+// L2), instead of 8-point stencils re-read through the caches per point.
+// Loads for the next plane are issued into registers before the current
+// plane's arithmetic.  Work items are (column tile, chunk of VZC planes),
+// chunk-major, so the blocks in flight share their rims and planes in L2.
+constexpr int VBX = 32, VBY = 8, VNT = VBX * VBY, VZC = 16;
+
+// central first difference of the 2R values c[-R*s .. R*s], times the
+// divisor of OCFD_Schemes.cpp:97-104 (CD6: /60) and :134-142 (CD8: /840),
+// which the caller folds into its 1/h factor (one multiply instead of an
+// IEEE division per derivative)
+template <int R>
+__device__ __forceinline__ double cd(const double* c, int s) {
+    if (R == 3) return 45.0 * (c[s] - c[-s]) - 9.0 * (c[2 * s] - c[-2 * s]) + (c[3 * s] - c[-3 * s]);
+    return 672.0 * (c[s] - c[-s]) - 168.0 * (c[2 * s] - c[-2 * s]) +
+           32.0 * (c[3 * s] - c[-3 * s]) - 3.0 * (c[4 * s] - c[-4 * s]);
 }
 
-// Blocks of 32 x 8 threads cover 32 x 8 cells of one plane, so the x and y
-// neighbours of a stencil are mostly read by the same block (L1); the grid
-// strides over the (x tile, y tile, plane) space.
+// the same difference over a window slot ring: w[slot(k + m)] for m = -R..R
 template <int R>
-__global__ void __launch_bounds__(256) vis_flux_kernel(const __grid_constant__ VisArgs a) {
-    const int tx = (a.nx + 31) / 32, ty = (a.ny + 7) / 8;
-    const long ntile = (long)tx * ty * a.nz;
-    for (long b = blockIdx.x; b < ntile; b += gridDim.x) {
-        const int i = (int)(b % tx) * 32 + threadIdx.x % 32;
-        const long r = b / tx;
-        const int j = (int)(r % ty) * 8 + threadIdx.x / 32, k = (int)(r / ty);
-        if (i >= a.nx || j >= a.ny) continue;
-        const int X = i + 4, Y = j + 4, Z = k + 4;
-        // derivatives along the computational directions: g[q][dir]
-        double g[4][3];
+__device__ __forceinline__ double cd_ring(const double* w, int k) {
+    constexpr int W = 2 * R + 1;
+    auto v = [&](int m) { return w[((k + m + 2 * W) % W) * 4 * VNT]; };
+    if (R == 3) return 45.0 * (v(1) - v(-1)) - 9.0 * (v(2) - v(-2)) + (v(3) - v(-3));
+    return 672.0 * (v(1) - v(-1)) - 168.0 * (v(2) - v(-2)) + 32.0 * (v(3) - v(-3)) -
+           3.0 * (v(4) - v(-4));
+}
+
+struct VisItem {
+    int x0, y0, k0, k1;
+};
+
+__device__ __forceinline__ long vis_items(const VisArgs& a) {
+    return (long)((a.nx + VBX - 1) / VBX) * ((a.ny + VBY - 1) / VBY) * ((a.nz + VZC - 1) / VZC);
+}
+
+__device__ __forceinline__ VisItem vis_item(const VisArgs& a, long it) {
+    const int ntx = (a.nx + VBX - 1) / VBX, nty = (a.ny + VBY - 1) / VBY;
+    const long t = it % ((long)ntx * nty);
+    VisItem w;
+    w.x0 = (int)(t % ntx) * VBX;
+    w.y0 = (int)(t / ntx) * VBY;
+    w.k0 = (int)(it / ((long)ntx * nty)) * VZC;
+    w.k1 = min(a.nz, w.k0 + VZC);
+    return w;
+}
+
+template <int R>
+constexpr size_t vis_flux_smem() {
+    return ((size_t)(2 * R + 1) * 4 * VNT + 4 * (VBY + 2 * R) * (VBX + 2 * R)) * sizeof(double);
+}
+template <int R>
+constexpr size_t vis_div_smem() {
+    return ((size_t)(2 * R + 1) * 4 * VNT + 4 * VBY * (VBX + 2 * R) + 4 * (VBY + 2 * R) * VBX) *
+           sizeof(double);
+}
+
+// Gradients of u, v, w, T (CD6/CD8, value / h), the Sutherland viscosity
+// (get_Amu_kernal, commen_kernel.cpp:123-132) and the viscous fluxes
+// Ev1..4 of all three directions (vis_flux_ker, OCFD_NS_Jacobian3d.cpp:477-624)
+// at every interior cell.
+template <int R, bool UNI>
+__global__ void __launch_bounds__(VNT, 2) vis_flux_kernel(const __grid_constant__ VisArgs a) {
+    constexpr int W = 2 * R + 1, TX = VBX + 2 * R, TY = VBY + 2 * R, TYX = TY * TX;
+    constexpr int PS = (TYX + VNT - 1) / VNT;     // tile positions a thread stages per field
+    extern __shared__ double vsm[];
+    double* ring = vsm;                            // [W][4][VNT], own column only
+    double* tile = vsm + W * 4 * VNT;              // [4][TY][TX], plane k with its rim
+    const int tid = threadIdx.x, lx = tid % VBX, ly = tid / VBX;
+    const size_t plane_rows = (size_t)(a.ny + 8);
+    const long items = vis_items(a);
+    for (long it = blockIdx.x; it < items; it += gridDim.x) {
+        const VisItem w = vis_item(a, it);
+        const int i = w.x0 + lx, j = w.y0 + ly;
+        const bool own = i < a.nx && j < a.ny;
+        const int X = min(i, a.nx - 1) + 4, Y = min(j, a.ny - 1) + 4;
+        // in-plane offsets of this thread's column and of its tile positions
+        // (LAP points clamped into the array: the clamped ones belong to no
+        // stencil of an own cell), per field
+        int col[4], so[4][PS];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            g[q][0] = cdiff<R, 0>(a.prim[q], a.ppitch[q], a.ny, X, Y, Z) * a.rh[0];
-            g[q][1] = cdiff<R, 1>(a.prim[q], a.ppitch[q], a.ny, X, Y, Z) * a.rh[1];
-            g[q][2] = cdiff<R, 2>(a.prim[q], a.ppitch[q], a.ny, X, Y, Z) * a.rh[2];
+        for (int q = 0; q < 4; ++q) col[q] = X + (int)a.ppitch[q] * Y;
+#pragma unroll
+        for (int p = 0; p < PS; ++p) {
+            const int t = min(tid + p * VNT, TYX - 1), yy = t / TX, xx = t - yy * TX;
+            const int tx = min(w.x0 - R + xx + 4, a.nx + 7), ty = min(w.y0 - R + yy + 4, a.ny + 7);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) so[q][p] = tx + (int)a.ppitch[q] * ty;
         }
-        double m[9], aj = 1.0;
-        if (a.uniform) {
+        auto plane = [&](int q, int k) {
+            return a.prim[q] + (size_t)a.ppitch[q] * plane_rows * (size_t)(k + 4);
+        };
+        // window: planes k0-R .. k0+R-1, loaded R planes at a time
 #pragma unroll
-            for (int c = 0; c < 9; ++c) m[c] = (c == 0 || c == 4 || c == 8) ? 1.0 : 0.0;
-        } else {
+        for (int h = 0; h < 2; ++h) {
+            double v[R][4];
 #pragma unroll
-            for (int c = 0; c < 9; ++c) m[c] = __ldg(a.met[c] + lapi(X, Y, Z, a.mpitch[c], a.ny));
-            aj = __ldg(a.met[9] + lapi(X, Y, Z, a.mpitch[9], a.ny));
+            for (int m = 0; m < R; ++m)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) v[m][q] = __ldg(plane(q, w.k0 - R + h * R + m) + col[q]);
+#pragma unroll
+            for (int m = 0; m < R; ++m)
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    ring[(((w.k0 - R + h * R + m + 2 * W) % W) * 4 + q) * VNT + tid] = v[m][q];
         }
-        // physical gradients (chain rule with akx..asz)
-        double gx[4], gy[4], gz[4];
+        double lead[4], nt[4][PS];
+        auto prefetch = [&](int k) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            gx[q] = g[q][0] * m[0] + g[q][1] * m[3] + g[q][2] * m[6];
-            gy[q] = g[q][0] * m[1] + g[q][1] * m[4] + g[q][2] * m[7];
-            gz[q] = g[q][0] * m[2] + g[q][1] * m[5] + g[q][2] * m[8];
-        }
-        const double Tc = __ldg(a.prim[3] + lapi(X, Y, Z, a.ppitch[3], a.ny));
-        const double amu = a.amu_c0 * sqrt(Tc * Tc * Tc) / (a.tsb + Tc);
-        const double div = gx[0] + gy[1] + gz[2];
-        const double s11 = (2.0 * gx[0] - 2.0 / 3.0 * div) * amu;
-        const double s22 = (2.0 * gy[1] - 2.0 / 3.0 * div) * amu;
-        const double s33 = (2.0 * gz[2] - 2.0 / 3.0 * div) * amu;
-        const double s12 = (gy[0] + gx[1]) * amu;
-        const double s13 = (gz[0] + gx[2]) * amu;
-        const double s23 = (gz[1] + gy[2]) * amu;
-        const double amuk = amu * a.vfc;
-        const double u = __ldg(a.prim[0] + lapi(X, Y, Z, a.ppitch[0], a.ny));
-        const double v = __ldg(a.prim[1] + lapi(X, Y, Z, a.ppitch[1], a.ny));
-        const double w = __ldg(a.prim[2] + lapi(X, Y, Z, a.ppitch[2], a.ny));
-        const double E1 = u * s11 + v * s12 + w * s13 + amuk * gx[3];
-        const double E2 = u * s12 + v * s22 + w * s23 + amuk * gy[3];
-        const double E3 = u * s13 + v * s23 + w * s33 + amuk * gz[3];
-        const size_t o = lapi(X, Y, Z, a.epitch, a.ny);
+            for (int q = 0; q < 4; ++q) {
+                const double* b = plane(q, k);
+                lead[q] = __ldg(plane(q, k + R) + col[q]);
 #pragma unroll
-        for (int dir = 0; dir < 3; ++dir) {
-            const double kx = m[3 * dir] * aj, ky = m[3 * dir + 1] * aj, kz = m[3 * dir + 2] * aj;
-            a.ev[4 * dir + 0][o] = kx * s11 + ky * s12 + kz * s13;
-            a.ev[4 * dir + 1][o] = kx * s12 + ky * s22 + kz * s23;
-            a.ev[4 * dir + 2][o] = kx * s13 + ky * s23 + kz * s33;
-            a.ev[4 * dir + 3][o] = kx * E1 + ky * E2 + kz * E3;
+                for (int p = 0; p < PS; ++p)
+                    if (tid + p * VNT < TYX) nt[q][p] = __ldg(b + so[q][p]);
+            }
+        };
+        prefetch(w.k0);
+        for (int k = w.k0; k < w.k1; ++k) {
+            __syncthreads();                       // the previous plane's tile is read
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                ring[(((k + R) % W) * 4 + q) * VNT + tid] = lead[q];
+#pragma unroll
+                for (int p = 0; p < PS; ++p)
+                    if (tid + p * VNT < TYX) tile[q * TYX + tid + p * VNT] = nt[q][p];
+            }
+            __syncthreads();
+            if (k + 1 < w.k1) prefetch(k + 1);     // next plane's loads in flight
+            if (!own) continue;
+            double g[4][3];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const double* c = tile + (q * TY + ly + R) * TX + lx + R;
+                g[q][0] = cd<R>(c, 1) * a.rh[0];
+                g[q][1] = cd<R>(c, TX) * a.rh[1];
+                g[q][2] = cd_ring<R>(ring + q * VNT + tid, k) * a.rh[2];
+            }
+            const int Z = k + 4;
+            double m[9], aj = 1.0;
+            if (UNI) {
+#pragma unroll
+                for (int c = 0; c < 9; ++c) m[c] = (c == 0 || c == 4 || c == 8) ? 1.0 : 0.0;
+            } else {
+#pragma unroll
+                for (int c = 0; c < 9; ++c) m[c] = __ldg(a.met[c] + lapi(X, Y, Z, a.mpitch[c], a.ny));
+                aj = __ldg(a.met[9] + lapi(X, Y, Z, a.mpitch[9], a.ny));
+            }
+            // physical gradients (chain rule with akx..asz)
+            double gx[4], gy[4], gz[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                gx[q] = g[q][0] * m[0] + g[q][1] * m[3] + g[q][2] * m[6];
+                gy[q] = g[q][0] * m[1] + g[q][1] * m[4] + g[q][2] * m[7];
+                gz[q] = g[q][0] * m[2] + g[q][1] * m[5] + g[q][2] * m[8];
+            }
+            const double* ctr = tile + (ly + R) * TX + lx + R;
+            const double Tc = ctr[3 * TY * TX];
+            const double amu = a.amu_c0 * sqrt(Tc * Tc * Tc) / (a.tsb + Tc);
+            const double div = gx[0] + gy[1] + gz[2];
+            const double s11 = (2.0 * gx[0] - 2.0 / 3.0 * div) * amu;
+            const double s22 = (2.0 * gy[1] - 2.0 / 3.0 * div) * amu;
+            const double s33 = (2.0 * gz[2] - 2.0 / 3.0 * div) * amu;
+            const double s12 = (gy[0] + gx[1]) * amu;
+            const double s13 = (gz[0] + gx[2]) * amu;
+            const double s23 = (gz[1] + gy[2]) * amu;
+            const double amuk = amu * a.vfc;
+            const double u = ctr[0], v = ctr[TY * TX], wv = ctr[2 * TY * TX];
+            const double E1 = u * s11 + v * s12 + wv * s13 + amuk * gx[3];
+            const double E2 = u * s12 + v * s22 + wv * s23 + amuk * gy[3];
+            const double E3 = u * s13 + v * s23 + wv * s33 + amuk * gz[3];
+            const size_t o = lapi(X, Y, Z, a.epitch, a.ny);
+#pragma unroll
+            for (int dir = 0; dir < 3; ++dir) {
+                const double kx = m[3 * dir] * aj, ky = m[3 * dir + 1] * aj, kz = m[3 * dir + 2] * aj;
+                a.ev[4 * dir + 0][o] = kx * s11 + ky * s12 + kz * s13;
+                a.ev[4 * dir + 1][o] = kx * s12 + ky * s22 + kz * s23;
+                a.ev[4 * dir + 2][o] = kx * s13 + ky * s23 + kz * s33;
+                a.ev[4 * dir + 3][o] = kx * E1 + ky * E2 + kz * E3;
+            }
         }
     }
 }
 
-template <int R>
-__global__ void __launch_bounds__(256) vis_div_kernel(const __grid_constant__ VisArgs a) {
-    const int tx = (a.nx + 31) / 32, ty = (a.ny + 7) / 8;
-    const long ntile = (long)tx * ty * a.nz;
-    for (long b = blockIdx.x; b < ntile; b += gridDim.x) {
-        const int i = (int)(b % tx) * 32 + threadIdx.x % 32;
-        const long r = b / tx;
-        const int j = (int)(r % ty) * 8 + threadIdx.x / 32, k = (int)(r / ty);
-        if (i >= a.nx || j >= a.ny) continue;
-        const int X = i + 4, Y = j + 4, Z = k + 4;
-        const double aj = a.uniform ? 1.0 : __ldg(a.met[9] + lapi(X, Y, Z, a.mpitch[9], a.ny));
+// du[1..4] (+)= J * (d Ev_x/dx + d Ev_y/dy + d Ev_z/dz), x then y then z as
+// the reference accumulates (YF_Pe_XF per direction); du[0] = 0 when storing.
+template <int R, bool UNI>
+__global__ void __launch_bounds__(VNT, 2) vis_div_kernel(const __grid_constant__ VisArgs a) {
+    constexpr int W = 2 * R + 1, XW = VBX + 2 * R, YH = VBY + 2 * R;
+    constexpr int XF = VBY * XW, YF = YH * VBX;               // x-rim, y-rim tile per field
+    constexpr int PX = (XF + VNT - 1) / VNT, PY = (YF + VNT - 1) / VNT;
+    extern __shared__ double vsm[];
+    double* ring = vsm;                            // Ev_z window [W][4][VNT]
+    double* xt = vsm + W * 4 * VNT;                // Ev_x [4][VBY][XW]
+    double* yt = xt + 4 * XF;                      // Ev_y [4][YH][VBX]
+    const int tid = threadIdx.x, lx = tid % VBX, ly = tid / VBX;
+    const size_t eplane = (size_t)a.epitch * (size_t)(a.ny + 8);
+    const long items = vis_items(a);
+    for (long it = blockIdx.x; it < items; it += gridDim.x) {
+        const VisItem w = vis_item(a, it);
+        const int i = w.x0 + lx, j = w.y0 + ly;
+        const bool own = i < a.nx && j < a.ny;
+        const int X = min(i, a.nx - 1) + 4, Y = min(j, a.ny - 1) + 4;
+        // in-plane offsets (the 12 flux fields share one pitch): this column,
+        // the x-rim and y-rim tile positions (clamped into the array)
+        const int col = X + (int)a.epitch * Y;
+        int xo[PX], yo[PY];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            double* d = a.du + (size_t)i +
-                        (size_t)a.du_pitch * ((size_t)j + (size_t)a.du_ly *
-                                                             ((size_t)k + (size_t)a.du_lz * (q + 1)));
-            double acc = a.accumulate ? *d : 0.0;
-            acc += aj * (cdiff<R, 0>(a.ev[q], a.epitch, a.ny, X, Y, Z) * a.rh[0]);
-            acc += aj * (cdiff<R, 1>(a.ev[4 + q], a.epitch, a.ny, X, Y, Z) * a.rh[1]);
-            acc += aj * (cdiff<R, 2>(a.ev[8 + q], a.epitch, a.ny, X, Y, Z) * a.rh[2]);
-            *d = acc;
+        for (int p = 0; p < PX; ++p) {
+            const int t = min(tid + p * VNT, XF - 1), yy = t / XW, xx = t - yy * XW;
+            xo[p] = min(w.x0 - R + xx + 4, a.nx + 7) + (int)a.epitch * (min(w.y0 + yy, a.ny - 1) + 4);
         }
-        if (!a.accumulate)
-            a.du[(size_t)i + (size_t)a.du_pitch * ((size_t)j + (size_t)a.du_ly * (size_t)k)] = 0.0;
+#pragma unroll
+        for (int p = 0; p < PY; ++p) {
+            const int t = min(tid + p * VNT, YF - 1), yy = t / VBX, xx = t - yy * VBX;
+            yo[p] = min(w.x0 + xx, a.nx - 1) + 4 + (int)a.epitch * min(w.y0 - R + yy + 4, a.ny + 7);
+        }
+        auto plane = [&](int c, int k) { return a.ev[c] + eplane * (size_t)(k + 4); };
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            double v[R][4];
+#pragma unroll
+            for (int m = 0; m < R; ++m)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) v[m][q] = __ldg(plane(8 + q, w.k0 - R + h * R + m) + col);
+#pragma unroll
+            for (int m = 0; m < R; ++m)
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    ring[(((w.k0 - R + h * R + m + 2 * W) % W) * 4 + q) * VNT + tid] = v[m][q];
+        }
+        // du of this column (accumulating): the plane's four values, loaded
+        // with the plane's other inputs
+        const size_t du_col = (size_t)min(i, a.nx - 1) + (size_t)a.du_pitch * (size_t)min(j, a.ny - 1);
+        const size_t du_plane = (size_t)a.du_pitch * a.du_ly, du_var = du_plane * a.du_lz;
+        double dn[4] = {0.0, 0.0, 0.0, 0.0}, lead[4], nx_[4][PX], ny_[4][PY];
+        auto prefetch = [&](int k) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if (a.accumulate) dn[q] = a.du[du_col + du_plane * k + du_var * (q + 1)];
+                lead[q] = __ldg(plane(8 + q, k + R) + col);
+                const double* bx = plane(q, k);
+                const double* by = plane(4 + q, k);
+#pragma unroll
+                for (int p = 0; p < PX; ++p)
+                    if (tid + p * VNT < XF) nx_[q][p] = __ldg(bx + xo[p]);
+#pragma unroll
+                for (int p = 0; p < PY; ++p)
+                    if (tid + p * VNT < YF) ny_[q][p] = __ldg(by + yo[p]);
+            }
+        };
+        prefetch(w.k0);
+        for (int k = w.k0; k < w.k1; ++k) {
+            __syncthreads();
+            double dc[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                dc[q] = dn[q];
+                ring[(((k + R) % W) * 4 + q) * VNT + tid] = lead[q];
+#pragma unroll
+                for (int p = 0; p < PX; ++p)
+                    if (tid + p * VNT < XF) xt[q * XF + tid + p * VNT] = nx_[q][p];
+#pragma unroll
+                for (int p = 0; p < PY; ++p)
+                    if (tid + p * VNT < YF) yt[q * YF + tid + p * VNT] = ny_[q][p];
+            }
+            __syncthreads();
+            if (k + 1 < w.k1) prefetch(k + 1);
+            if (!own) continue;
+            const int Z = k + 4;
+            const double aj = UNI ? 1.0 : __ldg(a.met[9] + lapi(X, Y, Z, a.mpitch[9], a.ny));
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                double acc = dc[q];
+                acc += aj * (cd<R>(xt + (q * VBY + ly) * XW + lx + R, 1) * a.rh[0]);
+                acc += aj * (cd<R>(yt + (q * YH + ly + R) * VBX + lx, VBX) * a.rh[1]);
+                acc += aj * (cd_ring<R>(ring + q * VNT + tid, k) * a.rh[2]);
+                a.du[du_col + du_plane * k + du_var * (q + 1)] = acc;
+            }
+            if (!a.accumulate) a.du[du_col + du_plane * k] = 0.0;
+        }
     }
 }
 
-int grid_for(const ws_grid* g) {
-    const long tiles = (long)((g->nx + 31) / 32) * ((g->ny + 7) / 8) * g->nz;
-    return (int)std::max(1L, std::min(tiles, 148L * 8));
+// Resident blocks of a viscous kernel on the current device, with its
+// shared-memory attribute set; computed once per device (0 on failure).
+template <typename K>
+int vis_resident(K kernel, size_t smem, int* cache) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+    if (cache[dev] > 0) return cache[dev];
+    int sms = 0, per = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, VNT, smem) != cudaSuccess)
+        return 0;
+    cache[dev] = sms * per;
+    return cache[dev];
 }
+
+// persistent launch: min(work items, resident blocks)
+template <typename K>
+int launch_vis(K kernel, size_t smem, int* cache, const ws_grid* g, const VisArgs& a,
+               cudaStream_t st) {
+    const int res = vis_resident(kernel, smem, cache);
+    if (res <= 0) return fail(WS_ERR_CUDA, "cannot prepare the viscous kernels");
+    const long items = (long)((g->nx + VBX - 1) / VBX) * ((g->ny + VBY - 1) / VBY) *
+                       ((g->nz + VZC - 1) / VZC);
+    const int blocks = (int)std::max(1L, std::min(items, (long)res));
+    kernel<<<blocks, VNT, smem, st>>>(a);
+    WS_CUDA(cudaGetLastError());
+    return WS_OK;
+}
+
+int flux_cache[4][64], div_cache[4][64];
 
 }  // namespace
 
@@ -186,26 +395,29 @@ int launch_du_vis(const ws_grid* g, const ws_viscous* vis, const ws_field prims[
     a.du_ly = du.length_Y;
     a.du_lz = du.length_Z;
     a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
-    a.rh[0] = 1.0 / g->hx; a.rh[1] = 1.0 / g->hy; a.rh[2] = 1.0 / g->hz;
+    const double dv = vis->scheme == 6 ? 60.0 : 840.0;
+    a.rh[0] = 1.0 / (g->hx * dv); a.rh[1] = 1.0 / (g->hy * dv); a.rh[2] = 1.0 / (g->hz * dv);
     // OCFD_init.cpp:380-396
     const double Cp = 1.0 / ((g->gamma - 1.0) * g->ama * g->ama);
     a.tsb = 110.4 / vis->ref_t;
     a.amu_c0 = 1.0 / vis->re * (1.0 + 110.4 / vis->ref_t);
     a.vfc = Cp / vis->pr;
     a.accumulate = accumulate ? 1 : 0;
-    const int blocks = grid_for(g);
-    if (vis->scheme == 6) vis_flux_kernel<3><<<blocks, 256, 0, st>>>(a);
-    else vis_flux_kernel<4><<<blocks, 256, 0, st>>>(a);
-    WS_CUDA(cudaGetLastError());
+    const bool cd6 = vis->scheme == 6, uni = a.uniform != 0;
+    int rc = cd6 ? (uni ? launch_vis(vis_flux_kernel<3, true>, vis_flux_smem<3>(), flux_cache[0], g, a, st)
+                        : launch_vis(vis_flux_kernel<3, false>, vis_flux_smem<3>(), flux_cache[1], g, a, st))
+                 : (uni ? launch_vis(vis_flux_kernel<4, true>, vis_flux_smem<4>(), flux_cache[2], g, a, st)
+                        : launch_vis(vis_flux_kernel<4, false>, vis_flux_smem<4>(), flux_cache[3], g, a, st));
+    if (rc) return rc;
     ws_field ef[12];
     for (int c = 0; c < 12; ++c) ef[c] = ws_field{a.ev[c], ep, 0};
-    int rc = launch_ghost_fill(g, ef, 8, st);
+    rc = launch_ghost_fill(g, ef, 8, st);
     if (!rc) rc = launch_ghost_fill(g, ef + 8, 4, st);
     if (rc) return rc;
-    if (vis->scheme == 6) vis_div_kernel<3><<<blocks, 256, 0, st>>>(a);
-    else vis_div_kernel<4><<<blocks, 256, 0, st>>>(a);
-    WS_CUDA(cudaGetLastError());
-    return WS_OK;
+    return cd6 ? (uni ? launch_vis(vis_div_kernel<3, true>, vis_div_smem<3>(), div_cache[0], g, a, st)
+                      : launch_vis(vis_div_kernel<3, false>, vis_div_smem<3>(), div_cache[1], g, a, st))
+               : (uni ? launch_vis(vis_div_kernel<4, true>, vis_div_smem<4>(), div_cache[2], g, a, st)
+                      : launch_vis(vis_div_kernel<4, false>, vis_div_smem<4>(), div_cache[3], g, a, st));
 }
 
 int check_viscous(const ws_viscous* vis) {
