@@ -318,6 +318,19 @@ WS_API int  ws_solver_stage(ws_solver* s, int krk, double dt, ws_stream_t stream
 /* The primitive fields d,u,v,w,T,cc that stage krk reads (stage 1: the
  * current state's). */
 WS_API int  ws_solver_stage_fields(ws_solver* s, int krk, ws_field prims[6]);
+/* ws_solver_stage in two halves, for a slab with viscous terms: the first
+ * (ghost fill, viscous flux pass with the fluxes' own ghost fill) and the
+ * second (viscous divergence, fused RHS + stage update).  Between them the
+ * caller exchanges the x halos of the four x-direction viscous fluxes
+ * (ws_solver_stage_flux_fields; they need x ghosts for d/dx), as the
+ * reference exchanges Ev1..4 between vis_flux_ker and its derivatives
+ * (OCFD_Stream.cpp:229-345).  ws_solver_stage with viscous terms on an
+ * EXTERNAL grid returns WS_ERR_UNSUPPORTED. */
+WS_API int  ws_solver_stage_begin(ws_solver* s, int krk, ws_stream_t stream);
+WS_API int  ws_solver_stage_end(ws_solver* s, int krk, double dt, ws_stream_t stream);
+/* The four x-direction viscous flux fields (Ev1..4 of the x direction, LAP)
+ * of the solver's workspace; WS_ERR_INVALID without viscous terms. */
+WS_API int  ws_solver_stage_flux_fields(ws_solver* s, ws_field ev_x[4]);
 /* Device status word (0 or WS_ERR_NONFINITE); synchronises `stream`. */
 WS_API int  ws_solver_status(ws_solver* s, int* status, ws_stream_t stream);
 WS_API int  ws_solver_set_tile(ws_solver* s, ws_tile tile);
@@ -330,7 +343,8 @@ WS_API int  ws_solver_load(ws_solver* s, const char* path, int32_t* istep, doubl
                            ws_stream_t stream);
 /* Navier-Stokes: every RHS adds the viscous terms (NULL: Euler again).  The
  * solver keeps their workspace; the RK stage adds them before its update.
- * WS_ERR_UNSUPPORTED for a grid with WS_FACE_EXTERNAL faces. */
+ * A grid with WS_FACE_EXTERNAL faces then steps with ws_solver_stage_begin /
+ * _end. */
 WS_API int  ws_solver_set_viscous(ws_solver* s, const ws_viscous* vis);
 
 /* ------------------------------------------------------------------------ */

@@ -500,9 +500,13 @@ void or_amu(const or_grid* g, const or_vis* vis, const double* T, double* amu) {
             }
 }
 
-void or_du_vis(const or_grid* g, const or_vis* vis, const double* u, const double* v,
-               const double* w, const double* T, const double* const* metrics,
-               const double* ajac, double* du) {
+// The viscous fluxes of all three directions (vis_flux_ker,
+// OCFD_NS_Jacobian3d.cpp:477-624, per direction) into 12 LAP fields, direction
+// dir component q at ev[(4 * dir + q) * lap_size]; interiors written, ghosts
+// left as they are.
+void or_vis_fluxes(const or_grid* g, const or_vis* vis, const double* u, const double* v,
+                   const double* w, const double* T, const double* const* metrics,
+                   const double* ajac, double* ev) {
     Dims D(g);
     const long N = D.cells();
     const double Cp = 1.0 / ((g->gamma - 1.0) * g->ama * g->ama);
@@ -517,9 +521,8 @@ void or_du_vis(const or_grid* g, const or_vis* vis, const double* u, const doubl
     auto met = [&](int m, long p) {       // akx..asz, Cartesian when metrics == NULL
         return metrics ? metrics[m][p] : (m == 0 || m == 4 || m == 8 ? 1.0 : 0.0);
     };
-    std::vector<double> Ev(4 * D.lap_size()), dv(N);
     for (int dir = 0; dir < 3; ++dir) {
-        std::fill(Ev.begin(), Ev.end(), 0.0);
+        double* Ev = ev + 4 * dir * D.lap_size();
 #pragma omp parallel for collapse(2) schedule(static)
         for (long k = 0; k < D.nz; ++k)
             for (long j = 0; j < D.ny; ++j)
@@ -563,20 +566,40 @@ void or_du_vis(const or_grid* g, const or_vis* vis, const double* u, const doubl
                     Ev[2 * L + p] = (akx * s13 + aky * s23 + akz * s33);
                     Ev[3 * L + p] = (akx * E1 + aky * E2 + akz * E3);
                 }
-        for (int q = 0; q < 4; ++q) {
-            double* e = Ev.data() + q * D.lap_size();
-            or_ghost_fill(g, e);
-            d0_field(g, vis->scheme, dir, e, dv.data());
-#pragma omp parallel for collapse(2) schedule(static)
-            for (long k = 0; k < D.nz; ++k)
-                for (long j = 0; j < D.ny; ++j)
-                    for (long i = 0; i < D.nx; ++i) {
-                        const long c = i + D.nx * (j + D.ny * k);
-                        const double aj = ajac ? ajac[D.lap(i, j, k)] : 1.0;
-                        du[D.soa(i, j, k, q + 1)] += aj * dv[c];
-                    }
-        }
     }
+}
+
+// du[1..4] += J * d(Ev_dir)/d(dir) for one direction (the derivative and
+// YF_Pe_XF accumulation of du_vis_Jacobian3d, OCFD_Stream.cpp:229-345), after
+// the ghost fill of its four flux fields ev4 (4 LAP fields); an EXTERNAL face
+// keeps the halo the caller put there.
+void or_vis_div_add(const or_grid* g, const or_vis* vis, int dir, double* ev4,
+                    const double* ajac, double* du) {
+    Dims D(g);
+    std::vector<double> dv(D.cells());
+    for (int q = 0; q < 4; ++q) {
+        double* e = ev4 + q * D.lap_size();
+        or_ghost_fill(g, e);
+        d0_field(g, vis->scheme, dir, e, dv.data());
+#pragma omp parallel for collapse(2) schedule(static)
+        for (long k = 0; k < D.nz; ++k)
+            for (long j = 0; j < D.ny; ++j)
+                for (long i = 0; i < D.nx; ++i) {
+                    const long c = i + D.nx * (j + D.ny * k);
+                    const double aj = ajac ? ajac[D.lap(i, j, k)] : 1.0;
+                    du[D.soa(i, j, k, q + 1)] += aj * dv[c];
+                }
+    }
+}
+
+void or_du_vis(const or_grid* g, const or_vis* vis, const double* u, const double* v,
+               const double* w, const double* T, const double* const* metrics,
+               const double* ajac, double* du) {
+    Dims D(g);
+    std::vector<double> ev(12 * D.lap_size(), 0.0);
+    or_vis_fluxes(g, vis, u, v, w, T, metrics, ajac, ev.data());
+    for (int dir = 0; dir < 3; ++dir)
+        or_vis_div_add(g, vis, dir, ev.data() + 4 * dir * D.lap_size(), ajac, du);
 }
 
 // Inviscid RHS (decomposed form of the BF3W operator), du overwritten.

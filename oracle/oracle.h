@@ -97,6 +97,15 @@ void   or_amu(const or_grid* g, const or_vis* vis, const double* T, double* amu)
 void   or_du_vis(const or_grid* g, const or_vis* vis, const double* u, const double* v,
                  const double* w, const double* T, const double* const* metrics,
                  const double* ajac, double* du);
+/* du_vis in two steps (for subdomains whose x-flux halos come from a
+ * neighbour between them): the 12 viscous flux fields (direction dir,
+ * component q at ev + (4*dir+q)*lap_size, interiors), then per direction the
+ * ghost fill of its 4 fields and du[1..4] += J * d(Ev_dir)/d(dir). */
+void   or_vis_fluxes(const or_grid* g, const or_vis* vis, const double* u, const double* v,
+                     const double* w, const double* T, const double* const* metrics,
+                     const double* ajac, double* ev);
+void   or_vis_div_add(const or_grid* g, const or_vis* vis, int dir, double* ev4,
+                      const double* ajac, double* du);
 /* Navier-Stokes forms of or_rhs_conserved / or_rk3_steps (vis may be NULL) */
 int    or_rhs_conserved_ns(const or_grid* g, const or_vis* vis, const double* f, double* du,
                            const double* const* metrics, const double* ajac);

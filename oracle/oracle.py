@@ -179,6 +179,20 @@ class Oracle:
                            _ptr_array(metrics), _p(ajac), _p(du))
         return du
 
+    def vis_fluxes(self, g: OrGrid, vis: OrVis, u, v, w, T, metrics=None, ajac=None):
+        """12 viscous flux LAP fields (3*4, nz+8, ny+8, nx+8): direction-major."""
+        shp = (12, g.nz + 2 * LAP, g.ny + 2 * LAP, g.nx + 2 * LAP)
+        ev = np.zeros(shp)
+        self.lib.or_vis_fluxes(C.byref(g), C.byref(vis), _p(u), _p(v), _p(w), _p(T),
+                               _ptr_array(metrics), _p(ajac), _p(ev))
+        return ev
+
+    def vis_div_add(self, g: OrGrid, vis: OrVis, direction: int, ev4: np.ndarray, du,
+                    ajac=None) -> None:
+        """Ghost fill of ev4 (4 LAP fields, in place) and du[1..4] += J d/d(dir)."""
+        assert ev4.flags.c_contiguous and ev4.shape[0] == 4
+        self.lib.or_vis_div_add(C.byref(g), C.byref(vis), direction, _p(ev4), _p(ajac), _p(du))
+
     def rhs_conserved_ns(self, g: OrGrid, vis: OrVis, f: np.ndarray, metrics=None,
                          ajac=None) -> np.ndarray:
         du = np.empty_like(f)

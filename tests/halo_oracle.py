@@ -1,15 +1,17 @@
 """A slab of windstencil_b200.halo stepped by the CPU oracle (test checker).
 
-OracleSlab has CudaSlab's methods (pack / unpack / stage / local_dt /
-set_state / get_state / status), so SlabStepper, LocalExchange and
-DistExchange run unchanged over it: on gloo ranks on the CPU, the
-decomposition, the exchange pattern and the stage sequence of the
+OracleSlab has CudaSlab's methods (send / recv / pack / unpack / begin / end
+/ local_dt / set_state / get_state / set_viscous / status), so SlabStepper,
+LocalExchange and DistExchange run unchanged over it: on gloo ranks on the
+CPU, the decomposition, the exchange pattern and the stage sequence of the
 multi-GPU path are checked against the oracle on the whole grid.
 
 Each stage follows the oracle's rhs_from_cons (oracle/oracle.cpp): prims of
 the stage's state, ghost fill of d, u, v, w, T (EXTERNAL x faces keep the
-unpacked halo), cc = sqrt(T)/ama on the padded field, inviscid RHS, SSP-RK3
-update (OCFD_time.cpp:15-65).
+unpacked halo), cc = sqrt(T)/ama on the padded field, inviscid RHS; with
+viscous terms the 12 flux fields, the x fluxes' halo, and per direction the
+flux ghost fill and divergence added to du; then the SSP-RK3 update
+(OCFD_time.cpp:15-65).
 """
 from __future__ import annotations
 
@@ -17,7 +19,8 @@ import numpy as np
 import torch
 
 from oracle.oracle import make_grid as or_make_grid
-from windstencil_b200.halo import HALO_FIELDS, Slab, slab_grid
+from oracle.oracle import make_vis
+from windstencil_b200.halo import FLUX, FLUX_FIELDS, HALO_FIELDS, PRIMS, Slab, slab_grid
 
 L = 4
 
@@ -30,13 +33,19 @@ class OracleSlab:
         self.grid = g
         self.og = or_make_grid(g.nx, g.ny, g.nz, hx=g.hx, hy=g.hy, hz=g.hz, gamma=g.gamma,
                                ama=g.ama, epsl_sw=g.epsl_sw, face_kind=g.faces)
-        n = HALO_FIELDS * g.nz * g.ny * 4
-        self.send = [torch.zeros(n, dtype=torch.float64) for _ in range(2)]
-        self.recv = [torch.zeros(n, dtype=torch.float64) for _ in range(2)]
-        self.f = None
-        self.fn = None
-        self.prims = None
+        plane = g.nz * g.ny * 4
+        self.n = {PRIMS: HALO_FIELDS * plane, FLUX: FLUX_FIELDS * plane}
+        self._send = [torch.zeros(self.n[PRIMS], dtype=torch.float64) for _ in range(2)]
+        self._recv = [torch.zeros(self.n[PRIMS], dtype=torch.float64) for _ in range(2)]
+        self.f = self.fn = self.prims = self.du = self.ev = None
+        self.vis = None
+        self.viscous = False
         self.krk = 1
+
+    def set_viscous(self, vis):
+        """vis: dict of re, pr, ref_t, scheme (as windstencil_b200.viscous) or None."""
+        self.vis = make_vis(**vis) if vis is not None else None
+        self.viscous = vis is not None
 
     def set_state(self, f_slab):
         self.f = np.array(f_slab, dtype=np.float64, order="C", copy=True)
@@ -46,12 +55,21 @@ class OracleSlab:
     def get_state(self):
         return self.f.copy()
 
+    def send(self, side, kind=PRIMS):
+        return self._send[side][:self.n[kind]]
+
+    def recv(self, side, kind=PRIMS):
+        return self._recv[side][:self.n[kind]]
+
     def _inputs(self):
         if self.prims is None:
             d, u, v, w, T, _ = self.o.cons_to_prim(self.og, self.f)
             cc = self.o.sound_speed(self.og, T)
             self.prims = [d, u, v, w, T, cc]
         return self.prims
+
+    def _fields(self, kind):
+        return self._inputs() if kind == PRIMS else [self.ev[q] for q in range(4)]
 
     def _planes(self, side, ghost):
         g = self.grid
@@ -61,28 +79,37 @@ class OracleSlab:
             x0 = L if side == 0 else g.nx
         return (slice(L, g.nz + L), slice(L, g.ny + L), slice(x0, x0 + 4))
 
-    def pack(self, side):
+    def pack(self, side, kind=PRIMS):
         sl = self._planes(side, ghost=False)
-        buf = np.stack([p[sl] for p in self._inputs()])
-        self.send[side].copy_(torch.from_numpy(buf.reshape(-1)))
+        buf = np.stack([p[sl] for p in self._fields(kind)])
+        self.send(side, kind).copy_(torch.from_numpy(buf.reshape(-1)))
 
-    def unpack(self, side, buf):
+    def unpack(self, side, buf, kind=PRIMS):
         g = self.grid
-        b = buf.cpu().numpy().reshape(HALO_FIELDS, g.nz, g.ny, 4)
+        fields = self._fields(kind)
+        b = buf.cpu().numpy().reshape(len(fields), g.nz, g.ny, 4)
         sl = self._planes(side, ghost=True)
-        for q, p in enumerate(self._inputs()):
+        for q, p in enumerate(fields):
             p[sl] = b[q]
 
-    def stage(self, dt):
+    def begin(self):
         d, u, v, w, T, _ = self._inputs()
         if self.krk == 1:
             self.fn = self.f.copy()
         for p in (d, u, v, w, T):
             self.o.ghost_fill(self.og, p)
         cc = self.o.sound_speed(self.og, T)
-        du = self.o.du_invis(self.og, d, u, v, w, cc)
-        self.o.time_advance(self.krk, dt, self.f, self.fn, du)
-        self.prims = None
+        self.du = self.o.du_invis(self.og, d, u, v, w, cc)
+        if self.viscous:
+            self.ev = self.o.vis_fluxes(self.og, self.vis, u, v, w, T)
+
+    def end(self, dt):
+        if self.viscous:     # du_comput: inviscid, then viscous (OCFD_Stream.cpp:27-45)
+            for direction in range(3):
+                self.o.vis_div_add(self.og, self.vis, direction,
+                                   self.ev[4 * direction:4 * direction + 4], self.du)
+        self.o.time_advance(self.krk, dt, self.f, self.fn, self.du)
+        self.prims = self.du = self.ev = None
         self.krk = self.krk % 3 + 1
 
     def local_dt(self, cfl):

@@ -105,14 +105,35 @@ def test_stage_rules(cuda):
         s.stage(2, 1e-4)                                   # stage 1 is due
     with pytest.raises(ws.WsError, match="WS_ERR_UNSUPPORTED"):
         s.step(1e-4, 1)                                    # EXTERNAL: staged only
-    with pytest.raises(ws.WsError, match="WS_ERR_UNSUPPORTED"):
-        s.set_viscous(ws.viscous())
     s.stage(1, 1e-4)
     s.set_state(wl.fourier_state(16, 16, 16, seed=2))      # a new state restarts at 1
     s.stage(1, 1e-4)
     s.close()
     with pytest.raises(ws.WsError, match="WS_ERR_UNSUPPORTED"):
         ws.Batch([g])
+
+
+def test_stage_halves_rules(cuda):
+    g = ws.Grid(16, 16, 16, faces=(XT, EX, PE, PE, PE, PE))
+    s = ws.Solver(g)
+    s.set_state(wl.fourier_state(16, 16, 16, seed=2))
+    with pytest.raises(ws.WsError, match="WS_ERR_INVALID"):
+        s.stage_flux_fields()                              # no viscous terms
+    with pytest.raises(ws.WsError, match="WS_ERR_INVALID"):
+        s.stage_end(1, 1e-4)                               # end without begin
+    s.set_viscous(ws.viscous())
+    assert len(s.stage_flux_fields()) == 4
+    with pytest.raises(ws.WsError, match="WS_ERR_UNSUPPORTED"):
+        s.stage(1, 1e-4)                                   # the flux halo is needed
+    with pytest.raises(ws.WsError, match="WS_ERR_UNSUPPORTED"):
+        s.rhs()
+    s.stage_begin(1)
+    with pytest.raises(ws.WsError, match="WS_ERR_INVALID"):
+        s.stage_begin(1)                                   # already begun
+    s.stage_end(1, 1e-4)
+    s.stage_begin(2)
+    s.stage_end(2, 1e-4)
+    s.close()
 
 
 CASES = [
@@ -154,3 +175,40 @@ def test_slabs_match_whole_grid(oracle, cuda, case):
     if prec == ws.FP64:
         ref = oracle.rk3_steps(or_grid(*shape, face_kind=faces), f0, dt, nsteps)
         assert rel_linf(got, ref).max() <= 1e-12
+
+
+NS_CASES = [
+    ("ns_periodic_2_cd8", (64, 20, 12), (PE,) * 6, 2, 8),
+    ("ns_extrap_3_cd6", (66, 16, 12), (EX, EX, PE, PE, PE, PE), 3, 6),
+]
+
+
+@pytest.mark.parametrize("case", NS_CASES, ids=[c[0] for c in NS_CASES])
+def test_ns_slabs_match_whole_grid(oracle, cuda, case):
+    """Navier-Stokes on slabs: the stage halo and, between the viscous flux
+    and divergence passes, the x fluxes' halo."""
+    from oracle.oracle import make_vis
+    _, shape, faces, parts, scheme = case
+    vis = dict(re=200.0, pr=0.72, ref_t=288.15, scheme=scheme)
+    g = ws.Grid(*shape, faces=faces)
+    f0 = wl.fourier_state(*shape, seed=23)
+    nsteps = 3
+    whole = ws.Solver(g)
+    whole.set_viscous(vis)
+    whole.set_state(f0)
+    dt = whole.compute_dt(0.3)
+    whole.step(dt, nsteps)
+    want = whole.get_state()
+    whole.close()
+    st = halo.in_process(g, parts)
+    try:
+        st.set_viscous(vis)
+        st.set_state(f0)
+        st.step(dt, nsteps)
+        got = halo.join_state(st.get_state())
+        assert st.status() == 0
+    finally:
+        st.close()
+    assert np.array_equal(got, want), rel_linf(got, want).max()
+    ref = oracle.rk3_steps_ns(or_grid(*shape, face_kind=faces), make_vis(**vis), f0, dt, nsteps)
+    assert rel_linf(got, ref).max() <= 1e-12

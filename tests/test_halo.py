@@ -84,28 +84,38 @@ def test_abi_rejects_external_outside_x():
 
 
 # -- whole runs over oracle slabs --------------------------------------------
+VIS = dict(re=200.0, pr=0.72, ref_t=288.15, scheme=8)
 CASES = {
-    "periodic_2": (Grid(40, 12, 10, faces=(FACE_PERIODIC,) * 6), 2),
-    "periodic_3": (Grid(37, 12, 10, faces=(FACE_PERIODIC,) * 6), 3),
-    "extrap_3": (Grid(36, 12, 10, faces=(FACE_EXTRAP, FACE_EXTRAP) + (FACE_PERIODIC,) * 4), 3),
+    "periodic_2": (Grid(40, 12, 10, faces=(FACE_PERIODIC,) * 6), 2, None),
+    "periodic_3": (Grid(37, 12, 10, faces=(FACE_PERIODIC,) * 6), 3, None),
+    "extrap_3": (Grid(36, 12, 10, faces=(FACE_EXTRAP, FACE_EXTRAP) + (FACE_PERIODIC,) * 4), 3,
+                 None),
     "closure_2": (Grid(32, 12, 10, faces=(FACE_CLOSURE, FACE_CLOSURE, FACE_CLOSURE,
-                                          FACE_CLOSURE, FACE_PERIODIC, FACE_PERIODIC)), 2),
+                                          FACE_CLOSURE, FACE_PERIODIC, FACE_PERIODIC)), 2, None),
+    "ns_periodic_2": (Grid(40, 12, 10, faces=(FACE_PERIODIC,) * 6), 2, VIS),
+    "ns_extrap_3": (Grid(36, 12, 10, faces=(FACE_EXTRAP, FACE_EXTRAP) + (FACE_PERIODIC,) * 4),
+                    3, dict(VIS, scheme=6)),
 }
 NSTEPS = 2
 
 
-def _reference_run(oracle, g, f, nsteps):
+def _reference_run(oracle, g, f, nsteps, vis=None):
+    from oracle.oracle import make_vis
     og = _or_grid(g)
     dt = oracle.compute_dt(og, f, 0.5)
-    return dt, oracle.rk3_steps(og, f, dt, nsteps)
+    if vis is None:
+        return dt, oracle.rk3_steps(og, f, dt, nsteps)
+    return dt, oracle.rk3_steps_ns(og, make_vis(**vis), f, dt, nsteps)
 
 
 @pytest.mark.parametrize("case", sorted(CASES))
 def test_slabs_in_one_process_match_whole_grid(oracle, case):
-    g, parts = CASES[case]
+    g, parts, vis = CASES[case]
     f = _state(g)
-    dt, want = _reference_run(oracle, g, f, NSTEPS)
+    dt, want = _reference_run(oracle, g, f, NSTEPS, vis)
     st = SlabStepper([OracleSlab(oracle, g, s) for s in decompose(g, parts)], LocalExchange())
+    st.set_viscous(vis)
+    assert st.viscous == (vis is not None)
     st.set_state(f)
     assert st.compute_dt(0.5) == dt
     st.step(dt, NSTEPS)
@@ -130,10 +140,11 @@ def _rank_main(rank, world, port, case, out_dir):
     try:
         oracle = Oracle()
         oracle.set_threads(1)
-        g, parts = CASES[case]
+        g, parts, vis = CASES[case]
         assert parts == world
         slab = decompose(g, world)[rank]
         st = SlabStepper([OracleSlab(oracle, g, slab)], DistExchange())
+        st.set_viscous(vis)
         st.set_state(_state(g))
         dt = st.compute_dt(0.5)
         st.step(dt, NSTEPS)
@@ -144,13 +155,15 @@ def _rank_main(rank, world, port, case, out_dir):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("case", ["periodic_2", "periodic_3", "closure_2"])
+@pytest.mark.parametrize("case", ["periodic_2", "periodic_3", "closure_2", "ns_periodic_2",
+                                  "ns_extrap_3"])
 def test_gloo_ranks_match_whole_grid(oracle, case):
     """One slab per gloo rank: DistExchange's sends / receives (a two-rank
-    periodic ring has the same rank on both sides) and the dt reduction."""
-    g, parts = CASES[case]
+    periodic ring has the same rank on both sides), the viscous fluxes' halo
+    and the dt reduction."""
+    g, parts, vis = CASES[case]
     f = _state(g)
-    dt, want = _reference_run(oracle, g, f, NSTEPS)
+    dt, want = _reference_run(oracle, g, f, NSTEPS, vis)
     with tempfile.TemporaryDirectory() as d:
         mp.start_processes(_rank_main, args=(parts, _free_port(), case, d), nprocs=parts,
                            join=True, start_method="spawn")

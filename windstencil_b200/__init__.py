@@ -343,6 +343,20 @@ class Solver:
         check(load().ws_solver_stage_fields(self.h, krk, prims))
         return list(prims)
 
+    def stage_begin(self, krk: int, stream=None):
+        """First half of a stage: ghost fill, viscous flux pass."""
+        check(load().ws_solver_stage_begin(self.h, krk, _stream(stream)))
+
+    def stage_end(self, krk: int, dt: float, stream=None):
+        """Second half: viscous divergence, fused RHS + stage update."""
+        check(load().ws_solver_stage_end(self.h, krk, dt, _stream(stream)))
+
+    def stage_flux_fields(self):
+        """WsField descriptors of the four x-direction viscous fluxes."""
+        ev = (WsField * 4)()
+        check(load().ws_solver_stage_flux_fields(self.h, ev))
+        return list(ev)
+
     def status(self, stream=None) -> int:
         s = C.c_int()
         check(load().ws_solver_status(self.h, C.byref(s), _stream(stream)))

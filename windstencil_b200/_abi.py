@@ -117,6 +117,9 @@ SIGNATURES = {
     "ws_solver_step": (_I, [_P, C.c_double, _I, _P]),
     "ws_solver_stage": (_I, [_P, _I, C.c_double, _P]),
     "ws_solver_stage_fields": (_I, [_P, _I, C.POINTER(WsField)]),
+    "ws_solver_stage_begin": (_I, [_P, _I, _P]),
+    "ws_solver_stage_end": (_I, [_P, _I, C.c_double, _P]),
+    "ws_solver_stage_flux_fields": (_I, [_P, C.POINTER(WsField)]),
     "ws_solver_status": (_I, [_P, C.POINTER(_I), _P]),
     "ws_solver_set_tile": (_I, [_P, WsTile]),
     "ws_solver_set_viscous": (_I, [_P, C.POINTER(WsViscous)]),

@@ -35,6 +35,7 @@ struct ws_solver {
     ws_viscous vis{};
     void* vis_ws = nullptr;
     int next_stage = 1;                      // ws_solver_stage: the stage due next
+    bool stage_begun = false;                // its first half is enqueued
 };
 
 namespace {
@@ -65,24 +66,38 @@ const ws_field* stage_input(const GridState& g, int c, int krk) {
     return g.pr[krk == 2 ? 1 - c : c];
 }
 
-// stage krk of the SSP-RK3 step from state buffer c into 1-c; primitives
+// Stage krk of the SSP-RK3 step from state buffer c into 1-c; primitives
 // pr[c] -> pr[1-c] (stage 1), pr[1-c] -> pr[c] (stage 2), pr[c] -> pr[1-c]
-// (stage 3)
-int enqueue_stage(ws_solver* s, int c, int krk, double dt, cudaStream_t st) {
+// (stage 3).  First half: ghost fill of the stage's input (faces that are
+// not EXTERNAL) and, with viscous terms, their flux pass.
+int enqueue_stage_begin(ws_solver* s, int c, int krk, cudaStream_t st) {
+    GridState& g = s->s;
+    const ws_field* pin = stage_input(g, c, krk);
+    int rc = launch_ghost_fill_prims(&g.g, pin, st);
+    if (rc || !s->viscous) return rc;
+    const ws_field p4[4] = {pin[1], pin[2], pin[3], pin[4]};
+    return launch_vis_flux(&g.g, &s->vis, p4, nullptr, s->vis_ws, st);
+}
+
+// Second half: the viscous terms' divergence into du (stored), then the fused
+// RHS with the stage update, which adds them to the inviscid RHS.
+int enqueue_stage_end(ws_solver* s, int c, int krk, double dt, cudaStream_t st) {
     GridState& g = s->s;
     const ws_field* pin = stage_input(g, c, krk);
     const ws_field* pout = g.pr[krk == 2 ? c : 1 - c];
-    int rc = launch_ghost_fill_prims(&g.g, pin, st);
-    if (rc) return rc;
     ws_soa dvis{};
-    if (s->viscous) {   // viscous terms of the stage's input into du
-        const ws_field p4[4] = {pin[1], pin[2], pin[3], pin[4]};
-        rc = launch_du_vis(&g.g, &s->vis, p4, nullptr, g.du, s->vis_ws, false, st);
+    if (s->viscous) {
+        int rc = launch_vis_div(&g.g, &s->vis, nullptr, g.du, s->vis_ws, false, st);
         if (rc) return rc;
         dvis = g.du;
     }
     return rhs_stage_enqueue(&g.g, pin, g.f[1 - c], g.f[c], g.f[1 - c], pout, dt, krk,
                              g.status, dvis, s->tile, st);
+}
+
+int enqueue_stage(ws_solver* s, int c, int krk, double dt, cudaStream_t st) {
+    int rc = enqueue_stage_begin(s, c, krk, st);
+    return rc ? rc : enqueue_stage_end(s, c, krk, dt, st);
 }
 
 // one SSP-RK3 step from state buffer c into 1-c
@@ -169,8 +184,6 @@ int ws_solver_set_viscous(ws_solver* s, const ws_viscous* vis) {
         return WS_OK;
     }
     if (int rc = check_viscous(vis)) return rc;
-    if (has_external(&s->s.g))
-        return fail(WS_ERR_UNSUPPORTED, "viscous terms on a grid with EXTERNAL faces");
     if (!s->vis_ws) {
         WS_CUDA(cudaMalloc(&s->vis_ws, vis_workspace_bytes(&s->s.g)));
         WS_CUDA(cudaMemset(s->vis_ws, 0, vis_workspace_bytes(&s->s.g)));
@@ -215,6 +228,7 @@ int ws_solver_load(ws_solver* s, const char* path, int32_t* istep, double* tt,
         f[4 * n + c] = d * ((u * u + v * v + w * w) * 0.5 + cv * p[4 * n + c]);
     }
     s->next_stage = 1;
+    s->stage_begun = false;
     rc = grid_state_upload(s->s, f.data(), (cudaStream_t)stream);
     if (rc) return rc;
     WS_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
@@ -224,6 +238,7 @@ int ws_solver_load(ws_solver* s, const char* path, int32_t* istep, double* tt,
 int ws_solver_set_state(ws_solver* s, const double* f_host, ws_stream_t stream) {
     if (!s || !f_host) return fail(WS_ERR_INVALID, "NULL argument");
     s->next_stage = 1;
+    s->stage_begun = false;
     return grid_state_upload(s->s, f_host, (cudaStream_t)stream);
 }
 
@@ -256,6 +271,9 @@ int ws_solver_fields(ws_solver* s, ws_soa* f, ws_soa* du, ws_field prims[6]) {
 
 int ws_solver_rhs(ws_solver* s, ws_stream_t stream) {
     if (!s) return fail(WS_ERR_INVALID, "solver is NULL");
+    if (s->viscous && has_external(&s->s.g))
+        return fail(WS_ERR_UNSUPPORTED, "viscous RHS of an EXTERNAL grid: the x fluxes' "
+                                        "halos come from ws_solver_stage_begin / _end");
     return enqueue_rhs(s, (cudaStream_t)stream);
 }
 
@@ -281,7 +299,8 @@ int ws_solver_step(ws_solver* s, double dt, int nsteps, ws_stream_t stream) {
     if (has_external(&s->s.g))
         return fail(WS_ERR_UNSUPPORTED, "a grid with EXTERNAL faces steps by stages "
                                         "(ws_solver_stage) with a halo exchange before each");
-    if (s->next_stage != 1) return fail(WS_ERR_INVALID, "a staged step is in progress");
+    if (s->next_stage != 1 || s->stage_begun)
+        return fail(WS_ERR_INVALID, "a staged step is in progress");
     if (!s->exec[0] || s->graph_dt != dt) {
         int rc = capture(s, dt);
         if (rc) return rc;
@@ -302,20 +321,65 @@ int ws_solver_stage_fields(ws_solver* s, int krk, ws_field prims[6]) {
     return WS_OK;
 }
 
-int ws_solver_stage(ws_solver* s, int krk, double dt, ws_stream_t stream) {
+namespace {
+int check_stage(ws_solver* s, int krk, bool begun) {
     if (!s) return fail(WS_ERR_INVALID, "solver is NULL");
-    if (!(dt > 0)) return fail(WS_ERR_INVALID, "need dt > 0");
     if (krk != s->next_stage)
         return fail(WS_ERR_INVALID, "stage " + std::to_string(krk) + " called when stage " +
                                         std::to_string(s->next_stage) + " is due");
-    int rc = enqueue_stage(s, s->s.cur, krk, dt, (cudaStream_t)stream);
-    if (rc) return rc;
+    if (s->stage_begun != begun)
+        return fail(WS_ERR_INVALID, begun ? "stage end without its begin"
+                                          : "the stage's first half is already enqueued");
+    return WS_OK;
+}
+
+void advance_stage(ws_solver* s, int krk) {
+    s->stage_begun = false;
     if (krk == 3) {
         s->s.cur ^= 1;
         s->next_stage = 1;
     } else {
         s->next_stage = krk + 1;
     }
+}
+}  // namespace
+
+int ws_solver_stage(ws_solver* s, int krk, double dt, ws_stream_t stream) {
+    if (int rc = check_stage(s, krk, false)) return rc;
+    if (!(dt > 0)) return fail(WS_ERR_INVALID, "need dt > 0");
+    if (s->viscous && has_external(&s->s.g))
+        return fail(WS_ERR_UNSUPPORTED, "with viscous terms an EXTERNAL grid stages in two "
+                                        "halves (ws_solver_stage_begin / _end) with the "
+                                        "x fluxes' halo exchange between them");
+    int rc = enqueue_stage(s, s->s.cur, krk, dt, (cudaStream_t)stream);
+    if (rc) return rc;
+    advance_stage(s, krk);
+    return WS_OK;
+}
+
+int ws_solver_stage_begin(ws_solver* s, int krk, ws_stream_t stream) {
+    if (int rc = check_stage(s, krk, false)) return rc;
+    int rc = enqueue_stage_begin(s, s->s.cur, krk, (cudaStream_t)stream);
+    if (rc) return rc;
+    s->stage_begun = true;
+    return WS_OK;
+}
+
+int ws_solver_stage_end(ws_solver* s, int krk, double dt, ws_stream_t stream) {
+    if (int rc = check_stage(s, krk, true)) return rc;
+    if (!(dt > 0)) return fail(WS_ERR_INVALID, "need dt > 0");
+    int rc = enqueue_stage_end(s, s->s.cur, krk, dt, (cudaStream_t)stream);
+    if (rc) return rc;
+    advance_stage(s, krk);
+    return WS_OK;
+}
+
+int ws_solver_stage_flux_fields(ws_solver* s, ws_field ev_x[4]) {
+    if (!s || !ev_x) return fail(WS_ERR_INVALID, "NULL argument");
+    if (!s->viscous) return fail(WS_ERR_INVALID, "the solver has no viscous terms");
+    ws_field ev[12];
+    vis_flux_fields(&s->s.g, s->vis_ws, ev);
+    for (int q = 0; q < 4; ++q) ev_x[q] = ev[q];
     return WS_OK;
 }
 

@@ -368,15 +368,15 @@ size_t vis_workspace_bytes(const ws_grid* g) {
     return 12 * (size_t)lap_pitch(g->nx) * (g->ny + 8) * (g->nz + 8) * sizeof(double);
 }
 
-// du[1..4] += (accumulate) or = viscous terms; du[0] = 0 when storing.
-// prims: u, v, w, T LAP fields with ghosts filled; ws: vis_workspace_bytes(g).
-int launch_du_vis(const ws_grid* g, const ws_viscous* vis, const ws_field prims[4],
-                  const ws_metrics* m, ws_soa du, void* ws, bool accumulate, cudaStream_t st) {
+namespace {
+VisArgs vis_args(const ws_grid* g, const ws_viscous* vis, const ws_field* prims,
+                 const ws_metrics* m, ws_soa du, void* ws, bool accumulate) {
     VisArgs a{};
-    for (int q = 0; q < 4; ++q) {
-        a.prim[q] = prims[q].ptr;
-        a.ppitch[q] = prims[q].pitch;
-    }
+    if (prims)
+        for (int q = 0; q < 4; ++q) {
+            a.prim[q] = prims[q].ptr;
+            a.ppitch[q] = prims[q].pitch;
+        }
     a.uniform = g->metrics_uniform ? 1 : 0;
     if (!a.uniform) {
         const ws_field* mf = &m->akx;
@@ -385,11 +385,10 @@ int launch_du_vis(const ws_grid* g, const ws_viscous* vis, const ws_field prims[
             a.mpitch[c] = mf[c].pitch;
         }
     }
-    const uint32_t ep = lap_pitch(g->nx);
-    const size_t nlap = (size_t)ep * (g->ny + 8) * (g->nz + 8);
-    double* e = static_cast<double*>(ws);
-    for (int c = 0; c < 12; ++c) a.ev[c] = e + c * nlap;
-    a.epitch = ep;
+    ws_field ef[12];
+    vis_flux_fields(g, ws, ef);
+    for (int c = 0; c < 12; ++c) a.ev[c] = ef[c].ptr;
+    a.epitch = ef[0].pitch;
     a.du = du.ptr;
     a.du_pitch = du.pitch;
     a.du_ly = du.length_Y;
@@ -403,6 +402,20 @@ int launch_du_vis(const ws_grid* g, const ws_viscous* vis, const ws_field prims[
     a.amu_c0 = 1.0 / vis->re * (1.0 + 110.4 / vis->ref_t);
     a.vfc = Cp / vis->pr;
     a.accumulate = accumulate ? 1 : 0;
+    return a;
+}
+}  // namespace
+
+void vis_flux_fields(const ws_grid* g, void* ws, ws_field ev[12]) {
+    const uint32_t ep = lap_pitch(g->nx);
+    const size_t nlap = (size_t)ep * (g->ny + 8) * (g->nz + 8);
+    double* e = static_cast<double*>(ws);
+    for (int c = 0; c < 12; ++c) ev[c] = ws_field{e + c * nlap, ep, 0};
+}
+
+int launch_vis_flux(const ws_grid* g, const ws_viscous* vis, const ws_field prims[4],
+                    const ws_metrics* m, void* ws, cudaStream_t st) {
+    const VisArgs a = vis_args(g, vis, prims, m, ws_soa{}, ws, false);
     const bool cd6 = vis->scheme == 6, uni = a.uniform != 0;
     int rc = cd6 ? (uni ? launch_vis(vis_flux_kernel<3, true>, vis_flux_smem<3>(), flux_cache[0], g, a, st)
                         : launch_vis(vis_flux_kernel<3, false>, vis_flux_smem<3>(), flux_cache[1], g, a, st))
@@ -410,14 +423,27 @@ int launch_du_vis(const ws_grid* g, const ws_viscous* vis, const ws_field prims[
                         : launch_vis(vis_flux_kernel<4, false>, vis_flux_smem<4>(), flux_cache[3], g, a, st));
     if (rc) return rc;
     ws_field ef[12];
-    for (int c = 0; c < 12; ++c) ef[c] = ws_field{a.ev[c], ep, 0};
+    vis_flux_fields(g, ws, ef);
     rc = launch_ghost_fill(g, ef, 8, st);
-    if (!rc) rc = launch_ghost_fill(g, ef + 8, 4, st);
-    if (rc) return rc;
+    return rc ? rc : launch_ghost_fill(g, ef + 8, 4, st);
+}
+
+int launch_vis_div(const ws_grid* g, const ws_viscous* vis, const ws_metrics* m, ws_soa du,
+                   void* ws, bool accumulate, cudaStream_t st) {
+    const VisArgs a = vis_args(g, vis, nullptr, m, du, ws, accumulate);
+    const bool cd6 = vis->scheme == 6, uni = a.uniform != 0;
     return cd6 ? (uni ? launch_vis(vis_div_kernel<3, true>, vis_div_smem<3>(), div_cache[0], g, a, st)
                       : launch_vis(vis_div_kernel<3, false>, vis_div_smem<3>(), div_cache[1], g, a, st))
                : (uni ? launch_vis(vis_div_kernel<4, true>, vis_div_smem<4>(), div_cache[2], g, a, st)
                       : launch_vis(vis_div_kernel<4, false>, vis_div_smem<4>(), div_cache[3], g, a, st));
+}
+
+// du[1..4] += (accumulate) or = viscous terms; du[0] = 0 when storing.
+// prims: u, v, w, T LAP fields with ghosts filled; ws: vis_workspace_bytes(g).
+int launch_du_vis(const ws_grid* g, const ws_viscous* vis, const ws_field prims[4],
+                  const ws_metrics* m, ws_soa du, void* ws, bool accumulate, cudaStream_t st) {
+    int rc = launch_vis_flux(g, vis, prims, m, ws, st);
+    return rc ? rc : launch_vis_div(g, vis, m, du, ws, accumulate, st);
 }
 
 int check_viscous(const ws_viscous* vis) {

@@ -21,9 +21,12 @@ share a process unpack straight from their neighbour's pack buffer.  Each
 slab steps with its fused RHS + stage kernel (ws_solver_stage) on a grid
 whose shared x faces are WS_FACE_EXTERNAL.
 
-The halo carries d, u, v, w, T and cc: every ghost value the stage reads
-(the reference exchanges d, u, v, w, T and recomputes cc on the padded
-field; cc travels here instead of being recomputed).
+The stage's halo carries d, u, v, w, T and cc: every ghost value the stage
+reads (the reference exchanges d, u, v, w, T and recomputes cc on the padded
+field; cc travels here instead of being recomputed).  With viscous terms a
+second halo per stage carries the four x-direction viscous fluxes between
+their flux pass and their divergence, as the reference exchanges Ev1..4
+between vis_flux_ker and their derivatives (OCFD_Stream.cpp:229-345).
 
 This module holds the decomposition, the exchange and the stage sequence;
 the per-slab kernels live in libwindstencil_b200.so (CudaSlab).  Anything
@@ -41,6 +44,8 @@ from . import (FACE_CLOSURE, FACE_EXTERNAL, FACE_PERIODIC, Grid, Solver, halo_pa
                halo_unpack_x, halo_x_bytes)
 
 HALO_FIELDS = 6          # d, u, v, w, T, cc
+FLUX_FIELDS = 4          # x-direction viscous fluxes Ev1..4
+PRIMS, FLUX = "prims", "flux"       # the two halos of a stage
 LO, HI = 0, 1            # x faces of a slab
 
 
@@ -116,18 +121,27 @@ def join_state(parts: list[np.ndarray]) -> np.ndarray:
 
 class CudaSlab:
     """One slab's state and kernels on the current CUDA device: a ws_solver
-    over the slab grid, plus its send and receive halo buffers."""
+    over the slab grid, plus its send and receive halo buffers (sized for the
+    larger halo; the flux halo uses their leading part)."""
 
     def __init__(self, grid: Grid, slab: Slab):
         import torch
         self.slab = slab
         self.grid = slab_grid(grid, slab)
         self.solver = Solver(self.grid)
-        n = halo_x_bytes(self.grid, HALO_FIELDS) // 8
+        self.n = {PRIMS: halo_x_bytes(self.grid, HALO_FIELDS) // 8,
+                  FLUX: halo_x_bytes(self.grid, FLUX_FIELDS) // 8}
         dev = torch.device("cuda", torch.cuda.current_device())
-        self.send = [torch.empty(n, dtype=torch.float64, device=dev) for _ in range(2)]
-        self.recv = [torch.empty(n, dtype=torch.float64, device=dev) for _ in range(2)]
+        self._send = [torch.empty(self.n[PRIMS], dtype=torch.float64, device=dev)
+                      for _ in range(2)]
+        self._recv = [torch.empty(self.n[PRIMS], dtype=torch.float64, device=dev)
+                      for _ in range(2)]
         self.krk = 1     # the stage due next
+        self.viscous = False
+
+    def set_viscous(self, vis) -> None:
+        self.solver.set_viscous(vis)
+        self.viscous = vis is not None
 
     def set_state(self, f_slab: np.ndarray) -> None:
         self.solver.set_state(f_slab)
@@ -136,16 +150,32 @@ class CudaSlab:
     def get_state(self) -> np.ndarray:
         return self.solver.get_state()
 
-    def pack(self, side: int) -> None:
-        """Planes next to face `side` of the due stage's input -> send[side]."""
-        halo_pack_x(self.grid, self.solver.stage_fields(self.krk), side, self.send[side])
+    def send(self, side: int, kind: str = PRIMS):
+        return self._send[side][:self.n[kind]]
 
-    def unpack(self, side: int, buf) -> None:
-        """buf -> ghost planes beyond face `side` of the due stage's input."""
-        halo_unpack_x(self.grid, self.solver.stage_fields(self.krk), side, buf)
+    def recv(self, side: int, kind: str = PRIMS):
+        return self._recv[side][:self.n[kind]]
 
-    def stage(self, dt: float) -> None:
-        self.solver.stage(self.krk, dt)
+    def _fields(self, kind):
+        if kind == PRIMS:
+            return self.solver.stage_fields(self.krk)
+        return self.solver.stage_flux_fields()
+
+    def pack(self, side: int, kind: str = PRIMS) -> None:
+        """Planes next to face `side` of the halo's fields -> send(side, kind)."""
+        halo_pack_x(self.grid, self._fields(kind), side, self.send(side, kind))
+
+    def unpack(self, side: int, buf, kind: str = PRIMS) -> None:
+        """buf -> ghost planes beyond face `side` of the halo's fields."""
+        halo_unpack_x(self.grid, self._fields(kind), side, buf)
+
+    def begin(self) -> None:
+        """First half of the due stage (ghost fill, viscous flux pass)."""
+        self.solver.stage_begin(self.krk)
+
+    def end(self, dt: float) -> None:
+        """Second half (viscous divergence, fused RHS + stage update)."""
+        self.solver.stage_end(self.krk, dt)
         self.krk = self.krk % 3 + 1
 
     def local_dt(self, cfl: float) -> float:
@@ -167,16 +197,16 @@ class LocalExchange:
     access): each slab's ghost planes come straight from its neighbour's
     send buffer; no copy in between."""
 
-    def run(self, runners: list) -> None:
+    def run(self, runners: list, kind: str = PRIMS) -> None:
         by_index = {r.slab.index: r for r in runners}
         for r in runners:
             for side in _sides(r.slab):
-                r.pack(side)
+                r.pack(side, kind)
         for r in runners:
             if r.slab.left is not None:
-                r.unpack(LO, by_index[r.slab.left].send[HI])
+                r.unpack(LO, by_index[r.slab.left].send(HI, kind), kind)
             if r.slab.right is not None:
-                r.unpack(HI, by_index[r.slab.right].send[LO])
+                r.unpack(HI, by_index[r.slab.right].send(LO, kind), kind)
 
     def min(self, x: float) -> float:
         return x
@@ -202,27 +232,31 @@ class DistExchange:
             return index
         return self.dist.get_global_rank(self.group, index)
 
-    def run(self, runners: list) -> None:
+    def run(self, runners: list, kind: str = PRIMS) -> None:
         dist = self.dist
         if len(runners) != 1:
             raise ValueError("DistExchange runs one slab per rank")
         r = runners[0]
         s = r.slab
         for side in _sides(s):
-            r.pack(side)
+            r.pack(side, kind)
         ops = []
         if s.left is not None:
-            ops.append(dist.P2POp(dist.isend, r.send[LO], self._peer(s.left), self.group, LO))
+            ops.append(dist.P2POp(dist.isend, r.send(LO, kind), self._peer(s.left), self.group,
+                                  LO))
         if s.right is not None:
-            ops.append(dist.P2POp(dist.isend, r.send[HI], self._peer(s.right), self.group, HI))
-            ops.append(dist.P2POp(dist.irecv, r.recv[HI], self._peer(s.right), self.group, LO))
+            ops.append(dist.P2POp(dist.isend, r.send(HI, kind), self._peer(s.right), self.group,
+                                  HI))
+            ops.append(dist.P2POp(dist.irecv, r.recv(HI, kind), self._peer(s.right), self.group,
+                                  LO))
         if s.left is not None:
-            ops.append(dist.P2POp(dist.irecv, r.recv[LO], self._peer(s.left), self.group, HI))
+            ops.append(dist.P2POp(dist.irecv, r.recv(LO, kind), self._peer(s.left), self.group,
+                                  HI))
         if ops:
             for w in dist.batch_isend_irecv(ops):
                 w.wait()
         for side in _sides(s):
-            r.unpack(side, r.recv[side])
+            r.unpack(side, r.recv(side, kind), kind)
 
     def min(self, x: float) -> float:
         import torch
@@ -243,9 +277,23 @@ class SlabStepper:
         self.exchange = exchange
 
     def stage(self, dt: float) -> None:
-        self.exchange.run(self.runners)
+        self.exchange.run(self.runners, PRIMS)
         for r in self.runners:
-            r.stage(dt)
+            r.begin()
+        if self.viscous:
+            self.exchange.run(self.runners, FLUX)
+        for r in self.runners:
+            r.end(dt)
+
+    @property
+    def viscous(self) -> bool:
+        return any(r.viscous for r in self.runners)
+
+    def set_viscous(self, vis) -> None:
+        """Navier-Stokes on every slab (ws_viscous constants; None: Euler).
+        Every rank must make the same choice: it adds an exchange per stage."""
+        for r in self.runners:
+            r.set_viscous(vis)
 
     def step(self, dt: float, nsteps: int = 1) -> None:
         if not dt > 0:
