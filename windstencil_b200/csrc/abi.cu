@@ -91,7 +91,11 @@ bool job_empty(ws_job j) {
 // latencies better than 16 within an 80-register budget; mixed 8x8 / 384
 // threads, two CTAs per SM (one CTA's barrier waits overlap the other's
 // arithmetic).
-int default_cfg(int precision) { return precision == WS_MIXED ? 3 : 0; }
+// Measured at 600x128x128 on B200: FP64 16x8/768 either way; the mixed
+// form's plain RHS 8x8/384 (two CTAs per SM), its stage kernel 16x8/768.
+int default_cfg(int precision, bool stage) {
+    return precision == WS_MIXED && !stage ? 3 : 0;
+}
 
 namespace {
 // sweep length cap: unlimited (each persistent CTA sweeps its whole share)
@@ -219,8 +223,8 @@ int rhs_ctas(const ws_grid* g, const RhsArgs& a, int cfg, bool stage) {
     return ctas;
 }
 
-int tile_index(const ws_grid* g, ws_tile tile, int* cfg) {
-    *cfg = default_cfg(g->precision);
+int tile_index(const ws_grid* g, ws_tile tile, bool stage, int* cfg) {
+    *cfg = default_cfg(g->precision, stage);
     if (tile.tile_x || tile.tile_y || tile.threads) {
         *cfg = find_tile_cfg(tile.tile_x, tile.tile_y, tile.threads);
         if (*cfg < 0) return fail(WS_ERR_UNSUPPORTED, "tile shape not compiled in this build");
@@ -232,7 +236,7 @@ int tile_index(const ws_grid* g, ws_tile tile, int* cfg) {
 int rhs_enqueue(const ws_grid* g, ws_job job, const ws_field prims[5], const ws_metrics* m,
                 ws_soa du, ws_tile tile, cudaStream_t st) {
     int cfg = 0;
-    int rc = tile_index(g, tile, &cfg);
+    int rc = tile_index(g, tile, false, &cfg);
     if (rc) return rc;
     const int scan = tile.scan_z > 0 ? tile.scan_z : default_scan(g);
     const RhsArgs a = make_rhs_args(g, job, prims, m, du, cfg, scan);
@@ -248,7 +252,7 @@ int rhs_stage_enqueue(const ws_grid* g, const ws_field p_in[6], ws_soa f_in, ws_
                       ws_soa f_out, const ws_field p_out[6], double dt, int krk, int* status,
                       ws_soa dvis, ws_tile tile, cudaStream_t st) {
     int cfg = 0;
-    int rc = tile_index(g, tile, &cfg);
+    int rc = tile_index(g, tile, true, &cfg);
     if (rc) return rc;
     const int scan = tile.scan_z > 0 ? tile.scan_z : default_scan(g);
     ws_job job{{4, 4, 4}, {g->nx + 4, g->ny + 4, g->nz + 4}};

@@ -325,7 +325,7 @@ int batch_ready(ws_batch* b, cudaStream_t st) {
     if (!b->dirty) return WS_OK;
     std::vector<GridState*> ptrs;
     for (auto& s : b->states) ptrs.push_back(&s);
-    int cfg = default_cfg(b->states.empty() ? WS_FP64 : b->states[0].g.precision);
+    int cfg = default_cfg(b->states.empty() ? WS_FP64 : b->states[0].g.precision, true);
     if (b->tile.tile_x || b->tile.tile_y || b->tile.threads) {
         cfg = find_tile_cfg(b->tile.tile_x, b->tile.tile_y, b->tile.threads);
         if (cfg < 0) return fail(WS_ERR_UNSUPPORTED, "tile shape not compiled in this build");

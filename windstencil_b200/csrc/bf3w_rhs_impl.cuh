@@ -20,10 +20,11 @@
 //     round-trips fpY/fmY/fpZ/fmZ through global scratch).
 //   * Per plane, two barrier intervals:
 //       A: x-split over (BX+8) x BY points and y-split over BX x (BY+8)
-//          points into shared memory, and the z-split of the plane 5 ahead
-//          into the ring;
-//       B: every x, y face of the plane and the z face above it as one work
-//          item (face, variable) evaluating its P and M WENO once;
+//          points into shared memory, the z-split of the plane 5 ahead into
+//          the ring, and (stage mode) the z faces above the plane, whose
+//          stencils are all in the ring already;
+//       B: every x, y face of the plane (and, plain RHS, the z faces) as one
+//          work item (face, variable) evaluating its P and M WENO once;
 //     then the FP64 face difference writes du (no barrier needed before the
 //     next plane's split interval: the arrays are disjoint).
 //   * Primitive planes are staged with TMA tile loads (one thread issues
@@ -68,7 +69,11 @@ struct RhsLayout {
     static constexpr int N_STG = 2 * STG;         // double
     static constexpr int N_FX = 5 * BY * (BX + 1);
     static constexpr int N_FY = 5 * (BY + 1) * BX;
-    static constexpr int N_FZ = 2 * 5 * BXY;
+    // z faces of the last planes: 3 slots in stage mode, whose z faces are
+    // computed in interval A while the previous plane's difference may still
+    // read two slots; 2 for the plain RHS (computed in B)
+    static constexpr int NFZS = EPI ? 3 : 2;
+    static constexpr int N_FZ = NFZS * 5 * BXY;
     static constexpr int N_FB = EPI ? 2 * 15 * BXY : 0;   // fn, f, viscous terms, x2
     static constexpr int N_RING = RING * RS;      // CT
     static constexpr int N_SX = 10 * BY * SXW;    // CT
@@ -322,7 +327,7 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
     double* stg = reinterpret_cast<double*>(smem);       // [2][STG]
     double* fx = stg + L::N_STG;                         // [5][BY][BX+1]
     double* fy = fx + L::N_FX;                           // [5][BY+1][BX]
-    double* fz = fy + L::N_FY;                           // [2][5][BXY]
+    double* fz = fy + L::N_FY;                           // [NFZS][5][BXY]
     double* fb = fz + L::N_FZ;                           // [2][15][BXY]   (stage mode)
     CT* ring = reinterpret_cast<CT*>(fb + L::N_FB);      // [9][10][BXY]
     CT* sxs = ring + L::N_RING;                          // [10][BY][SXW]
@@ -414,8 +419,9 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
             }
         }
         const bool more = z + 1 < z1;
+        ta -= NXS + NYS;
         if (more) {   // plane z+5 enters the ring (slot of plane z-4, last read by face z-1/2)
-            for (ta -= NXS + NYS; ta < BXY; ta += NT) {
+            for (; ta < BXY; ta += NT) {
                 const int col = ta;
                 const double* cb = sb + 5 * BOX + col;
                 const int Z = z + 5;
@@ -427,7 +433,21 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
 #pragma unroll
                 for (int c = 0; c < 10; ++c) dst[c * BXY] = out[c];
             }
+            ta -= BXY;
         }
+        // z face z+1/2 (stencil planes z-3 .. z+4, in the ring since the last
+        // interval) into the next slot.  Stage mode computes it here, beside
+        // the splits (the previous plane's difference may still read the two
+        // previous slots); the plain RHS in interval B (measured faster each
+        // way).
+        const int cur = prev + 1 == L::NFZS ? 0 : prev + 1;
+        constexpr bool ZA = EPI;
+        constexpr unsigned NZF = 5 * BXY;
+        const int s0 = (z - 3) % 9;
+        if (ZA)
+            for (; ta < NZF; ta += NT)
+                fz[cur * 5 * BXY + ta] =
+                    face_flux<CT>(ring + s0 * RS + ta, 5 * BXY, RS, 9 - s0, 9 * RS);
         if (more) {
             if (!tma) {
                 issue_stage<BX, BY, NT>(a, stg + (b ^ 1) * L::STG, x0, y0, z + 1);
@@ -439,14 +459,12 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
         }
         __syncthreads();
 
-        // ---- interval B: faces of plane z and the z face z+1/2
-        const int cur = prev ^ 1;
-        const int s0 = (z - 3) % 9;
+        // ---- interval B: x and y faces of plane z
         // One round robin over the plane's items, split into loops by item
         // kind (no per-item branch chain): the x face right of each column
-        // and the y face above each row (power-of-two index math), the z
-        // faces, then the left/bottom faces of the tile.
-        constexpr unsigned NXR = 5 * BXY, NYR = 5 * BXY, NZF = 5 * BXY;
+        // and the y face above each row (power-of-two index math), then the
+        // left/bottom faces of the tile.
+        constexpr unsigned NXR = 5 * BXY, NYR = 5 * BXY;
         constexpr unsigned NE = 5 * (BY + BX);
         unsigned t = tid;
         const bool clx = CLO && (a.clo[0] | a.clo[1]), cly = CLO && (a.clo[2] | a.clo[3]);
@@ -470,9 +488,14 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
                                         true)
                     : face_flux<CT>(bp, 5 * SYH * BX, BX, 8, 0);
         }
-        for (t -= NYR; t < NZF; t += NT)
-            fz[cur * 5 * BXY + t] = face_flux<CT>(ring + s0 * RS + t, 5 * BXY, RS, 9 - s0, 9 * RS);
-        for (t -= NZF; t < NE; t += NT) {
+        t -= NYR;
+        if (!ZA) {
+            for (; t < NZF; t += NT)
+                fz[cur * 5 * BXY + t] =
+                    face_flux<CT>(ring + s0 * RS + t, 5 * BXY, RS, 9 - s0, 9 * RS);
+            t -= NZF;
+        }
+        for (; t < NE; t += NT) {
             if (t < 5 * BY) {
                 const unsigned var = t / BY, yy = t % BY;
                 const CT* bp = sxs + (var * BY + yy) * SXW;

@@ -265,7 +265,7 @@ void loop(ws_server* s) {
                 const ws_tile& t = s->cfg.tile;
                 const int cfg = (t.tile_x || t.tile_y || t.threads)
                                     ? std::max(0, find_tile_cfg(t.tile_x, t.tile_y, t.threads))
-                                    : default_cfg(p);
+                                    : default_cfg(p, true);
                 s->runner[p].build(g, cfg, t.scan_z, st);
             }
             s->rebuild = false;

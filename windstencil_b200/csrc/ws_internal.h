@@ -104,7 +104,7 @@ struct TileCfg {
 int num_tile_cfgs();
 TileCfg tile_cfg(int i);
 int find_tile_cfg(int bx, int by, int threads);   // index or -1
-int default_cfg(int precision);                   // tuned default shape
+int default_cfg(int precision, bool stage);       // tuned default shape (stage kernel or plain RHS)
 
 // Launch the fused RHS for one grid; cfg indexes the compiled tile shapes.
 // krk == 0: write du; krk in 1..3: fused SSP-RK3 stage epilogue (Cartesian).
