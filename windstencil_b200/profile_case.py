@@ -9,11 +9,14 @@ epilogue), so that a profiler can capture exactly those launches, e.g.
         python -m windstencil_b200.profile_case --nx 600 --ny 128 --nz 64
 
 The default 600x128x64 case holds ~1 GB on the device and its inputs exceed
-the 126 MB L2, so DRAM counters stay meaningful.
+the 126 MB L2, so DRAM counters stay meaningful.  --viscous N adds N
+evaluations of the viscous terms (ws_du_vis_jacobian3d, CD8, Re 1e4) on the
+FP64 grid: the flux pass, the flux ghost fill and the divergence pass.
 """
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 
 
 def main() -> None:
@@ -24,6 +27,7 @@ def main() -> None:
     ap.add_argument("--precision", default="fp64,mixed")
     ap.add_argument("--tile", default="", help="tile_x,tile_y,scan_z,threads")
     ap.add_argument("--step", action="store_true", help="also one SSP-RK3 step")
+    ap.add_argument("--viscous", type=int, default=0, help="viscous-term evaluations")
     a = ap.parse_args()
 
     import torch
@@ -42,6 +46,17 @@ def main() -> None:
         s.rhs()
         if a.step:
             s.step(s.compute_dt(0.5), 1)
+        if a.viscous and prec == ws.FP64:
+            _, du, prims = s.fields()     # descriptors of the solver's state
+            lib, gc = ws.load(), g.c()
+            need = int(lib.ws_du_vis_workspace_bytes(C.byref(gc)))
+            work = torch.zeros(need // 8 + 2, dtype=torch.float64, device="cuda")
+            vis = ws.viscous(re=1.0e4, pr=0.72, ref_t=288.15, scheme=8)
+            for _ in range(a.viscous):
+                ws.check(lib.ws_du_vis_jacobian3d(
+                    C.byref(gc), C.byref(vis), prims[1], prims[2], prims[3], prims[4], None,
+                    du, C.c_void_p(work.data_ptr()), work.numel() * 8,
+                    torch.cuda.current_stream().cuda_stream))
         torch.cuda.synchronize()
         s.close()
     print("ok")
