@@ -214,8 +214,10 @@ class LocalExchange:
 
 class DistExchange:
     """One slab per rank of a torch.distributed group, slab index = group
-    rank: point-to-point sends of the packed planes (NCCL on CUDA tensors,
-    gloo on CPU tensors), issued as one batch.
+    rank: point-to-point sends of the packed planes, issued as one batch.
+    With NCCL the device buffers go straight over NVLink; with a backend
+    that moves host memory only (gloo) device buffers are staged through
+    pinned host copies, as the reference stages its packs for MPI.
 
     Order and tags make a two-slab periodic ring (both neighbours the same
     rank) match as well: sends go low planes first, receives take the high
@@ -226,6 +228,19 @@ class DistExchange:
         import torch.distributed as dist
         self.dist = dist
         self.group = group
+        self.device_p2p = dist.get_backend(group) == "nccl"
+        self._host = {}
+
+    def _staged(self, t, key):
+        """The buffer the transport moves: t itself, or its pinned host twin."""
+        if self.device_p2p or not t.is_cuda:
+            return t
+        h = self._host.get(key)
+        if h is None or h.numel() != t.numel():
+            import torch
+            h = torch.empty(t.numel(), dtype=t.dtype).pin_memory()
+            self._host[key] = h
+        return h
 
     def _peer(self, index: int) -> int:
         if self.group is None:
@@ -238,25 +253,30 @@ class DistExchange:
             raise ValueError("DistExchange runs one slab per rank")
         r = runners[0]
         s = r.slab
-        for side in _sides(s):
+        sides = _sides(s)
+        for side in sides:
             r.pack(side, kind)
+        send = {side: self._staged(r.send(side, kind), ("s", side, kind)) for side in sides}
+        recv = {side: self._staged(r.recv(side, kind), ("r", side, kind)) for side in sides}
+        for side in sides:
+            if send[side] is not r.send(side, kind):
+                send[side].copy_(r.send(side, kind))      # synchronous device -> host
         ops = []
         if s.left is not None:
-            ops.append(dist.P2POp(dist.isend, r.send(LO, kind), self._peer(s.left), self.group,
-                                  LO))
+            ops.append(dist.P2POp(dist.isend, send[LO], self._peer(s.left), self.group, LO))
         if s.right is not None:
-            ops.append(dist.P2POp(dist.isend, r.send(HI, kind), self._peer(s.right), self.group,
-                                  HI))
-            ops.append(dist.P2POp(dist.irecv, r.recv(HI, kind), self._peer(s.right), self.group,
-                                  LO))
+            ops.append(dist.P2POp(dist.isend, send[HI], self._peer(s.right), self.group, HI))
+            ops.append(dist.P2POp(dist.irecv, recv[HI], self._peer(s.right), self.group, LO))
         if s.left is not None:
-            ops.append(dist.P2POp(dist.irecv, r.recv(LO, kind), self._peer(s.left), self.group,
-                                  HI))
+            ops.append(dist.P2POp(dist.irecv, recv[LO], self._peer(s.left), self.group, HI))
         if ops:
             for w in dist.batch_isend_irecv(ops):
                 w.wait()
-        for side in _sides(s):
-            r.unpack(side, r.recv(side, kind), kind)
+        for side in sides:
+            buf = r.recv(side, kind)
+            if recv[side] is not buf:
+                buf.copy_(recv[side], non_blocking=True)  # pinned host -> device, stream-ordered
+            r.unpack(side, buf, kind)
 
     def min(self, x: float) -> float:
         import torch
