@@ -52,25 +52,47 @@ __device__ __forceinline__ size_t lapi(int X, int Y, int Z, uint32_t pitch, int 
 // chunk-major, so the blocks in flight share their rims and planes in L2.
 constexpr int VBX = 32, VBY = 8, VNT = VBX * VBY, VZC = 16;
 
-// central first difference of the 2R values c[-R*s .. R*s], times the
-// divisor of OCFD_Schemes.cpp:97-104 (CD6: /60) and :134-142 (CD8: /840),
+// central first difference from the differences d_m = f(+m) - f(-m), times
+// the divisor of OCFD_Schemes.cpp:97-104 (CD6: /60) and :134-142 (CD8: /840),
 // which the caller folds into its 1/h factor (one multiply instead of an
 // IEEE division per derivative)
 template <int R>
-__device__ __forceinline__ double cd(const double* c, int s) {
-    if (R == 3) return 45.0 * (c[s] - c[-s]) - 9.0 * (c[2 * s] - c[-2 * s]) + (c[3 * s] - c[-3 * s]);
-    return 672.0 * (c[s] - c[-s]) - 168.0 * (c[2 * s] - c[-2 * s]) +
-           32.0 * (c[3 * s] - c[-3 * s]) - 3.0 * (c[4 * s] - c[-4 * s]);
+__device__ __forceinline__ double cdv(double d1, double d2, double d3, double d4) {
+    if (R == 3) return 45.0 * d1 - 9.0 * d2 + d3;
+    return 672.0 * d1 - 168.0 * d2 + 32.0 * d3 - 3.0 * d4;
 }
 
-// the same difference over a window slot ring: w[slot(k + m)] for m = -R..R
+// The kernels keep their fields in shared memory as interleaved pairs
+// (double2: u|v, w|T; Ev1|Ev2, Ev3|Ev4), so one 16-byte load serves a stencil
+// point of two fields: half the shared-memory instructions, which is what
+// limits these passes (the MIO queue), at the same bytes.
+// Differences of a pair along stride s (in double2 elements):
 template <int R>
-__device__ __forceinline__ double cd_ring(const double* w, int k) {
+__device__ __forceinline__ double2 cd2(const double2* c, int s) {
+    double d[2][4] = {};
+#pragma unroll
+    for (int m = 1; m <= R; ++m) {
+        const double2 p = c[m * s], n = c[-m * s];
+        d[0][m - 1] = p.x - n.x;
+        d[1][m - 1] = p.y - n.y;
+    }
+    return make_double2(cdv<R>(d[0][0], d[0][1], d[0][2], d[0][3]),
+                        cdv<R>(d[1][0], d[1][1], d[1][2], d[1][3]));
+}
+
+// the same over a thread's window of planes: w[slot(k + m) * stride]
+template <int R>
+__device__ __forceinline__ double2 cd2_ring(const double2* w, int k, int stride) {
     constexpr int W = 2 * R + 1;
-    auto v = [&](int m) { return w[((k + m + 2 * W) % W) * 4 * VNT]; };
-    if (R == 3) return 45.0 * (v(1) - v(-1)) - 9.0 * (v(2) - v(-2)) + (v(3) - v(-3));
-    return 672.0 * (v(1) - v(-1)) - 168.0 * (v(2) - v(-2)) + 32.0 * (v(3) - v(-3)) -
-           3.0 * (v(4) - v(-4));
+    double d[2][4] = {};
+#pragma unroll
+    for (int m = 1; m <= R; ++m) {
+        const double2 p = w[((k + m + 2 * W) % W) * stride], n = w[((k - m + 2 * W) % W) * stride];
+        d[0][m - 1] = p.x - n.x;
+        d[1][m - 1] = p.y - n.y;
+    }
+    return make_double2(cdv<R>(d[0][0], d[0][1], d[0][2], d[0][3]),
+                        cdv<R>(d[1][0], d[1][1], d[1][2], d[1][3]));
 }
 
 struct VisItem {
@@ -110,9 +132,9 @@ template <int R, bool UNI>
 __global__ void __launch_bounds__(VNT, 2) vis_flux_kernel(const __grid_constant__ VisArgs a) {
     constexpr int W = 2 * R + 1, TX = VBX + 2 * R, TY = VBY + 2 * R, TYX = TY * TX;
     constexpr int PS = (TYX + VNT - 1) / VNT;     // tile positions a thread stages per field
-    extern __shared__ double vsm[];
-    double* ring = vsm;                            // [W][4][VNT], own column only
-    double* tile = vsm + W * 4 * VNT;              // [4][TY][TX], plane k with its rim
+    extern __shared__ __align__(16) double vsm[];
+    double2* ring = reinterpret_cast<double2*>(vsm);   // [W][2][VNT] pairs, own column only
+    double2* tile = ring + W * 2 * VNT;                // [2][TY][TX] pairs, plane k with its rim
     const int tid = threadIdx.x, lx = tid % VBX, ly = tid / VBX;
     const size_t plane_rows = (size_t)(a.ny + 8);
     const long items = vis_items(a);
@@ -148,8 +170,9 @@ __global__ void __launch_bounds__(VNT, 2) vis_flux_kernel(const __grid_constant_
 #pragma unroll
             for (int m = 0; m < R; ++m)
 #pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    ring[(((w.k0 - R + h * R + m + 2 * W) % W) * 4 + q) * VNT + tid] = v[m][q];
+                for (int pr = 0; pr < 2; ++pr)
+                    ring[(((w.k0 - R + h * R + m + 2 * W) % W) * 2 + pr) * VNT + tid] =
+                        make_double2(v[m][2 * pr], v[m][2 * pr + 1]);
         }
         double lead[4], nt[4][PS];
         auto prefetch = [&](int k) {
@@ -166,22 +189,30 @@ __global__ void __launch_bounds__(VNT, 2) vis_flux_kernel(const __grid_constant_
         for (int k = w.k0; k < w.k1; ++k) {
             __syncthreads();                       // the previous plane's tile is read
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                ring[(((k + R) % W) * 4 + q) * VNT + tid] = lead[q];
+            for (int pr = 0; pr < 2; ++pr) {
+                ring[(((k + R) % W) * 2 + pr) * VNT + tid] =
+                    make_double2(lead[2 * pr], lead[2 * pr + 1]);
 #pragma unroll
                 for (int p = 0; p < PS; ++p)
-                    if (tid + p * VNT < TYX) tile[q * TYX + tid + p * VNT] = nt[q][p];
+                    if (tid + p * VNT < TYX)
+                        tile[pr * TYX + tid + p * VNT] =
+                            make_double2(nt[2 * pr][p], nt[2 * pr + 1][p]);
             }
             __syncthreads();
             if (k + 1 < w.k1) prefetch(k + 1);     // next plane's loads in flight
             if (!own) continue;
             double g[4][3];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const double* c = tile + (q * TY + ly + R) * TX + lx + R;
-                g[q][0] = cd<R>(c, 1) * a.rh[0];
-                g[q][1] = cd<R>(c, TX) * a.rh[1];
-                g[q][2] = cd_ring<R>(ring + q * VNT + tid, k) * a.rh[2];
+            for (int pr = 0; pr < 2; ++pr) {
+                const double2* c = tile + (pr * TY + ly + R) * TX + lx + R;
+                const double2 dx = cd2<R>(c, 1), dy = cd2<R>(c, TX);
+                const double2 dz = cd2_ring<R>(ring + pr * VNT + tid, k, 2 * VNT);
+                g[2 * pr][0] = dx.x * a.rh[0];
+                g[2 * pr + 1][0] = dx.y * a.rh[0];
+                g[2 * pr][1] = dy.x * a.rh[1];
+                g[2 * pr + 1][1] = dy.y * a.rh[1];
+                g[2 * pr][2] = dz.x * a.rh[2];
+                g[2 * pr + 1][2] = dz.y * a.rh[2];
             }
             const int Z = k + 4;
             double m[9], aj = 1.0;
@@ -201,8 +232,9 @@ __global__ void __launch_bounds__(VNT, 2) vis_flux_kernel(const __grid_constant_
                 gy[q] = g[q][0] * m[1] + g[q][1] * m[4] + g[q][2] * m[7];
                 gz[q] = g[q][0] * m[2] + g[q][1] * m[5] + g[q][2] * m[8];
             }
-            const double* ctr = tile + (ly + R) * TX + lx + R;
-            const double Tc = ctr[3 * TY * TX];
+            const double2* ctr = tile + (ly + R) * TX + lx + R;
+            const double2 uv = ctr[0], wT = ctr[TYX];
+            const double Tc = wT.y;
             const double amu = a.amu_c0 * sqrt(Tc * Tc * Tc) / (a.tsb + Tc);
             const double div = gx[0] + gy[1] + gz[2];
             const double s11 = (2.0 * gx[0] - 2.0 / 3.0 * div) * amu;
@@ -212,7 +244,7 @@ __global__ void __launch_bounds__(VNT, 2) vis_flux_kernel(const __grid_constant_
             const double s13 = (gz[0] + gx[2]) * amu;
             const double s23 = (gz[1] + gy[2]) * amu;
             const double amuk = amu * a.vfc;
-            const double u = ctr[0], v = ctr[TY * TX], wv = ctr[2 * TY * TX];
+            const double u = uv.x, v = uv.y, wv = wT.x;
             const double E1 = u * s11 + v * s12 + wv * s13 + amuk * gx[3];
             const double E2 = u * s12 + v * s22 + wv * s23 + amuk * gy[3];
             const double E3 = u * s13 + v * s23 + wv * s33 + amuk * gz[3];
@@ -236,10 +268,10 @@ __global__ void __launch_bounds__(VNT, 2) vis_div_kernel(const __grid_constant__
     constexpr int W = 2 * R + 1, XW = VBX + 2 * R, YH = VBY + 2 * R;
     constexpr int XF = VBY * XW, YF = YH * VBX;               // x-rim, y-rim tile per field
     constexpr int PX = (XF + VNT - 1) / VNT, PY = (YF + VNT - 1) / VNT;
-    extern __shared__ double vsm[];
-    double* ring = vsm;                            // Ev_z window [W][4][VNT]
-    double* xt = vsm + W * 4 * VNT;                // Ev_x [4][VBY][XW]
-    double* yt = xt + 4 * XF;                      // Ev_y [4][YH][VBX]
+    extern __shared__ __align__(16) double vsm[];
+    double2* ring = reinterpret_cast<double2*>(vsm);   // Ev_z window [W][2][VNT] pairs
+    double2* xt = ring + W * 2 * VNT;                  // Ev_x [2][VBY][XW] pairs
+    double2* yt = xt + 2 * XF;                         // Ev_y [2][YH][VBX] pairs
     const int tid = threadIdx.x, lx = tid % VBX, ly = tid / VBX;
     const size_t eplane = (size_t)a.epitch * (size_t)(a.ny + 8);
     const long items = vis_items(a);
@@ -273,8 +305,9 @@ __global__ void __launch_bounds__(VNT, 2) vis_div_kernel(const __grid_constant__
 #pragma unroll
             for (int m = 0; m < R; ++m)
 #pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    ring[(((w.k0 - R + h * R + m + 2 * W) % W) * 4 + q) * VNT + tid] = v[m][q];
+                for (int pr = 0; pr < 2; ++pr)
+                    ring[(((w.k0 - R + h * R + m + 2 * W) % W) * 2 + pr) * VNT + tid] =
+                        make_double2(v[m][2 * pr], v[m][2 * pr + 1]);
         }
         // du of this column (accumulating): the plane's four values, loaded
         // with the plane's other inputs
@@ -301,15 +334,19 @@ __global__ void __launch_bounds__(VNT, 2) vis_div_kernel(const __grid_constant__
             __syncthreads();
             double dc[4];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                dc[q] = dn[q];
-                ring[(((k + R) % W) * 4 + q) * VNT + tid] = lead[q];
+            for (int q = 0; q < 4; ++q) dc[q] = dn[q];
+#pragma unroll
+            for (int pr = 0; pr < 2; ++pr) {
+                ring[(((k + R) % W) * 2 + pr) * VNT + tid] =
+                    make_double2(lead[2 * pr], lead[2 * pr + 1]);
 #pragma unroll
                 for (int p = 0; p < PX; ++p)
-                    if (tid + p * VNT < XF) xt[q * XF + tid + p * VNT] = nx_[q][p];
+                    if (tid + p * VNT < XF)
+                        xt[pr * XF + tid + p * VNT] = make_double2(nx_[2 * pr][p], nx_[2 * pr + 1][p]);
 #pragma unroll
                 for (int p = 0; p < PY; ++p)
-                    if (tid + p * VNT < YF) yt[q * YF + tid + p * VNT] = ny_[q][p];
+                    if (tid + p * VNT < YF)
+                        yt[pr * YF + tid + p * VNT] = make_double2(ny_[2 * pr][p], ny_[2 * pr + 1][p]);
             }
             __syncthreads();
             if (k + 1 < w.k1) prefetch(k + 1);
@@ -317,12 +354,20 @@ __global__ void __launch_bounds__(VNT, 2) vis_div_kernel(const __grid_constant__
             const int Z = k + 4;
             const double aj = UNI ? 1.0 : __ldg(a.met[9] + lapi(X, Y, Z, a.mpitch[9], a.ny));
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                double acc = dc[q];
-                acc += aj * (cd<R>(xt + (q * VBY + ly) * XW + lx + R, 1) * a.rh[0]);
-                acc += aj * (cd<R>(yt + (q * YH + ly + R) * VBX + lx, VBX) * a.rh[1]);
-                acc += aj * (cd_ring<R>(ring + q * VNT + tid, k) * a.rh[2]);
-                a.du[du_col + du_plane * k + du_var * (q + 1)] = acc;
+            for (int pr = 0; pr < 2; ++pr) {
+                const double2 dx = cd2<R>(xt + (pr * VBY + ly) * XW + lx + R, 1);
+                const double2 dy = cd2<R>(yt + (pr * YH + ly + R) * VBX + lx, VBX);
+                const double2 dz = cd2_ring<R>(ring + pr * VNT + tid, k, 2 * VNT);
+                const double ddx[2] = {dx.x, dx.y}, ddy[2] = {dy.x, dy.y}, ddz[2] = {dz.x, dz.y};
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int q = 2 * pr + h;
+                    double acc = dc[q];
+                    acc += aj * (ddx[h] * a.rh[0]);
+                    acc += aj * (ddy[h] * a.rh[1]);
+                    acc += aj * (ddz[h] * a.rh[2]);
+                    a.du[du_col + du_plane * k + du_var * (q + 1)] = acc;
+                }
             }
             if (!a.accumulate) a.du[du_col + du_plane * k] = 0.0;
         }
