@@ -143,6 +143,13 @@ WS_API int  ws_last_error(char* buf, size_t n);
 /* Elements of the LAP-field row pitch this library allocates for extent nx+8
  * (a multiple of 32). */
 WS_API uint32_t ws_lap_pitch(uint32_t nx);
+/* Device-side errors of the launches that carry no per-grid status word
+ * (the drop-in RHS entry points): bit value 2 = a staging wait of the fused
+ * RHS gave up (bounded wait on its TMA copies) and the launch stopped early,
+ * leaving du incomplete.  Reads and clears the word of the current device;
+ * synchronises `stream`.  The solver, batches and server report the same bit
+ * in their own status words (WS_ERR_TIMEOUT). */
+WS_API int ws_device_error(int* flags, ws_stream_t stream);
 /* Attainable FMA throughput of the current device in TFLOP/s (independent
  * FMA chains on every SM; the roofline denominator of the RHS kernels).
  * Synchronises `stream`.  No reference counterpart (measurement utility). */
@@ -331,7 +338,8 @@ WS_API int  ws_solver_stage_end(ws_solver* s, int krk, double dt, ws_stream_t st
 /* The four x-direction viscous flux fields (Ev1..4 of the x direction, LAP)
  * of the solver's workspace; WS_ERR_INVALID without viscous terms. */
 WS_API int  ws_solver_stage_flux_fields(ws_solver* s, ws_field ev_x[4]);
-/* Device status word (0 or WS_ERR_NONFINITE); synchronises `stream`. */
+/* Device status word: 0, WS_ERR_NONFINITE, or WS_ERR_TIMEOUT (a staging
+ * wait of the fused RHS gave up); synchronises `stream`. */
 WS_API int  ws_solver_status(ws_solver* s, int* status, ws_stream_t stream);
 WS_API int  ws_solver_set_tile(ws_solver* s, ws_tile tile);
 /* Current state to / from a restart file (d, u, v, w, T from / to the
@@ -373,7 +381,7 @@ WS_API int  ws_batch_get_tile(ws_batch* b, ws_tile* tile);
 WS_API int  ws_batch_rhs(ws_batch* b, ws_stream_t stream);
 /* nsteps SSP-RK3 steps of every grid */
 WS_API int  ws_batch_step(ws_batch* b, int nsteps, ws_stream_t stream);
-/* per-grid status (0 or WS_ERR_NONFINITE); synchronises `stream` */
+/* per-grid status (0, WS_ERR_NONFINITE or WS_ERR_TIMEOUT); synchronises `stream` */
 WS_API int  ws_batch_status(ws_batch* b, int* status, ws_stream_t stream);
 /* times the compiled tile shapes on this batch's RHS and keeps the fastest */
 WS_API int  ws_batch_autotune(ws_batch* b, ws_tile* chosen, ws_stream_t stream);

@@ -30,6 +30,7 @@ from ._abi import (FACE_CLOSURE, FACE_EXTERNAL, FACE_EXTRAP, FACE_PERIODIC, FP64
 __all__ = [
     "FACE_CLOSURE", "FACE_EXTERNAL", "FACE_EXTRAP", "FACE_PERIODIC", "FP64", "MIXED", "LAP",
     "WsError", "Grid", "make_grid", "halo_x_bytes", "halo_pack_x", "halo_unpack_x",
+    "device_error",
     "lap_tensor", "soa_tensor", "field_desc", "soa_desc", "interior_job", "du_invis_jacobian3d",
     "du_vis_jacobian3d", "viscous", "restart_write", "restart_read", "metrics_write",
     "metrics_read",
@@ -228,6 +229,14 @@ def ghost_fill(g: Grid, fields, stream=None) -> None:
     gc = g.c()
     arr = (WsField * len(fields))(*[field_desc(t) for t in fields])
     check(load().ws_ghost_fill(C.byref(gc), arr, len(fields), _stream(stream)))
+
+
+def device_error(stream=None) -> int:
+    """Read and clear the device error word of the launches without a
+    per-grid status (ws_device_error): 2 = a staging wait gave up."""
+    v = C.c_int()
+    check(load().ws_device_error(C.byref(v), _stream(stream)))
+    return v.value
 
 
 def halo_x_bytes(g: Grid, nfields: int) -> int:

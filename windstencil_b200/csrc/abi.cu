@@ -9,6 +9,8 @@
 #include <cstring>
 #include <string>
 
+#include <cstdlib>
+
 #include "ws_internal.h"
 
 namespace ws {
@@ -184,6 +186,9 @@ RhsArgs make_rhs_args(const ws_grid* g, ws_job job, const ws_field prims[5],
         tma = encode_lap_map(&a.tm_box[i], g, prims[i], c.bx + 8, c.by + 8) &&
               encode_lap_map(&a.tm_ctr[i], g, prims[i], c.bx, c.by);
     a.tma = tma ? 1 : 0;
+    a.status = device_error_word();     // the stage epilogue sets the grid's own
+    const char* hold = std::getenv("WS_TEST_STAGE_WAIT");
+    a.hold_polls = hold ? std::max(0, std::atoi(hold)) : 0;
     return a;
 }
 
@@ -271,6 +276,21 @@ int rhs_stage_enqueue(const ws_grid* g, const ws_field p_in[6], ws_soa f_in, ws_
 }
 
 int validate_grid(const ws_grid* g) { return check_grid(g); }
+
+// One word per device for the launches that have no per-grid status word.
+__device__ int g_ws_device_error;
+
+int* device_error_word() {
+    static int* cache[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    if (!cache[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_ws_device_error) != cudaSuccess) return nullptr;
+        cache[dev] = static_cast<int*>(p);
+    }
+    return cache[dev];
+}
 
 bool has_external(const ws_grid* g) {
     for (int i = 0; i < 6; ++i)
@@ -374,6 +394,19 @@ int ws_ghost_fill(const ws_grid* g, const ws_field* fields, int nfields, ws_stre
     for (int i = 0; i < nfields; ++i)
         if ((rc = check_field(g, fields[i], "field"))) return rc;
     return launch_ghost_fill(g, fields, nfields, (cudaStream_t)stream);
+}
+
+int ws_device_error(int* flags, ws_stream_t stream) {
+    if (!flags) return fail(WS_ERR_INVALID, "flags is NULL");
+    int* w = device_error_word();
+    if (!w) return fail(WS_ERR_CUDA, "cannot resolve the device error word");
+    cudaStream_t st = (cudaStream_t)stream;
+    int v = 0;
+    WS_CUDA(cudaMemcpyAsync(&v, w, sizeof v, cudaMemcpyDeviceToHost, st));
+    WS_CUDA(cudaMemsetAsync(w, 0, sizeof(int), st));
+    WS_CUDA(cudaStreamSynchronize(st));
+    *flags = v;
+    return WS_OK;
 }
 
 size_t ws_halo_x_bytes(const ws_grid* g, int nfields) {

@@ -93,6 +93,7 @@ void grid_state_free(GridState& s, cudaStream_t st) {
 
 int grid_state_upload(GridState& s, const double* f_host, cudaStream_t st) {
     const size_t n = (size_t)5 * s.g.nx * s.g.ny * s.g.nz;
+    WS_CUDA(cudaMemsetAsync(s.status, 0, sizeof(int), st));     // a new state, a new status
     WS_CUDA(cudaMemcpyAsync(s.f[s.cur].ptr, f_host, n * sizeof(double), cudaMemcpyHostToDevice,
                             st));
     const ws_field* p = s.pr[s.cur];
@@ -478,7 +479,7 @@ int ws_batch_status(ws_batch* b, int* status, ws_stream_t stream) {
         WS_CUDA(cudaMemcpyAsync(&status[i], b->states[i].status, sizeof(int),
                                 cudaMemcpyDeviceToHost, st));
     WS_CUDA(cudaStreamSynchronize(st));
-    for (size_t i = 0; i < b->states.size(); ++i) status[i] = status[i] ? WS_ERR_NONFINITE : WS_OK;
+    for (size_t i = 0; i < b->states.size(); ++i) status[i] = status_code(status[i]);
     return WS_OK;
 }
 

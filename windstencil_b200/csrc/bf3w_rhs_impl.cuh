@@ -274,10 +274,10 @@ __device__ __forceinline__ void issue_stage_tma(const RhsArgs& a, double* s, int
 
 // a staging wait that gave up: recorded in the grid's status word (bit 1)
 // or, for the drop-in path that has none, in this flag
-static __device__ int g_rhs_stage_timeout;
+// status bit 2: a staging wait gave up and the CTA stopped (every launch
+// carries a status word: the grid's own, or the library's device error word)
 __device__ __forceinline__ void report_stage_timeout(const RhsArgs& a) {
     if (a.status) atomicOr(a.status, 2);
-    else atomicOr(&g_rhs_stage_timeout, 1);
 }
 
 // stage mode: cp.async fn (and, after stage 1, f; with viscous terms,
@@ -373,12 +373,19 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
     }
     cp_async_wait<0>();
     {
-        const bool bad = tma && !mbar_wait_bounded(&bar[0], ph & 1u);
-        if (tma) ph ^= 1u;
+        // a.hold_polls > 0 (failure-path test): wait on bar[2], on which
+        // nothing ever arrives, for that many polls, so the timeout path runs
+        const uint32_t want = ph & 1u;
+        bool bad = false;
+        if (tma) {
+            bad = a.hold_polls > 0 ? !mbar_wait_bounded(&bar[2], 0u, a.hold_polls)
+                                   : !mbar_wait_bounded(&bar[0], want);
+            ph ^= 1u;
+        }
         if (__syncthreads_or(bad)) {
             if (tid == 0) {
                 report_stage_timeout(a);
-                mbar_wait_bounded(&bar[0], ph & 1u);   // copies in flight
+                mbar_wait_bounded(&bar[0], want);     // the copies still in flight
             }
             return false;
         }
@@ -519,12 +526,13 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
         cp_async_wait<0>();
         {   // the next plane's staging has landed (TMA: its barrier phase)
             const bool wt = tma && more;
-            const bool bad = wt && !mbar_wait_bounded(&bar[b ^ 1], (ph >> (b ^ 1)) & 1u);
+            const uint32_t want = (ph >> (b ^ 1)) & 1u;
+            const bool bad = wt && !mbar_wait_bounded(&bar[b ^ 1], want);
             if (wt) ph ^= 1u << (b ^ 1);
             if (__syncthreads_or(bad)) {
                 if (tid == 0) {
                     report_stage_timeout(a);
-                    mbar_wait_bounded(&bar[b ^ 1], (ph >> (b ^ 1)) & 1u);   // copies in flight
+                    mbar_wait_bounded(&bar[b ^ 1], want);   // the copies still in flight
                 }
                 return false;
             }
@@ -606,11 +614,13 @@ __device__ __forceinline__ bool run_sweep(const RhsArgs& a, const SplitK<CT>& k,
                                                         first);
 }
 
-// mbarriers of the two staging buffers (TMA path), set up once per CTA
+// mbarriers of the two staging buffers (TMA path) and one nothing arrives on
+// (the failure-path test waits on it), set up once per CTA
 __device__ __forceinline__ void init_stage_barriers(uint64_t* bar) {
     if (threadIdx.x == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
+        mbar_init(&bar[2], 1);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
     __syncthreads();
@@ -623,7 +633,7 @@ __global__ void __launch_bounds__(NT, (RhsLayout<BX, BY, CT, EPI>::MINB))
     // TMA tile destinations must be 128-byte aligned: align explicitly (the
     // launch adds 128 bytes of slack)
     unsigned char* smem_raw = smem_dyn + ((128 - (smem_addr(smem_dyn) & 127)) & 127);
-    __shared__ uint64_t bar[2];
+    __shared__ uint64_t bar[3];
     init_stage_barriers(bar);
     uint32_t ph = 0;
     bool first = true;
@@ -673,7 +683,7 @@ __global__ void __launch_bounds__(NT, (RhsLayout<BX, BY, CT, EPI>::MINB))
     // TMA tile destinations must be 128-byte aligned: align explicitly (the
     // launch adds 128 bytes of slack)
     unsigned char* smem_raw = smem_dyn + ((128 - (smem_addr(smem_dyn) & 127)) & 127);
-    __shared__ uint64_t bar[2];
+    __shared__ uint64_t bar[3];
     init_stage_barriers(bar);
     uint32_t ph = 0;
     const long total = cum[ngrids];

@@ -307,7 +307,7 @@ void loop(ws_server* s) {
                 grid_state_free(q->st, st);
                 s->active.erase(std::find(s->active.begin(), s->active.end(), q));
                 s->active_cells -= cells_of(q);
-                finish(s, q, err ? err : (status[i] ? WS_ERR_NONFINITE : WS_OK));
+                finish(s, q, err ? err : status_code(status[i]));
             }
             s->rebuild = true;
             s->cv_done.notify_all();

@@ -389,7 +389,7 @@ int ws_solver_status(ws_solver* s, int* status, ws_stream_t stream) {
     cudaStream_t st = (cudaStream_t)stream;
     WS_CUDA(cudaMemcpyAsync(&v, s->s.status, sizeof v, cudaMemcpyDeviceToHost, st));
     WS_CUDA(cudaStreamSynchronize(st));
-    *status = v ? WS_ERR_NONFINITE : WS_OK;
+    *status = status_code(v);
     return WS_OK;
 }
 

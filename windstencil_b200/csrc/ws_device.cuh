@@ -415,8 +415,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 // wait for the phase of parity `parity` to complete; false when it has not
 // after a bounded number of polls (each poll may suspend for a while)
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-    for (int i = 0; i < (1 << 22); ++i)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
+                                                  int polls = 1 << 22) {
+    for (int i = 0; i < polls; ++i)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }

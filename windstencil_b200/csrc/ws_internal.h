@@ -14,6 +14,14 @@ namespace ws {
 // Grid checks shared by every entry point (extents, constants, face kinds,
 // precision); WS_OK or the error code with its message set.
 int validate_grid(const ws_grid* g);
+// the library's device error word of the current device (launches without a
+// per-grid status word report into it); NULL when it cannot be resolved
+int* device_error_word();
+// a device status word as an error code: bit 2 (a staging wait gave up) ->
+// WS_ERR_TIMEOUT, bit 1 (non-finite or non-physical state) -> WS_ERR_NONFINITE
+inline int status_code(int v) {
+    return (v & 2) ? WS_ERR_TIMEOUT : v ? WS_ERR_NONFINITE : WS_OK;
+}
 // any face of kind WS_FACE_EXTERNAL (ghosts written by the caller's halo exchange)
 bool has_external(const ws_grid* g);
 // 4 x planes of nf LAP fields <-> halo buffer [nf][nz][ny][4]: pack reads the
@@ -63,6 +71,11 @@ struct RhsArgs {
     // Set only when every box start is 16-byte aligned (even job start x,
     // even pitches, 16-byte aligned fields); otherwise staging uses cp.async.
     int tma;
+    // > 0 only in the failure-path test (environment WS_TEST_STAGE_WAIT):
+    // the first staging wait polls, this many times, an mbarrier nothing
+    // arrives on, so the kernel takes its timeout path (status bit 2, early
+    // stop) without any fault
+    int hold_polls;
     CUtensorMap tm_box[5], tm_ctr[5];
 };
 
