@@ -44,7 +44,7 @@ def test_closure_rhs_fp64(oracle, cuda, faces, shape):
     assert rel_linf(out, ref).max() <= TOL
 
 
-@pytest.mark.parametrize("tile", [(16, 8, 0, 768), (8, 8, 0, 384), (16, 8, 3, 512),
+@pytest.mark.parametrize("tile", [(16, 8, 0, 768), (8, 8, 0, 384), (16, 8, 3, 704),
                                   (8, 8, 5, 256)])
 def test_closure_rhs_tiles(oracle, cuda, tile):
     shape, faces = (37, 21, 9), (CL, CL, CL, CL, PE, PE)

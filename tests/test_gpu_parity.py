@@ -82,8 +82,8 @@ def test_rhs_fp64_general_metrics(oracle, cuda):
     assert rel_linf(out, ref).max() <= TOL
 
 
-@pytest.mark.parametrize("tile", [(16, 8, 1, 768), (16, 8, 5, 512), (16, 8, 32, 768),
-                                  (16, 8, 0, 512), (16, 8, 3, 768), (8, 8, 0, 256),
+@pytest.mark.parametrize("tile", [(16, 8, 1, 768), (16, 8, 5, 704), (16, 8, 32, 768),
+                                  (16, 8, 0, 704), (16, 8, 3, 768), (8, 8, 0, 256),
                                   (8, 8, 7, 384), (8, 8, 0, 384)])
 def test_rhs_tiles_and_scans(oracle, cuda, tile):
     g = ws.Grid(37, 19, 23)

@@ -718,7 +718,7 @@ __global__ void __launch_bounds__(NT, (RhsLayout<BX, BY, CT, EPI>::MINB))
 // ---------------------------------------------------------------------------
 // Compiled tile shapes and per-slice launchers
 // ---------------------------------------------------------------------------
-inline constexpr TileCfg kCfgs[] = {{16, 8, 768}, {16, 8, 512}, {8, 8, 256}, {8, 8, 384}};
+inline constexpr TileCfg kCfgs[] = {{16, 8, 768}, {16, 8, 704}, {8, 8, 256}, {8, 8, 384}};
 inline constexpr int kNumCfgs = sizeof(kCfgs) / sizeof(kCfgs[0]);
 
 template <int BX, int BY, int NT, bool UNI, typename CT, bool EPI, bool CLO>
@@ -808,7 +808,7 @@ int RhsSlice<CT, CLO>::launch(int cfg, const RhsArgs& a, bool uni, int ctas, int
                               cudaStream_t st) {
     switch (cfg) {
         case 0: return launch_t<16, 8, 768>(a, uni, ctas, krk, st);
-        case 1: return launch_t<16, 8, 512>(a, uni, ctas, krk, st);
+        case 1: return launch_t<16, 8, 704>(a, uni, ctas, krk, st);
         case 2: return launch_t<8, 8, 256>(a, uni, ctas, krk, st);
         case 3: return launch_t<8, 8, 384>(a, uni, ctas, krk, st);
         default: return fail(WS_ERR_INVALID, "unknown tile configuration");
@@ -819,7 +819,7 @@ int RhsSlice<CT, CLO>::launch_batch(int cfg, const RhsArgs* g, const long* cum, 
                                     bool uni, int ctas, int krk, cudaStream_t st) {
     switch (cfg) {
         case 0: return batch_t<16, 8, 768>(g, cum, n, zc, uni, ctas, krk, st);
-        case 1: return batch_t<16, 8, 512>(g, cum, n, zc, uni, ctas, krk, st);
+        case 1: return batch_t<16, 8, 704>(g, cum, n, zc, uni, ctas, krk, st);
         case 2: return batch_t<8, 8, 256>(g, cum, n, zc, uni, ctas, krk, st);
         case 3: return batch_t<8, 8, 384>(g, cum, n, zc, uni, ctas, krk, st);
         default: return fail(WS_ERR_INVALID, "unknown tile configuration");
@@ -829,7 +829,7 @@ template <typename CT, bool CLO>
 int RhsSlice<CT, CLO>::max_ctas(int cfg, bool uni, bool stage) {
     switch (cfg) {
         case 0: return max_t<16, 8, 768>(uni, stage);
-        case 1: return max_t<16, 8, 512>(uni, stage);
+        case 1: return max_t<16, 8, 704>(uni, stage);
         case 2: return max_t<8, 8, 256>(uni, stage);
         case 3: return max_t<8, 8, 384>(uni, stage);
         default: return 0;
