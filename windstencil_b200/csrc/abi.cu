@@ -93,13 +93,12 @@ bool job_empty(ws_job j) {
 // latencies better than 16 within an 80-register budget; mixed 8x8 / 384
 // threads, two CTAs per SM (one CTA's barrier waits overlap the other's
 // arithmetic).
-// Measured at 600x128x128 on B200: the stage kernel 16x8/704 in both
-// precisions (its two intervals hold 1216 and 1400 items: 704 threads run
-// each in two nearly full rounds); the plain RHS 16x8/768 in FP64 and 8x8/384
-// (two CTAs per SM) in the mixed form.
+// Measured at 600x128x128 on B200: 16x8 with 704 threads (the sweep's two
+// intervals hold 1216 and 1400 items, which 704 threads run in two nearly
+// full rounds each), except the mixed form's plain RHS, 8x8/384 (two CTAs
+// per SM; 16x8/704 measures the same).
 int default_cfg(int precision, bool stage) {
-    if (stage) return 1;
-    return precision == WS_MIXED ? 3 : 0;
+    return precision == WS_MIXED && !stage ? 3 : 1;
 }
 
 namespace {

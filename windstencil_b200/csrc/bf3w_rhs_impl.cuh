@@ -21,10 +21,10 @@
 //   * Per plane, two barrier intervals:
 //       A: x-split over (BX+8) x BY points and y-split over BX x (BY+8)
 //          points into shared memory, the z-split of the plane 5 ahead into
-//          the ring, and (stage mode) the z faces above the plane, whose
-//          stencils are all in the ring already;
-//       B: every x, y face of the plane (and, plain RHS, the z faces) as one
-//          work item (face, variable) evaluating its P and M WENO once;
+//          the ring, and the z faces above the plane, whose stencils are all
+//          in the ring already (1216 items at 16x8);
+//       B: every x, y face of the plane as one work item (face, variable)
+//          evaluating its P and M WENO once (1400 items at 16x8);
 //     then the FP64 face difference writes du (no barrier needed before the
 //     next plane's split interval: the arrays are disjoint).
 //   * Primitive planes are staged with TMA tile loads (one thread issues
@@ -69,10 +69,9 @@ struct RhsLayout {
     static constexpr int N_STG = 2 * STG;         // double
     static constexpr int N_FX = 5 * BY * (BX + 1);
     static constexpr int N_FY = 5 * (BY + 1) * BX;
-    // z faces of the last planes: 3 slots in stage mode, whose z faces are
-    // computed in interval A while the previous plane's difference may still
-    // read two slots; 2 for the plain RHS (computed in B)
-    static constexpr int NFZS = EPI ? 3 : 2;
+    // z faces of the last 3 planes: a plane's z faces are computed in
+    // interval A while the previous plane's difference may still read two
+    static constexpr int NFZS = 3;
     static constexpr int N_FZ = NFZS * 5 * BXY;
     static constexpr int N_FB = EPI ? 2 * 15 * BXY : 0;   // fn, f, viscous terms, x2
     static constexpr int N_RING = RING * RS;      // CT
@@ -443,18 +442,16 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
             ta -= BXY;
         }
         // z face z+1/2 (stencil planes z-3 .. z+4, in the ring since the last
-        // interval) into the next slot.  Stage mode computes it here, beside
-        // the splits (the previous plane's difference may still read the two
-        // previous slots); the plain RHS in interval B (measured faster each
-        // way).
+        // interval) into the next slot, beside the splits (the previous
+        // plane's difference may still read the two previous slots)
         const int cur = prev + 1 == L::NFZS ? 0 : prev + 1;
-        constexpr bool ZA = EPI;
-        constexpr unsigned NZF = 5 * BXY;
-        const int s0 = (z - 3) % 9;
-        if (ZA)
+        {
+            constexpr unsigned NZF = 5 * BXY;
+            const int s0 = (z - 3) % 9;
             for (; ta < NZF; ta += NT)
                 fz[cur * 5 * BXY + ta] =
                     face_flux<CT>(ring + s0 * RS + ta, 5 * BXY, RS, 9 - s0, 9 * RS);
+        }
         if (more) {
             if (!tma) {
                 issue_stage<BX, BY, NT>(a, stg + (b ^ 1) * L::STG, x0, y0, z + 1);
@@ -495,14 +492,7 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
                                         true)
                     : face_flux<CT>(bp, 5 * SYH * BX, BX, 8, 0);
         }
-        t -= NYR;
-        if (!ZA) {
-            for (; t < NZF; t += NT)
-                fz[cur * 5 * BXY + t] =
-                    face_flux<CT>(ring + s0 * RS + t, 5 * BXY, RS, 9 - s0, 9 * RS);
-            t -= NZF;
-        }
-        for (; t < NE; t += NT) {
+        for (t -= NYR; t < NE; t += NT) {
             if (t < 5 * BY) {
                 const unsigned var = t / BY, yy = t % BY;
                 const CT* bp = sxs + (var * BY + yy) * SXW;
