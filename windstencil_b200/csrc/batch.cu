@@ -91,17 +91,21 @@ void grid_state_free(GridState& s, cudaStream_t st) {
     s.mem = nullptr;
 }
 
-int grid_state_upload(GridState& s, const double* f_host, cudaStream_t st) {
-    const size_t n = (size_t)5 * s.g.nx * s.g.ny * s.g.nz;
-    WS_CUDA(cudaMemsetAsync(s.status, 0, sizeof(int), st));     // a new state, a new status
-    WS_CUDA(cudaMemcpyAsync(s.f[s.cur].ptr, f_host, n * sizeof(double), cudaMemcpyHostToDevice,
-                            st));
+int grid_state_derive(GridState& s, cudaStream_t st) {
     const ws_field* p = s.pr[s.cur];
     int rc = launch_cons_to_prim(&s.g, s.f[s.cur], p[0], p[1], p[2], p[3], p[4],
                                  ws_field{nullptr, 0, 0}, s.status, st);
     if (rc) return rc;
     ws_job job{{4, 4, 4}, {s.g.nx + 4, s.g.ny + 4, s.g.nz + 4}};
     return launch_sound_speed(&s.g, job, p[4], p[5], st);
+}
+
+int grid_state_upload(GridState& s, const double* f_host, cudaStream_t st) {
+    const size_t n = (size_t)5 * s.g.nx * s.g.ny * s.g.nz;
+    WS_CUDA(cudaMemsetAsync(s.status, 0, sizeof(int), st));     // a new state, a new status
+    WS_CUDA(cudaMemcpyAsync(s.f[s.cur].ptr, f_host, n * sizeof(double), cudaMemcpyHostToDevice,
+                            st));
+    return grid_state_derive(s, st);
 }
 
 int grid_state_download(GridState& s, double* f_host, cudaStream_t st) {

@@ -179,13 +179,7 @@ int start_requests(ws_server* s, std::vector<Req*>& fresh) {
                 q->st.f[q->st.cur], g.nx, g.ny, g.nz, g.gamma, g.ama, q->r.synth_mach,
                 q->r.synth_x_jump, q->r.synth_seed);
             WS_CUDA(cudaGetLastError());
-            const ws_field* pr = q->st.prims();
-            rc = launch_cons_to_prim(&g, q->st.f[q->st.cur], pr[0], pr[1], pr[2], pr[3], pr[4],
-                                     ws_field{nullptr, 0, 0}, q->st.status, st);
-            if (!rc) {
-                ws_job job{{4, 4, 4}, {g.nx + 4, g.ny + 4, g.nz + 4}};
-                rc = launch_sound_speed(&g, job, pr[4], pr[5], st);
-            }
+            rc = grid_state_derive(q->st, st);
         }
         if (rc) return rc;
         if (q->r.dt > 0) continue;

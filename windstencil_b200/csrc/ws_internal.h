@@ -187,6 +187,8 @@ void grid_state_free(GridState& s, cudaStream_t st);
 // upload a dense conserved state and derive d,u,v,w,T,cc on the interior
 int grid_state_upload(GridState& s, const double* f_host, cudaStream_t st);
 int grid_state_download(GridState& s, double* f_host, cudaStream_t st);   // no sync
+// d,u,v,w,T,cc (interiors) of the current conserved state f[cur]
+int grid_state_derive(GridState& s, cudaStream_t st);
 
 // A set of grids stepped together: one batched launch per kernel per stage.
 class BatchRunner {
