@@ -82,7 +82,7 @@ def parse():
     ap.add_argument("--serial-grids", type=int, default=32)
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-rate-low", type=float, default=6.0)
-    ap.add_argument("--serve-seconds", type=float, default=20.0)
+    ap.add_argument("--serve-seconds", type=float, default=60.0)    # the configuration's window
     ap.add_argument("--serve-drain", type=float, default=20.0)
     return ap.parse_args()
 
