@@ -119,8 +119,8 @@ constexpr size_t vis_flux_smem() {
     return ((size_t)(2 * R + 1) * 4 * VNT + 4 * (VBY + 2 * R) * (VBX + 2 * R)) * sizeof(double);
 }
 template <int R>
-constexpr size_t vis_div_smem() {
-    return ((size_t)(2 * R + 1) * 4 * VNT + 4 * VBY * (VBX + 2 * R) + 4 * (VBY + 2 * R) * VBX) *
+constexpr size_t vis_div_smem() {   // two buffers of the Ev_x, Ev_y tiles and of du
+    return 2 * ((size_t)4 * VBY * (VBX + 2 * R) + 4 * (VBY + 2 * R) * VBX + 4 * VNT) *
            sizeof(double);
 }
 
@@ -261,17 +261,27 @@ __global__ void __launch_bounds__(VNT, 2) vis_flux_kernel(const __grid_constant_
     }
 }
 
+__device__ __forceinline__ void vcp8(void* smem, const void* gmem) {
+    const uint32_t sa = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void vcp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void vcp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 // du[1..4] (+)= J * (d Ev_x/dx + d Ev_y/dy + d Ev_z/dz), x then y then z as
 // the reference accumulates (YF_Pe_XF per direction); du[0] = 0 when storing.
+// The Ev_z window of a thread's column lives in registers; the next plane's
+// Ev_x / Ev_y tiles (and du, accumulating) arrive by cp.async into the other
+// of two shared-memory buffers while the current plane is processed.
 template <int R, bool UNI>
 __global__ void __launch_bounds__(VNT, 2) vis_div_kernel(const __grid_constant__ VisArgs a) {
     constexpr int W = 2 * R + 1, XW = VBX + 2 * R, YH = VBY + 2 * R;
     constexpr int XF = VBY * XW, YF = YH * VBX;               // x-rim, y-rim tile per field
     constexpr int PX = (XF + VNT - 1) / VNT, PY = (YF + VNT - 1) / VNT;
+    constexpr int BUF = 2 * XF + 2 * YF;                      // double2 per buffer
     extern __shared__ __align__(16) double vsm[];
-    double2* ring = reinterpret_cast<double2*>(vsm);   // Ev_z window [W][2][VNT] pairs
-    double2* xt = ring + W * 2 * VNT;                  // Ev_x [2][VBY][XW] pairs
-    double2* yt = xt + 2 * XF;                         // Ev_y [2][YH][VBX] pairs
+    double2* tiles = reinterpret_cast<double2*>(vsm);         // [2][Ev_x pairs | Ev_y pairs]
+    double* dus = vsm + 2 * 2 * BUF;                          // [2][4][VNT] du (accumulating)
     const int tid = threadIdx.x, lx = tid % VBX, ly = tid / VBX;
     const size_t eplane = (size_t)a.epitch * (size_t)(a.ny + 8);
     const long items = vis_items(a);
@@ -295,77 +305,79 @@ __global__ void __launch_bounds__(VNT, 2) vis_div_kernel(const __grid_constant__
             yo[p] = min(w.x0 + xx, a.nx - 1) + 4 + (int)a.epitch * min(w.y0 - R + yy + 4, a.ny + 7);
         }
         auto plane = [&](int c, int k) { return a.ev[c] + eplane * (size_t)(k + 4); };
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            double v[R][4];
-#pragma unroll
-            for (int m = 0; m < R; ++m)
-#pragma unroll
-                for (int q = 0; q < 4; ++q) v[m][q] = __ldg(plane(8 + q, w.k0 - R + h * R + m) + col);
-#pragma unroll
-            for (int m = 0; m < R; ++m)
-#pragma unroll
-                for (int pr = 0; pr < 2; ++pr)
-                    ring[(((w.k0 - R + h * R + m + 2 * W) % W) * 2 + pr) * VNT + tid] =
-                        make_double2(v[m][2 * pr], v[m][2 * pr + 1]);
-        }
-        // du of this column (accumulating): the plane's four values, loaded
-        // with the plane's other inputs
         const size_t du_col = (size_t)min(i, a.nx - 1) + (size_t)a.du_pitch * (size_t)min(j, a.ny - 1);
         const size_t du_plane = (size_t)a.du_pitch * a.du_ly, du_var = du_plane * a.du_lz;
-        double dn[4] = {0.0, 0.0, 0.0, 0.0}, lead[4], nx_[4][PX], ny_[4][PY];
-        auto prefetch = [&](int k) {
+        // plane k's Ev_x / Ev_y tiles (pairs interleaved) and du into buffer b
+        auto stage = [&](int k, int b) {
+            double2* xt = tiles + b * BUF;
+            double2* yt = xt + 2 * XF;
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                if (a.accumulate) dn[q] = a.du[du_col + du_plane * k + du_var * (q + 1)];
-                lead[q] = __ldg(plane(8 + q, k + R) + col);
                 const double* bx = plane(q, k);
                 const double* by = plane(4 + q, k);
 #pragma unroll
                 for (int p = 0; p < PX; ++p)
-                    if (tid + p * VNT < XF) nx_[q][p] = __ldg(bx + xo[p]);
-#pragma unroll
-                for (int p = 0; p < PY; ++p)
-                    if (tid + p * VNT < YF) ny_[q][p] = __ldg(by + yo[p]);
-            }
-        };
-        prefetch(w.k0);
-        for (int k = w.k0; k < w.k1; ++k) {
-            __syncthreads();
-            double dc[4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) dc[q] = dn[q];
-#pragma unroll
-            for (int pr = 0; pr < 2; ++pr) {
-                ring[(((k + R) % W) * 2 + pr) * VNT + tid] =
-                    make_double2(lead[2 * pr], lead[2 * pr + 1]);
-#pragma unroll
-                for (int p = 0; p < PX; ++p)
                     if (tid + p * VNT < XF)
-                        xt[pr * XF + tid + p * VNT] = make_double2(nx_[2 * pr][p], nx_[2 * pr + 1][p]);
+                        vcp8(reinterpret_cast<double*>(xt + (q >> 1) * XF + tid + p * VNT) + (q & 1),
+                             bx + xo[p]);
 #pragma unroll
                 for (int p = 0; p < PY; ++p)
                     if (tid + p * VNT < YF)
-                        yt[pr * YF + tid + p * VNT] = make_double2(ny_[2 * pr][p], ny_[2 * pr + 1][p]);
+                        vcp8(reinterpret_cast<double*>(yt + (q >> 1) * YF + tid + p * VNT) + (q & 1),
+                             by + yo[p]);
+                if (a.accumulate)
+                    vcp8(dus + (b * 4 + q) * VNT + tid, a.du + du_col + du_plane * k + du_var * (q + 1));
             }
-            __syncthreads();
-            if (k + 1 < w.k1) prefetch(k + 1);
+            vcp_commit();
+        };
+        __syncthreads();                  // the previous item's last buffer is read
+        stage(w.k0, 0);
+        // Ev_z window: zw[q][m] = plane k - R + m (m = 0..2R); filled with
+        // planes k0-R .. k0+R-1 in slots 1..2R, the lead plane k0+R apart
+        double zw[4][W], lead[4];
+#pragma unroll
+        for (int m = 0; m < 2 * R; ++m)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) zw[q][m + 1] = __ldg(plane(8 + q, w.k0 - R + m) + col);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            zw[q][0] = 0.0;
+            lead[q] = __ldg(plane(8 + q, w.k0 + R) + col);
+        }
+        for (int k = w.k0; k < w.k1; ++k) {
+            const int b = (k - w.k0) & 1;
+            vcp_wait_all();
+            __syncthreads();              // buffer b landed; buffer b^1 read by every thread
+            if (k + 1 < w.k1) stage(k + 1, b ^ 1);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+#pragma unroll
+                for (int m = 0; m < 2 * R; ++m) zw[q][m] = zw[q][m + 1];
+                zw[q][2 * R] = lead[q];
+            }
+            if (k + 1 < w.k1)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) lead[q] = __ldg(plane(8 + q, k + 1 + R) + col);
             if (!own) continue;
             const int Z = k + 4;
             const double aj = UNI ? 1.0 : __ldg(a.met[9] + lapi(X, Y, Z, a.mpitch[9], a.ny));
+            const double2* xt = tiles + b * BUF;
+            const double2* yt = xt + 2 * XF;
 #pragma unroll
             for (int pr = 0; pr < 2; ++pr) {
                 const double2 dx = cd2<R>(xt + (pr * VBY + ly) * XW + lx + R, 1);
                 const double2 dy = cd2<R>(yt + (pr * YH + ly + R) * VBX + lx, VBX);
-                const double2 dz = cd2_ring<R>(ring + pr * VNT + tid, k, 2 * VNT);
-                const double ddx[2] = {dx.x, dx.y}, ddy[2] = {dy.x, dy.y}, ddz[2] = {dz.x, dz.y};
+                const double ddx[2] = {dx.x, dx.y}, ddy[2] = {dy.x, dy.y};
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
                     const int q = 2 * pr + h;
-                    double acc = dc[q];
+                    const double* z = zw[q];
+                    const double dz = cdv<R>(z[R + 1] - z[R - 1], z[R + 2] - z[R - 2],
+                                             z[R + 3] - z[R - 3], R == 4 ? z[R + 4] - z[0] : 0.0);
+                    double acc = a.accumulate ? dus[(b * 4 + q) * VNT + tid] : 0.0;
                     acc += aj * (ddx[h] * a.rh[0]);
                     acc += aj * (ddy[h] * a.rh[1]);
-                    acc += aj * (ddz[h] * a.rh[2]);
+                    acc += aj * (dz * a.rh[2]);
                     a.du[du_col + du_plane * k + du_var * (q + 1)] = acc;
                 }
             }
