@@ -93,12 +93,14 @@ bool job_empty(ws_job j) {
 // latencies better than 16 within an 80-register budget; mixed 8x8 / 384
 // threads, two CTAs per SM (one CTA's barrier waits overlap the other's
 // arithmetic).
-// Measured at 600x128x128 on B200: 16x8 with 704 threads (the sweep's two
-// intervals hold 1216 and 1400 items, which 704 threads run in two nearly
-// full rounds each), except the mixed form's plain RHS, 8x8/384 (two CTAs
-// per SM; 16x8/704 measures the same).
+// Measured at 600x128x128 on B200: 16x8 with 704 threads in every form (the
+// sweep's two intervals hold 1216 and 1400 items, which 704 threads run in
+// two nearly full rounds each); the mixed form's 8x8/384 (two CTAs per SM)
+// measures 1% slower for the plain RHS and 7% for the stage kernel.
 int default_cfg(int precision, bool stage) {
-    return precision == WS_MIXED && !stage ? 3 : 1;
+    (void)precision;
+    (void)stage;
+    return 1;
 }
 
 namespace {

@@ -61,6 +61,11 @@ template <int BX, int BY, typename CT, bool EPI = false>
 struct RhsLayout {
     static constexpr int BXY = BX * BY;
     static constexpr int SXW = BX + 8;        // x-split row width
+    // x-split row pitch: for 4-byte types padded so that the 32 / BX rows a
+    // warp's x faces read start on disjoint bank groups (unpadded, two rows
+    // of a warp share banks and every such load takes two wavefronts)
+    static constexpr int SXP = sizeof(CT) == 8 ? SXW : BX == 8 ? 24 : BX == 16 ? 48 : SXW;
+    static_assert(SXP >= SXW, "x-split pitch");
     static constexpr int SYH = BY + 8;        // y-split rows
     static constexpr int BOXW = BX + 8, BOXH = BY + 8, BOX = BOXW * BOXH;
     static constexpr int STG = 5 * (BOX + BXY);   // doubles per staging buffer
@@ -75,7 +80,7 @@ struct RhsLayout {
     static constexpr int N_FZ = NFZS * 5 * BXY;
     static constexpr int N_FB = EPI ? 2 * 15 * BXY : 0;   // fn, f, viscous terms, x2
     static constexpr int N_RING = RING * RS;      // CT
-    static constexpr int N_SX = 10 * BY * SXW;    // CT
+    static constexpr int N_SX = 10 * BY * SXP;    // CT
     static constexpr int N_SY = 10 * SYH * BX;    // CT
     static constexpr size_t smem_bytes =
         (size_t)(N_STG + N_FX + N_FY + N_FZ + N_FB) * sizeof(double) +
@@ -321,7 +326,8 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
                                       int x0, int y0, int z0, int z1, int krk, uint64_t* bar,
                                       uint32_t& ph, bool& first) {
     using L = RhsLayout<BX, BY, CT, EPI>;
-    constexpr int BXY = L::BXY, SXW = L::SXW, SYH = L::SYH, BOXW = L::BOXW, BOX = L::BOX;
+    constexpr int BXY = L::BXY, SXW = L::SXW, SXP = L::SXP, SYH = L::SYH, BOXW = L::BOXW,
+                  BOX = L::BOX;
     constexpr int RS = L::RS;
     double* stg = reinterpret_cast<double*>(smem);       // [2][STG]
     double* fx = stg + L::N_STG;                         // [5][BY][BX+1]
@@ -329,7 +335,7 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
     double* fz = fy + L::N_FY;                           // [NFZS][5][BXY]
     double* fb = fz + L::N_FZ;                           // [2][15][BXY]   (stage mode)
     CT* ring = reinterpret_cast<CT*>(fb + L::N_FB);      // [9][10][BXY]
-    CT* sxs = ring + L::N_RING;                          // [10][BY][SXW]
+    CT* sxs = ring + L::N_RING;                          // [10][BY][SXP], rows of SXW
     CT* sys = sxs + L::N_SX;                             // [10][SYH][BX]
     const int tid = threadIdx.x;
     static_assert(NT >= BXY, "one thread per cell in the stage epilogue");
@@ -408,9 +414,9 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
                                         sb[3 * BOX + bi], sb[4 * BOX + bi],
                                         min(x0 - 4 + xi, a.nx + 7), min(y0 + yy, a.ny + 7), z,
                                         out);
-                CT* dst = sxs + yy * SXW + xi;
+                CT* dst = sxs + yy * SXP + xi;
 #pragma unroll
-                for (int c = 0; c < 10; ++c) dst[c * BY * SXW] = out[c];
+                for (int c = 0; c < 10; ++c) dst[c * BY * SXP] = out[c];
             } else {
                 const int t2 = t - NXS;
                 const int yi = t2 / BX, xx = t2 - yi * BX;
@@ -474,13 +480,13 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
         const bool clx = CLO && (a.clo[0] | a.clo[1]), cly = CLO && (a.clo[2] | a.clo[3]);
         for (; t < NXR; t += NT) {
             const unsigned var = t / BXY, r = t % BXY, yy = r / BX, xx = r % BX;
-            const CT* bp = sxs + (var * BY + yy) * SXW + xx + 1;
+            const CT* bp = sxs + (var * BY + yy) * SXP + xx + 1;
             const int f = x0 - 3 + (int)xx;
             fx[(var * BY + yy) * (BX + 1) + xx + 1] =
                 (clx && closure_face(f, a.nx, a.clo[0], a.clo[1]))
-                    ? closure_value<CT>(bp, bp + 5 * BY * SXW, 1, f, a.nx, a.clo[0], a.clo[1],
+                    ? closure_value<CT>(bp, bp + 5 * BY * SXP, 1, f, a.nx, a.clo[0], a.clo[1],
                                         false)
-                    : face_flux<CT>(bp, 5 * BY * SXW, 1, 8, 0);
+                    : face_flux<CT>(bp, 5 * BY * SXP, 1, 8, 0);
         }
         for (t -= NXR; t < NYR; t += NT) {
             const unsigned var = t / BXY, r = t % BXY, g = r / BX + 1, xx = r % BX;
@@ -495,13 +501,13 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
         for (t -= NYR; t < NE; t += NT) {
             if (t < 5 * BY) {
                 const unsigned var = t / BY, yy = t % BY;
-                const CT* bp = sxs + (var * BY + yy) * SXW;
+                const CT* bp = sxs + (var * BY + yy) * SXP;
                 const int f = x0 - 4;
                 fx[(var * BY + yy) * (BX + 1)] =
                     (clx && closure_face(f, a.nx, a.clo[0], a.clo[1]))
-                        ? closure_value<CT>(bp, bp + 5 * BY * SXW, 1, f, a.nx, a.clo[0],
+                        ? closure_value<CT>(bp, bp + 5 * BY * SXP, 1, f, a.nx, a.clo[0],
                                             a.clo[1], false)
-                        : face_flux<CT>(bp, 5 * BY * SXW, 1, 8, 0);
+                        : face_flux<CT>(bp, 5 * BY * SXP, 1, 8, 0);
             } else {
                 const unsigned var = (t - 5 * BY) / BX, xx = (t - 5 * BY) % BX;
                 const CT* bp = sys + var * SYH * BX + xx;
