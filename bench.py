@@ -97,10 +97,15 @@ def workload_name(a, world=1):
             "SSP-RK3 CFL 0.5")
 
 
+L2_BYTES = 126e6                # B200 L2
+
+
 def config_of(a, world, **kw):
+    # per GPU, the five primitive LAP fields a step reads (plus f, fn, du)
+    prim_bytes = 5 * 8 * (a.nx + 8) * (a.ny + 8) * (a.nz + 8)
     c = {"workload": workload_name(a, world), "grid": [a.nx * world, a.ny, a.nz],
          "grid_per_gpu": [a.nx, a.ny, a.nz], "rhs_per_step": 3, "cfl": 0.5,
-         "inputs_exceed_l2": True,
+         "inputs_exceed_l2": prim_bytes > L2_BYTES,
          "parallelism": "single" if world == 1 else f"xslab{world}"}
     c.update(kw)
     return c
