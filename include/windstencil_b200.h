@@ -72,12 +72,12 @@ enum ws_face_kind {
      * extrapolation / averages (x) or minmod2 forms (y) at the high end, and
      * the reference's dropped M term of the last y cell.  >= 8 cells.       */
     WS_FACE_CLOSURE = 2,
-    /* x faces only: the face is shared with a neighbouring subdomain (a slab
-     * of a grid split along x); its 4 ghost planes at interior y, z are
-     * written by the caller (ws_halo_unpack_x), as the reference's
-     * exchange_boundary_x_packed_dev does (OCFD_mpi_dev.cpp:185-218); the
-     * ghost fill leaves them and copies them into the y/z ghost edges.
-     * Faces next to it are reconstructed with WENO7 through those ghosts. */
+    /* the face is shared with a neighbouring subdomain (a block of a grid
+     * split along x, y and/or z); its 4 ghost planes over the interior of
+     * the other two axes are written by the caller (ws_halo_unpack), as the
+     * reference's exchange_boundary_{x,y,z}_packed_dev do
+     * (OCFD_mpi_dev.cpp:123-290); the ghost fill leaves them.  Faces next to
+     * it are reconstructed with WENO7 through those ghosts. */
     WS_FACE_EXTERNAL = 3
 };
 
@@ -203,8 +203,8 @@ WS_API size_t ws_du_vis_workspace_bytes(const ws_grid* g);
  * the fluxes' ghosts filled by g->face_kind.  workspace: caller-owned device
  * memory of ws_du_vis_workspace_bytes(g) (the reference keeps the same
  * fields as globals); the call allocates nothing.  WS_ERR_UNSUPPORTED for a
- * grid with WS_FACE_EXTERNAL faces: the fluxes' x halos would need an
- * exchange of their own between the two passes. */
+ * grid with WS_FACE_EXTERNAL faces: the fluxes' halos need an exchange of
+ * their own between the two passes (ws_solver_stage_begin / _end). */
 WS_API int ws_du_vis_jacobian3d(const ws_grid* g, const ws_viscous* vis, ws_field u, ws_field v,
                                 ws_field w, ws_field T, const ws_metrics* metrics, ws_soa du,
                                 void* workspace, size_t workspace_bytes, ws_stream_t stream);
@@ -233,21 +233,29 @@ WS_API int ws_metrics_read(const char* path, int nx, int ny, int nz, double* fie
  * GPU: no host staging, no MPI. */
 WS_API int ws_ghost_fill(const ws_grid* g, const ws_field* fields, int nfields, ws_stream_t stream);
 
-/* Halo planes of a grid split into slabs along x (the reference's MPI_COMM_X
- * decomposition, OCFD_mpi.c:124-145, with one subdomain per GPU).
- * side 0 is the low-x face, side 1 the high-x face.  A halo buffer holds
- * nfields x nz x ny x 4 doubles, [field][z][y][x], interior y and z only
- * (the packed layout of cudaFieldBoundaryPack_kernel, OCFD_mpi_dev.cpp:137-152).
- * Buffers are device memory, 8-byte aligned; 1 <= nfields <= 8. */
+/* Halo planes of a grid split into blocks (the reference's MPI decomposition
+ * NPX0 x NPY0 x NPZ0, OCFD_mpi.c:102-145, with one subdomain per GPU).
+ * axis 0, 1, 2 = x, y, z; side 0 is the low face, side 1 the high face.  A
+ * halo buffer holds nfields x the 4 planes along the axis over the interior
+ * of the other two, x fastest: [field][z][y][x] with 4 x planes (axis 0),
+ * [field][z][4][x] (axis 1), [field][4][y][x] (axis 2) -- the packed layout
+ * of cudaFieldBoundaryPack_kernel (OCFD_mpi_dev.cpp:137-152).  Buffers are
+ * device memory, 8-byte aligned; 1 <= nfields <= 8. */
+WS_API size_t ws_halo_bytes(const ws_grid* g, int axis, int nfields);
+/* Interior planes next to face (axis, side) (side 0: 4..7; side 1: n..n+3
+ * in LAP coordinates along the axis) -> buf: the sends of
+ * exchange_boundary_{x,y,z}_packed_dev; side 0 goes to the low neighbour. */
+WS_API int ws_halo_pack(const ws_grid* g, const ws_field* fields, int nfields, int axis,
+                        int side, void* buf, ws_stream_t stream);
+/* buf -> the ghost planes beyond face (axis, side) (side 0: 0..3; side 1:
+ * n+4..n+7): the receives.  The low ghosts take the low neighbour's side-1
+ * planes, and the reverse. */
+WS_API int ws_halo_unpack(const ws_grid* g, const ws_field* fields, int nfields, int axis,
+                          int side, const void* buf, ws_stream_t stream);
+/* The x-axis forms of the three above (axis 0). */
 WS_API size_t ws_halo_x_bytes(const ws_grid* g, int nfields);
-/* Interior planes next to face `side` (side 0: x = 4..7; side 1: x = nx..nx+3
- * in LAP coordinates) -> buf.  The sends of exchange_boundary_x_packed_dev
- * (OCFD_mpi_dev.cpp:185-218): side 0 goes to the low-x neighbour. */
 WS_API int ws_halo_pack_x(const ws_grid* g, const ws_field* fields, int nfields, int side,
                           void* buf, ws_stream_t stream);
-/* buf -> the ghost planes beyond face `side` (side 0: x = 0..3; side 1:
- * x = nx+4..nx+7): the receives of exchange_boundary_x_packed_dev.  The low
- * ghosts take the low-x neighbour's side-1 planes, and the reverse. */
 WS_API int ws_halo_unpack_x(const ws_grid* g, const ws_field* fields, int nfields, int side,
                             const void* buf, ws_stream_t stream);
 
@@ -325,19 +333,20 @@ WS_API int  ws_solver_stage(ws_solver* s, int krk, double dt, ws_stream_t stream
 /* The primitive fields d,u,v,w,T,cc that stage krk reads (stage 1: the
  * current state's). */
 WS_API int  ws_solver_stage_fields(ws_solver* s, int krk, ws_field prims[6]);
-/* ws_solver_stage in two halves, for a slab with viscous terms: the first
+/* ws_solver_stage in two halves, for a block with viscous terms: the first
  * (ghost fill, viscous flux pass with the fluxes' own ghost fill) and the
  * second (viscous divergence, fused RHS + stage update).  Between them the
- * caller exchanges the x halos of the four x-direction viscous fluxes
- * (ws_solver_stage_flux_fields; they need x ghosts for d/dx), as the
- * reference exchanges Ev1..4 between vis_flux_ker and its derivatives
- * (OCFD_Stream.cpp:229-345).  ws_solver_stage with viscous terms on an
- * EXTERNAL grid returns WS_ERR_UNSUPPORTED. */
+ * caller exchanges, along each axis with EXTERNAL faces, the halos of that
+ * direction's four viscous fluxes (ws_solver_stage_flux_fields; d/dx needs
+ * the x fluxes' x ghosts, and so on), as the reference exchanges Ev1..4
+ * between vis_flux_ker and its derivatives (OCFD_Stream.cpp:229-345).
+ * ws_solver_stage with viscous terms on an EXTERNAL grid returns
+ * WS_ERR_UNSUPPORTED. */
 WS_API int  ws_solver_stage_begin(ws_solver* s, int krk, ws_stream_t stream);
 WS_API int  ws_solver_stage_end(ws_solver* s, int krk, double dt, ws_stream_t stream);
-/* The four x-direction viscous flux fields (Ev1..4 of the x direction, LAP)
- * of the solver's workspace; WS_ERR_INVALID without viscous terms. */
-WS_API int  ws_solver_stage_flux_fields(ws_solver* s, ws_field ev_x[4]);
+/* The four viscous flux fields of direction `axis` (Ev1..4, LAP) in the
+ * solver's workspace; WS_ERR_INVALID without viscous terms. */
+WS_API int  ws_solver_stage_flux_fields(ws_solver* s, int axis, ws_field ev_axis[4]);
 /* Device status word: 0, WS_ERR_NONFINITE, or WS_ERR_TIMEOUT (a staging
  * wait of the fused RHS gave up); synchronises `stream`. */
 WS_API int  ws_solver_status(ws_solver* s, int* status, ws_stream_t stream);

@@ -398,14 +398,14 @@ void or_split_batch(const double* in, long n, double gamma, double epsl_sw,
 // OR_FACE_EXTRAP copies the nearest interior value (zero gradient).  Axes are
 // filled x, then y, then z over the full padded extent of the other axes,
 // so edge and corner ghosts are defined (the RHS never reads them).  An
-// OR_FACE_EXTERNAL x face keeps its ghost planes (a neighbouring subdomain's
-// halo, unpacked by the caller as exchange_boundary_x_packed_dev does,
-// OCFD_mpi_dev.cpp:185-218); the y and z passes copy them into the edges.
+// OR_FACE_EXTERNAL face keeps its ghost planes (a neighbouring subdomain's
+// halo, unpacked by the caller as exchange_boundary_{x,y,z}_packed_dev do,
+// OCFD_mpi_dev.cpp:185-290); the later axes' passes copy them into the edges.
 void or_ghost_fill(const or_grid* g, double* f) {
     Dims D(g);
     const long L = OR_LAP;
-    const bool ext_lo = g->face_kind[0] == OR_FACE_EXTERNAL;
-    const bool ext_hi = g->face_kind[1] == OR_FACE_EXTERNAL;
+    bool ext[6];
+    for (int i = 0; i < 6; ++i) ext[i] = g->face_kind[i] == OR_FACE_EXTERNAL;
     // x
 #pragma omp parallel for collapse(2) schedule(static)
     for (long k = -L; k < D.nz + L; ++k)
@@ -413,8 +413,8 @@ void or_ghost_fill(const or_grid* g, double* f) {
             for (long l = 1; l <= L; ++l) {
                 long lo = g->face_kind[0] == OR_FACE_PERIODIC ? D.nx - l : 0;
                 long hi = g->face_kind[1] == OR_FACE_PERIODIC ? l - 1 : D.nx - 1;
-                if (!ext_lo) f[D.lap(-l, j, k)] = f[D.lap(lo, j, k)];
-                if (!ext_hi) f[D.lap(D.nx - 1 + l, j, k)] = f[D.lap(hi, j, k)];
+                if (!ext[0]) f[D.lap(-l, j, k)] = f[D.lap(lo, j, k)];
+                if (!ext[1]) f[D.lap(D.nx - 1 + l, j, k)] = f[D.lap(hi, j, k)];
             }
     // y
 #pragma omp parallel for collapse(2) schedule(static)
@@ -423,8 +423,8 @@ void or_ghost_fill(const or_grid* g, double* f) {
             for (long i = -L; i < D.nx + L; ++i) {
                 long lo = g->face_kind[2] == OR_FACE_PERIODIC ? D.ny - l : 0;
                 long hi = g->face_kind[3] == OR_FACE_PERIODIC ? l - 1 : D.ny - 1;
-                f[D.lap(i, -l, k)] = f[D.lap(i, lo, k)];
-                f[D.lap(i, D.ny - 1 + l, k)] = f[D.lap(i, hi, k)];
+                if (!ext[2]) f[D.lap(i, -l, k)] = f[D.lap(i, lo, k)];
+                if (!ext[3]) f[D.lap(i, D.ny - 1 + l, k)] = f[D.lap(i, hi, k)];
             }
     // z
 #pragma omp parallel for collapse(2) schedule(static)
@@ -433,8 +433,8 @@ void or_ghost_fill(const or_grid* g, double* f) {
             for (long i = -L; i < D.nx + L; ++i) {
                 long lo = g->face_kind[4] == OR_FACE_PERIODIC ? D.nz - l : 0;
                 long hi = g->face_kind[5] == OR_FACE_PERIODIC ? l - 1 : D.nz - 1;
-                f[D.lap(i, j, -l)] = f[D.lap(i, j, lo)];
-                f[D.lap(i, j, D.nz - 1 + l)] = f[D.lap(i, j, hi)];
+                if (!ext[4]) f[D.lap(i, j, -l)] = f[D.lap(i, j, lo)];
+                if (!ext[5]) f[D.lap(i, j, D.nz - 1 + l)] = f[D.lap(i, j, hi)];
             }
 }
 

@@ -34,8 +34,8 @@ extern "C" {
 
 /* CLOSURE (x and y faces only): zero-gradient ghosts, and the faces next to
  * it take the boundary closures of the fused path's ring kernel.
- * EXTERNAL (x faces only): ghost planes written by the caller (a halo from a
- * neighbouring subdomain); the ghost fill keeps them. */
+ * EXTERNAL: ghost planes written by the caller (a halo from a neighbouring
+ * subdomain); the ghost fill keeps them. */
 enum { OR_FACE_PERIODIC = 0, OR_FACE_EXTRAP = 1, OR_FACE_CLOSURE = 2, OR_FACE_EXTERNAL = 3 };
 
 typedef struct or_grid {

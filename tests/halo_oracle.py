@@ -1,17 +1,18 @@
-"""A slab of windstencil_b200.halo stepped by the CPU oracle (test checker).
+"""A block of windstencil_b200.halo stepped by the CPU oracle (test checker).
 
-OracleSlab has CudaSlab's methods (send / recv / pack / unpack / begin / end
-/ local_dt / set_state / get_state / set_viscous / status), so SlabStepper,
-LocalExchange and DistExchange run unchanged over it: on gloo ranks on the
-CPU, the decomposition, the exchange pattern and the stage sequence of the
-multi-GPU path are checked against the oracle on the whole grid.
+OracleSlab has CudaBlock's methods (send / recv / pack / unpack / begin /
+end / local_dt / set_state / get_state / set_viscous / status), so
+SlabStepper, LocalExchange and DistExchange run unchanged over it: on gloo
+ranks on the CPU, the decomposition, the exchange pattern and the stage
+sequence of the multi-GPU path are checked against the oracle on the whole
+grid.
 
 Each stage follows the oracle's rhs_from_cons (oracle/oracle.cpp): prims of
-the stage's state, ghost fill of d, u, v, w, T (EXTERNAL x faces keep the
+the stage's state, ghost fill of d, u, v, w, T (EXTERNAL faces keep the
 unpacked halo), cc = sqrt(T)/ama on the padded field, inviscid RHS; with
-viscous terms the 12 flux fields, the x fluxes' halo, and per direction the
-flux ghost fill and divergence added to du; then the SSP-RK3 update
-(OCFD_time.cpp:15-65).
+viscous terms the 12 flux fields, each direction's fluxes' halo along its
+axis, and per direction the flux ghost fill and divergence added to du;
+then the SSP-RK3 update (OCFD_time.cpp:15-65).
 """
 from __future__ import annotations
 
@@ -20,23 +21,29 @@ import torch
 
 from oracle.oracle import make_grid as or_make_grid
 from oracle.oracle import make_vis
-from windstencil_b200.halo import FLUX, FLUX_FIELDS, HALO_FIELDS, PRIMS, Slab, slab_grid
+from windstencil_b200.halo import FLUX, HALO_FIELDS, PRIMS, Block, block_grid
 
 L = 4
 
 
 class OracleSlab:
-    def __init__(self, oracle, grid, slab: Slab):
+    def __init__(self, oracle, grid, block: Block):
         self.o = oracle
-        self.slab = slab
-        g = slab_grid(grid, slab)
+        self.slab = self.block = block
+        g = block_grid(grid, block)
         self.grid = g
         self.og = or_make_grid(g.nx, g.ny, g.nz, hx=g.hx, hy=g.hy, hz=g.hz, gamma=g.gamma,
                                ama=g.ama, epsl_sw=g.epsl_sw, face_kind=g.faces)
-        plane = g.nz * g.ny * 4
-        self.n = {PRIMS: HALO_FIELDS * plane, FLUX: FLUX_FIELDS * plane}
-        self._send = [torch.zeros(self.n[PRIMS], dtype=torch.float64) for _ in range(2)]
-        self._recv = [torch.zeros(self.n[PRIMS], dtype=torch.float64) for _ in range(2)]
+        n = (g.nx, g.ny, g.nz)
+        self.n, self._send, self._recv = {}, {}, {}
+        for ax in range(3):
+            plane = 4 * n[(ax + 1) % 3] * n[(ax + 2) % 3]
+            self.n[ax, PRIMS] = HALO_FIELDS * plane
+            self.n[ax, FLUX] = 4 * plane
+            self._send[ax] = [torch.zeros(self.n[ax, PRIMS], dtype=torch.float64)
+                              for _ in range(2)]
+            self._recv[ax] = [torch.zeros(self.n[ax, PRIMS], dtype=torch.float64)
+                              for _ in range(2)]
         self.f = self.fn = self.prims = self.du = self.ev = None
         self.vis = None
         self.viscous = False
@@ -55,11 +62,11 @@ class OracleSlab:
     def get_state(self):
         return self.f.copy()
 
-    def send(self, side, kind=PRIMS):
-        return self._send[side][:self.n[kind]]
+    def send(self, axis, side, kind=PRIMS):
+        return self._send[axis][side][:self.n[axis, kind]]
 
-    def recv(self, side, kind=PRIMS):
-        return self._recv[side][:self.n[kind]]
+    def recv(self, axis, side, kind=PRIMS):
+        return self._recv[axis][side][:self.n[axis, kind]]
 
     def _inputs(self):
         if self.prims is None:
@@ -68,27 +75,37 @@ class OracleSlab:
             self.prims = [d, u, v, w, T, cc]
         return self.prims
 
-    def _fields(self, kind):
-        return self._inputs() if kind == PRIMS else [self.ev[q] for q in range(4)]
+    def _fields(self, axis, kind):
+        if kind == PRIMS:
+            return self._inputs()
+        return [self.ev[4 * axis + q] for q in range(4)]
 
-    def _planes(self, side, ghost):
+    def _planes(self, axis, side, ghost):
+        """(z, y, x) slices of the 4 planes along `axis` (interior elsewhere)."""
         g = self.grid
+        n = (g.nx, g.ny, g.nz)
         if ghost:
-            x0 = 0 if side == 0 else g.nx + L
+            a0 = 0 if side == 0 else n[axis] + L
         else:
-            x0 = L if side == 0 else g.nx
-        return (slice(L, g.nz + L), slice(L, g.ny + L), slice(x0, x0 + 4))
+            a0 = L if side == 0 else n[axis]
+        sl = [slice(a0, a0 + 4) if ax == axis else slice(L, n[ax] + L) for ax in range(3)]
+        return (sl[2], sl[1], sl[0])
 
-    def pack(self, side, kind=PRIMS):
-        sl = self._planes(side, ghost=False)
-        buf = np.stack([p[sl] for p in self._fields(kind)])
-        self.send(side, kind).copy_(torch.from_numpy(buf.reshape(-1)))
-
-    def unpack(self, side, buf, kind=PRIMS):
+    def _shape(self, axis, nf):
         g = self.grid
-        fields = self._fields(kind)
-        b = buf.cpu().numpy().reshape(len(fields), g.nz, g.ny, 4)
-        sl = self._planes(side, ghost=True)
+        n = [g.nx, g.ny, g.nz]
+        n[axis] = 4
+        return (nf, n[2], n[1], n[0])
+
+    def pack(self, axis, side, kind=PRIMS):
+        sl = self._planes(axis, side, ghost=False)
+        buf = np.stack([p[sl] for p in self._fields(axis, kind)])
+        self.send(axis, side, kind).copy_(torch.from_numpy(buf.reshape(-1)))
+
+    def unpack(self, axis, side, buf, kind=PRIMS):
+        fields = self._fields(axis, kind)
+        b = buf.cpu().numpy().reshape(self._shape(axis, len(fields)))
+        sl = self._planes(axis, side, ghost=True)
         for q, p in enumerate(fields):
             p[sl] = b[q]
 

@@ -28,38 +28,51 @@ def _rand_fields(torch, g, n, seed):
     return [t[i] for i in range(n)]
 
 
+@pytest.mark.parametrize("axis", [0, 1, 2])
 @pytest.mark.parametrize("nf", [1, 6])
 @pytest.mark.parametrize("shape", [(19, 13, 7), (40, 24, 10)])
-def test_halo_pack_unpack(cuda, nf, shape):
+def test_halo_pack_unpack(cuda, nf, shape, axis):
     torch = cuda
-    g = ws.Grid(*shape, faces=(XT, XT, PE, PE, PE, PE))
-    nx, ny, nz = shape
+    faces = [PE] * 6
+    faces[2 * axis] = faces[2 * axis + 1] = XT
+    g = ws.Grid(*shape, faces=tuple(faces))
+    n = list(shape)
     fields = _rand_fields(torch, g, nf, 5)
-    nb = ws.halo_x_bytes(g, nf) // 8
-    assert nb == nf * nz * ny * 4
-    for side, x0 in ((0, 4), (1, nx)):
+    nb = ws.halo_bytes(g, axis, nf) // 8
+    box = [n[0], n[1], n[2]]
+    box[axis] = 4
+    assert nb == nf * box[0] * box[1] * box[2]
+    if axis == 0:
+        assert ws.halo_x_bytes(g, nf) // 8 == nb
+
+    def planes(f, a0):         # (z, y, x) slices: 4 planes along axis from a0
+        sl = [slice(a0, a0 + 4) if d == axis else slice(4, n[d] + 4) for d in range(3)]
+        return f[sl[2], sl[1], sl[0]]
+    for side, a0 in ((0, 4), (1, n[axis])):
         buf = torch.full((nb,), -1.0, dtype=torch.float64, device="cuda")
-        ws.halo_pack_x(g, fields, side, buf)
-        want = torch.stack([f[4:nz + 4, 4:ny + 4, x0:x0 + 4] for f in fields]).reshape(-1)
+        ws.halo_pack(g, fields, axis, side, buf)
+        want = torch.stack([planes(f, a0) for f in fields]).reshape(-1)
         assert torch.equal(buf, want)
-    for side, x0 in ((0, 0), (1, nx + 4)):
+    for side, a0 in ((0, 0), (1, n[axis] + 4)):
         before = [f.clone() for f in fields]
         buf = torch.rand(nb, dtype=torch.float64, device="cuda")
-        ws.halo_unpack_x(g, fields, side, buf)
-        b = buf.reshape(nf, nz, ny, 4)
+        ws.halo_unpack(g, fields, axis, side, buf)
+        b = buf.reshape(nf, box[2], box[1], box[0])
         for q, f in enumerate(fields):
-            assert torch.equal(f[4:nz + 4, 4:ny + 4, x0:x0 + 4], b[q])
+            assert torch.equal(planes(f, a0), b[q])
             mask = torch.ones_like(f, dtype=torch.bool)
-            mask[4:nz + 4, 4:ny + 4, x0:x0 + 4] = False
+            sl = [slice(a0, a0 + 4) if d == axis else slice(4, n[d] + 4) for d in range(3)]
+            mask[sl[2], sl[1], sl[0]] = False
             assert torch.equal(f[mask], before[q][mask])      # nothing else written
     torch.cuda.synchronize()
 
 
 @pytest.mark.parametrize("faces", [(XT, XT, PE, EX, PE, PE), (EX, XT, EX, EX, PE, EX),
-                                   (XT, CL, CL, CL, PE, PE)])
+                                   (XT, CL, CL, CL, PE, PE), (PE, PE, XT, XT, EX, XT),
+                                   (XT, XT, XT, XT, XT, XT)])
 def test_ghost_fill_external(oracle, cuda, faces):
-    """EXTERNAL x ghosts at interior y, z are kept; the y/z ghost edges take
-    them; every other ghost as the oracle's fill."""
+    """EXTERNAL ghosts over the interior of the other axes are kept; every
+    other ghost as the oracle's fill (edges from the kept planes)."""
     torch = cuda
     shape = (21, 11, 9)
     nx, ny, nz = shape
@@ -123,6 +136,7 @@ def test_stage_halves_rules(cuda):
         s.stage_end(1, 1e-4)                               # end without begin
     s.set_viscous(ws.viscous())
     assert len(s.stage_flux_fields()) == 4
+    assert [f.ptr for f in s.stage_flux_fields(2)] != [f.ptr for f in s.stage_flux_fields(0)]
     with pytest.raises(ws.WsError, match="WS_ERR_UNSUPPORTED"):
         s.stage(1, 1e-4)                                   # the flux halo is needed
     with pytest.raises(ws.WsError, match="WS_ERR_UNSUPPORTED"):
@@ -270,6 +284,94 @@ def test_distributed_slabs_gloo_match_whole_grid(cuda, case):
     s = ws.Solver(g)
     s.set_viscous(vis)
     s.set_state(f0)
+    dt = s.compute_dt(0.4)
+    s.step(dt, nsteps)
+    want = s.get_state()
+    s.close()
+    assert all(m[0] == dt and m[1] == 0 for m in meta)
+    assert np.array_equal(got, want), rel_linf(got, want).max()
+
+
+BLOCK_CASES = [
+    ("periodic_2x2x1", (48, 40, 12), (PE,) * 6, (2, 2, 1), ws.FP64, None),
+    ("mixedfaces_1x2x2", (40, 34, 20), (EX, EX, PE, PE, EX, EX), (1, 2, 2), ws.FP64, None),
+    ("periodic_2x2x2", (48, 32, 24), (PE,) * 6, (2, 2, 2), ws.FP64, None),
+    ("mixedprec_2x2x1", (48, 40, 12), (PE,) * 6, (2, 2, 1), ws.MIXED, None),
+    ("ns_2x2x1", (48, 40, 12), (EX, EX, PE, PE, PE, PE), (2, 2, 1), ws.FP64,
+     dict(re=200.0, pr=0.72, ref_t=288.15, scheme=8)),
+]
+
+
+@pytest.mark.parametrize("case", BLOCK_CASES, ids=[c[0] for c in BLOCK_CASES])
+def test_blocks_match_whole_grid(cuda, case):
+    """Blocks along several axes on one GPU, halos handed over in process."""
+    _, shape, faces, dims, prec, vis = case
+    g = ws.Grid(*shape, faces=faces, precision=prec)
+    f0 = wl.fourier_state(*shape, seed=19)
+    whole = ws.Solver(g)
+    whole.set_viscous(vis)
+    whole.set_state(f0)
+    dt = whole.compute_dt(0.3)
+    whole.step(dt, 3)
+    want = whole.get_state()
+    whole.close()
+    st = halo.in_process(g, dims=dims)
+    try:
+        st.set_viscous(vis)
+        st.set_state(f0)
+        assert st.compute_dt(0.3) == dt
+        st.step(dt, 3)
+        got = halo.join_state(st.get_state(), [r.block for r in st.runners])
+        assert st.status() == 0
+    finally:
+        st.close()
+    assert np.array_equal(got, want), rel_linf(got, want).max()
+
+
+def _gloo_block_rank(rank, world, port, shape, faces, dims, nsteps, out_dir):
+    import datetime
+    import os
+
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    torch.cuda.set_device(0)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=120))
+    try:
+        g = ws.Grid(*shape, faces=faces)
+        st = halo.distributed(g, dims=dims)
+        st.set_state(wl.fourier_state(*shape, seed=31))
+        dt = st.compute_dt(0.4)
+        st.step(dt, nsteps)
+        np.save(os.path.join(out_dir, f"block{rank}.npy"), st.get_state()[0])
+        np.save(os.path.join(out_dir, f"dt{rank}.npy"), np.array([dt, st.status()]))
+        st.close()
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_distributed_blocks_gloo_match_whole_grid(cuda):
+    """halo.distributed over a 2 x 2 x 1 process grid in four processes
+    sharing the GPU (gloo, host-staged), against the whole grid."""
+    import socket
+    import tempfile
+
+    import torch.multiprocessing as mp
+    shape, faces, dims, nsteps = (48, 40, 12), (EX, EX, PE, PE, PE, PE), (2, 2, 1), 2
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    blocks = halo.decompose_blocks(ws.Grid(*shape, faces=faces), dims)
+    with tempfile.TemporaryDirectory() as d:
+        mp.start_processes(_gloo_block_rank, args=(4, port, shape, faces, dims, nsteps, d),
+                           nprocs=4, join=True, start_method="spawn")
+        got = halo.join_state([np.load(f"{d}/block{r}.npy") for r in range(4)], blocks)
+        meta = [np.load(f"{d}/dt{r}.npy") for r in range(4)]
+    g = ws.Grid(*shape, faces=faces)
+    s = ws.Solver(g)
+    s.set_state(wl.fourier_state(*shape, seed=31))
     dt = s.compute_dt(0.4)
     s.step(dt, nsteps)
     want = s.get_state()

@@ -16,7 +16,7 @@ from oracle.oracle import make_grid as or_make_grid
 from windstencil_b200 import (FACE_CLOSURE, FACE_EXTERNAL, FACE_EXTRAP, FACE_PERIODIC, Grid,
                               WsError, workloads as wl)
 from windstencil_b200.halo import (DistExchange, LocalExchange, SlabStepper, decompose,
-                                   join_state, slab_extents, split_state)
+                                   decompose_blocks, join_state, slab_extents, split_state)
 
 from halo_oracle import OracleSlab
 
@@ -67,24 +67,39 @@ def test_decompose_rejects_thin_or_mixed():
         decompose(Grid(32, 8, 8, faces=(FACE_PERIODIC, FACE_EXTRAP) + (0,) * 4), 2)
 
 
-def test_abi_rejects_external_outside_x():
-    """EXTERNAL is an x-face kind only; the check runs before any device work."""
+def test_abi_halo_argument_checks():
+    """Halo entry points validate their arguments before any device work."""
     from windstencil_b200 import _abi
     lib = _abi.load()
-    g = Grid(16, 16, 16, faces=(0, 0, FACE_EXTERNAL, 0, 0, 0)).c()
-    h = C.c_void_p()
-    assert lib.ws_solver_create(C.byref(g), C.byref(h)) == 4        # WS_ERR_UNSUPPORTED
-    g = Grid(16, 16, 16, faces=(FACE_EXTERNAL, 0, 0, 0, 0, 0)).c()
+    g = Grid(16, 12, 10, faces=(FACE_EXTERNAL, 0, FACE_EXTERNAL, 0, 0, FACE_EXTERNAL)).c()
     fields = (_abi.WsField * 1)(_abi.WsField(8, 32, 0))
-    assert lib.ws_halo_pack_x(C.byref(g), fields, 1, 2, 8, None) == 1   # bad side
-    assert lib.ws_halo_unpack_x(C.byref(g), fields, 9, 0, 8, None) == 1  # 9 fields
-    assert lib.ws_halo_x_bytes(C.byref(g), 6) == 6 * 16 * 16 * 4 * 8
+    assert lib.ws_halo_pack(C.byref(g), fields, 1, 3, 0, 8, None) == 1      # bad axis
+    assert lib.ws_halo_pack(C.byref(g), fields, 1, 1, 2, 8, None) == 1      # bad side
+    assert lib.ws_halo_unpack(C.byref(g), fields, 9, 2, 0, 8, None) == 1    # 9 fields
+    assert lib.ws_halo_pack_x(C.byref(g), fields, 1, 2, 8, None) == 1
+    assert lib.ws_halo_bytes(C.byref(g), 0, 6) == 6 * 10 * 12 * 4 * 8
+    assert lib.ws_halo_bytes(C.byref(g), 1, 6) == 6 * 10 * 4 * 16 * 8
+    assert lib.ws_halo_bytes(C.byref(g), 2, 6) == 6 * 4 * 12 * 16 * 8
+    assert lib.ws_halo_x_bytes(C.byref(g), 6) == lib.ws_halo_bytes(C.byref(g), 0, 6)
     g.face_kind[0] = 7
     assert lib.ws_ghost_fill(C.byref(g), fields, 1, None) == 1
 
 
 # -- whole runs over oracle slabs --------------------------------------------
 VIS = dict(re=200.0, pr=0.72, ref_t=288.15, scheme=8)
+PE3 = (FACE_PERIODIC,) * 6
+MIX = (FACE_EXTRAP, FACE_EXTRAP, FACE_PERIODIC, FACE_PERIODIC, FACE_EXTRAP, FACE_EXTRAP)
+CLO = (FACE_CLOSURE, FACE_CLOSURE, FACE_CLOSURE, FACE_CLOSURE, FACE_PERIODIC, FACE_PERIODIC)
+# blocks: (grid, dims, viscous constants)
+BLOCK_CASES = {
+    "periodic_2x2x1": (Grid(24, 20, 10, faces=PE3), (2, 2, 1), None),
+    "periodic_1x2x2": (Grid(20, 18, 16, faces=PE3), (1, 2, 2), None),
+    "mixed_2x1x2": (Grid(26, 12, 17, faces=MIX), (2, 1, 2), None),
+    "closure_2x2x1": (Grid(32, 24, 8, faces=CLO), (2, 2, 1), None),
+    "periodic_2x2x2": (Grid(20, 16, 12, faces=PE3), (2, 2, 2), None),
+    "ns_mixed_2x2x1": (Grid(24, 20, 10, faces=MIX), (2, 2, 1), dict(VIS, scheme=6)),
+    "ns_periodic_1x2x2": (Grid(12, 18, 16, faces=PE3), (1, 2, 2), VIS),
+}
 CASES = {
     "periodic_2": (Grid(40, 12, 10, faces=(FACE_PERIODIC,) * 6), 2, None),
     "periodic_3": (Grid(37, 12, 10, faces=(FACE_PERIODIC,) * 6), 3, None),
@@ -121,6 +136,46 @@ def test_slabs_in_one_process_match_whole_grid(oracle, case):
     st.step(dt, NSTEPS)
     got = join_state(st.get_state())
     assert np.array_equal(got, want)
+
+
+def test_decompose_blocks_reference_order_and_neighbours():
+    """Rank = npx + NPX0 * (npy + NPY0 * npz) (OCFD_mpi.c:111-113); per-axis
+    extents by the reference's rule; periodic axes wrap, others end."""
+    g = Grid(30, 20, 12, faces=MIX)
+    blocks = decompose_blocks(g, (3, 2, 2))
+    assert [b.index for b in blocks] == list(range(12))
+    for b in blocks:
+        px, py, pz = b.coords
+        assert b.index == px + 3 * (py + 2 * pz)
+        assert (b.origin[0], b.n[0]) == slab_extents(30, 3)[px]
+        assert (b.origin[1], b.n[1]) == slab_extents(20, 2)[py]
+        assert (b.origin[2], b.n[2]) == slab_extents(12, 2)[pz]
+    b = blocks[0]                                       # (0, 0, 0)
+    assert b.nbr[0] == (None, 1) and b.nbr[1] == (3, 3) and b.nbr[2] == (None, 6)
+    assert b.faces == (FACE_EXTRAP, FACE_EXTERNAL, FACE_EXTERNAL, FACE_EXTERNAL,
+                       FACE_EXTRAP, FACE_EXTERNAL)
+    b = blocks[11]                                      # (2, 1, 1)
+    assert b.nbr[0] == (10, None) and b.nbr[1] == (8, 8) and b.nbr[2] == (5, None)
+    assert b.faces[0] == FACE_EXTERNAL and b.faces[1] == FACE_EXTRAP
+    f = np.random.default_rng(1).random((5, 12, 20, 30))
+    parts = [split_state(f, x) for x in blocks]
+    assert np.array_equal(join_state(parts, blocks), f)
+    with pytest.raises(ValueError):
+        decompose_blocks(Grid(30, 12, 12, faces=MIX), (3, 4, 1))      # 3 cells along y
+
+
+@pytest.mark.parametrize("case", sorted(BLOCK_CASES))
+def test_blocks_in_one_process_match_whole_grid(oracle, case):
+    g, dims, vis = BLOCK_CASES[case]
+    f = _state(g)
+    dt, want = _reference_run(oracle, g, f, NSTEPS, vis)
+    blocks = decompose_blocks(g, dims)
+    st = SlabStepper([OracleSlab(oracle, g, b) for b in blocks], LocalExchange())
+    st.set_viscous(vis)
+    st.set_state(f)
+    assert st.compute_dt(0.5) == dt
+    st.step(dt, NSTEPS)
+    assert np.array_equal(join_state(st.get_state(), blocks), want)
 
 
 def _free_port():
@@ -170,6 +225,50 @@ def test_gloo_ranks_match_whole_grid(oracle, case):
         got = join_state([np.load(os.path.join(d, f"slab{r}.npy")) for r in range(parts)])
         dts = [float(np.load(os.path.join(d, f"dt{r}.npy"))[0]) for r in range(parts)]
     assert dts == [dt] * parts
+    assert np.array_equal(got, want)
+
+
+def _block_rank_main(rank, world, port, case, out_dir):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import datetime
+
+    import torch.distributed as dist
+    from oracle.oracle import Oracle
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        oracle = Oracle()
+        oracle.set_threads(1)
+        g, dims, vis = BLOCK_CASES[case]
+        block = decompose_blocks(g, dims)[rank]
+        st = SlabStepper([OracleSlab(oracle, g, block)], DistExchange())
+        st.set_viscous(vis)
+        st.set_state(_state(g))
+        dt = st.compute_dt(0.5)
+        st.step(dt, NSTEPS)
+        np.save(os.path.join(out_dir, f"block{rank}.npy"), st.get_state()[0])
+        np.save(os.path.join(out_dir, f"dt{rank}.npy"), np.array([dt]))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("case", ["periodic_2x2x1", "mixed_2x1x2", "ns_periodic_1x2x2"])
+def test_gloo_block_ranks_match_whole_grid(oracle, case):
+    """One block per gloo rank (4 ranks): the exchange along every split axis,
+    two-rank periodic rings on each, the viscous fluxes' halos per direction."""
+    g, dims, vis = BLOCK_CASES[case]
+    world = dims[0] * dims[1] * dims[2]
+    f = _state(g)
+    dt, want = _reference_run(oracle, g, f, NSTEPS, vis)
+    blocks = decompose_blocks(g, dims)
+    with tempfile.TemporaryDirectory() as d:
+        mp.start_processes(_block_rank_main, args=(world, _free_port(), case, d), nprocs=world,
+                           join=True, start_method="spawn")
+        got = join_state([np.load(os.path.join(d, f"block{r}.npy")) for r in range(world)],
+                         blocks)
+        dts = [float(np.load(os.path.join(d, f"dt{r}.npy"))[0]) for r in range(world)]
+    assert dts == [dt] * world
     assert np.array_equal(got, want)
 
 

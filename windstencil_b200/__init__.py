@@ -9,7 +9,7 @@ Reference interface this mirrors (WindStencil, src/):
   du_invis_Jacobian3d_init  solver/OCFD_NS_Jacobian3d.cpp:24-33   -> du_invis_jacobian3d_init
   du_invis_Jacobian3d_x     solver/OCFD_NS_Jacobian3d.cpp:133-414 -> du_invis_jacobian3d
   exchange_boundary_xyz_packed_dev  mpi/OCFD_mpi_dev.cpp:123-290 -> ghost_fill (one domain),
-                                     halo_pack_x / halo_unpack_x + halo.SlabStepper (x slabs)
+                                     halo_pack / halo_unpack + halo.SlabStepper (blocks)
   get_duvwT / cons_to_pri_kernel     kernels/commen_kernel.cpp:78-119 -> cons_to_prim
   pri_to_cons_kernel_warp            kernels/commen_kernel.cpp:33-73  -> prim_to_cons
   OCFD_time_advance                  solver/OCFD_time.cpp:15-91        -> time_advance
@@ -29,7 +29,8 @@ from ._abi import (FACE_CLOSURE, FACE_EXTERNAL, FACE_EXTRAP, FACE_PERIODIC, FP64
 
 __all__ = [
     "FACE_CLOSURE", "FACE_EXTERNAL", "FACE_EXTRAP", "FACE_PERIODIC", "FP64", "MIXED", "LAP",
-    "WsError", "Grid", "make_grid", "halo_x_bytes", "halo_pack_x", "halo_unpack_x",
+    "WsError", "Grid", "make_grid", "halo_bytes", "halo_pack", "halo_unpack", "halo_x_bytes",
+    "halo_pack_x", "halo_unpack_x",
     "device_error",
     "lap_tensor", "soa_tensor", "field_desc", "soa_desc", "interior_job", "du_invis_jacobian3d",
     "du_vis_jacobian3d", "viscous", "restart_write", "restart_read", "metrics_write",
@@ -239,30 +240,43 @@ def device_error(stream=None) -> int:
     return v.value
 
 
-def halo_x_bytes(g: Grid, nfields: int) -> int:
-    """Bytes of one side's x halo: nfields x nz x ny x 4 doubles."""
+def halo_bytes(g: Grid, axis: int, nfields: int) -> int:
+    """Bytes of one side's halo along `axis`: nfields x 4 planes over the
+    interior of the other two axes."""
     gc = g.c()
-    return int(load().ws_halo_x_bytes(C.byref(gc), nfields))
+    return int(load().ws_halo_bytes(C.byref(gc), axis, nfields))
 
 
-def _halo(fn, g: Grid, fields, side: int, buf, stream):
+def halo_x_bytes(g: Grid, nfields: int) -> int:
+    return halo_bytes(g, 0, nfields)
+
+
+def _halo(fn, g: Grid, fields, axis: int, side: int, buf, stream):
     gc = g.c()
     arr = (WsField * len(fields))(*[f if isinstance(f, WsField) else field_desc(f)
                                     for f in fields])
     assert buf.dtype.itemsize == 8 and buf.is_contiguous()
-    assert buf.numel() * 8 >= halo_x_bytes(g, len(fields)), "halo buffer too small"
-    check(fn(C.byref(gc), arr, len(fields), side, buf.data_ptr(), _stream(stream)))
+    assert buf.numel() * 8 >= halo_bytes(g, axis, len(fields)), "halo buffer too small"
+    check(fn(C.byref(gc), arr, len(fields), axis, side, buf.data_ptr(), _stream(stream)))
+
+
+def halo_pack(g: Grid, fields, axis: int, side: int, buf, stream=None) -> None:
+    """Interior planes next to face (axis, side) (side 0 low, 1 high) of LAP
+    fields (tensors or WsField) -> buf (contiguous float64 device tensor)."""
+    _halo(load().ws_halo_pack, g, fields, axis, side, buf, stream)
+
+
+def halo_unpack(g: Grid, fields, axis: int, side: int, buf, stream=None) -> None:
+    """buf -> the ghost planes beyond face (axis, side) of the fields."""
+    _halo(load().ws_halo_unpack, g, fields, axis, side, buf, stream)
 
 
 def halo_pack_x(g: Grid, fields, side: int, buf, stream=None) -> None:
-    """Interior x planes next to face `side` (0 low, 1 high) of LAP fields
-    (tensors or WsField) -> buf (contiguous float64 device tensor)."""
-    _halo(load().ws_halo_pack_x, g, fields, side, buf, stream)
+    halo_pack(g, fields, 0, side, buf, stream)
 
 
 def halo_unpack_x(g: Grid, fields, side: int, buf, stream=None) -> None:
-    """buf -> the ghost x planes beyond face `side` of the fields."""
-    _halo(load().ws_halo_unpack_x, g, fields, side, buf, stream)
+    halo_unpack(g, fields, 0, side, buf, stream)
 
 
 def cons_to_prim(g: Grid, f, d, u, v, w, T, P=None, stream=None) -> None:
@@ -360,10 +374,10 @@ class Solver:
         """Second half: viscous divergence, fused RHS + stage update."""
         check(load().ws_solver_stage_end(self.h, krk, dt, _stream(stream)))
 
-    def stage_flux_fields(self):
-        """WsField descriptors of the four x-direction viscous fluxes."""
+    def stage_flux_fields(self, axis: int = 0):
+        """WsField descriptors of direction `axis`'s four viscous fluxes."""
         ev = (WsField * 4)()
-        check(load().ws_solver_stage_flux_fields(self.h, ev))
+        check(load().ws_solver_stage_flux_fields(self.h, axis, ev))
         return list(ev)
 
     def status(self, stream=None) -> int:

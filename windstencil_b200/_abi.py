@@ -101,6 +101,9 @@ SIGNATURES = {
     "ws_du_invis_jacobian3d_tiled": (_I, [C.POINTER(WsGrid), WsJob] + [WsField] * 5 +
                                      [C.POINTER(WsMetrics), WsSoa, WsTile, _P]),
     "ws_ghost_fill": (_I, [C.POINTER(WsGrid), C.POINTER(WsField), _I, _P]),
+    "ws_halo_bytes": (C.c_size_t, [C.POINTER(WsGrid), _I, _I]),
+    "ws_halo_pack": (_I, [C.POINTER(WsGrid), C.POINTER(WsField), _I, _I, _I, _P, _P]),
+    "ws_halo_unpack": (_I, [C.POINTER(WsGrid), C.POINTER(WsField), _I, _I, _I, _P, _P]),
     "ws_halo_x_bytes": (C.c_size_t, [C.POINTER(WsGrid), _I]),
     "ws_halo_pack_x": (_I, [C.POINTER(WsGrid), C.POINTER(WsField), _I, _I, _P, _P]),
     "ws_halo_unpack_x": (_I, [C.POINTER(WsGrid), C.POINTER(WsField), _I, _I, _P, _P]),
@@ -120,7 +123,7 @@ SIGNATURES = {
     "ws_solver_stage_fields": (_I, [_P, _I, C.POINTER(WsField)]),
     "ws_solver_stage_begin": (_I, [_P, _I, _P]),
     "ws_solver_stage_end": (_I, [_P, _I, C.c_double, _P]),
-    "ws_solver_stage_flux_fields": (_I, [_P, C.POINTER(WsField)]),
+    "ws_solver_stage_flux_fields": (_I, [_P, _I, C.POINTER(WsField)]),
     "ws_solver_status": (_I, [_P, C.POINTER(_I), _P]),
     "ws_solver_set_tile": (_I, [_P, WsTile]),
     "ws_solver_set_viscous": (_I, [_P, C.POINTER(WsViscous)]),

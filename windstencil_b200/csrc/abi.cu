@@ -44,9 +44,7 @@ int check_grid(const ws_grid* g) {
         if (k != WS_FACE_PERIODIC && k != WS_FACE_EXTRAP && k != WS_FACE_CLOSURE &&
             k != WS_FACE_EXTERNAL)
             return fail(WS_ERR_INVALID, "face_kind must be a ws_face_kind value");
-        if (k == WS_FACE_EXTERNAL && i >= 2)
-            return fail(WS_ERR_UNSUPPORTED, "EXTERNAL faces are x faces only "
-                                            "(slabs split along x)");
+
         if (k == WS_FACE_CLOSURE && i >= 4)
             return fail(WS_ERR_UNSUPPORTED, "CLOSURE faces are x and y faces only "
                                             "(the reference closes z through its ghosts)");
@@ -413,40 +411,54 @@ int ws_device_error(int* flags, ws_stream_t stream) {
     return WS_OK;
 }
 
-size_t ws_halo_x_bytes(const ws_grid* g, int nfields) {
-    if (!g || nfields < 1 || nfields > 8) return 0;
-    return (size_t)nfields * g->nz * g->ny * 4 * sizeof(double);
+size_t ws_halo_bytes(const ws_grid* g, int axis, int nfields) {
+    if (!g || nfields < 1 || nfields > 8 || axis < 0 || axis > 2) return 0;
+    const size_t n[3] = {g->nx, g->ny, g->nz};
+    size_t c = (size_t)nfields * 4 * sizeof(double);
+    for (int d = 0; d < 3; ++d)
+        if (d != axis) c *= n[d];
+    return c;
 }
 
-int ws_halo_pack_x(const ws_grid* g, const ws_field* fields, int nfields, int side, void* buf,
-                   ws_stream_t stream) {
+namespace {
+int halo_call(const ws_grid* g, const ws_field* fields, int nfields, int axis, int side,
+              const void* buf, bool pack, ws_stream_t stream) {
     int rc;
     if ((rc = check_grid(g))) return rc;
     if (!fields || nfields < 1 || nfields > 8)
-        return fail(WS_ERR_INVALID, "halo pack takes 1..8 fields");
+        return fail(WS_ERR_INVALID, "a halo takes 1..8 fields");
+    if (axis < 0 || axis > 2) return fail(WS_ERR_INVALID, "axis must be 0, 1 or 2");
     if (side != 0 && side != 1) return fail(WS_ERR_INVALID, "side must be 0 or 1");
     if (!buf || (reinterpret_cast<uintptr_t>(buf) & 7))
         return fail(WS_ERR_INVALID, "halo buffer NULL or not 8-byte aligned");
     for (int i = 0; i < nfields; ++i)
         if ((rc = check_field(g, fields[i], "field"))) return rc;
-    return launch_halo_x(g, fields, nfields, side, static_cast<double*>(buf), true,
-                         (cudaStream_t)stream);
+    return launch_halo(g, fields, nfields, axis, side,
+                       const_cast<double*>(static_cast<const double*>(buf)), pack,
+                       (cudaStream_t)stream);
+}
+}  // namespace
+
+int ws_halo_pack(const ws_grid* g, const ws_field* fields, int nfields, int axis, int side,
+                 void* buf, ws_stream_t stream) {
+    return halo_call(g, fields, nfields, axis, side, buf, true, stream);
+}
+
+int ws_halo_unpack(const ws_grid* g, const ws_field* fields, int nfields, int axis, int side,
+                   const void* buf, ws_stream_t stream) {
+    return halo_call(g, fields, nfields, axis, side, buf, false, stream);
+}
+
+size_t ws_halo_x_bytes(const ws_grid* g, int nfields) { return ws_halo_bytes(g, 0, nfields); }
+
+int ws_halo_pack_x(const ws_grid* g, const ws_field* fields, int nfields, int side, void* buf,
+                   ws_stream_t stream) {
+    return halo_call(g, fields, nfields, 0, side, buf, true, stream);
 }
 
 int ws_halo_unpack_x(const ws_grid* g, const ws_field* fields, int nfields, int side,
                      const void* buf, ws_stream_t stream) {
-    int rc;
-    if ((rc = check_grid(g))) return rc;
-    if (!fields || nfields < 1 || nfields > 8)
-        return fail(WS_ERR_INVALID, "halo unpack takes 1..8 fields");
-    if (side != 0 && side != 1) return fail(WS_ERR_INVALID, "side must be 0 or 1");
-    if (!buf || (reinterpret_cast<uintptr_t>(buf) & 7))
-        return fail(WS_ERR_INVALID, "halo buffer NULL or not 8-byte aligned");
-    for (int i = 0; i < nfields; ++i)
-        if ((rc = check_field(g, fields[i], "field"))) return rc;
-    return launch_halo_x(g, fields, nfields, side,
-                         const_cast<double*>(static_cast<const double*>(buf)), false,
-                         (cudaStream_t)stream);
+    return halo_call(g, fields, nfields, 0, side, buf, false, stream);
 }
 
 int ws_cons_to_prim(const ws_grid* g, ws_soa f, ws_field d, ws_field u, ws_field v, ws_field w,

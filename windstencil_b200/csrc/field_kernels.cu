@@ -6,8 +6,8 @@
 //                  LAP-extended job by OCFD_NS_Jacobian3d.cpp:24-33)
 //   ghost fill     src/mpi/OCFD_mpi_dev.cpp:123-290 (host-staged periodic
 //                  self-exchange; here an in-place device copy)
-//   x halo planes  cudaFieldBoundaryPack/Unpack_kernel with the jobs of
-//                  exchange_boundary_x_packed_dev, OCFD_mpi_dev.cpp:137-218
+//   halo planes    cudaFieldBoundaryPack/Unpack_kernel with the jobs of
+//                  exchange_boundary_{x,y,z}_packed_dev, OCFD_mpi_dev.cpp:137-290
 //   cons->prim     src/kernels/commen_kernel.cpp:78-119
 //   prim->cons     src/kernels/commen_kernel.cpp:33-73
 //   RK3 stages     src/solver/OCFD_time.cpp:15-91
@@ -78,10 +78,10 @@ struct GhostArgs {
 };
 
 // value at a ghost point = value at the wrapped / clamped coordinates.  The
-// source is an interior point, or an x ghost at interior y, z of an EXTERNAL
-// face (which this pass never writes), so one pass fills every face without
-// ordering between them; EXTERNAL ghosts at interior y, z map onto themselves
-// and are skipped.
+// source is an interior point, or a ghost of an EXTERNAL face at interior
+// coordinates of the two other axes (which this pass never writes), so one
+// pass fills every face without ordering between them; those EXTERNAL ghosts
+// map onto themselves and are skipped.
 __device__ __forceinline__ void ghost_fill_point(const GhostArgs& a, long t) {
     int i, j, k;
     ghost_point(t, a.nx, a.ny, a.nz, i, j, k);
@@ -105,24 +105,27 @@ __global__ void ghost_fill_kernel(const __grid_constant__ GhostArgs a) {
 struct HaloArgs {
     double* ptr[8];
     uint32_t pitch[8];
-    int nf, ny, nz;
-    int x0;          // first LAP x plane of the four
-    double* buf;     // [nf][nz][ny][4]
+    int nf, ny;
+    int b[3];        // box extents in x, y, z (4 along the halo's axis)
+    int o[3];        // box origin, LAP coordinates
+    double* buf;     // [nf][b2][b1][b0]
     int pack;        // 1: planes -> buf, 0: buf -> planes
 };
 
-// one double per thread in buffer order: a warp covers 8 rows of 4 planes
-__global__ void halo_x_kernel(const __grid_constant__ HaloArgs a) {
-    const long total = (long)a.nf * a.nz * a.ny * 4;
+// one double per thread in buffer order (x fastest): the 4 planes along the
+// halo's axis over the interior of the two other axes
+__global__ void halo_kernel(const __grid_constant__ HaloArgs a) {
+    const long per = (long)a.b[0] * a.b[1] * a.b[2];
+    const long total = (long)a.nf * per;
     for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total;
          t += (long)gridDim.x * blockDim.x) {
-        const int m = (int)(t & 3);
-        const long r = t >> 2;
-        const int j = (int)(r % a.ny);
-        const long r2 = r / a.ny;
-        const int k = (int)(r2 % a.nz);
-        const int f = (int)(r2 / a.nz);
-        double* p = a.ptr[f] + lap_idx(a.x0 + m, j + 4, k + 4, a.pitch[f], a.ny);
+        const int f = (int)(t / per);
+        long r = t - (long)f * per;
+        const int i = (int)(r % a.b[0]);
+        r /= a.b[0];
+        const int j = (int)(r % a.b[1]);
+        const int k = (int)(r / a.b[1]);
+        double* p = a.ptr[f] + lap_idx(a.o[0] + i, a.o[1] + j, a.o[2] + k, a.pitch[f], a.ny);
         if (a.pack)
             a.buf[t] = *p;
         else
@@ -267,9 +270,10 @@ int launch_ghost_fill(const ws_grid* g, const ws_field* f, int nf, cudaStream_t 
     return WS_OK;
 }
 
-int launch_halo_x(const ws_grid* g, const ws_field* f, int nf, int side, double* buf, bool pack,
-                  cudaStream_t st) {
+int launch_halo(const ws_grid* g, const ws_field* f, int nf, int axis, int side, double* buf,
+                bool pack, cudaStream_t st) {
     if (nf < 1 || nf > 8) return fail(WS_ERR_INVALID, "halo: 1..8 fields");
+    if (axis < 0 || axis > 2) return fail(WS_ERR_INVALID, "halo: axis must be 0, 1 or 2");
     HaloArgs a{};
     for (int i = 0; i < nf; ++i) {
         a.ptr[i] = f[i].ptr;
@@ -277,14 +281,18 @@ int launch_halo_x(const ws_grid* g, const ws_field* f, int nf, int side, double*
     }
     a.nf = nf;
     a.ny = g->ny;
-    a.nz = g->nz;
-    // pack: interior planes 4..7 (low) / nx..nx+3 (high);
-    // unpack: ghost planes 0..3 (low) / nx+4..nx+7 (high)
-    a.x0 = pack ? (side == 0 ? 4 : (int)g->nx) : (side == 0 ? 0 : (int)g->nx + 4);
+    const int n[3] = {(int)g->nx, (int)g->ny, (int)g->nz};
+    for (int d = 0; d < 3; ++d) {
+        a.b[d] = d == axis ? 4 : n[d];
+        a.o[d] = 4;
+    }
+    // pack: interior planes 4..7 (low) / n..n+3 (high);
+    // unpack: ghost planes 0..3 (low) / n+4..n+7 (high)
+    a.o[axis] = pack ? (side == 0 ? 4 : n[axis]) : (side == 0 ? 0 : n[axis] + 4);
     a.buf = buf;
     a.pack = pack ? 1 : 0;
-    const long n = (long)nf * g->nz * g->ny * 4;
-    halo_x_kernel<<<grid_for(n, 256), 256, 0, st>>>(a);
+    const long total = (long)nf * a.b[0] * a.b[1] * a.b[2];
+    halo_kernel<<<grid_for(total, 256), 256, 0, st>>>(a);
     WS_CUDA(cudaGetLastError());
     return WS_OK;
 }

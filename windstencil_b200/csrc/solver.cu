@@ -272,7 +272,7 @@ int ws_solver_fields(ws_solver* s, ws_soa* f, ws_soa* du, ws_field prims[6]) {
 int ws_solver_rhs(ws_solver* s, ws_stream_t stream) {
     if (!s) return fail(WS_ERR_INVALID, "solver is NULL");
     if (s->viscous && has_external(&s->s.g))
-        return fail(WS_ERR_UNSUPPORTED, "viscous RHS of an EXTERNAL grid: the x fluxes' "
+        return fail(WS_ERR_UNSUPPORTED, "viscous RHS of an EXTERNAL grid: the fluxes' "
                                         "halos come from ws_solver_stage_begin / _end");
     return enqueue_rhs(s, (cudaStream_t)stream);
 }
@@ -350,7 +350,7 @@ int ws_solver_stage(ws_solver* s, int krk, double dt, ws_stream_t stream) {
     if (s->viscous && has_external(&s->s.g))
         return fail(WS_ERR_UNSUPPORTED, "with viscous terms an EXTERNAL grid stages in two "
                                         "halves (ws_solver_stage_begin / _end) with the "
-                                        "x fluxes' halo exchange between them");
+                                        "fluxes' halo exchange between them");
     int rc = enqueue_stage(s, s->s.cur, krk, dt, (cudaStream_t)stream);
     if (rc) return rc;
     advance_stage(s, krk);
@@ -374,12 +374,13 @@ int ws_solver_stage_end(ws_solver* s, int krk, double dt, ws_stream_t stream) {
     return WS_OK;
 }
 
-int ws_solver_stage_flux_fields(ws_solver* s, ws_field ev_x[4]) {
-    if (!s || !ev_x) return fail(WS_ERR_INVALID, "NULL argument");
+int ws_solver_stage_flux_fields(ws_solver* s, int axis, ws_field ev_axis[4]) {
+    if (!s || !ev_axis) return fail(WS_ERR_INVALID, "NULL argument");
+    if (axis < 0 || axis > 2) return fail(WS_ERR_INVALID, "axis must be 0, 1 or 2");
     if (!s->viscous) return fail(WS_ERR_INVALID, "the solver has no viscous terms");
     ws_field ev[12];
     vis_flux_fields(&s->s.g, s->vis_ws, ev);
-    for (int q = 0; q < 4; ++q) ev_x[q] = ev[q];
+    for (int q = 0; q < 4; ++q) ev_axis[q] = ev[4 * axis + q];
     return WS_OK;
 }
 

@@ -24,10 +24,12 @@ inline int status_code(int v) {
 }
 // any face of kind WS_FACE_EXTERNAL (ghosts written by the caller's halo exchange)
 bool has_external(const ws_grid* g);
-// 4 x planes of nf LAP fields <-> halo buffer [nf][nz][ny][4]: pack reads the
-// interior planes next to face `side`, unpack writes the ghost planes beyond it
-int launch_halo_x(const ws_grid* g, const ws_field* f, int nf, int side, double* buf, bool pack,
-                  cudaStream_t st);
+// 4 planes along `axis` of nf LAP fields <-> halo buffer [nf][b2][b1][b0]
+// (b = the planes' box: 4 along the axis, the interior along the others):
+// pack reads the interior planes next to face `side`, unpack writes the ghost
+// planes beyond it
+int launch_halo(const ws_grid* g, const ws_field* f, int nf, int axis, int side, double* buf,
+                bool pack, cudaStream_t st);
 
 // Error reporting: the message of the last failure, per host thread.
 void set_error(const std::string& msg);

@@ -1,36 +1,43 @@
-"""halo -- one grid split into slabs along x, stepped with an x-halo exchange
-before every SSP-RK3 stage.
+"""halo -- one grid split into blocks along x, y and z (slabs along x are the
+common case), stepped with a halo exchange before every SSP-RK3 stage.
 
-Replaces the reference's MPI x decomposition and its per-RHS exchange:
+Replaces the reference's MPI decomposition and its per-RHS exchange:
 
-  slab extents   OCFD_mpi.c:124-145 (nx = NX_GLOBAL / NPX0; the first
-                 NX_GLOBAL % NPX0 subdomains one cell wider; offsets i_offset)
-  neighbours     ID_XM1 / ID_XP1 (OCFD_mpi.c:176-197): wrapped when x is
-                 periodic, none at the ends of a non-periodic x
-  exchange       exchange_boundary_x_packed_dev (OCFD_mpi_dev.cpp:185-218):
-                 the 4 interior planes next to each x face, packed
-                 [field][z][y][x] over interior y, z, go to the neighbour on
-                 that side and land in its ghost planes
+  process grid   NPX0 x NPY0 x NPZ0 ranks, rank = npx + NPX0 * (npy + NPY0 *
+                 npz) (OCFD_mpi.c:102-121)
+  extents        per axis n = N_GLOBAL / NP, the first N_GLOBAL % NP
+                 subdomains one cell wider (OCFD_mpi.c:124-145 and its y, z
+                 counterparts)
+  neighbours     ID_XM1 / ID_XP1 and the y, z ones (OCFD_mpi.c:176-197):
+                 wrapped when the axis is periodic, none at the ends of a
+                 non-periodic axis
+  exchange       exchange_boundary_{x,y,z}_packed_dev (OCFD_mpi_dev.cpp:
+                 123-290): the 4 interior planes next to each shared face,
+                 packed over the interior of the other two axes, go to the
+                 neighbour on that side and land in its ghost planes
   time loop      OCFD_NS_Solver.cpp:64-90: exchange, du_comput, time advance
 
 The reference copies every packed plane set through host memory and a
 blocking MPI_Sendrecv.  Here the planes stay on the device: a pack kernel,
 point-to-point sends over NVLink (NCCL through torch.distributed, one rank
-per GPU), an unpack kernel, all ordered on the current stream; slabs that
+per GPU), an unpack kernel, all ordered on the current stream; blocks that
 share a process unpack straight from their neighbour's pack buffer.  Each
-slab steps with its fused RHS + stage kernel (ws_solver_stage) on a grid
-whose shared x faces are WS_FACE_EXTERNAL.
+block steps with its fused RHS + stage kernel (ws_solver_stage) on a grid
+whose shared faces are WS_FACE_EXTERNAL.  The stencils are one-dimensional,
+so no edge or corner ghosts are needed and the axes' exchanges are
+independent of each other.
 
 The stage's halo carries d, u, v, w, T and cc: every ghost value the stage
 reads (the reference exchanges d, u, v, w, T and recomputes cc on the padded
 field; cc travels here instead of being recomputed).  With viscous terms a
-second halo per stage carries the four x-direction viscous fluxes between
-their flux pass and their divergence, as the reference exchanges Ev1..4
-between vis_flux_ker and their derivatives (OCFD_Stream.cpp:229-345).
+second halo per stage carries, along each axis, that direction's four
+viscous fluxes between their flux pass and their divergence, as the
+reference exchanges Ev1..4 between vis_flux_ker and their derivatives
+(OCFD_Stream.cpp:229-345).
 
 This module holds the decomposition, the exchange and the stage sequence;
-the per-slab kernels live in libwindstencil_b200.so (CudaSlab).  Anything
-with CudaSlab's methods can stand in for it (the CPU tests run the oracle
+the per-block kernels live in libwindstencil_b200.so (CudaBlock).  Anything
+with CudaBlock's methods can stand in for it (the CPU tests run the oracle
 that way over gloo ranks).
 """
 from __future__ import annotations
@@ -40,20 +47,20 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from . import (FACE_CLOSURE, FACE_EXTERNAL, FACE_PERIODIC, Grid, Solver, halo_pack_x,
-               halo_unpack_x, halo_x_bytes)
+from . import (FACE_CLOSURE, FACE_EXTERNAL, FACE_PERIODIC, Grid, Solver, halo_bytes, halo_pack,
+               halo_unpack)
 
 HALO_FIELDS = 6          # d, u, v, w, T, cc
-FLUX_FIELDS = 4          # x-direction viscous fluxes Ev1..4
+FLUX_FIELDS = 4          # one direction's viscous fluxes Ev1..4
 PRIMS, FLUX = "prims", "flux"       # the two halos of a stage
-LO, HI = 0, 1            # x faces of a slab
+LO, HI = 0, 1            # the faces of an axis
 
 
 def slab_extents(nx: int, parts: int) -> list[tuple[int, int]]:
-    """(first global x cell, cells) of each slab: the reference's split
-    (OCFD_mpi.c:124-145), the remainder going to the first slabs."""
+    """(first global cell, cells) of each part of an axis: the reference's
+    split (OCFD_mpi.c:124-145), the remainder going to the first parts."""
     if parts < 1 or nx < parts:
-        raise ValueError(f"cannot split {nx} cells into {parts} slabs")
+        raise ValueError(f"cannot split {nx} cells into {parts} parts")
     base, rem = divmod(nx, parts)
     out, x0 = [], 0
     for k in range(parts):
@@ -64,78 +71,160 @@ def slab_extents(nx: int, parts: int) -> list[tuple[int, int]]:
 
 
 @dataclass(frozen=True)
-class Slab:
-    """Slab `index` of `parts`: global x cells [x0, x0 + nx), its neighbours'
-    indices (None at a non-periodic end) and its face kinds."""
+class Block:
+    """Block `index` of a dims[0] x dims[1] x dims[2] process grid (index x
+    fastest): global cells [origin, origin + n) per axis, the neighbours'
+    indices per axis and side (None at a non-periodic end or when the axis
+    is not split) and the block's face kinds."""
     index: int
-    parts: int
-    x0: int
-    nx: int
-    left: int | None
-    right: int | None
+    dims: tuple
+    coords: tuple
+    origin: tuple
+    n: tuple
+    nbr: tuple          # ((lo, hi) for x, y, z)
     faces: tuple
 
+    # the x-slab view
+    @property
+    def parts(self) -> int:
+        return self.dims[0]
 
-def decompose(grid: Grid, parts: int) -> list[Slab]:
-    """Split `grid` into `parts` slabs along x.  Shared faces become
-    WS_FACE_EXTERNAL; the grid's own x faces stay at the two ends.  One slab
-    keeps the grid as it is (a periodic x wraps onto itself)."""
-    lo, hi = grid.faces[0], grid.faces[1]
-    if (lo == FACE_PERIODIC) != (hi == FACE_PERIODIC):
-        raise ValueError("x must be periodic at both faces or at neither")
-    if FACE_EXTERNAL in (lo, hi):
-        raise ValueError("the grid to split must not have EXTERNAL faces")
-    periodic = lo == FACE_PERIODIC
-    slabs = []
-    for k, (x0, n) in enumerate(slab_extents(grid.nx, parts)):
-        if parts == 1:
-            left = right = None
-            faces = tuple(grid.faces)
-        else:
-            left = k - 1 if k > 0 else (parts - 1 if periodic else None)
-            right = k + 1 if k < parts - 1 else (0 if periodic else None)
-            faces = (FACE_EXTERNAL if left is not None else lo,
-                     FACE_EXTERNAL if right is not None else hi) + tuple(grid.faces[2:])
-        # a ghost plane set comes from one neighbour's 4 nearest planes
-        need = 8 if FACE_CLOSURE in faces[:2] else 4
-        if n < need:
-            raise ValueError(f"slab {k} has {n} cells along x; needs >= {need}")
-        slabs.append(Slab(k, parts, x0, n, left, right, faces))
-    return slabs
+    @property
+    def x0(self) -> int:
+        return self.origin[0]
+
+    @property
+    def nx(self) -> int:
+        return self.n[0]
+
+    @property
+    def left(self):
+        return self.nbr[0][LO]
+
+    @property
+    def right(self):
+        return self.nbr[0][HI]
+
+    def sides(self, axis: int) -> list[int]:
+        return [s for s in (LO, HI) if self.nbr[axis][s] is not None]
 
 
-def slab_grid(grid: Grid, slab: Slab) -> Grid:
-    """The slab's own grid: its x extent and face kinds, the global spacing."""
-    return dataclasses.replace(grid, nx=slab.nx, hx=grid.hx, hy=grid.hy, hz=grid.hz,
-                               faces=tuple(slab.faces))
+Slab = Block
 
 
-def split_state(f: np.ndarray, slab: Slab) -> np.ndarray:
-    """The slab's part of a dense conserved state (5, nz, ny, nx)."""
-    return np.ascontiguousarray(f[..., slab.x0:slab.x0 + slab.nx])
+def block_index(dims, coords) -> int:
+    return coords[0] + dims[0] * (coords[1] + dims[1] * coords[2])
 
 
-def join_state(parts: list[np.ndarray]) -> np.ndarray:
-    return np.concatenate(parts, axis=-1)
+def decompose_blocks(grid: Grid, dims) -> list[Block]:
+    """Split `grid` into dims[0] x dims[1] x dims[2] blocks.  Faces shared
+    with a neighbour become WS_FACE_EXTERNAL; the grid's own faces stay at
+    the ends of each axis.  An axis split in one part keeps its faces (a
+    periodic axis wraps onto itself)."""
+    dims = tuple(int(d) for d in dims)
+    if len(dims) != 3 or min(dims) < 1:
+        raise ValueError("dims: three positive part counts")
+    n_glob = (grid.nx, grid.ny, grid.nz)
+    per = []
+    for ax in range(3):
+        lo, hi = grid.faces[2 * ax], grid.faces[2 * ax + 1]
+        if (lo == FACE_PERIODIC) != (hi == FACE_PERIODIC):
+            raise ValueError(f"axis {ax} must be periodic at both faces or at neither")
+        if FACE_EXTERNAL in (lo, hi):
+            raise ValueError("the grid to split must not have EXTERNAL faces")
+        per.append(slab_extents(n_glob[ax], dims[ax]))
+    blocks = []
+    for pz in range(dims[2]):
+        for py in range(dims[1]):
+            for px in range(dims[0]):
+                c = (px, py, pz)
+                origin, n, nbr, faces = [], [], [], []
+                for ax in range(3):
+                    P, k = dims[ax], c[ax]
+                    lo, hi = grid.faces[2 * ax], grid.faces[2 * ax + 1]
+                    o, m = per[ax][k]
+                    origin.append(o)
+                    n.append(m)
+                    if P == 1:
+                        nb = (None, None)
+                        fk = (lo, hi)
+                    else:
+                        periodic = lo == FACE_PERIODIC
+                        left = k - 1 if k > 0 else (P - 1 if periodic else None)
+                        right = k + 1 if k < P - 1 else (0 if periodic else None)
+                        nb = tuple(None if kk is None else
+                                   block_index(dims, c[:ax] + (kk,) + c[ax + 1:])
+                                   for kk in (left, right))
+                        fk = (FACE_EXTERNAL if left is not None else lo,
+                              FACE_EXTERNAL if right is not None else hi)
+                    # a ghost plane set comes from one neighbour's 4 nearest planes
+                    need = 8 if FACE_CLOSURE in fk else 4
+                    if m < need:
+                        raise ValueError(f"block {c} has {m} cells along axis {ax}; "
+                                         f"needs >= {need}")
+                    nbr.append(nb)
+                    faces.extend(fk)
+                blocks.append(Block(block_index(dims, c), dims, c, tuple(origin), tuple(n),
+                                    tuple(nbr), tuple(faces)))
+    return blocks
 
 
-class CudaSlab:
-    """One slab's state and kernels on the current CUDA device: a ws_solver
-    over the slab grid, plus its send and receive halo buffers (sized for the
-    larger halo; the flux halo uses their leading part)."""
+def decompose(grid: Grid, parts: int) -> list[Block]:
+    """Split `grid` into `parts` slabs along x."""
+    return decompose_blocks(grid, (parts, 1, 1))
 
-    def __init__(self, grid: Grid, slab: Slab):
+
+def block_grid(grid: Grid, block: Block) -> Grid:
+    """The block's own grid: its extents and face kinds, the global spacing."""
+    return dataclasses.replace(grid, nx=block.n[0], ny=block.n[1], nz=block.n[2], hx=grid.hx,
+                               hy=grid.hy, hz=grid.hz, faces=tuple(block.faces))
+
+
+slab_grid = block_grid
+
+
+def split_state(f: np.ndarray, block: Block) -> np.ndarray:
+    """The block's part of a dense conserved state (5, nz, ny, nx)."""
+    (x0, y0, z0), (nx, ny, nz) = block.origin, block.n
+    return np.ascontiguousarray(f[:, z0:z0 + nz, y0:y0 + ny, x0:x0 + nx])
+
+
+def join_state(parts: list[np.ndarray], blocks: list[Block] | None = None) -> np.ndarray:
+    """The whole state from the blocks' states (x slabs: in slab order)."""
+    if blocks is None:
+        return np.concatenate(parts, axis=-1)
+    ext = [0, 0, 0]
+    for b in blocks:
+        for ax in range(3):
+            ext[ax] = max(ext[ax], b.origin[ax] + b.n[ax])
+    out = np.empty((5, ext[2], ext[1], ext[0]))
+    for p, b in zip(parts, blocks):
+        (x0, y0, z0), (bx, by, bz) = b.origin, b.n
+        out[:, z0:z0 + bz, y0:y0 + by, x0:x0 + bx] = p
+    return out
+
+
+class CudaBlock:
+    """One block's state and kernels on the current CUDA device: a ws_solver
+    over the block grid, plus send and receive halo buffers per split axis
+    (sized for the larger halo; the flux halo uses their leading part)."""
+
+    def __init__(self, grid: Grid, block: Block):
         import torch
-        self.slab = slab
-        self.grid = slab_grid(grid, slab)
+        self.slab = self.block = block
+        self.grid = block_grid(grid, block)
         self.solver = Solver(self.grid)
-        self.n = {PRIMS: halo_x_bytes(self.grid, HALO_FIELDS) // 8,
-                  FLUX: halo_x_bytes(self.grid, FLUX_FIELDS) // 8}
         dev = torch.device("cuda", torch.cuda.current_device())
-        self._send = [torch.empty(self.n[PRIMS], dtype=torch.float64, device=dev)
-                      for _ in range(2)]
-        self._recv = [torch.empty(self.n[PRIMS], dtype=torch.float64, device=dev)
-                      for _ in range(2)]
+        self.n, self._send, self._recv = {}, {}, {}
+        for ax in range(3):
+            if not block.sides(ax):
+                continue
+            self.n[ax, PRIMS] = halo_bytes(self.grid, ax, HALO_FIELDS) // 8
+            self.n[ax, FLUX] = halo_bytes(self.grid, ax, FLUX_FIELDS) // 8
+            self._send[ax] = [torch.empty(self.n[ax, PRIMS], dtype=torch.float64, device=dev)
+                              for _ in range(2)]
+            self._recv[ax] = [torch.empty(self.n[ax, PRIMS], dtype=torch.float64, device=dev)
+                              for _ in range(2)]
         self.krk = 1     # the stage due next
         self.viscous = False
 
@@ -143,31 +232,31 @@ class CudaSlab:
         self.solver.set_viscous(vis)
         self.viscous = vis is not None
 
-    def set_state(self, f_slab: np.ndarray) -> None:
-        self.solver.set_state(f_slab)
+    def set_state(self, f_block: np.ndarray) -> None:
+        self.solver.set_state(f_block)
         self.krk = 1
 
     def get_state(self) -> np.ndarray:
         return self.solver.get_state()
 
-    def send(self, side: int, kind: str = PRIMS):
-        return self._send[side][:self.n[kind]]
+    def send(self, axis: int, side: int, kind: str = PRIMS):
+        return self._send[axis][side][:self.n[axis, kind]]
 
-    def recv(self, side: int, kind: str = PRIMS):
-        return self._recv[side][:self.n[kind]]
+    def recv(self, axis: int, side: int, kind: str = PRIMS):
+        return self._recv[axis][side][:self.n[axis, kind]]
 
-    def _fields(self, kind):
+    def _fields(self, axis, kind):
         if kind == PRIMS:
             return self.solver.stage_fields(self.krk)
-        return self.solver.stage_flux_fields()
+        return self.solver.stage_flux_fields(axis)
 
-    def pack(self, side: int, kind: str = PRIMS) -> None:
-        """Planes next to face `side` of the halo's fields -> send(side, kind)."""
-        halo_pack_x(self.grid, self._fields(kind), side, self.send(side, kind))
+    def pack(self, axis: int, side: int, kind: str = PRIMS) -> None:
+        """Planes next to face (axis, side) of the halo's fields -> send buffer."""
+        halo_pack(self.grid, self._fields(axis, kind), axis, side, self.send(axis, side, kind))
 
-    def unpack(self, side: int, buf, kind: str = PRIMS) -> None:
-        """buf -> ghost planes beyond face `side` of the halo's fields."""
-        halo_unpack_x(self.grid, self._fields(kind), side, buf)
+    def unpack(self, axis: int, side: int, buf, kind: str = PRIMS) -> None:
+        """buf -> ghost planes beyond face (axis, side) of the halo's fields."""
+        halo_unpack(self.grid, self._fields(axis, kind), axis, side, buf)
 
     def begin(self) -> None:
         """First half of the due stage (ghost fill, viscous flux pass)."""
@@ -188,41 +277,41 @@ class CudaSlab:
         self.solver.close()
 
 
-def _sides(slab: Slab):
-    return [s for s, nb in ((LO, slab.left), (HI, slab.right)) if nb is not None]
+CudaSlab = CudaBlock
 
 
 class LocalExchange:
-    """Every slab lives in this process (one or several devices with peer
-    access): each slab's ghost planes come straight from its neighbour's
+    """Every block lives in this process (one or several devices with peer
+    access): each block's ghost planes come straight from its neighbour's
     send buffer; no copy in between."""
 
     def run(self, runners: list, kind: str = PRIMS) -> None:
-        by_index = {r.slab.index: r for r in runners}
-        for r in runners:
-            for side in _sides(r.slab):
-                r.pack(side, kind)
-        for r in runners:
-            if r.slab.left is not None:
-                r.unpack(LO, by_index[r.slab.left].send(HI, kind), kind)
-            if r.slab.right is not None:
-                r.unpack(HI, by_index[r.slab.right].send(LO, kind), kind)
+        by_index = {r.block.index: r for r in runners}
+        for ax in range(3):
+            for r in runners:
+                for side in r.block.sides(ax):
+                    r.pack(ax, side, kind)
+            for r in runners:
+                for side in r.block.sides(ax):
+                    nb = by_index[r.block.nbr[ax][side]]
+                    r.unpack(ax, side, nb.send(ax, 1 - side, kind), kind)
 
     def min(self, x: float) -> float:
         return x
 
 
 class DistExchange:
-    """One slab per rank of a torch.distributed group, slab index = group
+    """One block per rank of a torch.distributed group, block index = group
     rank: point-to-point sends of the packed planes, issued as one batch.
     With NCCL the device buffers go straight over NVLink; with a backend
     that moves host memory only (gloo) device buffers are staged through
     pinned host copies, as the reference stages its packs for MPI.
 
-    Order and tags make a two-slab periodic ring (both neighbours the same
-    rank) match as well: sends go low planes first, receives take the high
-    ghosts first, and each message is tagged with the side it was packed
-    from (0 low, 1 high)."""
+    Per axis, sends go low planes first and receives take the high ghosts
+    first, and each message is tagged with its axis and the side it was
+    packed from, so a two-block periodic ring (the same rank on both sides)
+    matches too; the axes follow each other in the same order on every
+    rank."""
 
     def __init__(self, group=None):
         import torch.distributed as dist
@@ -230,6 +319,11 @@ class DistExchange:
         self.group = group
         self.device_p2p = dist.get_backend(group) == "nccl"
         self._host = {}
+
+    def _peer(self, index: int) -> int:
+        if self.group is None:
+            return index
+        return self.dist.get_global_rank(self.group, index)
 
     def _staged(self, t, key):
         """The buffer the transport moves: t itself, or its pinned host twin."""
@@ -242,41 +336,44 @@ class DistExchange:
             self._host[key] = h
         return h
 
-    def _peer(self, index: int) -> int:
-        if self.group is None:
-            return index
-        return self.dist.get_global_rank(self.group, index)
-
     def run(self, runners: list, kind: str = PRIMS) -> None:
         dist = self.dist
         if len(runners) != 1:
-            raise ValueError("DistExchange runs one slab per rank")
+            raise ValueError("DistExchange runs one block per rank")
         r = runners[0]
-        s = r.slab
-        sides = _sides(s)
-        for side in sides:
-            r.pack(side, kind)
-        send = {side: self._staged(r.send(side, kind), ("s", side, kind)) for side in sides}
-        recv = {side: self._staged(r.recv(side, kind), ("r", side, kind)) for side in sides}
-        for side in sides:
-            if send[side] is not r.send(side, kind):
-                send[side].copy_(r.send(side, kind))      # synchronous device -> host
+        b = r.block
+        axes = [ax for ax in range(3) if b.sides(ax)]
+        send, recv = {}, {}
+        for ax in axes:
+            for side in b.sides(ax):
+                r.pack(ax, side, kind)
+                send[ax, side] = self._staged(r.send(ax, side, kind), ("s", ax, side, kind))
+                recv[ax, side] = self._staged(r.recv(ax, side, kind), ("r", ax, side, kind))
+                if send[ax, side] is not r.send(ax, side, kind):
+                    send[ax, side].copy_(r.send(ax, side, kind))   # synchronous D2H
         ops = []
-        if s.left is not None:
-            ops.append(dist.P2POp(dist.isend, send[LO], self._peer(s.left), self.group, LO))
-        if s.right is not None:
-            ops.append(dist.P2POp(dist.isend, send[HI], self._peer(s.right), self.group, HI))
-            ops.append(dist.P2POp(dist.irecv, recv[HI], self._peer(s.right), self.group, LO))
-        if s.left is not None:
-            ops.append(dist.P2POp(dist.irecv, recv[LO], self._peer(s.left), self.group, HI))
+        for ax in axes:
+            lo, hi = b.nbr[ax]
+            if lo is not None:
+                ops.append(dist.P2POp(dist.isend, send[ax, LO], self._peer(lo), self.group,
+                                      2 * ax + LO))
+            if hi is not None:
+                ops.append(dist.P2POp(dist.isend, send[ax, HI], self._peer(hi), self.group,
+                                      2 * ax + HI))
+                ops.append(dist.P2POp(dist.irecv, recv[ax, HI], self._peer(hi), self.group,
+                                      2 * ax + LO))
+            if lo is not None:
+                ops.append(dist.P2POp(dist.irecv, recv[ax, LO], self._peer(lo), self.group,
+                                      2 * ax + HI))
         if ops:
             for w in dist.batch_isend_irecv(ops):
                 w.wait()
-        for side in sides:
-            buf = r.recv(side, kind)
-            if recv[side] is not buf:
-                buf.copy_(recv[side], non_blocking=True)  # pinned host -> device, stream-ordered
-            r.unpack(side, buf, kind)
+        for ax in axes:
+            for side in b.sides(ax):
+                buf = r.recv(ax, side, kind)
+                if recv[ax, side] is not buf:
+                    buf.copy_(recv[ax, side], non_blocking=True)   # pinned -> device, in order
+                r.unpack(ax, side, buf, kind)
 
     def min(self, x: float) -> float:
         import torch
@@ -288,9 +385,9 @@ class DistExchange:
 
 
 class SlabStepper:
-    """SSP-RK3 steps of a grid split into x slabs: before each stage the x
-    halos of the stage's input are exchanged, then every local slab runs its
-    fused stage.  `runners` are this process's slabs."""
+    """SSP-RK3 steps of a grid split into blocks: before each stage the halos
+    of the stage's input are exchanged, then every local block runs its
+    fused stage.  `runners` are this process's blocks."""
 
     def __init__(self, runners: list, exchange):
         self.runners = runners
@@ -310,7 +407,7 @@ class SlabStepper:
         return any(r.viscous for r in self.runners)
 
     def set_viscous(self, vis) -> None:
-        """Navier-Stokes on every slab (ws_viscous constants; None: Euler).
+        """Navier-Stokes on every block (ws_viscous constants; None: Euler).
         Every rank must make the same choice: it adds an exchange per stage."""
         for r in self.runners:
             r.set_viscous(vis)
@@ -322,16 +419,16 @@ class SlabStepper:
             self.stage(dt)
 
     def compute_dt(self, cfl: float) -> float:
-        """Global CFL time step: the minimum of the slabs' (the maximum wave
+        """Global CFL time step: the minimum of the blocks' (the maximum wave
         speed over the whole grid)."""
         return self.exchange.min(min(r.local_dt(cfl) for r in self.runners))
 
     def set_state(self, f_global: np.ndarray) -> None:
         for r in self.runners:
-            r.set_state(split_state(f_global, r.slab))
+            r.set_state(split_state(f_global, r.block))
 
     def get_state(self) -> list[np.ndarray]:
-        """This process's slabs' states, in slab order."""
+        """This process's blocks' states, in block order."""
         return [r.get_state() for r in self.runners]
 
     def status(self) -> int:
@@ -342,17 +439,26 @@ class SlabStepper:
             r.close()
 
 
-def in_process(grid: Grid, parts: int) -> SlabStepper:
-    """All `parts` slabs on the current CUDA device (a single-GPU stand-in
-    for a multi-GPU run: same kernels, same halos, no waits between slabs)."""
-    return SlabStepper([CudaSlab(grid, s) for s in decompose(grid, parts)], LocalExchange())
+BlockStepper = SlabStepper
 
 
-def distributed(grid: Grid, group=None) -> SlabStepper:
-    """This rank's slab of `grid` split over the ranks of `group` (one GPU
-    per rank, the current CUDA device)."""
+def in_process(grid: Grid, parts=None, dims=None) -> SlabStepper:
+    """All blocks on the current CUDA device (a single-GPU stand-in for a
+    multi-GPU run: same kernels, same halos, no waits between blocks):
+    `parts` x slabs, or a dims[0] x dims[1] x dims[2] process grid."""
+    dims = dims if dims is not None else (parts, 1, 1)
+    return SlabStepper([CudaBlock(grid, b) for b in decompose_blocks(grid, dims)],
+                       LocalExchange())
+
+
+def distributed(grid: Grid, group=None, dims=None) -> SlabStepper:
+    """This rank's block of `grid` split over the ranks of `group` (one GPU
+    per rank, the current CUDA device): x slabs, or `dims` whose product is
+    the group size."""
     import torch.distributed as dist
-    parts = dist.get_world_size(group)
-    index = dist.get_rank(group)
-    slab = decompose(grid, parts)[index]
-    return SlabStepper([CudaSlab(grid, slab)], DistExchange(group))
+    world = dist.get_world_size(group)
+    dims = tuple(dims) if dims is not None else (world, 1, 1)
+    if dims[0] * dims[1] * dims[2] != world:
+        raise ValueError(f"dims {dims} do not match {world} ranks")
+    block = decompose_blocks(grid, dims)[dist.get_rank(group)]
+    return SlabStepper([CudaBlock(grid, block)], DistExchange(group))
