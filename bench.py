@@ -37,9 +37,9 @@ from a CUDA graph.
 
 --impl reference runs only the CPU reference arm (rank 0) on the headline
 workload and metric.  --gpus N > 1 (one rank per GPU under torchrun) steps one
-grid of (N*nx) x ny x nz split into N x slabs of nx x ny x nz, one per GPU,
-with the x halos exchanged over NCCL before every RK stage (weak scaling: each
-GPU keeps the single-GPU workload's cells).
+grid split into N blocks of nx x ny x nz, one per GPU (x slabs, or the process
+grid --dims px,py,pz), with the halos exchanged over NCCL before every RK stage
+(weak scaling: each GPU keeps the single-GPU workload's cells).
 """
 from __future__ import annotations
 
@@ -76,6 +76,9 @@ def parse():
     ap.add_argument("--no-second", action="store_true")
     ap.add_argument("--no-ns", action="store_true")
     ap.add_argument("--no-slabs", action="store_true")
+    ap.add_argument("--dims", default="",
+                    help="with --gpus N > 1: the process grid px,py,pz (product N); "
+                         "default N,1,1 (x slabs)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--batch-grids", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=50)
@@ -87,14 +90,25 @@ def parse():
     return ap.parse_args()
 
 
+def process_dims(a, world):
+    """The process grid of a multi-GPU run: --dims px,py,pz, else N x 1 x 1."""
+    if a.dims:
+        d = tuple(int(v) for v in a.dims.split(","))
+        if len(d) != 3 or d[0] * d[1] * d[2] != world:
+            raise SystemExit(f"--dims {a.dims} does not match {world} GPUs")
+        return d
+    return (world, 1, 1)
+
+
 def workload_name(a, world=1):
     if world == 1:
         return (f"fp64 fused RHS {a.nx}x{a.ny}x{a.nz}, Sod (rho 1/0.125, p 1/0.1, 1% noise), "
                 "x extrapolation, y/z periodic, SSP-RK3 CFL 0.5")
-    return (f"fp64 fused RHS {a.nx * world}x{a.ny}x{a.nz} split into {world} x slabs of "
-            f"{a.nx}x{a.ny}x{a.nz} (one per GPU, x halo exchanged over NCCL every RK stage), "
-            "Sod per slab (rho 1/0.125, p 1/0.1, 1% noise), x extrapolation, y/z periodic, "
-            "SSP-RK3 CFL 0.5")
+    d = process_dims(a, world)
+    return (f"fp64 fused RHS {a.nx * d[0]}x{a.ny * d[1]}x{a.nz * d[2]} split into "
+            f"{d[0]}x{d[1]}x{d[2]} blocks of {a.nx}x{a.ny}x{a.nz} (one per GPU, halos "
+            "exchanged over NCCL every RK stage), Sod per block (rho 1/0.125, p 1/0.1, "
+            "1% noise), x extrapolation, y/z periodic, SSP-RK3 CFL 0.5")
 
 
 L2_BYTES = 126e6                # B200 L2
@@ -103,10 +117,12 @@ L2_BYTES = 126e6                # B200 L2
 def config_of(a, world, **kw):
     # per GPU, the five primitive LAP fields a step reads (plus f, fn, du)
     prim_bytes = 5 * 8 * (a.nx + 8) * (a.ny + 8) * (a.nz + 8)
-    c = {"workload": workload_name(a, world), "grid": [a.nx * world, a.ny, a.nz],
+    d = process_dims(a, world) if world > 1 else (1, 1, 1)
+    c = {"workload": workload_name(a, world),
+         "grid": [a.nx * d[0], a.ny * d[1], a.nz * d[2]],
          "grid_per_gpu": [a.nx, a.ny, a.nz], "rhs_per_step": 3, "cfl": 0.5,
          "inputs_exceed_l2": prim_bytes > L2_BYTES,
-         "parallelism": "single" if world == 1 else f"xslab{world}"}
+         "parallelism": "single" if world == 1 else "blocks%dx%dx%d" % d}
     c.update(kw)
     return c
 
@@ -573,17 +589,19 @@ def run_ours(a, rank, world, dist):
         def run_steps(n):
             s.step(dt, n, stream=stream)
     else:
-        # this rank's x slab of one (world*nx) x ny x nz grid; per stage: halo
-        # pack, NCCL send/recv with the x neighbours, unpack, fused stage
+        # this rank's block of one (px*nx) x (py*ny) x (pz*nz) grid (x slabs
+        # by default); per stage: halo pack, NCCL send/recv with the
+        # neighbours, unpack, ghost fill, fused stage
         from windstencil_b200 import halo
-        gg = ws.Grid(a.nx * world, a.ny, a.nz, faces=faces)
+        dims = process_dims(a, world)
+        gg = ws.Grid(a.nx * dims[0], a.ny * dims[1], a.nz * dims[2], faces=faces)
         with torch.cuda.stream(stream):
-            stepper = halo.distributed(gg)
+            stepper = halo.distributed(gg, dims=dims)
             runner = stepper.runners[0]
             runner.set_state(f0)
             dt = stepper.compute_dt(0.5)
         g, s = runner.grid, runner.solver
-        sides = (runner.slab.left is not None) + (runner.slab.right is not None)
+        sides = sum(len(runner.block.sides(ax)) for ax in range(3))
         launches_per_step = 3 * (2 + 2 * sides)
 
         def run_steps(n):
