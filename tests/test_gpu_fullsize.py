@@ -5,7 +5,8 @@ x, periodic y and z) at 600x128x128 and 480x512x64, checked against the CPU
 oracle on the same inputs, rel. L-inf per field <= 1e-12: one RHS through
 the drop-in entry (ws_du_invis_jacobian3d) at both sizes, and two SSP-RK3
 steps of the graph-captured solver (fused RHS + stage kernel) at
-600x128x128.  Beside them, two size-independent properties on the GPU
+600x128x128, and the Navier-Stokes RHS (inviscid + viscous terms) of the
+benchmark's viscous workload at 600x128x128.  Beside them, two size-independent properties on the GPU
 alone at 600x128x128: a uniform state has a zero RHS, and on a fully
 periodic grid the face differences telescope (sum of du = 0 to round-off).
 The oracle takes a few seconds per RHS at these sizes on the host cores.
@@ -73,3 +74,23 @@ def test_full_size_free_stream_and_conservation(cuda):
     assert np.all(np.isfinite(du))
     for v in range(5):
         assert abs(np.sum(du[v])) <= 1e-12 * np.sum(np.abs(du[v]))
+
+
+def test_full_size_navier_stokes_rhs_matches_oracle(oracle, cuda):
+    """The benchmark's Navier-Stokes workload (Re 1e4, Pr 0.72, Sutherland
+    Ref_T 288.15, CD8) at 600x128x128: inviscid + viscous RHS of the solver
+    against the oracle's rhs_conserved_ns."""
+    from oracle.oracle import make_vis
+    nx, ny, nz = 600, 128, 128
+    vis = dict(re=1e4, pr=0.72, ref_t=288.15, scheme=8)
+    og = or_grid(nx, ny, nz, face_kind=SOD_FACES)
+    f0 = wl.sod_state(nx, ny, nz, seed=2)
+    ref = oracle.rhs_conserved_ns(og, make_vis(**vis), f0)
+    s = ws.Solver(ws.Grid(nx, ny, nz, faces=SOD_FACES))
+    try:
+        s.set_viscous(vis)
+        s.set_state(f0)
+        s.rhs()
+        assert rel_linf(s.get_rhs(), ref).max() <= TOL
+    finally:
+        s.close()
