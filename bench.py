@@ -79,6 +79,10 @@ def parse():
     ap.add_argument("--dims", default="",
                     help="with --gpus N > 1: the process grid px,py,pz (product N); "
                          "default N,1,1 (x slabs)")
+    ap.add_argument("--backend", default="nccl", choices=["nccl", "gloo"],
+                    help="process group of --gpus N > 1; gloo stages the halos through "
+                         "host memory, so ranks may share a GPU (a test of the "
+                         "multi-rank path on one device)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--batch-grids", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=50)
@@ -123,6 +127,9 @@ def config_of(a, world, **kw):
          "grid_per_gpu": [a.nx, a.ny, a.nz], "rhs_per_step": 3, "cfl": 0.5,
          "inputs_exceed_l2": prim_bytes > L2_BYTES,
          "parallelism": "single" if world == 1 else "blocks%dx%dx%d" % d}
+    if world > 1 and a.impl == "ours":
+        c["halo_transport"] = ("NCCL point-to-point, device buffers" if a.backend == "nccl"
+                               else "gloo, staged through pinned host memory")
     c.update(kw)
     return c
 
@@ -568,13 +575,23 @@ def bench_serve(a, ws, wl, serial_rate, rate, seconds, drain, seed=5):
                 "work, executed all device work in the window"}
 
 
+def max_over_ranks(torch, dist, x):
+    """The maximum of x over the ranks (x itself on one GPU)."""
+    if dist is None:
+        return x
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(a, rank, world, dist):
     import torch
     import windstencil_b200 as ws
     from windstencil_b200 import workloads as wl
 
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
+    torch.cuda.set_device(local % torch.cuda.device_count())
     faces = (ws.FACE_EXTRAP, ws.FACE_EXTRAP, 0, 0, 0, 0)
     f0 = wl.sod_state(a.nx, a.ny, a.nz, seed=2 + rank)
     stream = torch.cuda.Stream()
@@ -626,11 +643,7 @@ def run_ours(a, rank, world, dist):
         e1.synchronize()
     torch.cuda.synchronize()
     barrier()
-    ms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(torch, dist, e0.elapsed_time(e1))
     status = s.status(stream=stream)
     value = world * cells * 3 * a.steps / (ms * 1e-3) / 1e9
 
@@ -677,11 +690,7 @@ def run_ours(a, rank, world, dist):
         q1.record(stream)
         q1.synchronize()
         wall = time.perf_counter() - w0
-        ems = q0.elapsed_time(q1)
-        if dist is not None:
-            t = torch.tensor([ems], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+        ems = max_over_ranks(torch, dist, q0.elapsed_time(q1))
         nbytes = 5 * cells * 8
         e2e = {"value": world * cells * 3 * n_e2e / (ems * 1e-3) / 1e9, "unit": "Gcell-RHS/s",
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
@@ -752,8 +761,9 @@ def main():
         import torch
         import torch.distributed as dist_
         if a.impl == "ours":
-            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-            dist_.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")) %
+                                  torch.cuda.device_count())
+            dist_.init_process_group(a.backend, timeout=datetime.timedelta(seconds=300))
         else:
             dist_.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
         dist = dist_

@@ -35,3 +35,32 @@ def test_reference_arm_line():
     c = d["config"]
     assert c["grid"] == [32, 16, 16] and c["inputs_exceed_l2"] is False
     assert "workload" in c and "model" not in c
+
+
+def _free_port():
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def torchrun_bench(nproc, *args, timeout=600):
+    """bench.py under torch.distributed.run, one rank per process, as the
+    multi-GPU runs launch it; returns (JSON lines printed, stderr)."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={nproc}", "--master-addr=127.0.0.1",
+           f"--master-port={_free_port()}", os.path.join(ROOT, "bench.py"), *args]
+    out = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-3000:]
+    return [json.loads(l) for l in out.stdout.splitlines() if l.startswith("{")], out.stderr
+
+
+def test_reference_arm_two_ranks_prints_once():
+    """Under torchrun the reference arm runs on rank 0 alone; the other ranks
+    exit 0 without work or output."""
+    lines, _ = torchrun_bench(2, "--impl", "reference", "--gpus", "2", "--steps", "2",
+                              "--warmup", "1", "--nx", "32", "--ny", "16", "--nz", "16")
+    assert len(lines) == 1
+    d = lines[0]
+    assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+    assert d["config"]["parallelism"] == "blocks2x1x1"
