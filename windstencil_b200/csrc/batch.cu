@@ -8,6 +8,8 @@
 #include <algorithm>
 #include <cstring>
 #include <memory>
+#include <utility>
+#include <vector>
 
 #include "ws_internal.h"
 
@@ -15,6 +17,31 @@ namespace ws {
 
 namespace {
 size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+// Work items of a batched RHS launch: every tile's z column cut into runs
+// of at most zc planes, {grid, tile, first plane, end plane} (LAP z),
+// longest first (a run costs its planes plus about one plane of prologue,
+// whatever the tile's fill), so that the CTAs, taking them in turn, start
+// the long runs early; equal runs keep grid and tile order, so CTAs that run
+// together sweep neighbouring columns.
+std::vector<int4> batch_items(const std::vector<GridState*>& grids, int cfg, int zc) {
+    const TileCfg t = tile_cfg(cfg);
+    std::vector<std::pair<int, int4>> w;
+    for (int i = 0; i < (int)grids.size(); ++i) {
+        const ws_grid& g = grids[i]->g;
+        const int ntiles = (((int)g.nx + t.bx - 1) / t.bx) * (((int)g.ny + t.by - 1) / t.by);
+        for (int tile = 0; tile < ntiles; ++tile)
+            for (int z = 0; z < (int)g.nz; z += zc) {
+                const int len = std::min(zc, (int)g.nz - z);
+                w.push_back({len + 1, make_int4(i, tile, 4 + z, 4 + z + len)});
+            }
+    }
+    std::stable_sort(w.begin(), w.end(),
+                     [](const auto& l, const auto& r) { return l.first > r.first; });
+    std::vector<int4> out(w.size());
+    for (size_t k = 0; k < w.size(); ++k) out[k] = w[k].second;
+    return out;
+}
 
 __global__ void max_speed_kernel(ws_field u, ws_field v, ws_field w, ws_field cc, int nx,
                                  int ny, int nz, double rx, double ry, double rz,
@@ -154,15 +181,36 @@ int BatchRunner::build(const std::vector<GridState*>& grids, int cfg, int zc, cu
     for (auto* s : grids) n_gtab += ghost_chunks(&s->g);
     if (n_gtab > (1L << 30)) return fail(WS_ERR_INVALID, "batch too large");
     n_gtab_ = (int)n_gtab;
-    // layout of the device tables: 4 RhsArgs sets, cum, 2 ghost sets, block table
+    // persistent CTAs of the RHS launches
+    closure_ = false;
+    for (auto* s : grids)
+        for (int i = 0; i < 4; ++i) closure_ |= s->g.face_kind[i] == WS_FACE_CLOSURE;
+    const int maxc = rhs_max_ctas(precision_, true, closure_, cfg_, true);
+    if (maxc <= 0) return fail(WS_ERR_CUDA, "cannot size the persistent grid");
+    const TileCfg tc = tile_cfg(cfg);
+    long planes = 0;
+    for (auto* s : grids)
+        planes += (long)(((int)s->g.nx + tc.bx - 1) / tc.bx) *
+                  (((int)s->g.ny + tc.by - 1) / tc.by) * s->g.nz;
+    ctas_ = (int)std::max(1L, std::min<long>(maxc, std::max<long>(1, planes / 16)));
+    // the RHS launches' work items: z runs of at most zc planes per tile, and
+    // short enough (down to 8 planes) that a small batch still gives every
+    // CTA two items or more (whole columns would leave most SMs idle on a few
+    // small grids)
+    const long fill = std::max(8L, (planes + 2L * ctas_ - 1) / (2L * ctas_));
+    const std::vector<int4> items = batch_items(grids, cfg, (int)std::min<long>(zc_, fill));
+    // layout of the device tables: 4 RhsArgs sets, work items + their
+    // counter, 2 ghost sets, block table
     const size_t gsz = ghost_args_size();
     size_t o = 0, o_rhs[4], o_gh[2];
     for (int k = 0; k < 4; ++k) {
         o_rhs[k] = o;
         o = align256(o + n * sizeof(RhsArgs));
     }
-    const size_t o_cum = o;
-    o = align256(o + (n + 1) * sizeof(long));
+    const size_t o_items = o;
+    o = align256(o + items.size() * sizeof(int4));
+    const size_t o_ctr = o;
+    o = align256(o + sizeof(unsigned));
     for (int k = 0; k < 2; ++k) {
         o_gh[k] = o;
         o = align256(o + n * gsz);
@@ -171,9 +219,9 @@ int BatchRunner::build(const std::vector<GridState*>& grids, int cfg, int zc, cu
     const size_t bytes = align256(o_gt + n_gtab * sizeof(int2));
     host_.assign(bytes, 0);
     unsigned char* h = host_.data();
-    long* hc = reinterpret_cast<long*>(h + o_cum);
+    if (!items.empty())
+        std::memcpy(h + o_items, items.data(), items.size() * sizeof(int4));
     int2* hgt = reinterpret_cast<int2*>(h + o_gt);
-    hc[0] = 0;
     long gi = 0;
     for (int i = 0; i < n; ++i) {
         GridState* s = grids[i];
@@ -204,7 +252,6 @@ int BatchRunner::build(const std::vector<GridState*>& grids, int cfg, int zc, cu
                             sizeof(RhsArgs));
             fill_ghost_args(h + o_gh[p] + i * gsz, &s->g, s->pr[c]);
         }
-        hc[i + 1] = hc[i] + (long)s->args[0].ntx * s->args[0].nty * s->g.nz;
         for (long c = 0; c < ghost_chunks(&s->g); ++c) hgt[gi++] = make_int2(i, (int)c);
     }
     if (bytes > dev_bytes_) {
@@ -215,18 +262,12 @@ int BatchRunner::build(const std::vector<GridState*>& grids, int cfg, int zc, cu
     }
     unsigned char* d = static_cast<unsigned char*>(dev_);
     for (int k = 0; k < 4; ++k) d_rhs_[k] = reinterpret_cast<RhsArgs*>(d + o_rhs[k]);
-    d_cum_ = reinterpret_cast<long*>(d + o_cum);
+    work_ = {reinterpret_cast<const int4*>(d + o_items), (int)items.size(),
+             reinterpret_cast<unsigned*>(d + o_ctr)};
     for (int k = 0; k < 2; ++k) d_ghost_[k] = d + o_gh[k];
     d_gtab_ = reinterpret_cast<int2*>(d + o_gt);
     int rc = upload_tables(st);
     if (rc) return rc;
-    closure_ = false;
-    for (auto* s : grids)
-        for (int i = 0; i < 4; ++i) closure_ |= s->g.face_kind[i] == WS_FACE_CLOSURE;
-    const int maxc = rhs_max_ctas(precision_, true, closure_, cfg_, true);
-    if (maxc <= 0) return fail(WS_ERR_CUDA, "cannot size the persistent grid");
-    const long planes = hc[n];
-    ctas_ = (int)std::max(1L, std::min<long>(maxc, std::max<long>(1, planes / 16)));
     return WS_OK;
 }
 
@@ -242,8 +283,8 @@ int BatchRunner::enqueue_rhs(cudaStream_t st) {
     if (grids_.empty()) return WS_OK;
     int rc = launch_ghost_fill_batch(d_ghost_[parity_], d_gtab_, n_gtab_, st);
     if (rc) return rc;
-    return launch_rhs_batch(d_rhs_[2 * parity_], d_cum_, (int)grids_.size(), zc_, precision_,
-                            true, closure_, cfg_, ctas_, 0, st);
+    return launch_rhs_batch(d_rhs_[2 * parity_], work_, precision_, true, closure_, cfg_, ctas_, 0,
+                            st);
 }
 
 // stage 1 alone: reads f[cur], pr[cur] and writes only the other buffers,
@@ -252,8 +293,8 @@ int BatchRunner::enqueue_stage1(cudaStream_t st) {
     if (grids_.empty()) return WS_OK;
     int rc = launch_ghost_fill_batch(d_ghost_[parity_], d_gtab_, n_gtab_, st);
     if (rc) return rc;
-    return launch_rhs_batch(d_rhs_[2 * parity_], d_cum_, (int)grids_.size(), zc_, precision_,
-                            true, closure_, cfg_, ctas_, 1, st);
+    return launch_rhs_batch(d_rhs_[2 * parity_], work_, precision_, true, closure_, cfg_, ctas_, 1,
+                            st);
 }
 
 int BatchRunner::enqueue_step(cudaStream_t st) {
@@ -262,8 +303,8 @@ int BatchRunner::enqueue_step(cudaStream_t st) {
         const int two = krk == 2;
         int rc = launch_ghost_fill_batch(d_ghost_[parity_ ^ two], d_gtab_, n_gtab_, st);
         if (rc) return rc;
-        rc = launch_rhs_batch(d_rhs_[2 * parity_ + two], d_cum_, (int)grids_.size(), zc_,
-                              precision_, true, closure_, cfg_, ctas_, krk, st);
+        rc = launch_rhs_batch(d_rhs_[2 * parity_ + two], work_, precision_, true, closure_, cfg_,
+                              ctas_, krk, st);
         if (rc) return rc;
     }
     return WS_OK;

@@ -26,18 +26,14 @@ int launch_rhs(const RhsArgs& a, int precision, bool uniform, int cfg, int ctas,
                : RhsSlice<double, false>::launch(cfg, a, uniform, ctas, krk, st);
 }
 
-int launch_rhs_batch(const RhsArgs* grids, const long* cum, int n, int zc, int precision,
-                     bool uniform, bool closure, int cfg, int ctas, int krk, cudaStream_t st) {
+int launch_rhs_batch(const RhsArgs* grids, const BatchWork& w, int precision, bool uniform,
+                     bool closure, int cfg, int ctas, int krk, cudaStream_t st) {
     if (precision == WS_MIXED)
-        return closure
-                   ? RhsSlice<float, true>::launch_batch(cfg, grids, cum, n, zc, uniform, ctas,
-                                                         krk, st)
-                   : RhsSlice<float, false>::launch_batch(cfg, grids, cum, n, zc, uniform, ctas,
-                                                          krk, st);
-    return closure ? RhsSlice<double, true>::launch_batch(cfg, grids, cum, n, zc, uniform, ctas,
-                                                          krk, st)
-                   : RhsSlice<double, false>::launch_batch(cfg, grids, cum, n, zc, uniform,
-                                                           ctas, krk, st);
+        return closure ? RhsSlice<float, true>::launch_batch(cfg, grids, w, uniform, ctas, krk, st)
+                       : RhsSlice<float, false>::launch_batch(cfg, grids, w, uniform, ctas, krk,
+                                                              st);
+    return closure ? RhsSlice<double, true>::launch_batch(cfg, grids, w, uniform, ctas, krk, st)
+                   : RhsSlice<double, false>::launch_batch(cfg, grids, w, uniform, ctas, krk, st);
 }
 
 int rhs_max_ctas(int precision, bool uniform, bool closure, int cfg, bool stage) {

@@ -666,48 +666,40 @@ __global__ void __launch_bounds__(NT, (RhsLayout<BX, BY, CT, EPI>::MINB))
     }
 }
 
-// Batched form: many independent grids, one persistent launch.  The work
-// space is the concatenation over grids of (tile, plane) in tile-major order;
-// cum[g] is the number of tile-planes before grid g.  Each CTA takes an equal
-// contiguous range, so a CTA sweeps neighbouring columns of one grid in turn
-// and every CTA ends with the same number of planes.
+// Batched form: one persistent launch over many grids.  The work is a list of
+// items {grid, tile, first plane, end plane} (z runs of at most the scan
+// length), longest first; each CTA takes the next item through an atomic
+// counter (zeroed before the launch), so the long runs start early and the
+// short ones fill in at the end.
 template <int BX, int BY, int NT, bool UNI, typename CT, bool EPI, bool CLO>
 __global__ void __launch_bounds__(NT, (RhsLayout<BX, BY, CT, EPI>::MINB))
-    bf3w_rhs_batch_kernel(const RhsArgs* __restrict__ grids, const long* __restrict__ cum,
-                          int ngrids, int zc, int krk) {
+    bf3w_rhs_batch_kernel(const RhsArgs* __restrict__ grids, const int4* __restrict__ items,
+                          int nitems, unsigned* __restrict__ counter, int krk) {
     extern __shared__ __align__(128) unsigned char smem_dyn[];
     // TMA tile destinations must be 128-byte aligned: align explicitly (the
     // launch adds 128 bytes of slack)
     unsigned char* smem_raw = smem_dyn + ((128 - (smem_addr(smem_dyn) & 127)) & 127);
     __shared__ uint64_t bar[3];
+    __shared__ int next;
     init_stage_barriers(bar);
     uint32_t ph = 0;
-    const long total = cum[ngrids];
-    const long lo = total * blockIdx.x / gridDim.x, hi = total * (blockIdx.x + 1) / gridDim.x;
-    if (lo >= hi) return;
-    int g = 0, top = ngrids;          // last g with cum[g] <= lo
-    while (top - g > 1) {
-        const int mid = (g + top) >> 1;
-        if (cum[mid] <= lo) g = mid; else top = mid;
-    }
-    long pos = lo;
     int fenced = -1;                  // grid whose tensor maps this CTA has fenced
-    while (pos < hi) {
-        while (cum[g + 1] <= pos) ++g;
-        const RhsArgs& a = grids[g];
+    for (;;) {
+        if (threadIdx.x == 0) next = (int)atomicAdd(counter, 1u);
+        __syncthreads();
+        const int it = next;
+        __syncthreads();              // every thread has read `next`
+        if (it >= nitems) return;
+        const int4 w = items[it];
+        const RhsArgs& a = grids[w.x];
         const SplitK<CT> k = {CT(a.eps2), CT(a.hrg), CT(a.c1), CT(a.c3), CT(a.gm1)};
-        const long nzj = a.ez - a.sz;
-        const long local = pos - cum[g];
-        const long tile = local / nzj;
-        const int zoff = (int)(local - tile * nzj);
-        const int len = (int)min(min(nzj - zoff, hi - pos), (long)zc);
-        bool first = fenced != g;
-        fenced = g;
-        if (!run_sweep<BX, BY, NT, UNI, CT, EPI, true, CLO>(a, k, smem_raw, a.sx + (int)(tile % a.ntx) * BX,
-                                                   a.sy + (int)(tile / a.ntx) * BY, a.sz + zoff,
-                                                   a.sz + zoff + len, krk, bar, ph, first))
+        bool first = fenced != w.x;
+        fenced = w.x;
+        if (!run_sweep<BX, BY, NT, UNI, CT, EPI, true, CLO>(a, k, smem_raw,
+                                                           a.sx + (w.y % a.ntx) * BX,
+                                                           a.sy + (w.y / a.ntx) * BY, w.z, w.w,
+                                                           krk, bar, ph, first))
             return;
-        pos += len;
     }
 }
 
@@ -749,11 +741,12 @@ struct Launcher {
         WS_CUDA(cudaGetLastError());
         return WS_OK;
     }
-    static int launch_batch(const RhsArgs* grids, const long* cum, int n, int zc, int ctas,
-                            int krk, cudaStream_t st) {
+    static int launch_batch(const RhsArgs* grids, const BatchWork& w, int ctas, int krk,
+                            cudaStream_t st) {
         if (max_ctas() <= 0) return fail(WS_ERR_CUDA, "cannot prepare the RHS kernel");
+        WS_CUDA(cudaMemsetAsync(w.counter, 0, sizeof(unsigned), st));
         bf3w_rhs_batch_kernel<BX, BY, NT, UNI, CT, EPI, CLO>
-            <<<ctas, NT, smem(), st>>>(grids, cum, n, zc, krk);
+            <<<ctas, NT, smem(), st>>>(grids, w.items, w.nitems, w.counter, krk);
         WS_CUDA(cudaGetLastError());
         return WS_OK;
     }
@@ -774,17 +767,14 @@ struct RhsSlice {
                    : Launcher<BX, BY, NT, false, CT, false, CLO>::launch(a, ctas, 0, st);
     }
     template <int BX, int BY, int NT>
-    static int batch_t(const RhsArgs* g, const long* cum, int n, int zc, bool uni, int ctas,
-                       int krk, cudaStream_t st) {
+    static int batch_t(const RhsArgs* g, const BatchWork& w, bool uni, int ctas, int krk,
+                       cudaStream_t st) {
         if (krk > 0) {
             if (!uni) return fail(WS_ERR_UNSUPPORTED, "stage epilogue needs Cartesian metrics");
-            return Launcher<BX, BY, NT, true, CT, true, CLO>::launch_batch(g, cum, n, zc, ctas,
-                                                                           krk, st);
+            return Launcher<BX, BY, NT, true, CT, true, CLO>::launch_batch(g, w, ctas, krk, st);
         }
-        return uni ? Launcher<BX, BY, NT, true, CT, false, CLO>::launch_batch(g, cum, n, zc,
-                                                                              ctas, 0, st)
-                   : Launcher<BX, BY, NT, false, CT, false, CLO>::launch_batch(g, cum, n, zc,
-                                                                               ctas, 0, st);
+        return uni ? Launcher<BX, BY, NT, true, CT, false, CLO>::launch_batch(g, w, ctas, 0, st)
+                   : Launcher<BX, BY, NT, false, CT, false, CLO>::launch_batch(g, w, ctas, 0, st);
     }
     template <int BX, int BY, int NT>
     static int max_t(bool uni, bool stage) {
@@ -794,8 +784,8 @@ struct RhsSlice {
     }
 
     static int launch(int cfg, const RhsArgs& a, bool uni, int ctas, int krk, cudaStream_t st);
-    static int launch_batch(int cfg, const RhsArgs* g, const long* cum, int n, int zc, bool uni,
-                            int ctas, int krk, cudaStream_t st);
+    static int launch_batch(int cfg, const RhsArgs* g, const BatchWork& w, bool uni, int ctas,
+                            int krk, cudaStream_t st);
     static int max_ctas(int cfg, bool uni, bool stage);
 };
 
@@ -811,13 +801,13 @@ int RhsSlice<CT, CLO>::launch(int cfg, const RhsArgs& a, bool uni, int ctas, int
     }
 }
 template <typename CT, bool CLO>
-int RhsSlice<CT, CLO>::launch_batch(int cfg, const RhsArgs* g, const long* cum, int n, int zc,
-                                    bool uni, int ctas, int krk, cudaStream_t st) {
+int RhsSlice<CT, CLO>::launch_batch(int cfg, const RhsArgs* g, const BatchWork& w, bool uni,
+                                    int ctas, int krk, cudaStream_t st) {
     switch (cfg) {
-        case 0: return batch_t<16, 8, 768>(g, cum, n, zc, uni, ctas, krk, st);
-        case 1: return batch_t<16, 8, 704>(g, cum, n, zc, uni, ctas, krk, st);
-        case 2: return batch_t<8, 8, 256>(g, cum, n, zc, uni, ctas, krk, st);
-        case 3: return batch_t<8, 8, 384>(g, cum, n, zc, uni, ctas, krk, st);
+        case 0: return batch_t<16, 8, 768>(g, w, uni, ctas, krk, st);
+        case 1: return batch_t<16, 8, 704>(g, w, uni, ctas, krk, st);
+        case 2: return batch_t<8, 8, 256>(g, w, uni, ctas, krk, st);
+        case 3: return batch_t<8, 8, 384>(g, w, uni, ctas, krk, st);
         default: return fail(WS_ERR_INVALID, "unknown tile configuration");
     }
 }

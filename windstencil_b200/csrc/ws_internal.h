@@ -128,11 +128,18 @@ int launch_rhs(const RhsArgs& a, int precision, bool uniform, int cfg, int ctas,
 // resident CTAs of the kernel for (precision, metric kind, CLOSURE faces
 // present, tile shape, stage epilogue)
 int rhs_max_ctas(int precision, bool uniform, bool closure, int cfg, bool stage);
-// Batched RHS over n grids (device array of RhsArgs, cum[n+1] tile-plane
-// prefix sums); all grids share precision, metric kind and tile shape;
-// closure: some grid has CLOSURE faces.
-int launch_rhs_batch(const RhsArgs* grids, const long* cum, int n, int zc, int precision,
-                     bool uniform, bool closure, int cfg, int ctas, int krk, cudaStream_t st);
+// Work of a batched RHS launch: items {grid, tile, first plane, end plane}
+// in the order the CTAs take them, and the counter they take them by (the
+// launch zeroes it first).
+struct BatchWork {
+    const int4* items;
+    int nitems;
+    unsigned* counter;
+};
+// Batched RHS over the grids of a device array of RhsArgs; all grids share
+// precision, metric kind and tile shape; closure: some grid has CLOSURE faces.
+int launch_rhs_batch(const RhsArgs* grids, const BatchWork& w, int precision, bool uniform,
+                     bool closure, int cfg, int ctas, int krk, cudaStream_t st);
 // Host-side RhsArgs of one grid and job (tile shape cfg, sweep cap scan).
 RhsArgs make_rhs_args(const ws_grid* g, ws_job job, const ws_field prims[5],
                       const ws_metrics* m, ws_soa du, int cfg, int scan);
@@ -230,7 +237,7 @@ class BatchRunner {
     // d_ghost_[s] the ghost-fill arguments of primitive set pr[cur ^ s].
     RhsArgs* d_rhs_[4] = {nullptr, nullptr, nullptr, nullptr};
     void* d_ghost_[2] = {nullptr, nullptr};
-    long* d_cum_ = nullptr;
+    BatchWork work_{nullptr, 0, nullptr};   // the RHS launches' work items
     int2* d_gtab_ = nullptr;
     int n_gtab_ = 0;
     int parity_ = 0;
