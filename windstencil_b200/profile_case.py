@@ -12,6 +12,10 @@ The default 600x128x64 case holds ~1 GB on the device and its inputs exceed
 the 126 MB L2, so DRAM counters stay meaningful.  --viscous N adds N
 evaluations of the viscous terms (ws_du_vis_jacobian3d, CD8, Re 1e4) on the
 FP64 grid: the flux pass, the flux ghost fill and the divergence pass.
+--batch N instead steps N grids of the batched workload (nx log-uniform in
+[32, 256], ny, nz in [16, 128], periodic) together, one SSP-RK3 step per
+precision after one warm-up step: three launches each of the batched ghost
+fill and of the batched RHS + stage kernel.
 """
 from __future__ import annotations
 
@@ -28,6 +32,7 @@ def main() -> None:
     ap.add_argument("--tile", default="", help="tile_x,tile_y,scan_z,threads")
     ap.add_argument("--step", action="store_true", help="also one SSP-RK3 step")
     ap.add_argument("--viscous", type=int, default=0, help="viscous-term evaluations")
+    ap.add_argument("--batch", type=int, default=0, help="grids of the batched workload")
     a = ap.parse_args()
 
     import torch
@@ -35,6 +40,9 @@ def main() -> None:
     import windstencil_b200 as ws
     from windstencil_b200 import workloads as wl
 
+    if a.batch:
+        _batch(a, ws, wl)
+        return
     f0 = wl.sod_state(a.nx, a.ny, a.nz, seed=2)
     for name in a.precision.split(","):
         prec = ws.MIXED if name == "mixed" else ws.FP64
@@ -59,6 +67,25 @@ def main() -> None:
                     torch.cuda.current_stream().cuda_stream))
         torch.cuda.synchronize()
         s.close()
+    print("ok")
+
+
+def _batch(a, ws, wl) -> None:
+    import torch
+    specs = wl.batch_specs(a.batch, seed=4)
+    states = [wl.batch_state(sp) for sp in specs]
+    for name in a.precision.split(","):
+        prec = ws.MIXED if name == "mixed" else ws.FP64
+        b = ws.Batch([ws.Grid(sp.nx, sp.ny, sp.nz, precision=prec) for sp in specs])
+        if a.tile:
+            b.set_tile(tuple(int(v) for v in a.tile.split(",")))
+        for i, f in enumerate(states):
+            b.set_state(i, f)
+        b.set_dt(b.compute_dt(0.5))
+        b.step(1)
+        b.step(1)
+        torch.cuda.synchronize()
+        b.close()
     print("ok")
 
 
