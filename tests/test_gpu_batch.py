@@ -92,3 +92,29 @@ def test_batch_nonfinite_status(cuda):
         b.set_state(i, f)
     assert b.status() == [0, 5, 0]
     b.close()
+
+
+def test_batch_whole_column_runs_match_single(cuda):
+    """A batch large enough that every work item is a whole tile column (the
+    small batches above cut their columns into runs of 8 or more planes):
+    the RHS equals the one-grid path bit for bit, two steps within 1e-13."""
+    shapes = [(128, 64, 40), (120, 56, 40), (96, 64, 33), (128, 50, 40)] * 2
+    grids = [ws.Grid(*s) for s in shapes]
+    states = _states(shapes, seed=20)
+    b = ws.Batch(grids)
+    for i, f in enumerate(states):
+        b.set_state(i, f)
+    b.rhs()
+    dts = b.compute_dt(0.5)
+    b.set_dt(dts)
+    b.step(2)
+    assert b.status() == [0] * len(grids)
+    for i, (g, f) in enumerate(zip(grids, states)):
+        s = ws.Solver(g)
+        s.set_state(f)
+        s.rhs()
+        assert np.array_equal(s.get_rhs(), b.get_rhs(i)), i
+        s.step(dts[i], 2)
+        assert rel_linf(b.get_state(i), s.get_state()).max() <= 1e-13, i
+        s.close()
+    b.close()
