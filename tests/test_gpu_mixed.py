@@ -8,7 +8,7 @@ configuration); one RHS evaluation within rel. L2 <= 5e-5, rel. L-inf <= 1e-4.
 
 The Sod-type states with 1% cell noise are chaotic under WENO: the FP64
 solution itself moves by ~10% in v, w after 100 steps when its initial state
-is perturbed by 1e-12, so long-horizon mixed-vs-FP64
+is perturbed by 1e-12 (the FP64 oracle shows the same), so long-horizon mixed-vs-FP64
 comparisons use the smooth Fourier workload; Sod is compared on one RHS.
 """
 import numpy as np
