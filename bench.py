@@ -91,6 +91,18 @@ def parse():
     ap.add_argument("--serve-rate-low", type=float, default=6.0)
     ap.add_argument("--serve-seconds", type=float, default=60.0)    # the configuration's window
     ap.add_argument("--serve-drain", type=float, default=20.0)
+    # --profile-case: a short fixed sequence of launches for ncu (no timing)
+    ap.add_argument("--profile-case", action="store_true",
+                    help="run a small profiling case instead of the benchmark: one fused "
+                         "RHS per --precision on the Sod grid --nx --ny --nz (and with "
+                         "--step one SSP-RK3 step, with --viscous N that many viscous-term "
+                         "evaluations); with --profile-batch N, one warm-up and one timed "
+                         "SSP-RK3 step of N grids of the batched workload per precision")
+    ap.add_argument("--precision", default="fp64,mixed")
+    ap.add_argument("--tile", default="", help="tile_x,tile_y,scan_z,threads")
+    ap.add_argument("--step", action="store_true")
+    ap.add_argument("--viscous", type=int, default=0)
+    ap.add_argument("--profile-batch", type=int, default=0)
     return ap.parse_args()
 
 
@@ -127,9 +139,6 @@ def config_of(a, world, **kw):
          "grid_per_gpu": [a.nx, a.ny, a.nz], "rhs_per_step": 3, "cfl": 0.5,
          "inputs_exceed_l2": prim_bytes > L2_BYTES,
          "parallelism": "single" if world == 1 else "blocks%dx%dx%d" % d}
-    if world > 1 and a.impl == "ours":
-        c["halo_transport"] = ("NCCL point-to-point, device buffers" if a.backend == "nccl"
-                               else "gloo, staged through pinned host memory")
     c.update(kw)
     return c
 
@@ -191,60 +200,69 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU arms (the oracle is the checker / reported baseline, never the product)
 # ---------------------------------------------------------------------------
-def _cpu_rhs_setup(nx, ny, nz, hz=None):
-    from oracle.oracle import Oracle, RefFunctions, make_grid
+def _cpu_stepper(nx, ny, nz):
+    """The headline workload stepped on the host: SSP-RK3 steps assembled from
+    the reference's own scalar kernels (oracle/_ref, kind "reference"), else
+    the oracle port's own step (kind "port")."""
+    from oracle.oracle import Oracle, RefFunctions, RefRK3, make_grid
     from windstencil_b200 import workloads as wl
     o = Oracle()
-    kind, rhs = "port", o.du_invis
-    if RefFunctions.available():
-        kind, rhs = "reference", RefFunctions().du_invis
-    og = make_grid(nx, ny, nz, hz=hz, face_kind=(1, 1, 0, 0, 0, 0))
+    og = make_grid(nx, ny, nz, face_kind=(1, 1, 0, 0, 0, 0))
     f = wl.sod_state(nx, ny, nz, seed=2)
-    d, u, v, w, T, _ = o.cons_to_prim(og, f)
-    for x in (d, u, v, w, T):
-        o.ghost_fill(og, x)
-    cc = o.sound_speed(og, T)
-    return o, kind, (lambda: rhs(og, d, u, v, w, cc))
+    dt = o.compute_dt(og, f, 0.5)
+    if RefFunctions.available():
+        st = RefRK3(og, f, oracle=o)
+        return o, "reference", (lambda: st.step(dt)), dt
+    state = {"f": f}
+
+    def port_step():
+        state["f"] = o.rk3_steps(og, state["f"], dt, 1)
+    return o, "port", port_step, dt
 
 
 def cpu_arm(a, seconds):
-    """Bounded sample: full RHS evaluations of the headline grid for ~`seconds`."""
-    o, kind, run = _cpu_rhs_setup(a.nx, a.ny, a.nz)
-    run()                           # warm-up (page-in, thread pool)
+    """Bounded sample: whole SSP-RK3 steps of the headline grid for ~`seconds`."""
+    o, kind, step, _ = _cpu_stepper(a.nx, a.ny, a.nz)
+    step()                          # warm-up (page-in, thread pool)
     n, t0 = 0, time.perf_counter()
     while True:
-        run()
+        step()
         n += 1
         el = time.perf_counter() - t0
-        if el >= seconds or n >= 50:
+        if el >= seconds or n >= 20:
             break
     what = ("reference scalar kernels built for the host" if kind == "reference"
             else "oracle port")
-    return {"value": a.nx * a.ny * a.nz * n / el / 1e9, "unit": "Gcell-RHS/s",
+    return {"value": a.nx * a.ny * a.nz * 3 * n / el / 1e9, "unit": "Gcell-RHS/s",
             "cores": o.threads(), "kind": kind,
-            "sample": f"{n} full inviscid RHS evaluation(s) of the {a.nx}x{a.ny}x{a.nz} grid "
-                      f"in {el:.1f} s ({what}, OpenMP over {o.threads()} threads)"}
+            "sample": f"{n} SSP-RK3 step(s) (3 inviscid RHS each) of the {a.nx}x{a.ny}x{a.nz} "
+                      f"grid in {el:.1f} s ({what}, OpenMP over {o.threads()} threads)"}
 
 
 def run_reference(a, rank, world):
+    """The reference arm: the headline workload's SSP-RK3 steps on the host
+    cores, one bench step = one time step (3 RHS evaluations and the stage
+    updates), on the same grid, state, dt and metric as the GPU arm."""
     if rank != 0:
         return
-    nzs = min(a.nz, 16)       # each step: one RHS on a 16-plane slab (bounded sample)
-    o, kind, run = _cpu_rhs_setup(a.nx, a.ny, nzs, hz=1.0 / (a.nz - 1.0))
+    o, kind, step, dt = _cpu_stepper(a.nx, a.ny, a.nz)
     for _ in range(a.warmup):
-        run()
+        step()
     t0 = time.perf_counter()
     for _ in range(a.steps):
-        run()
+        step()
     el = time.perf_counter() - t0
-    value = a.nx * a.ny * nzs * a.steps / el / 1e9
-    sample = (f"each step: one inviscid RHS on a {a.nx}x{a.ny}x{nzs} slab of the workload "
-              f"(same x/y extents, spacing and state recipe)")
+    value = a.nx * a.ny * a.nz * 3 * a.steps / el / 1e9
+    what = ("the reference's own scalar kernels built for the host (cons_to_pri, sound "
+            "speed, Steger-Warming split, WENO7-SYMBO P/M, time advance ker1/2/3), "
+            "decomposed RHS loop, OpenMP" if kind == "reference" else "the oracle port")
+    sample = (f"each step: one whole SSP-RK3 time step of the {a.nx}x{a.ny}x{a.nz} grid "
+              f"(3 inviscid RHS + stage updates) with {what}")
     line = {"metric": "Gcell-RHS/s", "value": value, "unit": "Gcell-RHS/s", "impl": "reference",
             "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": el / a.steps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config_of(a, world),
+            "config": config_of(a, world), "dt": dt,
             "cpu_baseline": {"value": value, "unit": "Gcell-RHS/s", "cores": o.threads(),
                              "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": "Gcell-RHS/s", "h2d_bytes_per_step": 0,
@@ -260,9 +278,17 @@ def _events(torch):
 
 
 def _peak(ws, name):
+    """Attainable FMA throughput (TFLOP/s) measured now by the measurement
+    utility libws_peaks.so (name: "fp64" or "fp32")."""
     import ctypes as C
+    lib = C.CDLL(os.path.join(ROOT, "windstencil_b200", "libws_peaks.so"))
+    fn = getattr(lib, f"wsp_{name}_fma_peak")
+    fn.argtypes = [C.POINTER(C.c_double), C.c_void_p]
+    fn.restype = C.c_int
     out = C.c_double()
-    ws._abi.check(getattr(ws.load(), name)(C.byref(out), None))
+    rc = fn(C.byref(out), None)
+    if rc != 0:
+        raise RuntimeError(f"FMA peak measurement failed (CUDA error {rc})")
     return out.value
 
 
@@ -317,7 +343,7 @@ def bench_mixed(a, torch, ws, wl, stream):
     l2 = [float(np.linalg.norm(a32[i] - a64[i]) / np.linalg.norm(a64[i])) for i in range(5)]
     li = [float(np.max(np.abs(a32[i] - a64[i])) / np.max(np.abs(a64[i]))) for i in range(5)]
     cells = nx * ny * nz
-    peak32 = _peak(ws, "ws_probe_fp32_peak")
+    peak32 = _peak(ws, "fp32")
     res.update({
         "kernel_ms_fp64": out["fp64_kernel_ms"], "kernel_ms_mixed": out["mixed_kernel_ms"],
         "kernel_speedup_vs_fp64": out["fp64_kernel_ms"] / out["mixed_kernel_ms"],
@@ -649,7 +675,7 @@ def run_ours(a, rank, world, dist):
 
     # ---- dominant kernel alone (drop-in entry point, same stream)
     rhs_ms = time_rhs_kernel(torch, ws, g, s, stream, max(3, min(a.steps, 20)))
-    peak = _peak(ws, "ws_probe_fp64_peak")
+    peak = _peak(ws, "fp64")
     achieved = FLOP_PER_CELL * cells / (rhs_ms * 1e-3) / 1e12
     peaks = {}
     try:
@@ -731,12 +757,74 @@ def run_ours(a, rank, world, dist):
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms / a.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64", "data": "synthetic",
-                "config": config_of(a, world, dt=dt),
+                "config": config_of(a, world), "dt": dt,
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": launches_per_step * a.steps, "clocks": clk.summary(),
                 "device_status": status}
+        if world > 1:
+            line["halo_transport"] = ("NCCL point-to-point, device buffers"
+                                      if a.backend == "nccl"
+                                      else "gloo, staged through pinned host memory")
         line.update(extra)
         print(json.dumps(line), flush=True)
+
+
+def profile_case(a):
+    """A small, fixed launch sequence for a profiler to capture, e.g.
+
+        ncu --set full --clock-control none -k regex:bf3w_rhs -c 2 -o prof \
+            python bench.py --profile-case --nz 64 --precision fp64
+
+    600x128x64 holds ~1 GB on the device and its inputs exceed the 126 MB L2,
+    so DRAM counters stay meaningful.  Nothing is timed or printed but "ok"."""
+    import torch
+    import windstencil_b200 as ws
+    from windstencil_b200 import workloads as wl
+    import ctypes as C
+
+    tile = tuple(int(v) for v in a.tile.split(",")) if a.tile else None
+    if a.profile_batch:
+        specs = wl.batch_specs(a.profile_batch, seed=4)
+        states = [wl.batch_state(sp) for sp in specs]
+        for name in a.precision.split(","):
+            prec = ws.MIXED if name == "mixed" else ws.FP64
+            b = ws.Batch([ws.Grid(sp.nx, sp.ny, sp.nz, precision=prec) for sp in specs])
+            if tile:
+                b.set_tile(tile)
+            for i, f in enumerate(states):
+                b.set_state(i, f)
+            b.set_dt(b.compute_dt(0.5))
+            b.step(1)
+            b.step(1)
+            torch.cuda.synchronize()
+            b.close()
+        print("ok")
+        return
+    f0 = wl.sod_state(a.nx, a.ny, a.nz, seed=2)
+    for name in a.precision.split(","):
+        prec = ws.MIXED if name == "mixed" else ws.FP64
+        g = ws.Grid(a.nx, a.ny, a.nz, faces=(1, 1, 0, 0, 0, 0), precision=prec)
+        s = ws.Solver(g)
+        if tile:
+            s.set_tile(tile)
+        s.set_state(f0)
+        s.rhs()
+        if a.step:
+            s.step(s.compute_dt(0.5), 1)
+        if a.viscous and prec == ws.FP64:
+            _, du, prims = s.fields()
+            lib, gc = ws.load(), g.c()
+            need = int(lib.ws_du_vis_workspace_bytes(C.byref(gc)))
+            work = torch.zeros(need // 8 + 2, dtype=torch.float64, device="cuda")
+            vis = ws.viscous(re=1.0e4, pr=0.72, ref_t=288.15, scheme=8)
+            for _ in range(a.viscous):
+                ws.check(lib.ws_du_vis_jacobian3d(
+                    C.byref(gc), C.byref(vis), prims[1], prims[2], prims[3], prims[4], None,
+                    du, C.c_void_p(work.data_ptr()), work.numel() * 8,
+                    torch.cuda.current_stream().cuda_stream))
+        torch.cuda.synchronize()
+        s.close()
+    print("ok")
 
 
 def measured_traffic(a):
@@ -753,6 +841,9 @@ def measured_traffic(a):
 
 def main():
     a = parse()
+    if a.profile_case:
+        profile_case(a)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     dist = None

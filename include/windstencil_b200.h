@@ -150,11 +150,6 @@ WS_API uint32_t ws_lap_pitch(uint32_t nx);
  * synchronises `stream`.  The solver, batches and server report the same bit
  * in their own status words (WS_ERR_TIMEOUT). */
 WS_API int ws_device_error(int* flags, ws_stream_t stream);
-/* Attainable FMA throughput of the current device in TFLOP/s (independent
- * FMA chains on every SM; the roofline denominator of the RHS kernels).
- * Synchronises `stream`.  No reference counterpart (measurement utility). */
-WS_API int ws_probe_fp64_peak(double* tflops, ws_stream_t stream);
-WS_API int ws_probe_fp32_peak(double* tflops, ws_stream_t stream);
 
 /* ------------------------------------------------------------------------ */
 /* Drop-in kernels (explicit arguments)                                      */
@@ -286,11 +281,14 @@ WS_API int ws_time_advance(const ws_grid* g, int krk, double dt, ws_soa f, ws_so
  * prims: 4 LAP fields per grid, in the order u, v, w, cc.
  * dt_out[i] = cfl / max over grid i's interior of
  *             |u|/hx + |v|/hy + |w|/hz + cc*sqrt(hx^-2 + hy^-2 + hz^-2).
- * n above WS_DT_STATIC_MAX_GRIDS is rejected with WS_ERR_INVALID.  The first
- * call with a given device current looks up the array's device address;
- * make that first call before any stream capture.  All calls share the
- * array (each clears the entries it uses first), so calls whose work
- * overlaps on the GPU race: serialise them.  Synchronises `stream`. */
+ * n above WS_DT_STATIC_MAX_GRIDS is rejected with WS_ERR_INVALID; a grid with
+ * a NaN or infinite wave speed in any cell gives WS_ERR_NONFINITE.  The first
+ * call with a given device current looks up the array's device address and
+ * keeps it until exit; make that first call before any stream capture, and
+ * do not call cudaDeviceReset after it.  All calls share the array (each
+ * clears the entries it uses first), so calls whose work overlaps on the GPU
+ * race: serialise them.  Every call copies the maxima to the host and
+ * synchronises `stream` before it returns. */
 #define WS_DT_STATIC_MAX_GRIDS 4096
 WS_API int ws_compute_dt_static(const ws_grid* grids, const ws_field* prims, int n, double cfl,
                                 double* dt_out, ws_stream_t stream);

@@ -36,6 +36,7 @@ ring kernel (OCFD_NS_Jacobian3d.cpp:1063-1085 x, :1515-1584 y).
 
 Only tests/ and bench.py's CPU-baseline legs use the result, as the checker.
 Usage:  python oracle/build_ref.py [--ref /path/to/reference] [--native]
+        (the tree defaults to $WS_REFERENCE, else the recipe's mount point)
 """
 from __future__ import annotations
 
@@ -48,7 +49,15 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "_ref")
-DEFAULT_REF = "/root/reference"
+# Where this recipe looks for the reference tree: --ref, else $WS_REFERENCE,
+# else the read-only mount of the machine the recipe was written for.
+MOUNT_REF = "/root/reference"
+
+
+def reference_tree() -> str | None:
+    """The reference tree to read, or None when none is mounted."""
+    ref = os.environ.get("WS_REFERENCE", MOUNT_REF)
+    return ref if os.path.isdir(os.path.join(ref, "src")) else None
 
 FUNCS = [
     ("src/kernels/OCFD_Schemes.cpp", "OCFD_weno7_SYMBO_kernel_P_opt"),
@@ -506,7 +515,7 @@ def build(ref: str, native: bool = False) -> str:
 
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default=os.environ.get("WS_REFERENCE", DEFAULT_REF))
+    ap.add_argument("--ref", default=os.environ.get("WS_REFERENCE", MOUNT_REF))
     ap.add_argument("--native", action="store_true")
     a = ap.parse_args()
     if not os.path.isdir(os.path.join(a.ref, "src")):

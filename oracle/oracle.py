@@ -280,9 +280,11 @@ class RefFunctions:
         self.lib.ref_split_batch(_p(pts), len(pts), gamma, epsl_sw, _p(fp), _p(fm))
         return fp, fm
 
-    def cons_to_prim(self, g: OrGrid, f):
-        shp = (g.nz + 2 * LAP, g.ny + 2 * LAP, g.nx + 2 * LAP)
-        out = [np.zeros(shp) for _ in range(6)]
+    def cons_to_prim(self, g: OrGrid, f, out=None):
+        """d, u, v, w, T, P as LAP fields (interiors written; `out` reused when given)."""
+        if out is None:
+            shp = (g.nz + 2 * LAP, g.ny + 2 * LAP, g.nx + 2 * LAP)
+            out = [np.zeros(shp) for _ in range(6)]
         self.lib.ref_cons_to_prim(g.nx, g.ny, g.nz, g.gamma, g.ama, _p(f), *[_p(a) for a in out])
         return out
 
@@ -292,16 +294,16 @@ class RefFunctions:
                                   _p(w), _p(T), _p(f))
         return f
 
-    def sound_speed(self, g: OrGrid, T):
-        cc = np.empty_like(T)
+    def sound_speed(self, g: OrGrid, T, out=None):
+        cc = np.empty_like(T) if out is None else out
         self.lib.ref_sound_speed(g.nx, g.ny, g.nz, g.ama, _p(T), _p(cc))
         return cc
 
     def time_advance(self, krk, dt, g: OrGrid, f, fn, du):
         self.lib.ref_time_advance(krk, dt, g.nx, g.ny, g.nz, _p(f), _p(fn), _p(du))
 
-    def du_invis(self, g: OrGrid, d, u, v, w, cc, metrics=None, ajac=None):
-        du = np.empty((5, g.nz, g.ny, g.nx))
+    def du_invis(self, g: OrGrid, d, u, v, w, cc, metrics=None, ajac=None, out=None):
+        du = np.empty((5, g.nz, g.ny, g.nx)) if out is None else out
         kinds = (C.c_int * 6)(*[g.face_kind[i] for i in range(6)])
         self.lib.ref_du_invis(g.nx, g.ny, g.nz, g.hx, g.hy, g.hz, g.gamma, g.epsl_sw,
                               _p(d), _p(u), _p(v), _p(w), _p(cc), _ptr_array(metrics),
@@ -315,3 +317,40 @@ class RefFunctions:
                             vis.pr, vis.ref_t, vis.scheme, _p(u), _p(v), _p(w), _p(T),
                             _ptr_array(metrics), _p(ajac), _p(du), kinds)
         return du
+
+
+class RefRK3:
+    """SSP-RK3 time steps assembled from the reference's own scalar kernels
+    built for the host (oracle/_ref): per stage cons_to_pri_kernel, the ghost
+    fill (the oracle's restatement of the periodic / boundary halo), the
+    sound speed, the decomposed inviscid RHS and OCFD_time_advance_ker1/2/3
+    (the solver loop of OCFD_NS_Solver.cpp:64-90 with all three stages, as
+    or_rk3_steps runs it).  Every array is allocated once; a step allocates
+    nothing.  Used by bench.py's reference arm and CPU baseline only."""
+
+    def __init__(self, g: OrGrid, f: np.ndarray, ref: RefFunctions | None = None,
+                 oracle: Oracle | None = None):
+        self.g = g
+        self.ref = ref or RefFunctions()
+        self.o = oracle or Oracle()
+        shp = (g.nz + 2 * LAP, g.ny + 2 * LAP, g.nx + 2 * LAP)
+        self.prims = [np.zeros(shp) for _ in range(6)]    # d, u, v, w, T, P
+        self.cc = np.zeros(shp)
+        self.f = np.array(f, dtype=np.float64, order="C", copy=True)
+        self.fn = np.empty_like(self.f)
+        self.du = np.empty_like(self.f)
+
+    def rhs(self) -> np.ndarray:
+        g = self.g
+        self.ref.cons_to_prim(g, self.f, out=self.prims)
+        for x in self.prims[:5]:
+            self.o.ghost_fill(g, x)
+        self.ref.sound_speed(g, self.prims[4], out=self.cc)
+        d, u, v, w = self.prims[:4]
+        return self.ref.du_invis(g, d, u, v, w, self.cc, out=self.du)
+
+    def step(self, dt: float) -> None:
+        np.copyto(self.fn, self.f)
+        for krk in (1, 2, 3):
+            self.rhs()
+            self.ref.time_advance(krk, dt, self.g, self.f, self.fn, self.du)

@@ -27,8 +27,8 @@ def reffn():
     from oracle.oracle import RefFunctions
     if not RefFunctions.available():
         from oracle import build_ref
-        ref = os.environ.get("WS_REFERENCE", build_ref.DEFAULT_REF)
-        if os.path.isdir(os.path.join(ref, "src")):
+        ref = build_ref.reference_tree()
+        if ref:
             build_ref.build(ref)
     if not RefFunctions.available():
         pytest.skip("reference functions not built (reference tree absent)")

@@ -35,6 +35,10 @@ def test_reference_arm_line():
     c = d["config"]
     assert c["grid"] == [32, 16, 16] and c["inputs_exceed_l2"] is False
     assert "workload" in c and "model" not in c
+    # one reference step is one whole SSP-RK3 time step of the full grid,
+    # as on the GPU arm (3 RHS evaluations per step)
+    assert c["rhs_per_step"] == 3 and "SSP-RK3 time step of the 32x16x16 grid" in cb["sample"]
+    assert d["dt"] > 0
 
 
 def _free_port():

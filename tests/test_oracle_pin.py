@@ -151,3 +151,19 @@ def test_du_vis_bitexact(oracle, reffn, scheme, general, faces):
     b = reffn.du_vis(g, vis, u, v, w, T, metrics, ajac, base.copy())
     assert np.array_equal(a, b)
     assert np.array_equal(a[0], base[0])        # no viscous mass term
+
+
+def test_ref_rk3_steps_bitexact(oracle, reffn):
+    """The reference arm's time step (the reference's scalar kernels per
+    stage: cons_to_pri, ghost fill, sound speed, decomposed RHS, time advance
+    ker1/2/3) equals the oracle's SSP-RK3 steps bit for bit, on the headline
+    face kinds (extrapolation in x, periodic y and z)."""
+    from oracle.oracle import RefRK3, make_grid
+    from windstencil_b200 import workloads as wl
+    g = make_grid(24, 16, 12, face_kind=(1, 1, 0, 0, 0, 0))
+    f = wl.sod_state(24, 16, 12, seed=2)
+    dt = oracle.compute_dt(g, f, 0.5)
+    st = RefRK3(g, f, ref=reffn, oracle=oracle)
+    for _ in range(2):
+        st.step(dt)
+    assert np.array_equal(st.f, oracle.rk3_steps(g, f, dt, 2))

@@ -62,6 +62,44 @@ def test_dt_static_matches_allocating_entry_points(cuda):
         s.close()
 
 
+def test_dt_static_full_table(cuda):
+    """n = WS_DT_STATIC_MAX_GRIDS: every slot, the last included, is cleared,
+    reduced and read back (one small grid's fields behind every slot)."""
+    n = ws_max()
+    g = ws.Grid(16, 8, 8)
+    s = ws.Solver(g)
+    s.set_state(wl.fourier_state(16, 8, 8, seed=3))
+    ref = s.compute_dt(0.5)
+    _, _, p = s.fields()
+    stream = cuda.cuda.current_stream().cuda_stream
+    out = _static_dt([g] * n, [(p[1], p[2], p[3], p[5])] * n, 0.5, stream)
+    assert out.shape == (n,) and np.all(out == ref)
+    s.close()
+
+
+@pytest.mark.parametrize("kind", ["nan", "inf"])
+def test_dt_static_nonfinite(cuda, kind):
+    """A NaN or infinite wave speed in one cell of the second grid gives
+    WS_ERR_NONFINITE naming that grid, not a dt."""
+    shp = (24, 16, 12)
+    f_ok = wl.fourier_state(*shp, seed=31)
+    f_bad = f_ok.copy()
+    f_bad[1, 5, 7, 11] = np.nan if kind == "nan" else np.inf
+    solvers, quads = [], []
+    for f in (f_ok, f_bad):
+        s = ws.Solver(ws.Grid(*shp))
+        s.set_state(f)
+        _, _, p = s.fields()
+        quads.append((p[1], p[2], p[3], p[5]))
+        solvers.append(s)
+    stream = cuda.cuda.current_stream().cuda_stream
+    with pytest.raises(ws.WsError) as e:
+        _static_dt([ws.Grid(*shp)] * 2, quads, 0.5, stream)
+    assert e.value.code == 5 and "grid 1" in str(e.value)
+    for s in solvers:
+        s.close()
+
+
 def test_dt_static_rejects_too_many_grids(cuda):
     g = ws.Grid(8, 8, 8).c()
     f = _abi.WsField(0x10000, 32, 0)

@@ -93,8 +93,6 @@ SIGNATURES = {
     "ws_last_error": (_I, [C.c_char_p, C.c_size_t]),
     "ws_lap_pitch": (C.c_uint32, [C.c_uint32]),
     "ws_device_error": (_I, [C.POINTER(_I), _P]),
-    "ws_probe_fp64_peak": (_I, [C.POINTER(C.c_double), _P]),
-    "ws_probe_fp32_peak": (_I, [C.POINTER(C.c_double), _P]),
     "ws_du_invis_jacobian3d_init": (_I, [C.POINTER(WsGrid), WsJob, WsField, WsField, _P]),
     "ws_du_invis_jacobian3d": (_I, [C.POINTER(WsGrid), WsJob] + [WsField] * 5 +
                                [C.POINTER(WsMetrics), WsSoa, _P]),

@@ -6,6 +6,7 @@
 // (ghost fill; fused RHS with the stage update), the step replayed from a CUDA
 // graph, and an autotuner that times the compiled tile shapes on the batch.
 #include <algorithm>
+#include <cfloat>
 #include <cstring>
 #include <memory>
 #include <utility>
@@ -49,6 +50,7 @@ __global__ void max_speed_kernel(ws_field u, ws_field v, ws_field w, ws_field cc
     const long n = (long)nx * ny * nz;
     const double rr = sqrt(rx * rx + ry * ry + rz * rz);
     double m = 0.0;
+    bool bad = false;
     for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n;
          t += (long)gridDim.x * blockDim.x) {
         const int i = (int)(t % nx) + 4;
@@ -58,15 +60,24 @@ __global__ void max_speed_kernel(ws_field u, ws_field v, ws_field w, ws_field cc
             return f.ptr[(size_t)i + (size_t)f.pitch * ((size_t)j + (size_t)(ny + 8) * k)];
         };
         const double s = fabs(at(u)) * rx + fabs(at(v)) * ry + fabs(at(w)) * rz + at(cc) * rr;
+        // a NaN or infinite speed must reach the result, which fmax would
+        // drop (NaN) or the host could read as a valid maximum (+inf)
+        bad |= !(s <= DBL_MAX);
         m = fmax(m, s);
     }
     for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+    // positive doubles order like their bit patterns; the quiet-NaN pattern
+    // 0x7ff8... lies above every finite value and +inf, so it wins the max
+    const unsigned long long bits =
+        __any_sync(0xffffffffu, bad) ? 0x7ff8000000000000ull
+                                     : (unsigned long long)__double_as_longlong(m);
+    if ((threadIdx.x & 31) == 0) atomicMax(out, bits);
 }
 }  // namespace
 
 // max over the interior of |u|/hx + |v|/hy + |w|/hz + c*sqrt(hx^-2+hy^-2+hz^-2)
-// as the bits of a non-negative double, atomically max-ed into *out
+// as the bits of a non-negative double, atomically max-ed into *out (*out must
+// start at 0); a NaN or infinite speed in any cell yields NaN bits instead
 int launch_max_speed(const ws_grid* g, const ws_field prims[6], unsigned long long* out,
                      cudaStream_t st) {
     const long n = (long)g->nx * g->ny * g->nz;
@@ -469,7 +480,9 @@ int ws_batch_compute_dt(ws_batch* b, double cfl, double* dt_out, ws_stream_t str
     for (int i = 0; i < n; ++i) {
         double m;
         std::memcpy(&m, &h[i], sizeof m);
-        if (!(m > 0)) return fail(WS_ERR_NONFINITE, "maximum wave speed is not positive");
+        if (!wave_speed_ok(m))
+            return fail(WS_ERR_NONFINITE, "grid " + std::to_string(i) +
+                                              ": maximum wave speed is not finite and positive");
         dt_out[i] = cfl / m;
     }
     return WS_OK;

@@ -19,7 +19,9 @@
 // host threads) race on it: serialise them.  Host code never dereferences
 // the array's name -- in host code that name stands for a host-side shadow,
 // not the device address -- the device address is looked up once per device
-// with cudaGetSymbolAddress on the first call made with that device current.
+// with cudaGetSymbolAddress on the first call made with that device current
+// and kept for the life of the process, so a cudaDeviceReset after that
+// first call is not supported (the module reloads at another address).
 #include <cstring>
 #include <mutex>
 
@@ -90,18 +92,18 @@ extern "C" int ws_compute_dt_static(const ws_grid* grids, const ws_field* prims,
         rc = launch_max_speed(&grids[i], six, scratch + i, st);
         if (rc) return rc;
     }
-    unsigned long long bits[64];
-    for (int b = 0; b < n; b += 64) {
-        const int m = n - b < 64 ? n - b : 64;
-        WS_CUDA(cudaMemcpyAsync(bits, scratch + b, m * sizeof(unsigned long long),
-                                cudaMemcpyDeviceToHost, st));
-        WS_CUDA(cudaStreamSynchronize(st));
-        for (int i = 0; i < m; ++i) {
-            double v;
-            std::memcpy(&v, &bits[i], sizeof v);
-            if (!(v > 0)) return fail(WS_ERR_NONFINITE, "maximum wave speed is not positive");
-            dt_out[b + i] = cfl / v;
-        }
+    // one copy of the n maxima, one synchronisation (32 KB on the stack at most)
+    unsigned long long bits[WS_DT_STATIC_MAX_GRIDS];
+    WS_CUDA(cudaMemcpyAsync(bits, scratch, (size_t)n * sizeof(unsigned long long),
+                            cudaMemcpyDeviceToHost, st));
+    WS_CUDA(cudaStreamSynchronize(st));
+    for (int i = 0; i < n; ++i) {
+        double v;
+        std::memcpy(&v, &bits[i], sizeof v);
+        if (!wave_speed_ok(v))
+            return fail(WS_ERR_NONFINITE, "grid " + std::to_string(i) +
+                                              ": maximum wave speed is not finite and positive");
+        dt_out[i] = cfl / v;
     }
     return WS_OK;
 }

@@ -198,7 +198,7 @@ int start_requests(ws_server* s, std::vector<Req*>& fresh) {
         } else {
             double m;
             std::memcpy(&m, &h[i], sizeof m);
-            q->st.dt = m > 0 ? q->r.cfl / m : 0.0;
+            q->st.dt = wave_speed_ok(m) ? q->r.cfl / m : 0.0;   // 0: the request fails
         }
     }
     return WS_OK;

@@ -288,7 +288,8 @@ int ws_solver_compute_dt(ws_solver* s, double cfl, double* dt, ws_stream_t strea
     WS_CUDA(cudaStreamSynchronize(st));
     double m;
     std::memcpy(&m, &bits, sizeof m);
-    if (!(m > 0)) return fail(WS_ERR_NONFINITE, "maximum wave speed is not positive");
+    if (!wave_speed_ok(m))
+        return fail(WS_ERR_NONFINITE, "maximum wave speed is not finite and positive");
     *dt = cfl / m;
     return WS_OK;
 }

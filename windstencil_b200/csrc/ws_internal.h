@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cmath>
+
 #include <string>
 #include <vector>
 
@@ -19,6 +21,11 @@ int validate_grid(const ws_grid* g);
 int* device_error_word();
 // a device status word as an error code: bit 2 (a staging wait gave up) ->
 // WS_ERR_TIMEOUT, bit 1 (non-finite or non-physical state) -> WS_ERR_NONFINITE
+// A maximum wave speed read back from launch_max_speed usable for a CFL time
+// step: finite and positive (the reduction carries NaN and +inf through as
+// NaN bits, so one bad cell makes the whole grid's maximum unusable).
+inline bool wave_speed_ok(double m) { return std::isfinite(m) && m > 0; }
+
 inline int status_code(int v) {
     return (v & 2) ? WS_ERR_TIMEOUT : v ? WS_ERR_NONFINITE : WS_OK;
 }
