@@ -25,7 +25,7 @@ def test_bench_multi_rank_line(cuda, nproc, dims, par):
     assert d["scaling"] == "weak" and d["value"] > 0 and d["device_status"] == 0
     c = d["config"]
     assert c["parallelism"] == par and c["grid_per_gpu"] == [64, 32, 32]
-    assert c["halo_transport"].startswith("gloo")
+    assert d["halo_transport"].startswith("gloo")
     px, py, pz = (int(v) for v in (dims or f"{nproc},1,1").split(","))
     assert c["grid"] == [64 * px, 32 * py, 32 * pz]
     assert d["e2e"]["value"] > 0 and d["gpu_launches"] > 0
