@@ -124,30 +124,54 @@ __device__ __forceinline__ void split_point(const RhsArgs& a, const SplitK<CT>& 
 // values each.  Element k of the P stencil is at bp[k*stride], minus `wrap`
 // once k >= kw (the z ring wraps; x and y rows pass kw = 8); the M stencil is
 // the reversed F- row at +pmoff.
-template <typename CT>
+// CHOL: FP64 indicators in the Cholesky form (plain RHS kernels), else the
+// difference-chain form (stage kernels, which are at their register limit)
+template <typename CT, bool CHOL = true>
 __device__ __forceinline__ double face_flux(const CT* bp, int pmoff, int stride, int kw,
                                             int wrap);
 
 template <>
-__device__ __forceinline__ double face_flux<double>(const double* bp, int pmoff, int stride,
-                                                    int kw, int wrap) {
+__device__ __forceinline__ double face_flux<double, true>(const double* bp, int pmoff,
+                                                          int stride, int kw, int wrap);
+template <>
+__device__ __forceinline__ double face_flux<double, false>(const double* bp, int pmoff,
+                                                           int stride, int kw, int wrap);
+
+template <bool CHOL>
+__device__ __forceinline__ double face_flux_f64(const double* bp, int pmoff, int stride, int kw,
+                                                int wrap) {
     double t[8], np, dp, nm, dm;
 #pragma unroll
     for (int k = 0; k < 8; ++k) t[k] = bp[k * stride - (k >= kw ? wrap : 0)];
-    weno7_symbo_nd(t, np, dp);
+    weno7_symbo_nd<CHOL>(t, np, dp);
     const double p3 = t[3];
 #pragma unroll
     for (int k = 0; k < 8; ++k) t[k] = bp[pmoff + (7 - k) * stride - ((7 - k) >= kw ? wrap : 0)];
-    weno7_symbo_nd(t, nm, dm);
+    weno7_symbo_nd<CHOL>(t, nm, dm);
     const double m3 = t[3];
     return (p3 + m3) + (np * dm + nm * dp) / (dp * dm);
+}
+template <>
+__device__ __forceinline__ double face_flux<double, true>(const double* bp, int pmoff,
+                                                          int stride, int kw, int wrap) {
+    return face_flux_f64<true>(bp, pmoff, stride, kw, wrap);
+}
+template <>
+__device__ __forceinline__ double face_flux<double, false>(const double* bp, int pmoff,
+                                                           int stride, int kw, int wrap) {
+    return face_flux_f64<false>(bp, pmoff, stride, kw, wrap);
 }
 
 // mixed form: P and M in the two lanes of packed FP32x2 arithmetic; the face
 // value is summed in FP32 and widened once (the face difference is FP64)
 template <>
-__device__ __forceinline__ double face_flux<float>(const float* bp, int pmoff, int stride,
-                                                   int kw, int wrap) {
+__device__ __forceinline__ double face_flux<float, true>(const float* bp, int pmoff, int stride,
+                                                         int kw, int wrap);
+template <>
+__device__ __forceinline__ double face_flux<float, false>(const float* bp, int pmoff,
+                                                          int stride, int kw, int wrap);
+__device__ __forceinline__ double face_flux_f32(const float* bp, int pmoff, int stride, int kw,
+                                                int wrap) {
     float2 t[8], n, d;
 #pragma unroll
     for (int k = 0; k < 8; ++k)
@@ -156,6 +180,16 @@ __device__ __forceinline__ double face_flux<float>(const float* bp, int pmoff, i
     weno7_symbo_pm_f32x2(t, n, d);
     const float q = (n.x * d.y + n.y * d.x) * rcp_approx(d.x * d.y);
     return (double)((t[3].x + t[3].y) + q);
+}
+template <>
+__device__ __forceinline__ double face_flux<float, true>(const float* bp, int pmoff, int stride,
+                                                         int kw, int wrap) {
+    return face_flux_f32(bp, pmoff, stride, kw, wrap);
+}
+template <>
+__device__ __forceinline__ double face_flux<float, false>(const float* bp, int pmoff,
+                                                          int stride, int kw, int wrap) {
+    return face_flux_f32(bp, pmoff, stride, kw, wrap);
 }
 
 // CLOSURE face mode: value P + M of face f (between cells f-1 and f, f in
@@ -190,7 +224,7 @@ __device__ __forceinline__ double closure_value(const CT* prow, const CT* mrow, 
         double t[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) t[k] = sp[k];
-        weno7_symbo_nd(t, num, den);
+        weno7_symbo_nd<false>(t, num, den);
         P = sp[3] + num / den;
     }
     if (lo && f == 0) M = w5::m_lift(sm + 2);
@@ -207,7 +241,7 @@ __device__ __forceinline__ double closure_value(const CT* prow, const CT* mrow, 
         double t[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) t[k] = sm[7 - k];
-        weno7_symbo_nd(t, num, den);
+        weno7_symbo_nd<false>(t, num, den);
         M = sm[4] + num / den;
     }
     return P + M;
@@ -373,7 +407,7 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
         const int s0 = (z0 - 4) % 9;
         for (int t = tid; t < 5 * BXY; t += NT) {
             const int var = t / BXY, col = t - var * BXY;
-            fz[t] = face_flux<CT>(ring + s0 * RS + var * BXY + col, 5 * BXY, RS, 9 - s0, 9 * RS);
+            fz[t] = face_flux<CT, !EPI>(ring + s0 * RS + var * BXY + col, 5 * BXY, RS, 9 - s0, 9 * RS);
         }
     }
     cp_async_wait<0>();
@@ -456,7 +490,7 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
             const int s0 = (z - 3) % 9;
             for (; ta < NZF; ta += NT)
                 fz[cur * 5 * BXY + ta] =
-                    face_flux<CT>(ring + s0 * RS + ta, 5 * BXY, RS, 9 - s0, 9 * RS);
+                    face_flux<CT, !EPI>(ring + s0 * RS + ta, 5 * BXY, RS, 9 - s0, 9 * RS);
         }
         if (more) {
             if (!tma) {
@@ -486,7 +520,7 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
                 (clx && closure_face(f, a.nx, a.clo[0], a.clo[1]))
                     ? closure_value<CT>(bp, bp + 5 * BY * SXP, 1, f, a.nx, a.clo[0], a.clo[1],
                                         false)
-                    : face_flux<CT>(bp, 5 * BY * SXP, 1, 8, 0);
+                    : face_flux<CT, !EPI>(bp, 5 * BY * SXP, 1, 8, 0);
         }
         for (t -= NXR; t < NYR; t += NT) {
             const unsigned var = t / BXY, r = t % BXY, g = r / BX + 1, xx = r % BX;
@@ -496,7 +530,7 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
                 (cly && closure_face(f, a.ny, a.clo[2], a.clo[3]))
                     ? closure_value<CT>(bp, bp + 5 * SYH * BX, BX, f, a.ny, a.clo[2], a.clo[3],
                                         true)
-                    : face_flux<CT>(bp, 5 * SYH * BX, BX, 8, 0);
+                    : face_flux<CT, !EPI>(bp, 5 * SYH * BX, BX, 8, 0);
         }
         for (t -= NYR; t < NE; t += NT) {
             if (t < 5 * BY) {
@@ -507,7 +541,7 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
                     (clx && closure_face(f, a.nx, a.clo[0], a.clo[1]))
                         ? closure_value<CT>(bp, bp + 5 * BY * SXP, 1, f, a.nx, a.clo[0],
                                             a.clo[1], false)
-                        : face_flux<CT>(bp, 5 * BY * SXP, 1, 8, 0);
+                        : face_flux<CT, !EPI>(bp, 5 * BY * SXP, 1, 8, 0);
             } else {
                 const unsigned var = (t - 5 * BY) / BX, xx = (t - 5 * BY) % BX;
                 const CT* bp = sys + var * SYH * BX + xx;
@@ -516,7 +550,7 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
                     (cly && closure_face(f, a.ny, a.clo[2], a.clo[3]))
                         ? closure_value<CT>(bp, bp + 5 * SYH * BX, BX, f, a.ny, a.clo[2],
                                             a.clo[3], true)
-                        : face_flux<CT>(bp, 5 * SYH * BX, BX, 8, 0);
+                        : face_flux<CT, !EPI>(bp, 5 * SYH * BX, BX, 8, 0);
             }
         }
         cp_async_wait<0>();
@@ -538,8 +572,14 @@ __device__ __forceinline__ bool sweep(const RhsArgs& a, const SplitK<CT>& k, uns
         if (EPI) {
             if (dcell) {
                 const double* fbz = fb + b * 15 * BXY;
-                const size_t cell = fc0 + (size_t)z * fps;
+                // the cell's coordinates and offsets are recomputed here rather
+                // than kept live across the sweep (register pressure)
+                const int dcol = tid - (NT - BXY);
                 const int xx = dcol % BX, yy = dcol / BX;
+                const int dX = x0 + xx, dY = y0 + yy;
+                const size_t fps = (size_t)a.fn.pitch * a.fn.length_Y;
+                const size_t fvs = fps * a.fn.length_Z;
+                const size_t cell = soa_index(a.fn, dX - 4, dY - 4, z - 4, 0);
                 double q[5];
 #pragma unroll
                 for (int var = 0; var < 5; ++var) {

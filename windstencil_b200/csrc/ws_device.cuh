@@ -125,16 +125,18 @@ __device__ __forceinline__ void sw_split_gen(T d, T u, T v, T w, T c, T a1, T a2
 
 // ---------------------------------------------------------------------------
 // WENO7-SYMBO face value from t[0..7] = points i-3..i+4 (P orientation),
-// evaluated on the first, second and third differences of the stencil:
-//   D_j = t_{j+1}-t_j,  S_j = D_{j+1}-D_j,  T_j = S_{j+1}-S_j.
-// In these variables the reference's three derivative rounds of candidate k
-// (OCFD_Schemes.cpp:306-368) are a 3-term first-difference form r_k, 6 x a
-// 1-2 term second-difference form s_k and 6 x T_k, so
-//   beta_k / (720 * 39) = (r_k/sqrt 39)^2 + s_k^2 + (39.05/39) T_k^2.
-// The common factor 720*39 is taken out of every indicator and of eps, which
-// leaves the normalised weights unchanged; 1/sqrt(39) is folded into the
-// r_k coefficients and eps into the sum, so e_k = eps' + beta'_k costs three
-// FMAs.  Each candidate's coefficients sum to 12, so q_k = 12 t_3 + l_k(D)
+// evaluated on the first differences of the stencil D_j = t_{j+1}-t_j, with
+// S_j = D_{j+1}-D_j and T_j = S_{j+1}-S_j.  In these variables the
+// reference's three derivative rounds of candidate k (OCFD_Schemes.cpp:
+// 306-368) are a 3-term first-difference form r_k, 6 x a 1-2 term
+// second-difference form s_k and 6 x T_k, so
+//   beta_k / (720 * 39) = (r_k/sqrt 39)^2 + s_k^2 + (39.05/39) T_k^2,
+// a positive-definite quadratic form in three consecutive D_j.  The common
+// factor 720*39 is taken out of every indicator and of eps, which leaves the
+// normalised weights unchanged, and each form is evaluated through its
+// Cholesky factor (wk::UF below): e_k = eps' + beta'_k costs nine operations
+// on the D_j and needs no S_j / T_j.  Each candidate's coefficients sum to
+// 12, so q_k = 12 t_3 + l_k(D)
 // and face = t_3 + sum d_k P_k l_k / (12 sum d_k P_k), P_k the product of the
 // other four e_j (the reference's product weights); d_k is folded into the
 // l_k coefficients.  All of this is an exact algebraic rewrite (agreement
@@ -150,11 +152,6 @@ constexpr double D0 = 0.0401954833730, D1 = 0.2493800006710, D2 = 0.480268625626
                  D3 = 0.2009775476730, D4 = 0.0291783426580;
 }  // namespace wk
 
-template <typename T>
-struct WenoDiffs {
-    T D0, D1, D2, D3, D4, D5, D6;
-    T e0, e1, e2, e3, e4;     // eps' + beta'_k (e4 before the SYMBO max)
-};
 
 // The FP64 coefficients live in constant memory: a DFMA/DMUL takes a
 // constant-bank operand directly, whereas a 64-bit literal that does not fit
@@ -163,38 +160,58 @@ struct WenoDiffs {
 // The array is never written; its values are the constexpr ones above.
 namespace wk {
 enum Coef {
-    R11, RM7, R2, R5, RM1, RM31, R26, CC, EPSC,                // indicators
+    E0, E1 = E0 + 6, E2 = E1 + 6, E3 = E2 + 6, E4 = E3 + 6,     // indicator factors
+    EPSC = E4 + 6,
+    R11, RM7, R2, R5, RM1, RM31, R26, CC,                       // chain form
+
     L0A, L0B, L0C, L1A, L1B, L1C, L2A, L2B, L2C, L3A, L3B, L3C,   // d_k l_k
     L4A, L4B, L4C, L4D,
     Q0, Q1, Q2, Q3, Q4,                                       // 12 d_k
     NCOEF
 };
+// Cholesky factors of the five indicator forms.  In the variables above,
+// e_k - eps' = r_k^2 + s_k^2 + (39.05/39) T_k^2 is a positive-definite
+// quadratic form Q_k in three consecutive first differences; with those
+// taken in the order (v0, v1, v2) below, Q_k = U^T U for an upper-triangular
+// U, so e_k = eps' + y0^2 + y1^2 + y2^2 with
+//   y0 = U00 v0 + U01 v1 + U02 v2,  y1 = U11 v1 + U12 v2,  y2 = U22 v2
+// (nine operations, and no second / third difference chains).  The factors
+// follow from the reference's derivative-round weights alone (rounded from a
+// 40-digit evaluation); the identity holds to 1e-16 relative.
+//   e0: (D2, D0, D1)  e1: (D3, D1, D2)  e2: (D2, D4, D3)
+//   e3: (D3, D4, D5)  e4: (D4, D5, D6)
+constexpr double UF[30] = {
+    2.8467255143139729562, 1.2524511398998827387, -3.5047014637543644273,
+    0.73158205008709597394, -1.3287246702332208323, 0.4616241568745027212,
+    1.4504641167040823579, 0.65496277299069166801, -1.8932931980378698419,
+    0.77327022632416193136, -1.1519034838986927736, 0.85715405628127057224,
+    1.0506408300871206129, 0.90421005237462993517, -1.6619893270367691926,
+    1.0996941657150618495, -1.4803950271616324632, 0.83209127295316749707,
+    2.8467255143139729562, -3.5047014637543644273, 1.2524511398998827387,
+    1.4066293440336288338, -0.69106415444385934995, 0.24008879701567067037,
+    5.22825165658802088, -7.2049383318732343462, 2.7417607885329328577,
+    1.3172006225543553721, -0.75306405648544262277, 0.13960107141105386569};
 }  // namespace wk
 static __constant__ double wkc[wk::NCOEF] = {
-    11 * wk::R, -7 * wk::R, 2 * wk::R, 5 * wk::R, -wk::R, -31 * wk::R, 26 * wk::R, wk::C, wk::EPS,
+    wk::UF[0], wk::UF[1], wk::UF[2], wk::UF[3], wk::UF[4], wk::UF[5],
+    wk::UF[6], wk::UF[7], wk::UF[8], wk::UF[9], wk::UF[10], wk::UF[11],
+    wk::UF[12], wk::UF[13], wk::UF[14], wk::UF[15], wk::UF[16], wk::UF[17],
+    wk::UF[18], wk::UF[19], wk::UF[20], wk::UF[21], wk::UF[22], wk::UF[23],
+    wk::UF[24], wk::UF[25], wk::UF[26], wk::UF[27], wk::UF[28], wk::UF[29],
+    wk::EPS,
+    11 * wk::R, -7 * wk::R, 2 * wk::R, 5 * wk::R, -wk::R, -31 * wk::R, 26 * wk::R, wk::C,
     13 * wk::D0, -10 * wk::D0, 3 * wk::D0, 3 * wk::D1, 4 * wk::D1, -wk::D1,
     -wk::D2, 6 * wk::D2, wk::D2, wk::D3, -4 * wk::D3, 9 * wk::D3,
     -3 * wk::D4, 10 * wk::D4, -13 * wk::D4, 12 * wk::D4,
     12 * wk::D0, 12 * wk::D1, 12 * wk::D2, 12 * wk::D3, 12 * wk::D4};
 
-__device__ __forceinline__ double weno_e(double r, double s, double t3) {
-    return fma(r, r, fma(s, s, fma(wkc[wk::CC] * t3, t3, wkc[wk::EPSC])));
-}
-
-__device__ __forceinline__ void weno7_indicators(const double t[8], WenoDiffs<double>& o) {
-    using namespace wk;
-    o.D0 = t[1] - t[0]; o.D1 = t[2] - t[1]; o.D2 = t[3] - t[2]; o.D3 = t[4] - t[3];
-    o.D4 = t[5] - t[4]; o.D5 = t[6] - t[5]; o.D6 = t[7] - t[6];
-    const double S0 = o.D1 - o.D0, S1 = o.D2 - o.D1, S2 = o.D3 - o.D2, S3 = o.D4 - o.D3;
-    const double S4 = o.D5 - o.D4, S5 = o.D6 - o.D5;
-    const double T0 = S1 - S0, T1 = S2 - S1, T2 = S3 - S2, T3 = S4 - S3, T4 = S5 - S4;
-    const double* k = wkc;
-    o.e0 = weno_e(fma(k[R11], o.D2, fma(k[RM7], o.D1, k[R2] * o.D0)), fma(2.0, S1, -S0), T0);
-    o.e1 = weno_e(fma(k[R2], o.D3, fma(k[R5], o.D2, k[RM1] * o.D1)), S2, T1);
-    o.e2 = weno_e(fma(k[RM1], o.D4, fma(k[R5], o.D3, k[R2] * o.D2)), S3, T2);
-    o.e3 = weno_e(fma(k[R2], o.D5, fma(k[RM7], o.D4, k[R11] * o.D3)), fma(2.0, S3, -S4), T3);
-    o.e4 = weno_e(fma(k[R11], o.D6, fma(k[RM31], o.D5, k[R26] * o.D4)),
-                  fma(-2.0, S5, 3.0 * S4), T4);
+// eps' + the Cholesky form of factor set `f` (wk::E0 .. wk::E4) on (v0, v1, v2)
+__device__ __forceinline__ double weno_e(double v0, double v1, double v2, int f) {
+    const double* k = wkc + f;
+    const double y0 = fma(k[2], v2, fma(k[1], v1, k[0] * v0));
+    const double y1 = fma(k[4], v2, k[3] * v1);
+    const double y2 = k[5] * v2;
+    return fma(y0, y0, fma(y1, y1, fma(y2, y2, wkc[wk::EPSC])));
 }
 
 // max of two indicators (both > 0): positive doubles order like their bit
@@ -207,22 +224,51 @@ __device__ __forceinline__ double pos_max(double a, double b) {
 }
 
 // face value = t[3] + num/den
+// The same indicators in the difference-chain form: r_k from the D_j, s_k from
+// the S_j and C T_k^2 from the T_j (ten operations per indicator counting the
+// shared S_j / T_j chains, against nine for the Cholesky form).  It holds
+// fewer values live at once, which is what the stage kernels (EPI), at the
+// 80-register limit of 704 threads, need: with the Cholesky form they spill.
+__device__ __forceinline__ double weno_e_chain(double r, double s, double t3) {
+    return fma(r, r, fma(s, s, fma(wkc[wk::CC] * t3, t3, wkc[wk::EPSC])));
+}
+
+// face value = t[3] + num/den; CHOL selects the indicator form (identical
+// values up to rounding)
+template <bool CHOL>
 __device__ __forceinline__ void weno7_symbo_nd(const double t[8], double& num, double& den) {
     using namespace wk;
-    WenoDiffs<double> o;
-    weno7_indicators(t, o);
-    const double e0 = o.e0, e1 = o.e1, e2 = o.e2, e3 = o.e3;
-    const double e4 = pos_max(pos_max(pos_max(e0, e1), pos_max(e2, e3)), o.e4);   // SYMBO
+    const double* k = wkc;
+    const double D0 = t[1] - t[0], D1 = t[2] - t[1], D2 = t[3] - t[2], D3 = t[4] - t[3];
+    const double D4 = t[5] - t[4], D5 = t[6] - t[5], D6 = t[7] - t[6];
+    double e0, e1, e2, e3, e4;
+    if (CHOL) {
+        e0 = weno_e(D2, D0, D1, E0);
+        e1 = weno_e(D3, D1, D2, E1);
+        e2 = weno_e(D2, D4, D3, E2);
+        e3 = weno_e(D3, D4, D5, E3);
+        e4 = weno_e(D4, D5, D6, E4);
+    } else {
+        const double S0 = D1 - D0, S1 = D2 - D1, S2 = D3 - D2, S3 = D4 - D3;
+        const double S4 = D5 - D4, S5 = D6 - D5;
+        const double T0 = S1 - S0, T1 = S2 - S1, T2 = S3 - S2, T3 = S4 - S3, T4 = S5 - S4;
+        e0 = weno_e_chain(fma(k[R11], D2, fma(k[RM7], D1, k[R2] * D0)), fma(2.0, S1, -S0), T0);
+        e1 = weno_e_chain(fma(k[R2], D3, fma(k[R5], D2, k[RM1] * D1)), S2, T1);
+        e2 = weno_e_chain(fma(k[RM1], D4, fma(k[R5], D3, k[R2] * D2)), S3, T2);
+        e3 = weno_e_chain(fma(k[R2], D5, fma(k[RM7], D4, k[R11] * D3)), fma(2.0, S3, -S4), T3);
+        e4 = weno_e_chain(fma(k[R11], D6, fma(k[RM31], D5, k[R26] * D4)),
+                          fma(-2.0, S5, 3.0 * S4), T4);
+    }
+    e4 = pos_max(pos_max(pos_max(e0, e1), pos_max(e2, e3)), e4);   // SYMBO
     // leave-one-out products from prefix / suffix partial products
     const double p01 = e0 * e1, p34 = e3 * e4;
     const double p012 = p01 * e2, p234 = e2 * p34;
     const double P0 = e1 * p234, P1 = e0 * p234, P2 = p01 * p34, P3 = p012 * e4, P4 = p012 * e3;
-    const double* k = wkc;
-    const double l0 = fma(k[L0A], o.D2, fma(k[L0B], o.D1, k[L0C] * o.D0));
-    const double l1 = fma(k[L1A], o.D3, fma(k[L1B], o.D2, k[L1C] * o.D1));
-    const double l2 = fma(k[L2A], o.D4, fma(k[L2B], o.D3, k[L2C] * o.D2));
-    const double l3 = fma(k[L3A], o.D5, fma(k[L3B], o.D4, k[L3C] * o.D3));
-    const double l4 = fma(k[L4A], o.D6, fma(k[L4B], o.D5, fma(k[L4C], o.D4, k[L4D] * o.D3)));
+    const double l0 = fma(k[L0A], D2, fma(k[L0B], D1, k[L0C] * D0));
+    const double l1 = fma(k[L1A], D3, fma(k[L1B], D2, k[L1C] * D1));
+    const double l2 = fma(k[L2A], D4, fma(k[L2B], D3, k[L2C] * D2));
+    const double l3 = fma(k[L3A], D5, fma(k[L3B], D4, k[L3C] * D3));
+    const double l4 = fma(k[L4A], D6, fma(k[L4B], D5, fma(k[L4C], D4, k[L4D] * D3)));
     num = fma(P4, l4, fma(P3, l3, fma(P2, l2, fma(P1, l1, P0 * l0))));
     den = fma(k[Q4], P4, fma(k[Q3], P3, fma(k[Q2], P2, fma(k[Q1], P1, k[Q0] * P0))));
 }
@@ -332,29 +378,28 @@ __device__ __forceinline__ float rcp_approx(float x) {
 __device__ __forceinline__ float2 rcp2(float2 x) {
     return make_float2(rcp_approx(x.x), rcp_approx(x.y));
 }
-__device__ __forceinline__ float2 weno_e2(float2 r, float2 s, float2 t3) {
-    return fma2(r, r, fma2(s, s, fma2(mul2(f2((float)wk::C), t3), t3, f2((float)wk::EPS))));
+// eps' + the Cholesky form of factor set F (wk::E0 .. wk::E4) on (v0, v1, v2),
+// both lanes
+template <int F>
+__device__ __forceinline__ float2 weno_e2(float2 v0, float2 v1, float2 v2) {
+    constexpr float u0 = (float)wk::UF[F], u1 = (float)wk::UF[F + 1], u2 = (float)wk::UF[F + 2];
+    constexpr float u3 = (float)wk::UF[F + 3], u4 = (float)wk::UF[F + 4];
+    constexpr float u5 = (float)wk::UF[F + 5];
+    const float2 y0 = fma2(f2(u2), v2, fma2(f2(u1), v1, mul2(f2(u0), v0)));
+    const float2 y1 = fma2(f2(u4), v2, mul2(f2(u3), v1));
+    const float2 y2 = mul2(f2(u5), v2);
+    return fma2(y0, y0, fma2(y1, y1, fma2(y2, y2, f2((float)wk::EPS))));
 }
 
 // face value of lane L = t[3].L + num.L / den.L
 __device__ __forceinline__ void weno7_symbo_pm_f32x2(const float2 t[8], float2& num,
                                                      float2& den) {
-    constexpr float R = (float)wk::R;
     const float2 D0 = sub2(t[1], t[0]), D1 = sub2(t[2], t[1]), D2 = sub2(t[3], t[2]);
     const float2 D3 = sub2(t[4], t[3]), D4 = sub2(t[5], t[4]), D5 = sub2(t[6], t[5]);
     const float2 D6 = sub2(t[7], t[6]);
-    const float2 S0 = sub2(D1, D0), S1 = sub2(D2, D1), S2 = sub2(D3, D2), S3 = sub2(D4, D3);
-    const float2 S4 = sub2(D5, D4), S5 = sub2(D6, D5);
-    const float2 T0 = sub2(S1, S0), T1 = sub2(S2, S1), T2 = sub2(S3, S2), T3 = sub2(S4, S3);
-    const float2 T4 = sub2(S5, S4);
-    const float2 e0 = weno_e2(fma2(f2(11 * R), D2, fma2(f2(-7 * R), D1, mul2(f2(2 * R), D0))),
-                              fma2(f2(2.f), S1, mul2(f2(-1.f), S0)), T0);
-    const float2 e1 = weno_e2(fma2(f2(2 * R), D3, fma2(f2(5 * R), D2, mul2(f2(-R), D1))), S2, T1);
-    const float2 e2 = weno_e2(fma2(f2(-R), D4, fma2(f2(5 * R), D3, mul2(f2(2 * R), D2))), S3, T2);
-    const float2 e3 = weno_e2(fma2(f2(2 * R), D5, fma2(f2(-7 * R), D4, mul2(f2(11 * R), D3))),
-                              fma2(f2(2.f), S3, mul2(f2(-1.f), S4)), T3);
-    float2 e4 = weno_e2(fma2(f2(11 * R), D6, fma2(f2(-31 * R), D5, mul2(f2(26 * R), D4))),
-                        fma2(f2(3.f), S4, mul2(f2(-2.f), S5)), T4);
+    const float2 e0 = weno_e2<wk::E0>(D2, D0, D1), e1 = weno_e2<wk::E1>(D3, D1, D2);
+    const float2 e2 = weno_e2<wk::E2>(D2, D4, D3), e3 = weno_e2<wk::E3>(D3, D4, D5);
+    float2 e4 = weno_e2<wk::E4>(D4, D5, D6);
     e4.x = fmaxf(fmaxf(fmaxf(e0.x, e1.x), fmaxf(e2.x, e3.x)), e4.x);
     e4.y = fmaxf(fmaxf(fmaxf(e0.y, e1.y), fmaxf(e2.y, e3.y)), e4.y);
     const float2 r01 = rcp2(mul2(e0, e1)), r23 = rcp2(mul2(e2, e3)), r4 = rcp2(e4);
