@@ -23,6 +23,10 @@ from tests.conftest import rel_linf
 pytestmark = pytest.mark.gpu
 SHAPE = (64, 32, 16)
 HOLD = "64"
+# the fused kernel's tile shape: the waits are its TMA staging waits (the
+# default FP64 path, the line passes, loads with plain global loads and has
+# no wait to run out)
+FUSED = (16, 8, 0, 704)
 
 
 def _rhs_drop_in(s, g):
@@ -30,8 +34,9 @@ def _rhs_drop_in(s, g):
     lib, gc = ws.load(), g.c()
     _, du, prims = s.fields()
     ws.check(lib.ws_ghost_fill(C.byref(gc), (ws.WsField * 6)(*prims), 6, None))
-    ws.check(lib.ws_du_invis_jacobian3d(C.byref(gc), ws.interior_job(g), prims[0], prims[1],
-                                        prims[2], prims[3], prims[5], None, du, None))
+    ws.check(lib.ws_du_invis_jacobian3d_tiled(C.byref(gc), ws.interior_job(g), prims[0],
+                                              prims[1], prims[2], prims[3], prims[5], None, du,
+                                              ws.WsTile(*FUSED), None))
 
 
 def test_drop_in_wait_timeout_reported(oracle, cuda, monkeypatch):
@@ -58,6 +63,7 @@ def test_stage_kernel_wait_timeout_reported(oracle, cuda, monkeypatch):
     og = or_grid(*SHAPE)
     dt = oracle.compute_dt(og, f0, 0.5)
     s = ws.Solver(g)
+    s.set_tile(FUSED)
     s.set_state(f0)
     monkeypatch.setenv("WS_TEST_STAGE_WAIT", HOLD)
     s.step(dt * 0.5, 1)                           # captured with the forced wait

@@ -240,8 +240,33 @@ int tile_index(const ws_grid* g, ws_tile tile, bool stage, int* cfg) {
 }
 
 // Fill RhsArgs and launch; shared by the drop-in entry and the solver.
+bool use_pencil(const ws_grid* g, ws_tile tile) {
+    if (tile.tile_x < 0) return true;
+    if (tile.tile_x || tile.tile_y || tile.threads) return false;
+    for (int i = 0; i < 4; ++i)
+        if (g->face_kind[i] == WS_FACE_CLOSURE) return false;
+    return g->precision == WS_FP64;
+}
+
+namespace {
+int check_pencil(const ws_grid* g, ws_tile tile) {
+    for (int i = 0; i < 4; ++i)
+        if (g->face_kind[i] == WS_FACE_CLOSURE)
+            return fail(WS_ERR_UNSUPPORTED, "line passes: no CLOSURE faces");
+    if (tile.threads % 32) return fail(WS_ERR_INVALID, "line passes: threads = 32 x warps");
+    return WS_OK;
+}
+}  // namespace
+
 int rhs_enqueue(const ws_grid* g, ws_job job, const ws_field prims[5], const ws_metrics* m,
                 ws_soa du, ws_tile tile, cudaStream_t st) {
+    if (use_pencil(g, tile)) {
+        int rc = check_pencil(g, tile);
+        if (rc) return rc;
+        const RhsArgs a = make_rhs_args(g, job, prims, m, du, 0, 1);
+        return launch_rhs_pencil(a, g->precision, g->metrics_uniform != 0, tile.threads / 32, 0,
+                                 false, st);
+    }
     int cfg = 0;
     int rc = tile_index(g, tile, false, &cfg);
     if (rc) return rc;
@@ -257,7 +282,19 @@ int rhs_enqueue(const ws_grid* g, ws_job job, const ws_field prims[5], const ws_
 // new primitives p_out.
 int rhs_stage_enqueue(const ws_grid* g, const ws_field p_in[6], ws_soa f_in, ws_soa fn,
                       ws_soa f_out, const ws_field p_out[6], double dt, int krk, int* status,
-                      ws_soa dvis, ws_tile tile, cudaStream_t st) {
+                      ws_soa dvis, ws_soa du, ws_tile tile, cudaStream_t st) {
+    if (use_pencil(g, tile)) {
+        int rc = check_pencil(g, tile);
+        if (rc) return rc;
+        if (du.pitch != fn.pitch || du.length_Y != fn.length_Y || du.length_Z != fn.length_Z)
+            return fail(WS_ERR_INVALID, "line passes: du needs the state's shape");
+        ws_job job{{4, 4, 4}, {g->nx + 4, g->ny + 4, g->nz + 4}};
+        const ws_field p5[5] = {p_in[0], p_in[1], p_in[2], p_in[3], p_in[5]};
+        RhsArgs a = make_rhs_args(g, job, p5, nullptr, du, 0, 1);
+        if ((rc = set_rhs_stage(a, g, f_in, fn, f_out, p_out, dt, status))) return rc;
+        return launch_rhs_pencil(a, g->precision, true, tile.threads / 32, krk,
+                                 dvis.ptr != nullptr, st);
+    }
     int cfg = 0;
     int rc = tile_index(g, tile, true, &cfg);
     if (rc) return rc;

@@ -1,0 +1,209 @@
+// pencil_impl.cuh -- BF3W inviscid RHS as three barrier-free line passes.
+//
+// Replaces, like the fused kernel (bf3w_rhs_impl.cuh), the reference's
+// split_Jac3d_Stager_Warming_ker (src/kernels/OCFD_split.cpp:36-3918) and
+// its boundary-ring kernel (src/solver/OCFD_NS_Jacobian3d.cpp:828-2530), with
+// the same per-point arithmetic (ws_device.cuh).  The fused kernel sweeps a
+// 2D column footprint along z with CTA barriers between its split and face
+// intervals and recomputes the footprint's halo splits and edge faces.  Here
+// every lane owns one grid line along the pass direction and marches it
+// alone: per point it computes the Steger-Warming split of the point four
+// ahead into a private 8-slot ring in shared memory, reconstructs the face
+// above the current point from the ring (WENO7-SYMBO P and M), and adds the
+// face difference of the point to du.  No lane reads another lane's ring, so
+// there is no barrier and no halo work across lines; a warp's lanes own 32
+// consecutive lines of the flattened pair of the other two axes, so there
+// are no partial tiles, and each warp takes an equal contiguous share of the
+// (line group, position) space.  The primitives of the next split and the
+// du of the next point are loaded a step ahead, so that their latency
+// overlaps the current step's reconstructions.
+//
+// A RHS is three passes, x (du =, or += onto viscous terms already stored in
+// du), y (+=) and z (+=, or in stage mode the SSP-RK3 stage update and the
+// primitives of the new state, as the fused kernel's epilogue).  du goes
+// through HBM between the passes, which the compute-bound passes absorb
+// (~320 B/cell against ~7.3 kFLOP/cell).
+#pragma once
+#include "bf3w_rhs_impl.cuh"
+
+namespace ws {
+
+template <typename CT>
+struct PencilLayout {
+    static constexpr int RS = 10 * 32;            // ring slot stride (CT), lanes inner
+    static constexpr int WARP = 8 * RS;           // one warp's ring
+};
+
+enum PencilMode { P_STORE = 0, P_ADD = 1, P_STAGE = 2 };
+
+// One pass along DIR (0 x, 1 y, 2 z) over the job of `a`.
+template <int DIR, int WPB, typename CT, bool UNI, int MODE>
+__global__ void __launch_bounds__(WPB * 32, 1)
+    pencil_rhs_kernel(const __grid_constant__ RhsArgs a, int krk) {
+    static_assert(MODE != P_STAGE || (DIR == 2 && UNI), "stage update: z pass, Cartesian");
+    constexpr bool ADD = MODE != P_STORE;
+    using P = PencilLayout<CT>;
+    extern __shared__ __align__(16) unsigned char pencil_smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    CT* ring = reinterpret_cast<CT*>(pencil_smem) + warp * P::WARP + lane;
+    const SplitK<CT> k = {CT(a.eps2), CT(a.hrg), CT(a.c1), CT(a.c3), CT(a.gm1)};
+    const int nxj = a.ex - a.sx, nyj = a.ey - a.sy, nzj = a.ez - a.sz;
+    const int n1 = DIR == 0 ? nyj : nxj;              // fastest line axis
+    const int n2 = DIR == 2 ? nyj : nzj;
+    const int L = DIR == 0 ? nxj : (DIR == 1 ? nyj : nzj);
+    const int m0 = DIR == 0 ? a.sx : (DIR == 1 ? a.sy : a.sz);
+    const int mlast = (DIR == 0 ? a.nx : (DIR == 1 ? a.ny : a.nz)) + 7;   // last LAP index
+    const double rh = DIR == 0 ? a.rhx : (DIR == 1 ? a.rhy : a.rhz);
+    const size_t vs = (size_t)a.du_pitch * a.du_ly * a.du_lz;            // du variable stride
+    const size_t fvs = MODE == P_STAGE ? (size_t)a.fn.pitch * a.fn.length_Y * a.fn.length_Z : 0;
+    const long NL = (long)n1 * n2, NG = (NL + 31) / 32, total = NG * L;
+    const long S = (long)gridDim.x * WPB, s = (long)blockIdx.x * WPB + warp;
+    long pos = total * s / S;
+    const long end = total * (s + 1) / S;
+    while (pos < end) {
+        const long grp = pos / L;
+        const int p0 = (int)(pos - grp * L);
+        const int len = (int)min((long)(L - p0), end - pos);
+        pos += len;
+        long l = grp * 32 + lane;
+        const bool valid = l < NL;
+        if (!valid) l = NL - 1;
+        const int c1 = (int)(l % n1), c2 = (int)(l / n1);
+        // LAP coordinates of march position m on this lane's line
+        auto X = [&](int m) { return DIR == 0 ? m : a.sx + c1; };
+        auto Y = [&](int m) { return DIR == 1 ? m : (DIR == 0 ? a.sy + c1 : a.sy + c2); };
+        auto Z = [&](int m) { return DIR == 2 ? m : a.sz + c2; };
+        auto load = [&](int m, double q[5]) {
+            const int x = X(m), y = Y(m), z = Z(m);
+#pragma unroll
+            for (int f = 0; f < 5; ++f) q[f] = ldg_prim(a, f, x, y, z);
+        };
+        auto split_into = [&](int m, const double q[5]) {
+            const int x = X(m), y = Y(m), z = Z(m);
+            CT out[10];
+            split_point<DIR, UNI, CT>(a, k, q[0], q[1], q[2], q[3], q[4], x, y, z, out);
+            CT* dst = ring + (m & 7) * P::RS;
+#pragma unroll
+            for (int c = 0; c < 10; ++c) dst[c * 32] = out[c];
+        };
+        // du offset of march position m (job-relative); in stage mode the
+        // conserved state has du's shape, offset by the interior origin
+        auto du_at = [&](int m) {
+            return (size_t)(X(m) - a.sx) +
+                   (size_t)a.du_pitch * ((size_t)(Y(m) - a.sy) + (size_t)a.du_ly * (size_t)(Z(m) - a.sz));
+        };
+        auto f_at = [&](int m) { return soa_index(a.fn, X(m) - 4, Y(m) - 4, Z(m) - 4, 0); };
+
+        const int ms = m0 + p0;
+        for (int m = ms - 4; m < ms + 4; ++m) {
+            double q[5];
+            load(m, q);
+            split_into(m, q);
+        }
+        double qn[5], dn[5], fnn[5], fin[5];
+        load(ms + 4, qn);
+        auto load_cell = [&](int m) {      // du (and the stage operands) of point m
+            if (ADD) {
+                const size_t o = du_at(m);
+#pragma unroll
+                for (int v = 0; v < 5; ++v) dn[v] = a.du[o + v * vs];
+            }
+            if (MODE == P_STAGE) {
+                const size_t o = f_at(m);
+#pragma unroll
+                for (int v = 0; v < 5; ++v) {
+                    fnn[v] = __ldg(a.fn.ptr + o + v * fvs);
+                    fin[v] = krk == 1 ? 0.0 : a.f_in.ptr[o + v * fvs];
+                }
+            }
+        };
+        if (valid) load_cell(ms);
+        double fprev[5];
+        {
+            const int s0 = (ms - 4) & 7;
+#pragma unroll
+            for (int v = 0; v < 5; ++v)
+                fprev[v] = face_flux<CT, true>(ring + s0 * P::RS + v * 32, 5 * 32, P::RS, 8 - s0,
+                                               8 * P::RS);
+        }
+        for (int m = ms; m < ms + len; ++m) {
+            double q[5], dc[5], fnc[5], fic[5];
+#pragma unroll
+            for (int f = 0; f < 5; ++f) {
+                q[f] = qn[f];
+                dc[f] = dn[f];
+                fnc[f] = fnn[f];
+                fic[f] = fin[f];
+            }
+            load(min(m + 5, mlast), qn);
+            if (valid && m + 1 < ms + len) load_cell(m + 1);
+            split_into(m + 4, q);
+            const int s0 = (m - 3) & 7;
+            const double J = UNI ? 1.0 : ldg_met(a, 9, X(m), Y(m), Z(m));
+            double r[5];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+                const double fc = face_flux<CT, true>(ring + s0 * P::RS + v * 32, 5 * 32, P::RS,
+                                                      8 - s0, 8 * P::RS);
+                r[v] = -J * ((fc - fprev[v]) * rh);
+                fprev[v] = fc;
+            }
+            if (!valid) continue;
+            if (MODE == P_STAGE) {
+                const size_t o = f_at(m);
+                double qs[5];
+#pragma unroll
+                for (int v = 0; v < 5; ++v) {
+                    qs[v] = ws_rk_stage(krk, fnc[v], fic[v], dc[v] + r[v], a.dt);
+                    a.f_out.ptr[o + v * fvs] = qs[v];
+                }
+                store_prims(a, qs, X(m), Y(m), Z(m));
+            } else {
+                const size_t o = du_at(m);
+#pragma unroll
+                for (int v = 0; v < 5; ++v) a.du[o + v * vs] = ADD ? dc[v] + r[v] : r[v];
+            }
+        }
+    }
+}
+
+template <int WPB, typename CT, bool UNI>
+struct PencilLauncher {
+    static size_t smem() { return (size_t)WPB * PencilLayout<CT>::WARP * sizeof(CT); }
+    template <int DIR, int MODE>
+    static int one(const RhsArgs& a, int krk, cudaStream_t st) {
+        auto kern = pencil_rhs_kernel<DIR, WPB, CT, UNI, MODE>;
+        static int blocks[64] = {0};       // attributes set and SM count read once per device
+        int dev = 0;
+        WS_CUDA(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= 64) return fail(WS_ERR_UNSUPPORTED, "device ordinal >= 64");
+        if (!blocks[dev]) {
+            int sms = 0;
+            WS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            WS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem()));
+            blocks[dev] = sms;
+        }
+        kern<<<blocks[dev], WPB * 32, smem(), st>>>(a, krk);
+        WS_CUDA(cudaGetLastError());
+        return WS_OK;
+    }
+    // plain RHS: x (=, or += with add_x), y (+=), z (+=)
+    static int rhs(const RhsArgs& a, bool add_x, cudaStream_t st) {
+        int rc = add_x ? one<0, P_ADD>(a, 0, st) : one<0, P_STORE>(a, 0, st);
+        if (rc || (rc = one<1, P_ADD>(a, 0, st))) return rc;
+        return one<2, P_ADD>(a, 0, st);
+    }
+    // stage: x, y into du, then z with the stage update
+    static int stage(const RhsArgs& a, bool add_x, int krk, cudaStream_t st) {
+        if constexpr (UNI) {
+            int rc = add_x ? one<0, P_ADD>(a, 0, st) : one<0, P_STORE>(a, 0, st);
+            if (rc || (rc = one<1, P_ADD>(a, 0, st))) return rc;
+            return one<2, P_STAGE>(a, krk, st);
+        } else {
+            return fail(WS_ERR_UNSUPPORTED, "stage update needs Cartesian metrics");
+        }
+    }
+};
+
+}  // namespace ws

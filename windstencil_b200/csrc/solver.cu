@@ -92,7 +92,7 @@ int enqueue_stage_end(ws_solver* s, int c, int krk, double dt, cudaStream_t st) 
         dvis = g.du;
     }
     return rhs_stage_enqueue(&g.g, pin, g.f[1 - c], g.f[c], g.f[1 - c], pout, dt, krk,
-                             g.status, dvis, s->tile, st);
+                             g.status, dvis, g.du, s->tile, st);
 }
 
 int enqueue_stage(ws_solver* s, int c, int krk, double dt, cudaStream_t st) {
@@ -168,7 +168,7 @@ void ws_solver_destroy(ws_solver* s) {
 
 int ws_solver_set_tile(ws_solver* s, ws_tile tile) {
     if (!s) return fail(WS_ERR_INVALID, "solver is NULL");
-    if ((tile.tile_x || tile.tile_y || tile.threads) &&
+    if (tile.tile_x >= 0 && (tile.tile_x || tile.tile_y || tile.threads) &&
         find_tile_cfg(tile.tile_x, tile.tile_y, tile.threads) < 0)
         return fail(WS_ERR_UNSUPPORTED, "tile shape not compiled in this build");
     s->tile = tile;

@@ -19,13 +19,12 @@ int validate_grid(const ws_grid* g);
 // the library's device error word of the current device (launches without a
 // per-grid status word report into it); NULL when it cannot be resolved
 int* device_error_word();
-// a device status word as an error code: bit 2 (a staging wait gave up) ->
-// WS_ERR_TIMEOUT, bit 1 (non-finite or non-physical state) -> WS_ERR_NONFINITE
 // A maximum wave speed read back from launch_max_speed usable for a CFL time
 // step: finite and positive (the reduction carries NaN and +inf through as
 // NaN bits, so one bad cell makes the whole grid's maximum unusable).
 inline bool wave_speed_ok(double m) { return std::isfinite(m) && m > 0; }
-
+// a device status word as an error code: bit 2 (a staging wait gave up) ->
+// WS_ERR_TIMEOUT, bit 1 (non-finite or non-physical state) -> WS_ERR_NONFINITE
 inline int status_code(int v) {
     return (v & 2) ? WS_ERR_TIMEOUT : v ? WS_ERR_NONFINITE : WS_OK;
 }
@@ -98,9 +97,11 @@ int rhs_ctas(const ws_grid* g, const RhsArgs& a, int cfg, bool stage);
 // reads primitives p_in (ghosts filled), f_in and fn; writes f_out and the
 // new primitives p_out.
 // dvis.ptr may be NULL (no viscous terms).
+// du: the grid's RHS buffer, which the line passes accumulate into (with
+// viscous terms it holds them, and dvis is the same buffer).
 int rhs_stage_enqueue(const ws_grid* g, const ws_field p_in[6], ws_soa f_in, ws_soa fn,
                       ws_soa f_out, const ws_field p_out[6], double dt, int krk, int* status,
-                      ws_soa dvis, ws_tile tile, cudaStream_t st);
+                      ws_soa dvis, ws_soa du, ws_tile tile, cudaStream_t st);
 
 // Viscous terms (viscous.cu): workspace size, parameter check, and du[1..4]
 // += (accumulate) or = the viscous terms (du[0] = 0 when storing) from the
@@ -127,6 +128,18 @@ int num_tile_cfgs();
 TileCfg tile_cfg(int i);
 int find_tile_cfg(int bx, int by, int threads);   // index or -1
 int default_cfg(int precision, bool stage);       // tuned default shape (stage kernel or plain RHS)
+
+// The RHS as three line passes x, y, z (pencil_impl.cuh), wpb warps per CTA
+// (0: the default), one CTA per SM; no CLOSURE faces.  krk 0: the RHS into
+// a.du; krk 1..3: the RHS into a.du, the z pass applying stage krk (a.f_in,
+// a.fn -> a.f_out, primitives to a.p_out).  add_x: a.du already holds terms
+// the RHS adds to (the viscous terms).
+int launch_rhs_pencil(const RhsArgs& a, int precision, bool uniform, int wpb, int krk,
+                      bool add_x, cudaStream_t st);
+// Whether a launch with tile selection `tile` runs the line passes: an
+// explicit request (tile_x < 0, threads = 32 x warps per CTA or 0), or the
+// default (all zeros) for FP64 grids without CLOSURE faces.
+bool use_pencil(const ws_grid* g, ws_tile tile);
 
 // Launch the fused RHS for one grid; cfg indexes the compiled tile shapes.
 // krk == 0: write du; krk in 1..3: fused SSP-RK3 stage epilogue (Cartesian).
