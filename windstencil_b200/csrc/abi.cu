@@ -245,7 +245,7 @@ bool use_pencil(const ws_grid* g, ws_tile tile) {
     if (tile.tile_x || tile.tile_y || tile.threads) return false;
     for (int i = 0; i < 4; ++i)
         if (g->face_kind[i] == WS_FACE_CLOSURE) return false;
-    return g->precision == WS_FP64;
+    return true;
 }
 
 namespace {

@@ -167,6 +167,147 @@ __global__ void __launch_bounds__(WPB * 32, 1)
     }
 }
 
+// The x pass of the mixed form, cooperative: the lanes still own 32 lines
+// (consecutive y) and reconstruct their own faces, but the loads and splits
+// of the next 4 points of all 32 lines, and the stores of 4 points of du,
+// are done by the warp together, lane (xi, yi) = (lane % 4, lane / 4) taking
+// point xi of lines yi, yi+8, yi+16, yi+24.  Each global access then covers
+// 8 lines x 4 consecutive x instead of 32 lines x 1 x: a quarter of the L1
+// transactions, which bound the per-lane form (the split is then written
+// into the owning lane's ring column, hence a 12-slot ring: the 8-point
+// stencils of a chunk of 4 faces span 11 points).  The FP64 passes are
+// compute-bound and keep the per-lane form.
+template <typename CT>
+struct PencilXLayout {
+    static constexpr int C = 4;                   // points per chunk
+    static constexpr int SLOTS = 12;
+    static constexpr int RS = 10 * 32;
+    static constexpr int RING = SLOTS * RS;       // CT
+    static constexpr int DUS = 5 * C * 32;        // du staging, doubles
+    static constexpr size_t WARP_BYTES = RING * sizeof(CT) + DUS * sizeof(double);
+};
+
+template <int WPB, typename CT, bool UNI, int MODE>
+__global__ void __launch_bounds__(WPB * 32, 1)
+    pencil_x_coop_kernel(const __grid_constant__ RhsArgs a) {
+    static_assert(MODE != P_STAGE, "the x pass never applies the stage");
+    constexpr bool ADD = MODE == P_ADD;
+    using P = PencilXLayout<CT>;
+    constexpr int C = P::C, NS = P::SLOTS;
+    extern __shared__ __align__(16) unsigned char pencil_smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned char* wbase = pencil_smem + warp * P::WARP_BYTES;
+    CT* ringw = reinterpret_cast<CT*>(wbase);                       // [12][10][32]
+    double* dus = reinterpret_cast<double*>(wbase + P::RING * sizeof(CT));   // [5][C][32]
+    CT* ring = ringw + lane;                                        // this lane's column
+    const SplitK<CT> k = {CT(a.eps2), CT(a.hrg), CT(a.c1), CT(a.c3), CT(a.gm1)};
+    const int nxj = a.ex - a.sx, nyj = a.ey - a.sy, nzj = a.ez - a.sz;
+    const int L = nxj, mlast = a.nx + 7;
+    const size_t vs = (size_t)a.du_pitch * a.du_ly * a.du_lz;
+    const long NL = (long)nyj * nzj, NG = (NL + 31) / 32, total = NG * L;
+    const long S = (long)gridDim.x * WPB, s = (long)blockIdx.x * WPB + warp;
+    const int xi = lane & 3, yi = lane >> 2;
+    long pos = total * s / S;
+    const long end = total * (s + 1) / S;
+    while (pos < end) {
+        const long grp = pos / L;
+        const int p0 = (int)(pos - grp * L);
+        const int len = (int)min((long)(L - p0), end - pos);
+        pos += len;
+        // this lane's own line, and the four lines it loads / stores for
+        const long lo = min(grp * 32 + lane, NL - 1);
+        const bool valid = grp * 32 + lane < NL;
+        const int oy = a.sy + (int)(lo % nyj), oz = a.sz + (int)(lo / nyj);
+        int cy[4], cz[4];
+        bool cv[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const long l = grp * 32 + yi + 8 * r;
+            cv[r] = l < NL;
+            const long lc = min(l, NL - 1);
+            cy[r] = a.sy + (int)(lc % nyj);
+            cz[r] = a.sz + (int)(lc / nyj);
+        }
+        // primitives of point x0 + xi of the four lines (x clamped), and their
+        // splits into the owning lanes' ring columns (only xi < cnt)
+        auto coop_load = [&](int x0, double q[4][5]) {
+            const int x = min(x0 + xi, mlast);
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int f = 0; f < 5; ++f) q[r][f] = ldg_prim(a, f, x, cy[r], cz[r]);
+        };
+        auto coop_split = [&](int x0, int cnt, const double q[4][5]) {
+            if (xi >= cnt) return;
+            const int x = x0 + xi;
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                CT out[10];
+                split_point<0, UNI, CT>(a, k, q[r][0], q[r][1], q[r][2], q[r][3], q[r][4], x,
+                                        cy[r], cz[r], out);
+                CT* dst = ringw + (x % NS) * P::RS + yi + 8 * r;
+#pragma unroll
+                for (int c = 0; c < 10; ++c) dst[c * 32] = out[c];
+            }
+        };
+        const int ms = a.sx + p0;
+        double qb[4][5];
+        coop_load(ms - 4, qb);
+        coop_split(ms - 4, 4, qb);
+        coop_load(ms, qb);
+        coop_split(ms, 4, qb);
+        coop_load(ms + 4, qb);              // the first chunk's new points
+        __syncwarp();
+        double fprev[5];
+        {
+            const int s0 = (ms - 4) % NS;
+#pragma unroll
+            for (int v = 0; v < 5; ++v)
+                fprev[v] = face_flux<CT, true>(ring + s0 * P::RS + v * 32, 5 * 32, P::RS,
+                                               NS - s0, NS * P::RS);
+        }
+        for (int mc = ms; mc < ms + len; mc += C) {
+            const int cnt = min(C, ms + len - mc);
+            coop_split(mc + 4, cnt, qb);     // points mc+4 .. (slots of mc-8 ..: dead)
+            __syncwarp();
+            if (mc + C < ms + len) coop_load(mc + C + 4, qb);
+            // faces of this lane's line, steps mc .. mc+cnt-1, into the staging
+            for (int i = 0; i < cnt; ++i) {
+                const int m = mc + i;
+                const int s0 = (m - 3) % NS;
+                const double J = UNI ? 1.0 : ldg_met(a, 9, m, oy, oz);
+#pragma unroll
+                for (int v = 0; v < 5; ++v) {
+                    const double fc = face_flux<CT, true>(ring + s0 * P::RS + v * 32, 5 * 32,
+                                                          P::RS, NS - s0, NS * P::RS);
+                    dus[(v * C + i) * 32 + lane] = -J * ((fc - fprev[v]) * a.rhx);
+                    fprev[v] = fc;
+                }
+            }
+            __syncwarp();
+            // du of the chunk: point mc + xi of lines yi + 8r
+            if (xi < cnt) {
+                const int x = mc + xi;
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    if (!cv[r]) continue;
+                    const size_t o = (size_t)(x - a.sx) +
+                                     (size_t)a.du_pitch * ((size_t)(cy[r] - a.sy) +
+                                                           (size_t)a.du_ly * (size_t)(cz[r] - a.sz));
+#pragma unroll
+                    for (int v = 0; v < 5; ++v) {
+                        const double r_ = dus[(v * C + xi) * 32 + yi + 8 * r];
+                        double* p = a.du + o + v * vs;
+                        *p = ADD ? *p + r_ : r_;
+                    }
+                }
+            }
+            (void)valid;
+        }
+        __syncwarp();
+    }
+}
+
 template <int WPB, typename CT, bool UNI>
 struct PencilLauncher {
     static size_t smem() { return (size_t)WPB * PencilLayout<CT>::WARP * sizeof(CT); }
@@ -188,18 +329,49 @@ struct PencilLauncher {
         WS_CUDA(cudaGetLastError());
         return WS_OK;
     }
+    // the mixed form's x pass: the cooperative kernel, 8 warps per CTA
+    template <int MODE>
+    static int xcoop(const RhsArgs& a, cudaStream_t st) {
+        constexpr int XW = 8;
+        const size_t bytes = XW * PencilXLayout<CT>::WARP_BYTES;
+        auto kern = pencil_x_coop_kernel<XW, CT, UNI, MODE>;
+        static int blocks[64] = {0};
+        int dev = 0;
+        WS_CUDA(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= 64) return fail(WS_ERR_UNSUPPORTED, "device ordinal >= 64");
+        if (!blocks[dev]) {
+            int sms = 0;
+            WS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            WS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)bytes));
+            blocks[dev] = sms;
+        }
+        kern<<<blocks[dev], XW * 32, bytes, st>>>(a);
+        WS_CUDA(cudaGetLastError());
+        return WS_OK;
+    }
+    static int xpass(const RhsArgs& a, bool add_x, cudaStream_t st) {
+        if constexpr (sizeof(CT) == 4)
+            return add_x ? xcoop<P_ADD>(a, st) : xcoop<P_STORE>(a, st);
+        else
+            return add_x ? one<0, P_ADD>(a, 0, st) : one<0, P_STORE>(a, 0, st);
+    }
     // plain RHS: x (=, or += with add_x), y (+=), z (+=)
     static int rhs(const RhsArgs& a, bool add_x, cudaStream_t st) {
-        int rc = add_x ? one<0, P_ADD>(a, 0, st) : one<0, P_STORE>(a, 0, st);
+        int rc = xpass(a, add_x, st);
         if (rc || (rc = one<1, P_ADD>(a, 0, st))) return rc;
         return one<2, P_ADD>(a, 0, st);
     }
-    // stage: x, y into du, then z with the stage update
+    // stage: x, y into du, then z with the stage update (the mixed form's
+    // stage pass holds more operands than 16 warps' 128 registers: 12 warps)
     static int stage(const RhsArgs& a, bool add_x, int krk, cudaStream_t st) {
         if constexpr (UNI) {
-            int rc = add_x ? one<0, P_ADD>(a, 0, st) : one<0, P_STORE>(a, 0, st);
+            int rc = xpass(a, add_x, st);
             if (rc || (rc = one<1, P_ADD>(a, 0, st))) return rc;
-            return one<2, P_STAGE>(a, krk, st);
+            if constexpr (sizeof(CT) == 4 && WPB > 12)
+                return PencilLauncher<12, CT, UNI>::template one<2, P_STAGE>(a, krk, st);
+            else
+                return one<2, P_STAGE>(a, krk, st);
         } else {
             return fail(WS_ERR_UNSUPPORTED, "stage update needs Cartesian metrics");
         }

@@ -138,7 +138,7 @@ int launch_rhs_pencil(const RhsArgs& a, int precision, bool uniform, int wpb, in
                       bool add_x, cudaStream_t st);
 // Whether a launch with tile selection `tile` runs the line passes: an
 // explicit request (tile_x < 0, threads = 32 x warps per CTA or 0), or the
-// default (all zeros) for FP64 grids without CLOSURE faces.
+// default (all zeros) for grids without CLOSURE faces.
 bool use_pencil(const ws_grid* g, ws_tile tile);
 
 // Launch the fused RHS for one grid; cfg indexes the compiled tile shapes.
