@@ -307,7 +307,8 @@ WS_API void ws_solver_destroy(ws_solver* s);
 WS_API int  ws_solver_set_state(ws_solver* s, const double* f_host, ws_stream_t stream);
 /* Downloads the conserved state; synchronises `stream`. */
 WS_API int  ws_solver_get_state(ws_solver* s, double* f_host, ws_stream_t stream);
-/* Downloads du of the last ws_solver_rhs(); synchronises `stream`. */
+/* Downloads du of the last ws_solver_rhs() (a step uses du as its
+ * accumulator, so read it before stepping); synchronises `stream`. */
 WS_API int  ws_solver_get_rhs(ws_solver* s, double* du_host, ws_stream_t stream);
 /* Device descriptors of the state (f, du SoA; d,u,v,w,T,cc LAP). */
 WS_API int  ws_solver_fields(ws_solver* s, ws_soa* f, ws_soa* du, ws_field prims[6]);
@@ -378,6 +379,8 @@ WS_API int  ws_batch_size(ws_batch* b);
 /* dense conserved state [5][nz][ny][nx] of grid i */
 WS_API int  ws_batch_set_state(ws_batch* b, int i, const double* f_host, ws_stream_t stream);
 WS_API int  ws_batch_get_state(ws_batch* b, int i, double* f_host, ws_stream_t stream);
+/* du of grid i after the last ws_batch_rhs() (a step overwrites it, as for
+ * the solver); synchronises `stream`. */
 WS_API int  ws_batch_get_rhs(ws_batch* b, int i, double* du_host, ws_stream_t stream);
 /* CFL time step of every grid (dt_out[n]); synchronises `stream` */
 WS_API int  ws_batch_compute_dt(ws_batch* b, double cfl, double* dt_out, ws_stream_t stream);

@@ -334,6 +334,7 @@ class Solver:
         return out
 
     def get_rhs(self, stream=None):
+        """du of the last rhs() (a step uses du as scratch: read it first)."""
         import numpy as np
         out = np.empty((5, self.g.nz, self.g.ny, self.g.nx))
         check(load().ws_solver_get_rhs(self.h, out.ctypes.data, _stream(stream)))
@@ -447,6 +448,7 @@ class Batch:
         return out
 
     def get_rhs(self, i, stream=None):
+        """du of grid i after the last rhs() (a step overwrites it)."""
         import numpy as np
         g = self.grids[i]
         out = np.empty((5, g.nz, g.ny, g.nx))

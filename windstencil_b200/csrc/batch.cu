@@ -176,9 +176,24 @@ void BatchRunner::release(cudaStream_t st) {
     grids_.clear();
 }
 
+int batch_kernel_cfg(const std::vector<GridState*>& grids, ws_tile tile) {
+    if (tile.tile_x < 0) return -1;
+    const int prec = grids.empty() ? WS_FP64 : grids[0]->g.precision;
+    if (tile.tile_x || tile.tile_y || tile.threads) {
+        const int c = find_tile_cfg(tile.tile_x, tile.tile_y, tile.threads);
+        return c < 0 ? -2 : c;
+    }
+    for (auto* s : grids)
+        for (int i = 0; i < 4; ++i)
+            if (s->g.face_kind[i] == WS_FACE_CLOSURE) return default_cfg(prec, true);
+    return -1;
+}
+
 int BatchRunner::build(const std::vector<GridState*>& grids, int cfg, int zc, cudaStream_t st) {
     drop_graphs();
     grids_ = grids;
+    pencil_ = cfg < 0;
+    if (pencil_) cfg = 0;       // argument tables as for tile 0 (its fields unused)
     cfg_ = cfg;
     zc_ = zc > 0 ? zc : (1 << 30);
     parity_ = 0;
@@ -227,12 +242,20 @@ int BatchRunner::build(const std::vector<GridState*>& grids, int cfg, int zc, cu
         o = align256(o + n * gsz);
     }
     const size_t o_gt = o;
-    const size_t bytes = align256(o_gt + n_gtab * sizeof(int2));
+    o = align256(o_gt + n_gtab * sizeof(int2));
+    const size_t o_woff = o;           // line passes: 3 x (n + 1) work prefixes
+    const size_t bytes = align256(o_woff + 3 * (size_t)(n + 1) * sizeof(long));
     host_.assign(bytes, 0);
     unsigned char* h = host_.data();
     if (!items.empty())
         std::memcpy(h + o_items, items.data(), items.size() * sizeof(int4));
     int2* hgt = reinterpret_cast<int2*>(h + o_gt);
+    long* hw = reinterpret_cast<long*>(h + o_woff);
+    for (int dir = 0; dir < 3; ++dir) {
+        long* w = hw + dir * (n + 1);
+        w[0] = 0;
+        for (int i = 0; i < n; ++i) w[i + 1] = w[i] + pencil_pass_work(grids[i]->g, dir);
+    }
     long gi = 0;
     for (int i = 0; i < n; ++i) {
         GridState* s = grids[i];
@@ -277,6 +300,7 @@ int BatchRunner::build(const std::vector<GridState*>& grids, int cfg, int zc, cu
              reinterpret_cast<unsigned*>(d + o_ctr)};
     for (int k = 0; k < 2; ++k) d_ghost_[k] = d + o_gh[k];
     d_gtab_ = reinterpret_cast<int2*>(d + o_gt);
+    d_woff_ = reinterpret_cast<const long*>(d + o_woff);
     int rc = upload_tables(st);
     if (rc) return rc;
     return WS_OK;
@@ -294,6 +318,9 @@ int BatchRunner::enqueue_rhs(cudaStream_t st) {
     if (grids_.empty()) return WS_OK;
     int rc = launch_ghost_fill_batch(d_ghost_[parity_], d_gtab_, n_gtab_, st);
     if (rc) return rc;
+    if (pencil_)
+        return launch_rhs_pencil_batch(d_rhs_[2 * parity_], d_woff_, (int)grids_.size(),
+                                       precision_, 0, st);
     return launch_rhs_batch(d_rhs_[2 * parity_], work_, precision_, true, closure_, cfg_, ctas_, 0,
                             st);
 }
@@ -304,6 +331,9 @@ int BatchRunner::enqueue_stage1(cudaStream_t st) {
     if (grids_.empty()) return WS_OK;
     int rc = launch_ghost_fill_batch(d_ghost_[parity_], d_gtab_, n_gtab_, st);
     if (rc) return rc;
+    if (pencil_)
+        return launch_rhs_pencil_batch(d_rhs_[2 * parity_], d_woff_, (int)grids_.size(),
+                                       precision_, 1, st);
     return launch_rhs_batch(d_rhs_[2 * parity_], work_, precision_, true, closure_, cfg_, ctas_, 1,
                             st);
 }
@@ -314,8 +344,10 @@ int BatchRunner::enqueue_step(cudaStream_t st) {
         const int two = krk == 2;
         int rc = launch_ghost_fill_batch(d_ghost_[parity_ ^ two], d_gtab_, n_gtab_, st);
         if (rc) return rc;
-        rc = launch_rhs_batch(d_rhs_[2 * parity_ + two], work_, precision_, true, closure_, cfg_,
-                              ctas_, krk, st);
+        rc = pencil_ ? launch_rhs_pencil_batch(d_rhs_[2 * parity_ + two], d_woff_,
+                                               (int)grids_.size(), precision_, krk, st)
+                     : launch_rhs_batch(d_rhs_[2 * parity_ + two], work_, precision_, true,
+                                        closure_, cfg_, ctas_, krk, st);
         if (rc) return rc;
     }
     return WS_OK;
@@ -382,11 +414,8 @@ int batch_ready(ws_batch* b, cudaStream_t st) {
     if (!b->dirty) return WS_OK;
     std::vector<GridState*> ptrs;
     for (auto& s : b->states) ptrs.push_back(&s);
-    int cfg = default_cfg(b->states.empty() ? WS_FP64 : b->states[0].g.precision, true);
-    if (b->tile.tile_x || b->tile.tile_y || b->tile.threads) {
-        cfg = find_tile_cfg(b->tile.tile_x, b->tile.tile_y, b->tile.threads);
-        if (cfg < 0) return fail(WS_ERR_UNSUPPORTED, "tile shape not compiled in this build");
-    }
+    const int cfg = batch_kernel_cfg(ptrs, b->tile);
+    if (cfg == -2) return fail(WS_ERR_UNSUPPORTED, "tile shape not compiled in this build");
     int rc = b->runner.build(ptrs, cfg, b->tile.scan_z, st);
     if (rc == WS_OK) b->dirty = false;
     return rc;
@@ -500,7 +529,7 @@ int ws_batch_set_dt(ws_batch* b, const double* dt) {
 
 int ws_batch_set_tile(ws_batch* b, ws_tile tile) {
     if (!b) return fail(WS_ERR_INVALID, "batch is NULL");
-    if ((tile.tile_x || tile.tile_y || tile.threads) &&
+    if (tile.tile_x >= 0 && (tile.tile_x || tile.tile_y || tile.threads) &&
         find_tile_cfg(tile.tile_x, tile.tile_y, tile.threads) < 0)
         return fail(WS_ERR_UNSUPPORTED, "tile shape not compiled in this build");
     b->tile = tile;
@@ -541,9 +570,11 @@ int ws_batch_status(ws_batch* b, int* status, ws_stream_t stream) {
     return WS_OK;
 }
 
-// Times every compiled tile shape (and two sweep caps) on the first RK stage
-// of this batch (ghost fill + fused RHS and stage update; the current state
-// is left as it was) and keeps the fastest; returns it in *chosen.
+// Times the candidate kernels on the first RK stage of this batch (ghost
+// fill + RHS and stage update; the current state is left as it was) and
+// keeps the fastest; returns its tile selection in *chosen.  Candidates: the
+// line passes (tile_x = -1), unless a grid has CLOSURE faces, and every
+// compiled tile shape of the fused kernel with two sweep caps.
 int ws_batch_autotune(ws_batch* b, ws_tile* chosen, ws_stream_t stream) {
     if (!b) return fail(WS_ERR_INVALID, "batch is NULL");
     cudaStream_t st = (cudaStream_t)stream;
@@ -552,30 +583,37 @@ int ws_batch_autotune(ws_batch* b, ws_tile* chosen, ws_stream_t stream) {
     WS_CUDA(cudaEventCreate(&e1));
     float best = 1e30f;
     ws_tile best_tile{0, 0, 0, 0};
-    const int caps[2] = {0, 32};
+    std::vector<ws_tile> cand;
+    bool closure = false;
+    for (auto& s : b->states)
+        for (int i = 0; i < 4; ++i) closure |= s.g.face_kind[i] == WS_FACE_CLOSURE;
+    if (!closure) cand.push_back(ws_tile{-1, 0, 0, 0});
     for (int c = 0; c < num_tile_cfgs(); ++c)
-        for (int cap : caps) {
+        for (int cap : {0, 32}) {
             const TileCfg tc = tile_cfg(c);
-            b->tile = ws_tile{tc.bx, tc.by, cap, tc.threads};
-            b->dirty = true;
-            int rc = batch_ready(b, st);
-            if (rc == WS_OK) rc = b->runner.enqueue_stage1(st);    // warm-up
-            if (rc) {
-                cudaEventDestroy(e0);
-                cudaEventDestroy(e1);
-                return rc;
-            }
-            cudaEventRecord(e0, st);
-            for (int r = 0; r < 2; ++r) b->runner.enqueue_stage1(st);
-            cudaEventRecord(e1, st);
-            WS_CUDA(cudaEventSynchronize(e1));
-            float ms = 0;
-            cudaEventElapsedTime(&ms, e0, e1);
-            if (ms < best) {
-                best = ms;
-                best_tile = b->tile;
-            }
+            cand.push_back(ws_tile{tc.bx, tc.by, cap, tc.threads});
         }
+    for (const ws_tile& t : cand) {
+        b->tile = t;
+        b->dirty = true;
+        int rc = batch_ready(b, st);
+        if (rc == WS_OK) rc = b->runner.enqueue_stage1(st);    // warm-up
+        if (rc) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return rc;
+        }
+        cudaEventRecord(e0, st);
+        for (int r = 0; r < 2; ++r) b->runner.enqueue_stage1(st);
+        cudaEventRecord(e1, st);
+        WS_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) {
+            best = ms;
+            best_tile = b->tile;
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     b->tile = best_tile;

@@ -22,4 +22,20 @@ int launch_rhs_pencil(const RhsArgs& a, int precision, bool uniform, int wpb, in
                    : PencilLauncher<8, double, false>::rhs(a, add_x, st);
 }
 
+// the batched form over the argument table g of n Cartesian grids (woff: the
+// x, y, z passes' work prefix tables, n + 1 entries each)
+int launch_rhs_pencil_batch(const RhsArgs* g, const long* woff, int n, int precision, int krk,
+                            cudaStream_t st) {
+    if (precision == WS_MIXED) return PencilLauncher<12, float, true>::batch(g, woff, n, krk, st);
+    return PencilLauncher<8, double, true>::batch(g, woff, n, krk, st);
+}
+
+// work of pass dir over the interior of grid g: line groups x march length
+long pencil_pass_work(const ws_grid& g, int dir) {
+    const long nx = g.nx, ny = g.ny, nz = g.nz;
+    const long nl = dir == 0 ? ny * nz : (dir == 1 ? nx * nz : nx * ny);
+    const long L = dir == 0 ? nx : (dir == 1 ? ny : nz);
+    return (nl + 31) / 32 * L;
+}
+
 }  // namespace ws

@@ -36,27 +36,147 @@ struct PencilLayout {
 
 enum PencilMode { P_STORE = 0, P_ADD = 1, P_STAGE = 2 };
 
-// One pass along DIR (0 x, 1 y, 2 z) over the job of `a`.
-template <int DIR, int WPB, typename CT, bool UNI, int MODE>
-__global__ void __launch_bounds__(WPB * 32, 1)
-    pencil_rhs_kernel(const __grid_constant__ RhsArgs a, int krk) {
+// March length, first LAP position and line count of pass DIR over the job
+// of `a`; the pass's work is its line groups (32 lines) x positions.
+template <int DIR>
+__device__ __forceinline__ long pencil_work(const RhsArgs& a, int& L) {
+    const int nxj = a.ex - a.sx, nyj = a.ey - a.sy, nzj = a.ez - a.sz;
+    L = DIR == 0 ? nxj : (DIR == 1 ? nyj : nzj);
+    const long NL = DIR == 0 ? (long)nyj * nzj : (DIR == 1 ? (long)nxj * nzj : (long)nxj * nyj);
+    return (NL + 31) / 32 * L;
+}
+
+// One segment of pass DIR (0 x, 1 y, 2 z): positions p0 .. p0+len-1 of the
+// lines of group grp of the job of `a`, this lane's line marched with the
+// lane's ring column `ring`.
+template <int DIR, typename CT, bool UNI, int MODE>
+__device__ __forceinline__ void pencil_segment(const RhsArgs& a, int krk, CT* ring, long grp,
+                                               int p0, int len) {
     static_assert(MODE != P_STAGE || (DIR == 2 && UNI), "stage update: z pass, Cartesian");
     constexpr bool ADD = MODE != P_STORE;
     using P = PencilLayout<CT>;
-    extern __shared__ __align__(16) unsigned char pencil_smem[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    CT* ring = reinterpret_cast<CT*>(pencil_smem) + warp * P::WARP + lane;
+    const int lane = threadIdx.x & 31;
     const SplitK<CT> k = {CT(a.eps2), CT(a.hrg), CT(a.c1), CT(a.c3), CT(a.gm1)};
     const int nxj = a.ex - a.sx, nyj = a.ey - a.sy, nzj = a.ez - a.sz;
     const int n1 = DIR == 0 ? nyj : nxj;              // fastest line axis
-    const int n2 = DIR == 2 ? nyj : nzj;
-    const int L = DIR == 0 ? nxj : (DIR == 1 ? nyj : nzj);
+    const long NL = (long)n1 * (DIR == 2 ? nyj : nzj);
     const int m0 = DIR == 0 ? a.sx : (DIR == 1 ? a.sy : a.sz);
     const int mlast = (DIR == 0 ? a.nx : (DIR == 1 ? a.ny : a.nz)) + 7;   // last LAP index
     const double rh = DIR == 0 ? a.rhx : (DIR == 1 ? a.rhy : a.rhz);
     const size_t vs = (size_t)a.du_pitch * a.du_ly * a.du_lz;            // du variable stride
     const size_t fvs = MODE == P_STAGE ? (size_t)a.fn.pitch * a.fn.length_Y * a.fn.length_Z : 0;
-    const long NL = (long)n1 * n2, NG = (NL + 31) / 32, total = NG * L;
+    long l = grp * 32 + lane;
+    const bool valid = l < NL;
+    if (!valid) l = NL - 1;
+    const int c1 = (int)(l % n1), c2 = (int)(l / n1);
+    // LAP coordinates of march position m on this lane's line
+    auto X = [&](int m) { return DIR == 0 ? m : a.sx + c1; };
+    auto Y = [&](int m) { return DIR == 1 ? m : (DIR == 0 ? a.sy + c1 : a.sy + c2); };
+    auto Z = [&](int m) { return DIR == 2 ? m : a.sz + c2; };
+    auto load = [&](int m, double q[5]) {
+        const int x = X(m), y = Y(m), z = Z(m);
+#pragma unroll
+        for (int f = 0; f < 5; ++f) q[f] = ldg_prim(a, f, x, y, z);
+    };
+    auto split_into = [&](int m, const double q[5]) {
+        const int x = X(m), y = Y(m), z = Z(m);
+        CT out[10];
+        split_point<DIR, UNI, CT>(a, k, q[0], q[1], q[2], q[3], q[4], x, y, z, out);
+        CT* dst = ring + (m & 7) * P::RS;
+#pragma unroll
+        for (int c = 0; c < 10; ++c) dst[c * 32] = out[c];
+    };
+    // du offset of march position m (job-relative); in stage mode the
+    // conserved state has du's shape, offset by the interior origin
+    auto du_at = [&](int m) {
+        return (size_t)(X(m) - a.sx) +
+               (size_t)a.du_pitch * ((size_t)(Y(m) - a.sy) + (size_t)a.du_ly * (size_t)(Z(m) - a.sz));
+    };
+    auto f_at = [&](int m) { return soa_index(a.fn, X(m) - 4, Y(m) - 4, Z(m) - 4, 0); };
+
+    const int ms = m0 + p0;
+    for (int m = ms - 4; m < ms + 4; ++m) {
+        double q[5];
+        load(m, q);
+        split_into(m, q);
+    }
+    double qn[5], dn[5], fnn[5], fin[5];
+    load(ms + 4, qn);
+    auto load_cell = [&](int m) {      // du (and the stage operands) of point m
+        if (ADD) {
+            const size_t o = du_at(m);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) dn[v] = a.du[o + v * vs];
+        }
+        if (MODE == P_STAGE) {
+            const size_t o = f_at(m);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+                fnn[v] = __ldg(a.fn.ptr + o + v * fvs);
+                fin[v] = krk == 1 ? 0.0 : a.f_in.ptr[o + v * fvs];
+            }
+        }
+    };
+    if (valid) load_cell(ms);
+    double fprev[5];
+    {
+        const int s0 = (ms - 4) & 7;
+#pragma unroll
+        for (int v = 0; v < 5; ++v)
+            fprev[v] = face_flux<CT, true>(ring + s0 * P::RS + v * 32, 5 * 32, P::RS, 8 - s0,
+                                           8 * P::RS);
+    }
+    for (int m = ms; m < ms + len; ++m) {
+        double q[5], dc[5], fnc[5], fic[5];
+#pragma unroll
+        for (int f = 0; f < 5; ++f) {
+            q[f] = qn[f];
+            dc[f] = dn[f];
+            fnc[f] = fnn[f];
+            fic[f] = fin[f];
+        }
+        load(min(m + 5, mlast), qn);
+        if (valid && m + 1 < ms + len) load_cell(m + 1);
+        split_into(m + 4, q);
+        const int s0 = (m - 3) & 7;
+        const double J = UNI ? 1.0 : ldg_met(a, 9, X(m), Y(m), Z(m));
+        double r[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            const double fc = face_flux<CT, true>(ring + s0 * P::RS + v * 32, 5 * 32, P::RS,
+                                                  8 - s0, 8 * P::RS);
+            r[v] = -J * ((fc - fprev[v]) * rh);
+            fprev[v] = fc;
+        }
+        if (!valid) continue;
+        if (MODE == P_STAGE) {
+            const size_t o = f_at(m);
+            double qs[5];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+                qs[v] = ws_rk_stage(krk, fnc[v], fic[v], dc[v] + r[v], a.dt);
+                a.f_out.ptr[o + v * fvs] = qs[v];
+            }
+            store_prims(a, qs, X(m), Y(m), Z(m));
+        } else {
+            const size_t o = du_at(m);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) a.du[o + v * vs] = ADD ? dc[v] + r[v] : r[v];
+        }
+    }
+}
+
+// One pass along DIR over the job of `a`: every warp takes an equal
+// contiguous share of the (line group, position) space.
+template <int DIR, int WPB, typename CT, bool UNI, int MODE>
+__global__ void __launch_bounds__(WPB * 32, 1)
+    pencil_rhs_kernel(const __grid_constant__ RhsArgs a, int krk) {
+    using P = PencilLayout<CT>;
+    extern __shared__ __align__(16) unsigned char pencil_smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    CT* ring = reinterpret_cast<CT*>(pencil_smem) + warp * P::WARP + lane;
+    int L = 0;
+    const long total = pencil_work<DIR>(a, L);
     const long S = (long)gridDim.x * WPB, s = (long)blockIdx.x * WPB + warp;
     long pos = total * s / S;
     const long end = total * (s + 1) / S;
@@ -64,106 +184,43 @@ __global__ void __launch_bounds__(WPB * 32, 1)
         const long grp = pos / L;
         const int p0 = (int)(pos - grp * L);
         const int len = (int)min((long)(L - p0), end - pos);
+        pencil_segment<DIR, CT, UNI, MODE>(a, krk, ring, grp, p0, len);
         pos += len;
-        long l = grp * 32 + lane;
-        const bool valid = l < NL;
-        if (!valid) l = NL - 1;
-        const int c1 = (int)(l % n1), c2 = (int)(l / n1);
-        // LAP coordinates of march position m on this lane's line
-        auto X = [&](int m) { return DIR == 0 ? m : a.sx + c1; };
-        auto Y = [&](int m) { return DIR == 1 ? m : (DIR == 0 ? a.sy + c1 : a.sy + c2); };
-        auto Z = [&](int m) { return DIR == 2 ? m : a.sz + c2; };
-        auto load = [&](int m, double q[5]) {
-            const int x = X(m), y = Y(m), z = Z(m);
-#pragma unroll
-            for (int f = 0; f < 5; ++f) q[f] = ldg_prim(a, f, x, y, z);
-        };
-        auto split_into = [&](int m, const double q[5]) {
-            const int x = X(m), y = Y(m), z = Z(m);
-            CT out[10];
-            split_point<DIR, UNI, CT>(a, k, q[0], q[1], q[2], q[3], q[4], x, y, z, out);
-            CT* dst = ring + (m & 7) * P::RS;
-#pragma unroll
-            for (int c = 0; c < 10; ++c) dst[c * 32] = out[c];
-        };
-        // du offset of march position m (job-relative); in stage mode the
-        // conserved state has du's shape, offset by the interior origin
-        auto du_at = [&](int m) {
-            return (size_t)(X(m) - a.sx) +
-                   (size_t)a.du_pitch * ((size_t)(Y(m) - a.sy) + (size_t)a.du_ly * (size_t)(Z(m) - a.sz));
-        };
-        auto f_at = [&](int m) { return soa_index(a.fn, X(m) - 4, Y(m) - 4, Z(m) - 4, 0); };
+    }
+}
 
-        const int ms = m0 + p0;
-        for (int m = ms - 4; m < ms + 4; ++m) {
-            double q[5];
-            load(m, q);
-            split_into(m, q);
-        }
-        double qn[5], dn[5], fnn[5], fin[5];
-        load(ms + 4, qn);
-        auto load_cell = [&](int m) {      // du (and the stage operands) of point m
-            if (ADD) {
-                const size_t o = du_at(m);
-#pragma unroll
-                for (int v = 0; v < 5; ++v) dn[v] = a.du[o + v * vs];
-            }
-            if (MODE == P_STAGE) {
-                const size_t o = f_at(m);
-#pragma unroll
-                for (int v = 0; v < 5; ++v) {
-                    fnn[v] = __ldg(a.fn.ptr + o + v * fvs);
-                    fin[v] = krk == 1 ? 0.0 : a.f_in.ptr[o + v * fvs];
-                }
-            }
-        };
-        if (valid) load_cell(ms);
-        double fprev[5];
-        {
-            const int s0 = (ms - 4) & 7;
-#pragma unroll
-            for (int v = 0; v < 5; ++v)
-                fprev[v] = face_flux<CT, true>(ring + s0 * P::RS + v * 32, 5 * 32, P::RS, 8 - s0,
-                                               8 * P::RS);
-        }
-        for (int m = ms; m < ms + len; ++m) {
-            double q[5], dc[5], fnc[5], fic[5];
-#pragma unroll
-            for (int f = 0; f < 5; ++f) {
-                q[f] = qn[f];
-                dc[f] = dn[f];
-                fnc[f] = fnn[f];
-                fic[f] = fin[f];
-            }
-            load(min(m + 5, mlast), qn);
-            if (valid && m + 1 < ms + len) load_cell(m + 1);
-            split_into(m + 4, q);
-            const int s0 = (m - 3) & 7;
-            const double J = UNI ? 1.0 : ldg_met(a, 9, X(m), Y(m), Z(m));
-            double r[5];
-#pragma unroll
-            for (int v = 0; v < 5; ++v) {
-                const double fc = face_flux<CT, true>(ring + s0 * P::RS + v * 32, 5 * 32, P::RS,
-                                                      8 - s0, 8 * P::RS);
-                r[v] = -J * ((fc - fprev[v]) * rh);
-                fprev[v] = fc;
-            }
-            if (!valid) continue;
-            if (MODE == P_STAGE) {
-                const size_t o = f_at(m);
-                double qs[5];
-#pragma unroll
-                for (int v = 0; v < 5; ++v) {
-                    qs[v] = ws_rk_stage(krk, fnc[v], fic[v], dc[v] + r[v], a.dt);
-                    a.f_out.ptr[o + v * fvs] = qs[v];
-                }
-                store_prims(a, qs, X(m), Y(m), Z(m));
-            } else {
-                const size_t o = du_at(m);
-#pragma unroll
-                for (int v = 0; v < 5; ++v) a.du[o + v * vs] = ADD ? dc[v] + r[v] : r[v];
-            }
-        }
+// The same pass over the grids of a batch: argument table `grids`, and
+// woff[i] the pass's work before grid i (woff[n] the total).  A warp's share
+// may cross grids.
+template <int DIR, int WPB, typename CT, int MODE>
+__global__ void __launch_bounds__(WPB * 32, 1)
+    pencil_batch_kernel(const RhsArgs* __restrict__ grids, const long* __restrict__ woff, int n,
+                        int krk) {
+    using P = PencilLayout<CT>;
+    extern __shared__ __align__(16) unsigned char pencil_smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    CT* ring = reinterpret_cast<CT*>(pencil_smem) + warp * P::WARP + lane;
+    const long total = woff[n];
+    const long S = (long)gridDim.x * WPB, s = (long)blockIdx.x * WPB + warp;
+    long pos = total * s / S;
+    const long end = total * (s + 1) / S;
+    int lo = 0, hi = n;                    // the grid holding pos: woff[i] <= pos < woff[i+1]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (woff[mid] <= pos) lo = mid; else hi = mid;
+    }
+    int i = lo;
+    while (pos < end) {
+        while (woff[i + 1] <= pos) ++i;
+        const RhsArgs& a = grids[i];
+        int L = 0;
+        pencil_work<DIR>(a, L);
+        const long local = pos - woff[i];
+        const long grp = local / L;
+        const int p0 = (int)(local - grp * L);
+        const int len = (int)min((long)(L - p0), end - pos);
+        pencil_segment<DIR, CT, true, MODE>(a, krk, ring, grp, p0, len);
+        pos += len;
     }
 }
 
@@ -187,168 +244,212 @@ struct PencilXLayout {
     static constexpr size_t WARP_BYTES = RING * sizeof(CT) + DUS * sizeof(double);
 };
 
-template <int WPB, typename CT, bool UNI, int MODE>
-__global__ void __launch_bounds__(WPB * 32, 1)
-    pencil_x_coop_kernel(const __grid_constant__ RhsArgs a) {
+// One segment of the cooperative x pass (positions p0 .. p0+len-1 of the 32
+// lines of group grp); wbase: the warp's ring and du staging.
+template <typename CT, bool UNI, int MODE>
+__device__ __forceinline__ void pencil_x_segment(const RhsArgs& a, unsigned char* wbase,
+                                                 long grp, int p0, int len) {
     static_assert(MODE != P_STAGE, "the x pass never applies the stage");
     constexpr bool ADD = MODE == P_ADD;
     using P = PencilXLayout<CT>;
     constexpr int C = P::C, NS = P::SLOTS;
-    extern __shared__ __align__(16) unsigned char pencil_smem[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    unsigned char* wbase = pencil_smem + warp * P::WARP_BYTES;
+    const int lane = threadIdx.x & 31;
     CT* ringw = reinterpret_cast<CT*>(wbase);                       // [12][10][32]
     double* dus = reinterpret_cast<double*>(wbase + P::RING * sizeof(CT));   // [5][C][32]
     CT* ring = ringw + lane;                                        // this lane's column
     const SplitK<CT> k = {CT(a.eps2), CT(a.hrg), CT(a.c1), CT(a.c3), CT(a.gm1)};
-    const int nxj = a.ex - a.sx, nyj = a.ey - a.sy, nzj = a.ez - a.sz;
-    const int L = nxj, mlast = a.nx + 7;
+    const int nyj = a.ey - a.sy, nzj = a.ez - a.sz;
+    const int mlast = a.nx + 7;
     const size_t vs = (size_t)a.du_pitch * a.du_ly * a.du_lz;
-    const long NL = (long)nyj * nzj, NG = (NL + 31) / 32, total = NG * L;
-    const long S = (long)gridDim.x * WPB, s = (long)blockIdx.x * WPB + warp;
+    const long NL = (long)nyj * nzj;
     const int xi = lane & 3, yi = lane >> 2;
+    // this lane's own line, and the four lines it loads / stores for
+    const long lo = min(grp * 32 + lane, NL - 1);
+    const bool valid = grp * 32 + lane < NL;
+    const int oy = a.sy + (int)(lo % nyj), oz = a.sz + (int)(lo / nyj);
+    int cy[4], cz[4];
+    bool cv[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const long l = grp * 32 + yi + 8 * r;
+        cv[r] = l < NL;
+        const long lc = min(l, NL - 1);
+        cy[r] = a.sy + (int)(lc % nyj);
+        cz[r] = a.sz + (int)(lc / nyj);
+    }
+    // primitives of point x0 + xi of the four lines (x clamped), and their
+    // splits into the owning lanes' ring columns (only xi < cnt)
+    auto coop_load = [&](int x0, double q[4][5]) {
+        const int x = min(x0 + xi, mlast);
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int f = 0; f < 5; ++f) q[r][f] = ldg_prim(a, f, x, cy[r], cz[r]);
+    };
+    auto coop_split = [&](int x0, int cnt, const double q[4][5]) {
+        if (xi >= cnt) return;
+        const int x = x0 + xi;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            CT out[10];
+            split_point<0, UNI, CT>(a, k, q[r][0], q[r][1], q[r][2], q[r][3], q[r][4], x,
+                                    cy[r], cz[r], out);
+            CT* dst = ringw + (x % NS) * P::RS + yi + 8 * r;
+#pragma unroll
+            for (int c = 0; c < 10; ++c) dst[c * 32] = out[c];
+        }
+    };
+    const int ms = a.sx + p0;
+    double qb[4][5];
+    coop_load(ms - 4, qb);
+    coop_split(ms - 4, 4, qb);
+    coop_load(ms, qb);
+    coop_split(ms, 4, qb);
+    coop_load(ms + 4, qb);              // the first chunk's new points
+    __syncwarp();
+    double fprev[5];
+    {
+        const int s0 = (ms - 4) % NS;
+#pragma unroll
+        for (int v = 0; v < 5; ++v)
+            fprev[v] = face_flux<CT, true>(ring + s0 * P::RS + v * 32, 5 * 32, P::RS,
+                                           NS - s0, NS * P::RS);
+    }
+    for (int mc = ms; mc < ms + len; mc += C) {
+        const int cnt = min(C, ms + len - mc);
+        coop_split(mc + 4, cnt, qb);     // points mc+4 .. (slots of mc-8 ..: dead)
+        __syncwarp();
+        if (mc + C < ms + len) coop_load(mc + C + 4, qb);
+        // faces of this lane's line, steps mc .. mc+cnt-1, into the staging
+        for (int i = 0; i < cnt; ++i) {
+            const int m = mc + i;
+            const int s0 = (m - 3) % NS;
+            const double J = UNI ? 1.0 : ldg_met(a, 9, m, oy, oz);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+                const double fc = face_flux<CT, true>(ring + s0 * P::RS + v * 32, 5 * 32,
+                                                      P::RS, NS - s0, NS * P::RS);
+                dus[(v * C + i) * 32 + lane] = -J * ((fc - fprev[v]) * a.rhx);
+                fprev[v] = fc;
+            }
+        }
+        __syncwarp();
+        // du of the chunk: point mc + xi of lines yi + 8r
+        if (xi < cnt) {
+            const int x = mc + xi;
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                if (!cv[r]) continue;
+                const size_t o = (size_t)(x - a.sx) +
+                                 (size_t)a.du_pitch * ((size_t)(cy[r] - a.sy) +
+                                                       (size_t)a.du_ly * (size_t)(cz[r] - a.sz));
+#pragma unroll
+                for (int v = 0; v < 5; ++v) {
+                    const double r_ = dus[(v * C + xi) * 32 + yi + 8 * r];
+                    double* p = a.du + o + v * vs;
+                    *p = ADD ? *p + r_ : r_;
+                }
+            }
+        }
+        (void)valid;
+    }
+    __syncwarp();
+}
+
+template <int WPB, typename CT, bool UNI, int MODE>
+__global__ void __launch_bounds__(WPB * 32, 1)
+    pencil_x_coop_kernel(const __grid_constant__ RhsArgs a) {
+    extern __shared__ __align__(16) unsigned char pencil_smem[];
+    const int warp = threadIdx.x >> 5;
+    unsigned char* wbase = pencil_smem + warp * PencilXLayout<CT>::WARP_BYTES;
+    int L = 0;
+    const long total = pencil_work<0>(a, L);
+    const long S = (long)gridDim.x * WPB, s = (long)blockIdx.x * WPB + warp;
     long pos = total * s / S;
     const long end = total * (s + 1) / S;
     while (pos < end) {
         const long grp = pos / L;
         const int p0 = (int)(pos - grp * L);
         const int len = (int)min((long)(L - p0), end - pos);
+        pencil_x_segment<CT, UNI, MODE>(a, wbase, grp, p0, len);
         pos += len;
-        // this lane's own line, and the four lines it loads / stores for
-        const long lo = min(grp * 32 + lane, NL - 1);
-        const bool valid = grp * 32 + lane < NL;
-        const int oy = a.sy + (int)(lo % nyj), oz = a.sz + (int)(lo / nyj);
-        int cy[4], cz[4];
-        bool cv[4];
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const long l = grp * 32 + yi + 8 * r;
-            cv[r] = l < NL;
-            const long lc = min(l, NL - 1);
-            cy[r] = a.sy + (int)(lc % nyj);
-            cz[r] = a.sz + (int)(lc / nyj);
-        }
-        // primitives of point x0 + xi of the four lines (x clamped), and their
-        // splits into the owning lanes' ring columns (only xi < cnt)
-        auto coop_load = [&](int x0, double q[4][5]) {
-            const int x = min(x0 + xi, mlast);
-#pragma unroll
-            for (int r = 0; r < 4; ++r)
-#pragma unroll
-                for (int f = 0; f < 5; ++f) q[r][f] = ldg_prim(a, f, x, cy[r], cz[r]);
-        };
-        auto coop_split = [&](int x0, int cnt, const double q[4][5]) {
-            if (xi >= cnt) return;
-            const int x = x0 + xi;
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                CT out[10];
-                split_point<0, UNI, CT>(a, k, q[r][0], q[r][1], q[r][2], q[r][3], q[r][4], x,
-                                        cy[r], cz[r], out);
-                CT* dst = ringw + (x % NS) * P::RS + yi + 8 * r;
-#pragma unroll
-                for (int c = 0; c < 10; ++c) dst[c * 32] = out[c];
-            }
-        };
-        const int ms = a.sx + p0;
-        double qb[4][5];
-        coop_load(ms - 4, qb);
-        coop_split(ms - 4, 4, qb);
-        coop_load(ms, qb);
-        coop_split(ms, 4, qb);
-        coop_load(ms + 4, qb);              // the first chunk's new points
-        __syncwarp();
-        double fprev[5];
-        {
-            const int s0 = (ms - 4) % NS;
-#pragma unroll
-            for (int v = 0; v < 5; ++v)
-                fprev[v] = face_flux<CT, true>(ring + s0 * P::RS + v * 32, 5 * 32, P::RS,
-                                               NS - s0, NS * P::RS);
-        }
-        for (int mc = ms; mc < ms + len; mc += C) {
-            const int cnt = min(C, ms + len - mc);
-            coop_split(mc + 4, cnt, qb);     // points mc+4 .. (slots of mc-8 ..: dead)
-            __syncwarp();
-            if (mc + C < ms + len) coop_load(mc + C + 4, qb);
-            // faces of this lane's line, steps mc .. mc+cnt-1, into the staging
-            for (int i = 0; i < cnt; ++i) {
-                const int m = mc + i;
-                const int s0 = (m - 3) % NS;
-                const double J = UNI ? 1.0 : ldg_met(a, 9, m, oy, oz);
-#pragma unroll
-                for (int v = 0; v < 5; ++v) {
-                    const double fc = face_flux<CT, true>(ring + s0 * P::RS + v * 32, 5 * 32,
-                                                          P::RS, NS - s0, NS * P::RS);
-                    dus[(v * C + i) * 32 + lane] = -J * ((fc - fprev[v]) * a.rhx);
-                    fprev[v] = fc;
-                }
-            }
-            __syncwarp();
-            // du of the chunk: point mc + xi of lines yi + 8r
-            if (xi < cnt) {
-                const int x = mc + xi;
-#pragma unroll
-                for (int r = 0; r < 4; ++r) {
-                    if (!cv[r]) continue;
-                    const size_t o = (size_t)(x - a.sx) +
-                                     (size_t)a.du_pitch * ((size_t)(cy[r] - a.sy) +
-                                                           (size_t)a.du_ly * (size_t)(cz[r] - a.sz));
-#pragma unroll
-                    for (int v = 0; v < 5; ++v) {
-                        const double r_ = dus[(v * C + xi) * 32 + yi + 8 * r];
-                        double* p = a.du + o + v * vs;
-                        *p = ADD ? *p + r_ : r_;
-                    }
-                }
-            }
-            (void)valid;
-        }
-        __syncwarp();
     }
+}
+
+template <int WPB, typename CT, int MODE>
+__global__ void __launch_bounds__(WPB * 32, 1)
+    pencil_x_coop_batch_kernel(const RhsArgs* __restrict__ grids, const long* __restrict__ woff,
+                               int n) {
+    extern __shared__ __align__(16) unsigned char pencil_smem[];
+    const int warp = threadIdx.x >> 5;
+    unsigned char* wbase = pencil_smem + warp * PencilXLayout<CT>::WARP_BYTES;
+    const long total = woff[n];
+    const long S = (long)gridDim.x * WPB, s = (long)blockIdx.x * WPB + warp;
+    long pos = total * s / S;
+    const long end = total * (s + 1) / S;
+    int lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (woff[mid] <= pos) lo = mid; else hi = mid;
+    }
+    int i = lo;
+    while (pos < end) {
+        while (woff[i + 1] <= pos) ++i;
+        const RhsArgs& a = grids[i];
+        int L = 0;
+        pencil_work<0>(a, L);
+        const long local = pos - woff[i];
+        const long grp = local / L;
+        const int p0 = (int)(local - grp * L);
+        const int len = (int)min((long)(L - p0), end - pos);
+        pencil_x_segment<CT, true, MODE>(a, wbase, grp, p0, len);
+        pos += len;
+    }
+}
+
+// Launch of a persistent line-pass kernel, one CTA per SM; the dynamic
+// shared memory size is set and the SM count read once per device per kernel.
+template <typename Kern, typename... Args>
+int pencil_launch(Kern kern, int* blocks, int threads, size_t smem, cudaStream_t st,
+                  Args... args) {
+    int dev = 0;
+    WS_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(WS_ERR_UNSUPPORTED, "device ordinal >= 64");
+    if (!blocks[dev]) {
+        int sms = 0;
+        WS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        WS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+        blocks[dev] = sms;
+    }
+    kern<<<blocks[dev], threads, smem, st>>>(args...);
+    WS_CUDA(cudaGetLastError());
+    return WS_OK;
 }
 
 template <int WPB, typename CT, bool UNI>
 struct PencilLauncher {
-    static size_t smem() { return (size_t)WPB * PencilLayout<CT>::WARP * sizeof(CT); }
+    static constexpr size_t SMEM = (size_t)WPB * PencilLayout<CT>::WARP * sizeof(CT);
+    static constexpr int XW = 8;                       // warps of the cooperative x pass
+    static constexpr size_t XSMEM = XW * PencilXLayout<CT>::WARP_BYTES;
+    // the mixed form's stage pass holds more operands than 16 warps' 128
+    // registers allow: it runs with 12
+    static constexpr int SW = (sizeof(CT) == 4 && WPB > 12) ? 12 : WPB;
+    static constexpr size_t SSMEM = (size_t)SW * PencilLayout<CT>::WARP * sizeof(CT);
+
+    // one grid (job of a)
     template <int DIR, int MODE>
     static int one(const RhsArgs& a, int krk, cudaStream_t st) {
-        auto kern = pencil_rhs_kernel<DIR, WPB, CT, UNI, MODE>;
-        static int blocks[64] = {0};       // attributes set and SM count read once per device
-        int dev = 0;
-        WS_CUDA(cudaGetDevice(&dev));
-        if (dev < 0 || dev >= 64) return fail(WS_ERR_UNSUPPORTED, "device ordinal >= 64");
-        if (!blocks[dev]) {
-            int sms = 0;
-            WS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-            WS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem()));
-            blocks[dev] = sms;
-        }
-        kern<<<blocks[dev], WPB * 32, smem(), st>>>(a, krk);
-        WS_CUDA(cudaGetLastError());
-        return WS_OK;
+        constexpr int W = MODE == P_STAGE ? SW : WPB;
+        static int blocks[64] = {0};
+        return pencil_launch(pencil_rhs_kernel<DIR, W, CT, UNI, MODE>, blocks, W * 32,
+                             MODE == P_STAGE ? SSMEM : SMEM, st, a, krk);
     }
-    // the mixed form's x pass: the cooperative kernel, 8 warps per CTA
     template <int MODE>
     static int xcoop(const RhsArgs& a, cudaStream_t st) {
-        constexpr int XW = 8;
-        const size_t bytes = XW * PencilXLayout<CT>::WARP_BYTES;
-        auto kern = pencil_x_coop_kernel<XW, CT, UNI, MODE>;
         static int blocks[64] = {0};
-        int dev = 0;
-        WS_CUDA(cudaGetDevice(&dev));
-        if (dev < 0 || dev >= 64) return fail(WS_ERR_UNSUPPORTED, "device ordinal >= 64");
-        if (!blocks[dev]) {
-            int sms = 0;
-            WS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-            WS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)bytes));
-            blocks[dev] = sms;
-        }
-        kern<<<blocks[dev], XW * 32, bytes, st>>>(a);
-        WS_CUDA(cudaGetLastError());
-        return WS_OK;
+        return pencil_launch(pencil_x_coop_kernel<XW, CT, UNI, MODE>, blocks, XW * 32, XSMEM, st,
+                             a);
     }
     static int xpass(const RhsArgs& a, bool add_x, cudaStream_t st) {
         if constexpr (sizeof(CT) == 4)
@@ -362,19 +463,44 @@ struct PencilLauncher {
         if (rc || (rc = one<1, P_ADD>(a, 0, st))) return rc;
         return one<2, P_ADD>(a, 0, st);
     }
-    // stage: x, y into du, then z with the stage update (the mixed form's
-    // stage pass holds more operands than 16 warps' 128 registers: 12 warps)
+    // stage: x, y into du, then z with the stage update
     static int stage(const RhsArgs& a, bool add_x, int krk, cudaStream_t st) {
         if constexpr (UNI) {
             int rc = xpass(a, add_x, st);
             if (rc || (rc = one<1, P_ADD>(a, 0, st))) return rc;
-            if constexpr (sizeof(CT) == 4 && WPB > 12)
-                return PencilLauncher<12, CT, UNI>::template one<2, P_STAGE>(a, krk, st);
-            else
-                return one<2, P_STAGE>(a, krk, st);
+            return one<2, P_STAGE>(a, krk, st);
         } else {
             return fail(WS_ERR_UNSUPPORTED, "stage update needs Cartesian metrics");
         }
+    }
+
+    // a batch: argument table g of n grids, woff = the three passes' work
+    // prefix tables of n + 1 entries each (x, y, z); krk 0: RHS into each du
+    template <int DIR, int MODE>
+    static int one_batch(const RhsArgs* g, const long* woff, int n, int krk, cudaStream_t st) {
+        constexpr int W = MODE == P_STAGE ? SW : WPB;
+        static int blocks[64] = {0};
+        return pencil_launch(pencil_batch_kernel<DIR, W, CT, MODE>, blocks, W * 32,
+                             MODE == P_STAGE ? SSMEM : SMEM, st, g, woff, n, krk);
+    }
+    static int batch(const RhsArgs* g, const long* woff, int n, int krk, cudaStream_t st) {
+        int rc;
+        if constexpr (sizeof(CT) == 4) {
+            static int blocks[64] = {0};
+            rc = pencil_launch(pencil_x_coop_batch_kernel<XW, CT, P_STORE>, blocks, XW * 32,
+                               XSMEM, st, g, woff, n);
+        } else {
+            rc = one_batch<0, P_STORE>(g, woff, n, 0, st);
+        }
+        if (rc || (rc = one_batch<1, P_ADD>(g, woff + (n + 1), n, 0, st))) return rc;
+        if (!krk) return one_batch<2, P_ADD>(g, woff + 2 * (n + 1), n, 0, st);
+        // the batched mixed stage pass (arguments read from global memory)
+        // needs the registers of 8 warps per CTA
+        if constexpr (sizeof(CT) == 4 && WPB != 8)
+            return PencilLauncher<8, CT, true>::template one_batch<2, P_STAGE>(
+                g, woff + 2 * (n + 1), n, krk, st);
+        else
+            return one_batch<2, P_STAGE>(g, woff + 2 * (n + 1), n, krk, st);
     }
 };
 

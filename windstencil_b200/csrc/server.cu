@@ -257,9 +257,8 @@ void loop(ws_server* s) {
                 for (Req* q : s->active)
                     if (q->r.grid.precision == p) g.push_back(&q->st);
                 const ws_tile& t = s->cfg.tile;
-                const int cfg = (t.tile_x || t.tile_y || t.threads)
-                                    ? std::max(0, find_tile_cfg(t.tile_x, t.tile_y, t.threads))
-                                    : default_cfg(p, true);
+                int cfg = batch_kernel_cfg(g, t);
+                if (cfg == -2) cfg = -1;        // a shape not compiled: the line passes
                 s->runner[p].build(g, cfg, t.scan_z, st);
             }
             s->rebuild = false;

@@ -136,6 +136,12 @@ int default_cfg(int precision, bool stage);       // tuned default shape (stage 
 // the RHS adds to (the viscous terms).
 int launch_rhs_pencil(const RhsArgs& a, int precision, bool uniform, int wpb, int krk,
                       bool add_x, cudaStream_t st);
+// The line passes over a batch: g the argument table of n Cartesian grids
+// (each with its du), woff the x, y and z passes' work prefix tables (n + 1
+// entries each, pencil_pass_work); krk as launch_rhs_pencil (no add_x).
+int launch_rhs_pencil_batch(const RhsArgs* g, const long* woff, int n, int precision, int krk,
+                            cudaStream_t st);
+long pencil_pass_work(const ws_grid& g, int dir);
 // Whether a launch with tile selection `tile` runs the line passes: an
 // explicit request (tile_x < 0, threads = 32 x warps per CTA or 0), or the
 // default (all zeros) for grids without CLOSURE faces.
@@ -220,6 +226,11 @@ int grid_state_download(GridState& s, double* f_host, cudaStream_t st);   // no 
 int grid_state_derive(GridState& s, cudaStream_t st);
 
 // A set of grids stepped together: one batched launch per kernel per stage.
+// The kernel a batch of these grids runs for tile selection `tile`: -1 for
+// the line passes (the default, unless a grid has CLOSURE faces; or asked for
+// by tile_x < 0), else a fused tile configuration (-2: not compiled).
+int batch_kernel_cfg(const std::vector<GridState*>& grids, ws_tile tile);
+
 class BatchRunner {
   public:
     BatchRunner() = default;
@@ -228,6 +239,7 @@ class BatchRunner {
     BatchRunner& operator=(const BatchRunner&) = delete;
     // (re)build the device tables for `grids` (all of one precision);
     // invalidates captured graphs
+    // cfg < 0: the line passes (pencil_impl.cuh), else the fused kernel's tile
     int build(const std::vector<GridState*>& grids, int cfg, int zc, cudaStream_t st);
     int enqueue_rhs(cudaStream_t st);
     // the first RK stage only (leaves the current state unchanged; tuning)
@@ -248,6 +260,8 @@ class BatchRunner {
     std::vector<GridState*> grids_;
     int precision_ = 0, cfg_ = 0, zc_ = 1 << 30, ctas_ = 0;
     bool closure_ = false;          // some grid has CLOSURE faces
+    bool pencil_ = false;           // line passes instead of the fused kernel
+    const long* d_woff_ = nullptr;  // line passes: x, y, z work prefix tables
     void* dev_ = nullptr;           // device tables
     size_t dev_bytes_ = 0;
     // With c = cur ^ p (p = step parity since build), a step reads f[c] and
