@@ -224,25 +224,31 @@ __global__ void __launch_bounds__(WPB * 32, 1)
     }
 }
 
-// The x pass of the mixed form, cooperative: the lanes still own 32 lines
-// (consecutive y) and reconstruct their own faces, but the loads and splits
-// of the next 4 points of all 32 lines, and the stores of 4 points of du,
-// are done by the warp together, lane (xi, yi) = (lane % 4, lane / 4) taking
-// point xi of lines yi, yi+8, yi+16, yi+24.  Each global access then covers
-// 8 lines x 4 consecutive x instead of 32 lines x 1 x: a quarter of the L1
-// transactions, which bound the per-lane form (the split is then written
-// into the owning lane's ring column, hence a 12-slot ring: the 8-point
-// stencils of a chunk of 4 faces span 11 points).  The FP64 passes are
-// compute-bound and keep the per-lane form.
-template <typename CT>
+// The x pass, cooperative.  In the other passes a warp's 32 lines are
+// consecutive in x, so the per-lane loads and du stores coalesce; in the x
+// pass they are 32 consecutive y, and per lane every access is a separate
+// L1 transaction (measured: MIO-throttle-bound, 3x the y pass's time in the
+// mixed form).  Here the lanes still own their lines and reconstruct their
+// own faces, but the loads and splits of the next C points of all 32 lines,
+// and the stores of C points of du, are done by the warp together: lane
+// (xi, yi) = (lane % C, lane / C) takes point xi of lines yi + r (32 / C),
+// r < C, so each access covers 32 / C lines x C consecutive x.  A split is
+// then written into the owning lane's ring column, so the ring holds 8 + C
+// slots (a chunk of C faces spans 7 + C stencil points).  C = 4 for the
+// mixed form; C = 2 for FP64, whose larger ring must leave room for 8 warps.
+template <typename CT, int C_>
 struct PencilXLayout {
-    static constexpr int C = 4;                   // points per chunk
-    static constexpr int SLOTS = 12;
+    static constexpr int C = C_;                  // points per chunk (and lanes per line row)
+    static constexpr int SLOTS = 8 + C;           // a chunk's 8-point stencils span 7 + C points
     static constexpr int RS = 10 * 32;
     static constexpr int RING = SLOTS * RS;       // CT
     static constexpr int DUS = 5 * C * 32;        // du staging, doubles
     static constexpr size_t WARP_BYTES = RING * sizeof(CT) + DUS * sizeof(double);
 };
+// chunk of the cooperative x pass: 4 for the mixed form, 2 for FP64 (whose
+// ring is twice as large; 8 warps per CTA then still fit)
+template <typename CT>
+constexpr int pencil_x_chunk() { return sizeof(CT) == 4 ? 4 : 2; }
 
 // One segment of the cooperative x pass (positions p0 .. p0+len-1 of the 32
 // lines of group grp); wbase: the warp's ring and du staging.
@@ -251,8 +257,8 @@ __device__ __forceinline__ void pencil_x_segment(const RhsArgs& a, unsigned char
                                                  long grp, int p0, int len) {
     static_assert(MODE != P_STAGE, "the x pass never applies the stage");
     constexpr bool ADD = MODE == P_ADD;
-    using P = PencilXLayout<CT>;
-    constexpr int C = P::C, NS = P::SLOTS;
+    using P = PencilXLayout<CT, pencil_x_chunk<CT>()>;
+    constexpr int C = P::C, NS = P::SLOTS, LR = 32 / C;   // lines per load round
     const int lane = threadIdx.x & 31;
     CT* ringw = reinterpret_cast<CT*>(wbase);                       // [12][10][32]
     double* dus = reinterpret_cast<double*>(wbase + P::RING * sizeof(CT));   // [5][C][32]
@@ -262,49 +268,49 @@ __device__ __forceinline__ void pencil_x_segment(const RhsArgs& a, unsigned char
     const int mlast = a.nx + 7;
     const size_t vs = (size_t)a.du_pitch * a.du_ly * a.du_lz;
     const long NL = (long)nyj * nzj;
-    const int xi = lane & 3, yi = lane >> 2;
-    // this lane's own line, and the four lines it loads / stores for
+    const int xi = lane % C, yi = lane / C;
+    // this lane's own line, and the C lines it loads / stores for
     const long lo = min(grp * 32 + lane, NL - 1);
     const bool valid = grp * 32 + lane < NL;
     const int oy = a.sy + (int)(lo % nyj), oz = a.sz + (int)(lo / nyj);
-    int cy[4], cz[4];
-    bool cv[4];
+    int cy[C], cz[C];
+    bool cv[C];
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-        const long l = grp * 32 + yi + 8 * r;
+    for (int r = 0; r < C; ++r) {
+        const long l = grp * 32 + yi + LR * r;
         cv[r] = l < NL;
         const long lc = min(l, NL - 1);
         cy[r] = a.sy + (int)(lc % nyj);
         cz[r] = a.sz + (int)(lc / nyj);
     }
-    // primitives of point x0 + xi of the four lines (x clamped), and their
+    // primitives of point x0 + xi of the C lines (x clamped), and their
     // splits into the owning lanes' ring columns (only xi < cnt)
-    auto coop_load = [&](int x0, double q[4][5]) {
+    auto coop_load = [&](int x0, double q[C][5]) {
         const int x = min(x0 + xi, mlast);
 #pragma unroll
-        for (int r = 0; r < 4; ++r)
+        for (int r = 0; r < C; ++r)
 #pragma unroll
             for (int f = 0; f < 5; ++f) q[r][f] = ldg_prim(a, f, x, cy[r], cz[r]);
     };
-    auto coop_split = [&](int x0, int cnt, const double q[4][5]) {
+    auto coop_split = [&](int x0, int cnt, const double q[C][5]) {
         if (xi >= cnt) return;
         const int x = x0 + xi;
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
+        for (int r = 0; r < C; ++r) {
             CT out[10];
             split_point<0, UNI, CT>(a, k, q[r][0], q[r][1], q[r][2], q[r][3], q[r][4], x,
                                     cy[r], cz[r], out);
-            CT* dst = ringw + (x % NS) * P::RS + yi + 8 * r;
+            CT* dst = ringw + (x % NS) * P::RS + yi + LR * r;
 #pragma unroll
             for (int c = 0; c < 10; ++c) dst[c * 32] = out[c];
         }
     };
     const int ms = a.sx + p0;
-    double qb[4][5];
-    coop_load(ms - 4, qb);
-    coop_split(ms - 4, 4, qb);
-    coop_load(ms, qb);
-    coop_split(ms, 4, qb);
+    double qb[C][5];
+    for (int p = ms - 4; p < ms + 4; p += C) {   // the first 8 points
+        coop_load(p, qb);
+        coop_split(p, C, qb);
+    }
     coop_load(ms + 4, qb);              // the first chunk's new points
     __syncwarp();
     double fprev[5];
@@ -317,7 +323,7 @@ __device__ __forceinline__ void pencil_x_segment(const RhsArgs& a, unsigned char
     }
     for (int mc = ms; mc < ms + len; mc += C) {
         const int cnt = min(C, ms + len - mc);
-        coop_split(mc + 4, cnt, qb);     // points mc+4 .. (slots of mc-8 ..: dead)
+        coop_split(mc + 4, cnt, qb);     // points mc+4 .. (slots of mc-4-C ..: dead)
         __syncwarp();
         if (mc + C < ms + len) coop_load(mc + C + 4, qb);
         // faces of this lane's line, steps mc .. mc+cnt-1, into the staging
@@ -334,18 +340,18 @@ __device__ __forceinline__ void pencil_x_segment(const RhsArgs& a, unsigned char
             }
         }
         __syncwarp();
-        // du of the chunk: point mc + xi of lines yi + 8r
+        // du of the chunk: point mc + xi of lines yi + LR r
         if (xi < cnt) {
             const int x = mc + xi;
 #pragma unroll
-            for (int r = 0; r < 4; ++r) {
+            for (int r = 0; r < C; ++r) {
                 if (!cv[r]) continue;
                 const size_t o = (size_t)(x - a.sx) +
                                  (size_t)a.du_pitch * ((size_t)(cy[r] - a.sy) +
                                                        (size_t)a.du_ly * (size_t)(cz[r] - a.sz));
 #pragma unroll
                 for (int v = 0; v < 5; ++v) {
-                    const double r_ = dus[(v * C + xi) * 32 + yi + 8 * r];
+                    const double r_ = dus[(v * C + xi) * 32 + yi + LR * r];
                     double* p = a.du + o + v * vs;
                     *p = ADD ? *p + r_ : r_;
                 }
@@ -361,7 +367,7 @@ __global__ void __launch_bounds__(WPB * 32, 1)
     pencil_x_coop_kernel(const __grid_constant__ RhsArgs a) {
     extern __shared__ __align__(16) unsigned char pencil_smem[];
     const int warp = threadIdx.x >> 5;
-    unsigned char* wbase = pencil_smem + warp * PencilXLayout<CT>::WARP_BYTES;
+    unsigned char* wbase = pencil_smem + warp * PencilXLayout<CT, pencil_x_chunk<CT>()>::WARP_BYTES;
     int L = 0;
     const long total = pencil_work<0>(a, L);
     const long S = (long)gridDim.x * WPB, s = (long)blockIdx.x * WPB + warp;
@@ -382,7 +388,7 @@ __global__ void __launch_bounds__(WPB * 32, 1)
                                int n) {
     extern __shared__ __align__(16) unsigned char pencil_smem[];
     const int warp = threadIdx.x >> 5;
-    unsigned char* wbase = pencil_smem + warp * PencilXLayout<CT>::WARP_BYTES;
+    unsigned char* wbase = pencil_smem + warp * PencilXLayout<CT, pencil_x_chunk<CT>()>::WARP_BYTES;
     const long total = woff[n];
     const long S = (long)gridDim.x * WPB, s = (long)blockIdx.x * WPB + warp;
     long pos = total * s / S;
@@ -431,7 +437,7 @@ template <int WPB, typename CT, bool UNI>
 struct PencilLauncher {
     static constexpr size_t SMEM = (size_t)WPB * PencilLayout<CT>::WARP * sizeof(CT);
     static constexpr int XW = 8;                       // warps of the cooperative x pass
-    static constexpr size_t XSMEM = XW * PencilXLayout<CT>::WARP_BYTES;
+    static constexpr size_t XSMEM = XW * PencilXLayout<CT, pencil_x_chunk<CT>()>::WARP_BYTES;
     // the mixed form's stage pass holds more operands than 16 warps' 128
     // registers allow: it runs with 12
     static constexpr int SW = (sizeof(CT) == 4 && WPB > 12) ? 12 : WPB;
@@ -452,10 +458,7 @@ struct PencilLauncher {
                              a);
     }
     static int xpass(const RhsArgs& a, bool add_x, cudaStream_t st) {
-        if constexpr (sizeof(CT) == 4)
-            return add_x ? xcoop<P_ADD>(a, st) : xcoop<P_STORE>(a, st);
-        else
-            return add_x ? one<0, P_ADD>(a, 0, st) : one<0, P_STORE>(a, 0, st);
+        return add_x ? xcoop<P_ADD>(a, st) : xcoop<P_STORE>(a, st);
     }
     // plain RHS: x (=, or += with add_x), y (+=), z (+=)
     static int rhs(const RhsArgs& a, bool add_x, cudaStream_t st) {
@@ -485,12 +488,10 @@ struct PencilLauncher {
     }
     static int batch(const RhsArgs* g, const long* woff, int n, int krk, cudaStream_t st) {
         int rc;
-        if constexpr (sizeof(CT) == 4) {
+        {
             static int blocks[64] = {0};
             rc = pencil_launch(pencil_x_coop_batch_kernel<XW, CT, P_STORE>, blocks, XW * 32,
                                XSMEM, st, g, woff, n);
-        } else {
-            rc = one_batch<0, P_STORE>(g, woff, n, 0, st);
         }
         if (rc || (rc = one_batch<1, P_ADD>(g, woff + (n + 1), n, 0, st))) return rc;
         if (!krk) return one_batch<2, P_ADD>(g, woff + 2 * (n + 1), n, 0, st);
