@@ -577,28 +577,50 @@ def bench_batch(a, torch, ws, wl, stream):
     return res, serial
 
 
-def bench_serve(a, ws, wl, serial_rate, rate, seconds, drain, seed=5):
-    """Poisson arrivals into the continuous-batching server (bounded run)."""
+def bench_serve(a, ws, wl, serial_rate, rate, seconds, drain, seed=5, host_io=False):
+    """Poisson arrivals into the continuous-batching server (bounded run).
+    host_io: every request uploads its initial state from host memory and
+    copies its final state back (latency includes both); else the initial
+    state is generated on the device and no result is copied."""
     rng = np.random.default_rng(seed)
     specs = wl.batch_specs(int(rate * seconds * 1.2) + 16, seed=seed)
+    pool = []
+    if host_io:         # a pool of host states, reused in turn (grid matches state)
+        pool = [(sp, wl.batch_state(sp)) for sp in specs[:32]]
     srv = ws.Server(hbm_budget_bytes=80 << 30)
     t0 = time.perf_counter()
     t_next = 0.0
     ids, offered_work = [], 0.0
+    pending = []
+
+    def release_done():
+        keep = []
+        for rid in pending:
+            state = srv.poll(rid)[0]
+            if state >= 2:              # done or failed: free its host buffers
+                srv.release(rid)
+            else:
+                keep.append(rid)
+        pending[:] = keep
     i = 0
     while True:
         now = time.perf_counter() - t0
         if now >= seconds:
             break
         if now < t_next:
+            if host_io:
+                release_done()
             time.sleep(min(t_next - now, 0.01))
             continue
-        s = specs[i % len(specs)]
+        s, f0 = pool[i % len(pool)] if host_io else (specs[i % len(specs)], None)
         nsteps = int(rng.integers(50, 501))
         prec = ws.FP64 if rng.random() < 0.5 else ws.MIXED
         g = ws.Grid(s.nx, s.ny, s.nz, precision=prec)
-        ids.append(srv.submit(g, nsteps, cfl=0.5, seed=s.seed, mach=s.mach, x_jump=s.x_jump,
-                              want_result=False))
+        rid = srv.submit(g, nsteps, cfl=0.5, f0=f0, seed=s.seed, mach=s.mach, x_jump=s.x_jump,
+                         want_result=host_io)
+        ids.append(rid)
+        if host_io:
+            pending.append(rid)
         offered_work += 3.0 * nsteps * s.cells
         i += 1
         t_next += rng.exponential(1.0 / rate)
@@ -607,6 +629,8 @@ def bench_serve(a, ws, wl, serial_rate, rate, seconds, drain, seed=5):
         st = srv.stats()
         if st["completed"] + st["failed"] >= len(ids):
             break
+        if host_io:
+            release_done()
         time.sleep(0.2)
     st = srv.stats()
     wall = time.perf_counter() - t0
@@ -619,14 +643,19 @@ def bench_serve(a, ws, wl, serial_rate, rate, seconds, drain, seed=5):
         "unfinished_at_stop": len(ids) - st["completed"] - st["failed"],
         "wall_s": wall, "p50_latency_s": st["p50_latency_s"],
         "p99_latency_s": st["p99_latency_s"], "mean_latency_s": st["mean_latency_s"],
-        "latency_over": "completed requests (submit -> result on the device)",
+        "latency_over": ("completed requests (submit -> initial state uploaded from host "
+                         "memory, steps, result copied to host memory)" if host_io else
+                         "completed requests (submit -> result on the device)"),
         "max_concurrent_grids": st["max_active"], "ticks": st["ticks"],
+        "loop_seconds": {k: st[k] for k in ("admit_s", "rebuild_s", "steps_s", "retire_s")},
         "offered_gcell_rhs_s": offered_work / seconds / 1e9,
         "served_gcell_rhs_s": served, "executed_gcell_rhs_s": executed, "unit": "Gcell-RHS/s",
         "served_vs_one_at_a_time_fp64": served / serial_rate if serial_rate else None,
         "executed_vs_one_at_a_time_fp64": executed / serial_rate if serial_rate else None,
         "requests": "grid as the batched workload, steps U[50,500], FP64 or mixed 50/50, "
-                    "80 GiB state budget, seeded initial state generated on the device",
+                    "80 GiB state budget, " +
+                    ("initial states from a pool of 32 host states (seeded), results copied "
+                     "back" if host_io else "seeded initial state generated on the device"),
         "note": "admission: FIFO under the HBM budget and a 3.2e7 active-cell cap; "
                 "arrivals stop at the end of the window, latency percentiles cover the "
                 "requests finished by the drain deadline; served counts finished requests' "
@@ -781,6 +810,9 @@ def run_ours(a, rank, world, dist):
                                           a.serve_drain)
             extra["served_sustainable"] = bench_serve(a, ws, wl, serial, a.serve_rate_low,
                                                       a.serve_seconds, a.serve_drain, seed=6)
+            extra["served_host_io"] = bench_serve(a, ws, wl, serial, a.serve_rate_low,
+                                                  a.serve_seconds, a.serve_drain, seed=7,
+                                                  host_io=True)
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
         cpu = cpu_arm(a, a.cpu_seconds)

@@ -434,6 +434,10 @@ typedef struct ws_server_stats {
     double served_cell_rhs;    /* cell-RHS evaluations of completed requests  */
     double executed_cell_rhs;  /* cell-RHS evaluations run, finished or not   */
     double busy_s, elapsed_s;
+    /* host clock spent by the loop in each phase: admission (allocation,
+     * initial state, time step), batch table rebuild, the steps (launch to
+     * completion), retirement (result copies, status) */
+    double admit_s, rebuild_s, steps_s, retire_s;
 } ws_server_stats;
 
 enum ws_request_state { WS_RQ_QUEUED = 0, WS_RQ_RUNNING = 1, WS_RQ_DONE = 2, WS_RQ_FAILED = 3 };

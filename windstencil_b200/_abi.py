@@ -82,7 +82,8 @@ class WsServerStats(C.Structure):
         ("hbm_in_use", C.c_size_t), ("p50_latency_s", C.c_double),
         ("p99_latency_s", C.c_double), ("mean_latency_s", C.c_double),
         ("served_cell_rhs", C.c_double), ("executed_cell_rhs", C.c_double),
-        ("busy_s", C.c_double), ("elapsed_s", C.c_double)]
+        ("busy_s", C.c_double), ("elapsed_s", C.c_double), ("admit_s", C.c_double),
+        ("rebuild_s", C.c_double), ("steps_s", C.c_double), ("retire_s", C.c_double)]
 
 
 _P = C.c_void_p

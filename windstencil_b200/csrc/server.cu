@@ -73,6 +73,11 @@ __global__ void synth_state_kernel(ws_soa f, int nx, int ny, int nz, double gamm
     }
 }
 
+// status words of the active grids, gathered into one array for one copy
+__global__ void gather_status_kernel(int* const* words, int n, int* out) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) out[i] = *words[i];
+}
+
 double now_s() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch())
         .count();
@@ -111,11 +116,20 @@ struct ws_server {
     cudaStream_t stream = nullptr;
     BatchRunner runner[2];          // per precision
     bool rebuild = true;
+    // status words of the active grids (device table of pointers, gathered
+    // after every tick so that a request whose state turned non-finite stops
+    // at once instead of stepping NaNs to its step count)
+    int** d_words = nullptr;
+    int* d_status = nullptr;
+    int* h_status = nullptr;        // pinned
+    int** h_words = nullptr;        // pinned: the pointer table's upload source
+    int n_words = 0, cap_words = 0;
     // statistics
     std::vector<double> latencies;
     double served_cell_rhs = 0, executed_cell_rhs = 0, t_start = 0, t_last = 0;
     long ticks = 0, admitted = 0, completed = 0, failed = 0, max_active_seen = 0;
     double busy_s = 0;
+    double t_admit = 0, t_rebuild = 0, t_steps = 0, t_retire = 0;   // per-phase host clock
     double active_cells = 0;
 };
 
@@ -233,6 +247,12 @@ void loop(ws_server* s) {
             admit_locked(s, fresh);
         }
         const double t0 = now_s();
+        double tp = t0;
+        auto phase = [&](double& acc) {
+            const double t = now_s();
+            acc += t - tp;
+            tp = t;
+        };
         if (!fresh.empty()) {
             int rc = start_requests(s, fresh);
             std::lock_guard<std::mutex> lk(s->mu);
@@ -250,6 +270,7 @@ void loop(ws_server* s) {
             s->max_active_seen = std::max<long>(s->max_active_seen, (long)s->active.size());
             s->cv_done.notify_all();
         }
+        phase(s->t_admit);
         if (s->active.empty()) continue;
         if (s->rebuild) {
             for (int p = 0; p < 2; ++p) {
@@ -261,8 +282,38 @@ void loop(ws_server* s) {
                 if (cfg == -2) cfg = -1;        // a shape not compiled: the line passes
                 s->runner[p].build(g, cfg, t.scan_z, st);
             }
+            const int na = (int)s->active.size();
+            if (na > s->cap_words) {
+                cudaStreamSynchronize(st);      // the old tables are idle
+                cudaFree(s->d_words);
+                cudaFree(s->d_status);
+                if (s->h_status) cudaFreeHost(s->h_status);
+                if (s->h_words) cudaFreeHost(s->h_words);
+                s->cap_words = std::max(na, 2 * s->cap_words);
+                if (cudaMalloc(&s->d_words, s->cap_words * sizeof(int*)) != cudaSuccess ||
+                    cudaMalloc(&s->d_status, s->cap_words * sizeof(int)) != cudaSuccess ||
+                    cudaMallocHost(&s->h_status, s->cap_words * sizeof(int)) != cudaSuccess ||
+                    cudaMallocHost(&s->h_words, s->cap_words * sizeof(int*)) != cudaSuccess) {
+                    cudaGetLastError();
+                    s->d_words = nullptr;
+                    s->d_status = nullptr;
+                    s->h_status = nullptr;
+                    s->h_words = nullptr;
+                    s->cap_words = 0;
+                }
+            }
+            s->n_words = 0;
+            if (s->cap_words >= na) {
+                // the previous upload from h_words was complete at the last
+                // tick's synchronisation
+                for (int i = 0; i < na; ++i) s->h_words[i] = s->active[i]->st.status;
+                cudaMemcpyAsync(s->d_words, s->h_words, na * sizeof(int*), cudaMemcpyHostToDevice,
+                                st);
+                s->n_words = na;
+            }
             s->rebuild = false;
         }
+        phase(s->t_rebuild);
         // steps this tick: up to the first completion; at most kTickSteps
         // while nothing waits in the queue (a request arriving now is then
         // admitted within that many steps)
@@ -276,12 +327,24 @@ void loop(ws_server* s) {
         // the batch changes every few ticks: launch the steps directly
         // rather than capture a graph for each new batch
         for (int p = 0; p < 2; ++p) s->runner[p].step_eager(k, st);
+        if (s->n_words > 0) {
+            gather_status_kernel<<<1, 256, 0, st>>>(s->d_words, s->n_words, s->d_status);
+            cudaMemcpyAsync(s->h_status, s->d_status, s->n_words * sizeof(int),
+                            cudaMemcpyDeviceToHost, st);
+        }
         cudaStreamSynchronize(st);
+        phase(s->t_steps);
         s->ticks++;
         s->executed_cell_rhs += 3.0 * k * s->active_cells;
         std::vector<Req*> done;
-        for (Req* q : s->active)
-            if ((q->steps_done += k) >= q->r.nsteps) done.push_back(q);
+        for (size_t i = 0; i < s->active.size(); ++i) {
+            Req* q = s->active[i];
+            q->steps_done += k;
+            // finished, or already failed (its status word is set)
+            if (q->steps_done >= q->r.nsteps ||
+                ((int)i < s->n_words && s->h_status[i] != 0))
+                done.push_back(q);
+        }
         if (!done.empty()) {
             int err = WS_OK;
             for (Req* q : done) {
@@ -305,6 +368,7 @@ void loop(ws_server* s) {
             s->rebuild = true;
             s->cv_done.notify_all();
         }
+        phase(s->t_retire);
         s->busy_s += now_s() - t0;
         s->t_last = now_s();
     }
@@ -327,11 +391,23 @@ int ws_server_create(const ws_server_config* cfg, ws_server** out) {
     if (s->cfg.max_active_cells <= 0) s->cfg.max_active_cells = 32.0e6;
     WS_CUDA(cudaGetDevice(&s->dev));
     WS_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
-    // keep freed request memory in the pool instead of returning it to the OS
+    // keep freed request memory in the pool instead of returning it to the OS,
+    // and grow the pool once now to the working set the active-cell cap allows
+    // (~330 B of state per cell): growing it request by request maps new
+    // memory at every admission (measured ~23 ms per request, a fifth of the
+    // loop's time under load)
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, s->dev) == cudaSuccess) {
         uint64_t thr = UINT64_MAX;
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        const size_t warm = std::min<size_t>(s->cfg.hbm_budget_bytes,
+                                             (size_t)(s->cfg.max_active_cells * 400.0));
+        void* p = nullptr;
+        if (cudaMallocAsync(&p, warm, s->stream) == cudaSuccess) {
+            cudaFreeAsync(p, s->stream);
+            cudaStreamSynchronize(s->stream);
+        }
+        cudaGetLastError();     // a device too small to warm this much is not an error
     }
     s->t_start = now_s();
     ws_server* raw = s.get();
@@ -352,6 +428,10 @@ void ws_server_destroy(ws_server* s) {
         if (kv.second->st.mem) grid_state_free(kv.second->st, s->stream);
     for (auto& r : s->runner) r.release(s->stream);
     cudaStreamSynchronize(s->stream);
+    if (s->d_words) cudaFree(s->d_words);
+    if (s->d_status) cudaFree(s->d_status);
+    if (s->h_status) cudaFreeHost(s->h_status);
+    if (s->h_words) cudaFreeHost(s->h_words);
     cudaStreamDestroy(s->stream);
     delete s;
 }
@@ -436,6 +516,10 @@ int ws_server_get_stats(ws_server* s, ws_server_stats* out) {
     out->served_cell_rhs = s->served_cell_rhs;
     out->executed_cell_rhs = s->executed_cell_rhs;
     out->busy_s = s->busy_s;
+    out->admit_s = s->t_admit;
+    out->rebuild_s = s->t_rebuild;
+    out->steps_s = s->t_steps;
+    out->retire_s = s->t_retire;
     out->elapsed_s = now_s() - s->t_start;
     return WS_OK;
 }
