@@ -745,7 +745,8 @@ def run_ours(a, rank, world, dist):
         pass
     roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": achieved / peak if peak else None, "traffic": measured_traffic(a),
-            "kernel": "pencil_rhs_kernel x, y, z line passes (<DIR,8,double,1,mode>), one RHS",
+            "kernel": "one RHS = pencil_x_coop_kernel<8,double,1,0> + "
+                      "pencil_rhs_kernel<1|2,8,double,1,1> (x, y, z line passes)",
             "kernel_ms": rhs_ms,
             "peak_source": "DFMA microkernel measured in this run (of measured)",
             "algorithmic_flop_per_cell": FLOP_PER_CELL,
@@ -753,6 +754,8 @@ def run_ours(a, rank, world, dist):
             "rhs_gcell_s": cells / (rhs_ms * 1e-3) / 1e9,
             "hbm_achieved_gbs": BYTES_PER_CELL * cells / (rhs_ms * 1e-3) / 1e9,
             "hbm_peak_gbs": peaks.get("hbm_gbs"), "hbm_peak_source": "MEASURED_PEAKS.json"}
+    if roof["traffic"]:
+        roof["hbm_measured_gbs"] = roof["traffic"] / (rhs_ms * 1e-3) / 1e9
 
     # ---- end to end through the C ABI with host buffers
     e2e = None
@@ -893,8 +896,9 @@ def profile_case(a):
 
 
 def measured_traffic(a):
-    """DRAM bytes per RHS launch from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "bf3w_rhs_fp64_600x128x128.json")
+    """DRAM bytes of one RHS (the three line passes) from the committed ncu
+    summary, if it was measured on this grid."""
+    p = os.path.join(ROOT, "profiles", "pencil_rhs_fp64_600x128x128.json")
     try:
         d = json.load(open(p))
         if d.get("grid") == [a.nx, a.ny, a.nz]:
