@@ -180,11 +180,20 @@ WS_API int ws_du_invis_jacobian3d_tiled(const ws_grid* g, ws_job job, ws_field d
 /* Viscous constants of the Navier-Stokes RHS: Reynolds number, Prandtl
  * number, Sutherland reference temperature Ref_T (Sutherland constant
  * 110.4 K, viscosity 1/Re at T = 1) and the central-difference order of the
- * derivatives, 6 or 8 (the reference's Scheme_vis_ID 203 / 204). */
+ * derivatives, 6 or 8 (the reference's Scheme_vis_ID 203 / 204).
+ * d0_bound: the reference's DIF_BOUND flags (D0_bound, parameters.c:175,
+ * :225), faces x-, x+, y-, y+, z-, z+.  Nonzero: in the four cells next to
+ * that face the viscous derivatives (gradients and flux divergence) take the
+ * reference's reduced forms (OCFD_bound, OCFD_bound_Scheme.cpp:432-452, and
+ * OCFD_D0bound_scheme_kernel, :82-240): a one-sided first difference at the
+ * face, then 2nd-, 4th- and 6th-order central differences; zero: the central
+ * difference through the ghosts.  Ignored on EXTERNAL faces (a neighbouring
+ * block's, not a physical, boundary). */
 typedef struct ws_viscous {
     double re, pr, ref_t;
     int32_t scheme;
     int32_t dummy0;
+    int32_t d0_bound[6];
 } ws_viscous;
 
 /* Device workspace that ws_du_vis_jacobian3d needs for grid g (bytes). */

@@ -72,6 +72,7 @@ FUNCS = [
     ("src/boundary/OCFD_bound_Scheme.cpp", "OCFD_weno5_kernel_M_lift"),
     ("src/boundary/OCFD_bound_Scheme.cpp", "OCFD_weno5_kernel_M_lift_plus"),
     ("src/boundary/OCFD_bound_Scheme.cpp", "OCFD_weno5_kernel_M_right_plus"),
+    ("src/boundary/OCFD_bound_Scheme.cpp", "OCFD_D0bound_scheme_kernel"),
     ("src/kernels/OCFD_Schemes.cpp", "OCFD_kernel_CD6"),
     ("src/kernels/OCFD_Schemes.cpp", "OCFD_kernel_CD8"),
     ("src/solver/OCFD_NS_Jacobian3d.cpp", "vis_flux_ker"),
@@ -354,7 +355,7 @@ void ref_du_invis(int nx, int ny, int nz, double hx, double hy, double hz, doubl
 void ref_du_vis(int nx, int ny, int nz, double hx, double hy, double hz, double gamma,
                 double ama, double re, double pr, double ref_t, int scheme, double* u,
                 double* v, double* w, double* T, const double* const* metrics,
-                const double* ajac, double* du, const int* face_kind) {
+                const double* ajac, double* du, const int* face_kind, const int* d0b) {
   const long px = nx + 2 * LAP, py = ny + 2 * LAP, pz = nz + 2 * LAP, L = px * py * pz;
   const long N = (long)nx * ny * nz;
   auto lap = [&](long i, long j, long k) { return (i + LAP) + px * ((j + LAP) + py * (k + LAP)); };
@@ -368,13 +369,28 @@ void ref_du_vis(int nx, int ny, int nz, double hx, double hy, double hz, double 
   const double* J = ajac ? ajac : unit.data();
   auto cf = [&](const double* p, long pitch) { cudaField f; f.ptr = const_cast<double*>(p);
     f.pitch = (unsigned)pitch; f.dummy0 = 0; return f; };
+  // the flags OCFD_bound (OCFD_bound_Scheme.cpp:432-452) sets for one domain
+  // whose job spans the interior: x = 4/5/6 with the low face's DIF_BOUND,
+  // y = 4/5/6 with the high face's; EXTERNAL faces are a neighbour's boundary
+  auto flags = [&](int dir) {
+    dim3 fl(dir + 1, 0, 0);
+    if (d0b[2 * dir] && face_kind[2 * dir] != 3) fl.x = dir + 4;
+    if (d0b[2 * dir + 1] && face_kind[2 * dir + 1] != 3) fl.y = dir + 4;
+    return fl;
+  };
   auto d0 = [&](const double* f, int dir, double* out) {
+    const dim3 fl = flags(dir);
+    const cudaJobPackage job(dim3(LAP, LAP, LAP), dim3(nx + LAP, ny + LAP, nz + LAP));
     #pragma omp parallel for collapse(2) schedule(static)
     for (long k = 0; k < nz; ++k) for (long j = 0; j < ny; ++j) for (long i = 0; i < nx; ++i) {
       REAL st[9];
       for (long q = -r; q <= r; ++q)
         st[q + r] = f[dir == 0 ? lap(i + q, j, k) : dir == 1 ? lap(i, j + q, k) : lap(i, j, k + q)];
-      const REAL tmp = scheme == 6 ? OCFD_kernel_CD6(st) : OCFD_kernel_CD8(st);
+      REAL tmp;
+      // OCFD_CD6_kernel / OCFD_CD8_kernel (OCFD_Schemes.cpp:107-160): the
+      // boundary forms first, the central scheme where they do not apply
+      int flag = OCFD_D0bound_scheme_kernel(&tmp, fl, dim3(i, j, k), &st[0], (int)-r, job);
+      if (flag != 0) tmp = scheme == 6 ? OCFD_kernel_CD6(st) : OCFD_kernel_CD8(st);
       out[i + nx * (j + ny * k)] = tmp / h[dir];
     }
   };

@@ -468,11 +468,41 @@ double cd8(const double* s) {
     return (672.0 * (s[5] - s[3]) - 168.0 * (s[6] - s[2]) + 32.0 * (s[7] - s[1]) -
             3.0 * (s[8] - s[0])) / 840.0;
 }
-// derivative along dir of LAP field f on the interior (dense out)
-void d0_field(const or_grid* g, int scheme, int dir, const double* f, double* out) {
+// The reduced forms of the derivative next to a face whose DIF_BOUND flag is
+// set (OCFD_D0bound_scheme_kernel, OCFD_bound_Scheme.cpp:82-240): at distance
+// e = 0..3 from the face, a one-sided first difference, then 2nd-, 4th- and
+// 6th-order central differences; c points at the stencil's centre.  Returns
+// false where the central scheme applies.  The low face is tested first, as
+// the reference does.
+bool d0_bound_form(const double* c, long pos, long n, bool lo, bool hi, double* tmp) {
+    long e;
+    bool low;
+    if (lo && pos < 4) {
+        e = pos;
+        low = true;
+    } else if (hi && pos >= n - 4) {
+        e = n - 1 - pos;
+        low = false;
+    } else {
+        return false;
+    }
+    if (e == 0) *tmp = low ? (c[1] - c[0]) : (c[0] - c[-1]);
+    else if (e == 1) *tmp = (c[1] - c[-1]) * 0.5;
+    else if (e == 2) *tmp = (c[-2] - 8.0 * c[-1] + 8.0 * c[1] - c[2]) / 12.0;
+    else *tmp = (c[3] - c[-3] - 9.0 * (c[2] - c[-2]) + 45.0 * (c[1] - c[-1])) / 60.0;
+    return true;
+}
+
+// derivative along dir of LAP field f on the interior (dense out); d0b: the
+// DIF_BOUND flags of the six faces (NULL: none), ignored on EXTERNAL faces
+void d0_field(const or_grid* g, int scheme, int dir, const double* f, double* out,
+              const int* d0b = nullptr) {
     Dims D(g);
     const long r = scheme == 6 ? 3 : 4;
     const double h = dir == 0 ? g->hx : dir == 1 ? g->hy : g->hz;
+    const bool lo = d0b && d0b[2 * dir] && g->face_kind[2 * dir] != OR_FACE_EXTERNAL;
+    const bool hi = d0b && d0b[2 * dir + 1] && g->face_kind[2 * dir + 1] != OR_FACE_EXTERNAL;
+    const long n = dir == 0 ? D.nx : dir == 1 ? D.ny : D.nz;
 #pragma omp parallel for collapse(2) schedule(static)
     for (long k = 0; k < D.nz; ++k)
         for (long j = 0; j < D.ny; ++j)
@@ -481,7 +511,10 @@ void d0_field(const or_grid* g, int scheme, int dir, const double* f, double* ou
                 for (long q = -r; q <= r; ++q)
                     st[q + r] = f[dir == 0 ? D.lap(i + q, j, k)
                                            : dir == 1 ? D.lap(i, j + q, k) : D.lap(i, j, k + q)];
-                const double tmp = scheme == 6 ? cd6(st) : cd8(st);
+                double tmp;
+                const long pos = dir == 0 ? i : dir == 1 ? j : k;
+                if (!d0_bound_form(st + r, pos, n, lo, hi, &tmp))
+                    tmp = scheme == 6 ? cd6(st) : cd8(st);
                 out[i + D.nx * (j + D.ny * k)] = tmp / h;
             }
 }
@@ -516,7 +549,8 @@ void or_vis_fluxes(const or_grid* g, const or_vis* vis, const double* u, const d
     const double* prim[4] = {u, v, w, T};
     for (int dir = 0; dir < 3; ++dir)
         for (int q = 0; q < 4; ++q)
-            d0_field(g, vis->scheme, dir, prim[q], grad.data() + (4 * dir + q) * N);
+            d0_field(g, vis->scheme, dir, prim[q], grad.data() + (4 * dir + q) * N,
+                     vis->d0_bound);
     or_amu(g, vis, T, amu.data());
     auto met = [&](int m, long p) {       // akx..asz, Cartesian when metrics == NULL
         return metrics ? metrics[m][p] : (m == 0 || m == 4 || m == 8 ? 1.0 : 0.0);
@@ -580,7 +614,7 @@ void or_vis_div_add(const or_grid* g, const or_vis* vis, int dir, double* ev4,
     for (int q = 0; q < 4; ++q) {
         double* e = ev4 + q * D.lap_size();
         or_ghost_fill(g, e);
-        d0_field(g, vis->scheme, dir, e, dv.data());
+        d0_field(g, vis->scheme, dir, e, dv.data(), vis->d0_bound);
 #pragma omp parallel for collapse(2) schedule(static)
         for (long k = 0; k < D.nz; ++k)
             for (long j = 0; j < D.ny; ++j)

@@ -54,6 +54,7 @@ typedef struct or_grid {
 typedef struct or_vis {
     double re, pr, ref_t;
     int scheme;
+    int d0_bound[6];   /* DIF_BOUND per face (x-, x+, y-, y+, z-, z+): reduced forms */
 } or_vis;
 
 /* scalar kernels ------------------------------------------------------------ */

@@ -35,14 +35,17 @@ class OrGrid(C.Structure):
 
 
 class OrVis(C.Structure):
-    """Viscous constants: Re, Pr, Sutherland Ref_T, central-difference order 6 or 8."""
+    """Viscous constants: Re, Pr, Sutherland Ref_T, central-difference order 6 or 8,
+    DIF_BOUND flags per face (the reduced boundary forms of the derivatives)."""
     _fields_ = [("re", C.c_double), ("pr", C.c_double), ("ref_t", C.c_double),
-                ("scheme", C.c_int)]
+                ("scheme", C.c_int), ("d0_bound", C.c_int * 6)]
 
 
-def make_vis(re=500.0, pr=0.72, ref_t=288.15, scheme=8) -> OrVis:
+def make_vis(re=500.0, pr=0.72, ref_t=288.15, scheme=8, d0_bound=(0,) * 6) -> OrVis:
     v = OrVis()
     v.re, v.pr, v.ref_t, v.scheme = re, pr, ref_t, scheme
+    for i, b in enumerate(d0_bound):
+        v.d0_bound[i] = int(b)
     return v
 
 
@@ -253,7 +256,8 @@ class RefFunctions:
         L.ref_du_invis.argtypes = ([C.c_int] * 3 + [C.c_double] * 5 + [_dp] * 5 +
                                    [C.POINTER(_dp), _dp, _dp, C.POINTER(C.c_int)])
         L.ref_du_vis.argtypes = ([C.c_int] * 3 + [C.c_double] * 8 + [C.c_int] + [_dp] * 4 +
-                                 [C.POINTER(_dp), _dp, _dp, C.POINTER(C.c_int)])
+                                 [C.POINTER(_dp), _dp, _dp, C.POINTER(C.c_int),
+                                  C.POINTER(C.c_int)])
 
     def weno_p(self, s):
         s = np.ascontiguousarray(s, dtype=np.float64).reshape(-1, 8)
@@ -313,9 +317,10 @@ class RefFunctions:
     def du_vis(self, g: OrGrid, vis: OrVis, u, v, w, T, metrics=None, ajac=None, du=None):
         du = np.zeros((5, g.nz, g.ny, g.nx)) if du is None else du
         kinds = (C.c_int * 6)(*[g.face_kind[i] for i in range(6)])
+        d0b = (C.c_int * 6)(*[vis.d0_bound[i] for i in range(6)])
         self.lib.ref_du_vis(g.nx, g.ny, g.nz, g.hx, g.hy, g.hz, g.gamma, g.ama, vis.re,
                             vis.pr, vis.ref_t, vis.scheme, _p(u), _p(v), _p(w), _p(T),
-                            _ptr_array(metrics), _p(ajac), _p(du), kinds)
+                            _ptr_array(metrics), _p(ajac), _p(du), kinds, d0b)
         return du
 
 

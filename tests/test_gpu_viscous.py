@@ -102,3 +102,57 @@ def test_viscous_rejects_bad_input(cuda):
     small = cuda.empty(16, dtype=cuda.float64, device="cuda")
     with pytest.raises(ws.WsError):
         ws.du_vis_jacobian3d(g, _vis(8), *f, du, workspace=small)
+
+
+@pytest.mark.parametrize("scheme", [6, 8])
+@pytest.mark.parametrize("faces,d0b", [((1, 1, 0, 0, 1, 1), (1, 1, 0, 0, 0, 0)),
+                                       ((1, 1, 1, 1, 0, 0), (1, 1, 1, 1, 1, 1)),
+                                       ((1, 1, 0, 0, 1, 1), (0, 1, 1, 0, 1, 0))])
+def test_du_vis_dif_bound(oracle, cuda, scheme, faces, d0b):
+    """DIF_BOUND: the reference's reduced derivative forms in the four cells
+    next to flagged faces (gradients and flux divergence), against the oracle
+    (pinned to the reference's OCFD_D0bound_scheme_kernel), general metrics in
+    the last case."""
+    nx, ny, nz = 22, 13, 11
+    general = d0b == (0, 1, 1, 0, 1, 0)
+    g = ws.Grid(nx, ny, nz, faces=faces, metrics_uniform=not general)
+    og = or_grid(nx, ny, nz, face_kind=faces)
+    d, u, v, w, T, cc = oracle_prims(oracle, og, wl.fourier_state(nx, ny, nz, seed=37))
+    metrics = ajac = mdev = None
+    if general:
+        rng = np.random.default_rng(38)
+        shp = d.shape
+        metrics = [rng.uniform(0.6, 1.4, shp) if i % 4 == 0 else rng.uniform(-0.3, 0.3, shp)
+                   for i in range(9)]
+        ajac = rng.uniform(0.8, 1.2, shp)
+        mdev = [to_lap(cuda, g, a) for a in metrics + [ajac]]
+    vis = dict(_vis(scheme), d0_bound=d0b)
+    base = np.random.default_rng(39).normal(size=(5, nz, ny, nx))
+    ref = oracle.du_vis(og, make_vis(**vis), u, v, w, T, metrics, ajac, du=base.copy())
+    plain = oracle.du_vis(og, make_vis(**_vis(scheme)), u, v, w, T, metrics, ajac,
+                          du=base.copy())
+    assert not np.array_equal(ref, plain)         # the flags change the boundary cells
+    du = cuda.from_numpy(base.copy()).cuda()
+    ws.du_vis_jacobian3d(g, vis, *(to_lap(cuda, g, a) for a in (u, v, w, T)), du, metrics=mdev)
+    cuda.cuda.synchronize()
+    assert rel_linf(du.cpu().numpy(), ref).max() <= TOL
+
+
+def test_ns_solver_dif_bound_steps(oracle, cuda):
+    """The solver with DIF_BOUND on the x faces: RHS and 3 steps against the
+    oracle."""
+    nx, ny, nz = 28, 14, 10
+    faces = (1, 1, 0, 0, 0, 0)
+    vis = dict(_vis(8), d0_bound=(1, 1, 0, 0, 0, 0))
+    og = or_grid(nx, ny, nz, face_kind=faces)
+    f0 = wl.fourier_state(nx, ny, nz, seed=40)
+    s = ws.Solver(ws.Grid(nx, ny, nz, faces=faces))
+    s.set_viscous(vis)
+    s.set_state(f0)
+    s.rhs()
+    assert rel_linf(s.get_rhs(), oracle.rhs_conserved_ns(og, make_vis(**vis), f0)).max() <= TOL
+    dt = oracle.compute_dt(og, f0, 0.4)
+    s.step(dt, 3)
+    ref = oracle.rk3_steps_ns(og, make_vis(**vis), f0, dt, 3)
+    assert rel_linf(s.get_state(), ref).max() <= TOL
+    s.close()

@@ -129,13 +129,19 @@ def test_du_invis_closure_bitexact(oracle, reffn, faces):
 
 @pytest.mark.parametrize("scheme", [6, 8])
 @pytest.mark.parametrize("general", [False, True])
-@pytest.mark.parametrize("faces", [(0, 0, 0, 0, 0, 0), (1, 1, 0, 0, 1, 1)])
-def test_du_vis_bitexact(oracle, reffn, scheme, general, faces):
+@pytest.mark.parametrize("faces,d0b", [((0, 0, 0, 0, 0, 0), (0,) * 6),
+                                       ((1, 1, 0, 0, 1, 1), (0,) * 6),
+                                       ((1, 1, 0, 0, 1, 1), (1, 1, 0, 1, 1, 0)),
+                                       ((1, 1, 1, 1, 0, 0), (1, 1, 1, 1, 1, 1))])
+def test_du_vis_bitexact(oracle, reffn, scheme, general, faces, d0b):
     # viscous terms: CD6/CD8 gradients, Sutherland viscosity, viscous fluxes
-    # per direction and their divergence, added to du[1..4]
+    # per direction and their divergence, added to du[1..4]; with DIF_BOUND
+    # flags the reduced forms next to flagged faces come from the reference's
+    # OCFD_D0bound_scheme_kernel (periodic faces included, as the reference
+    # applies them wherever the flag is set)
     from oracle.oracle import make_vis
     g = make_grid(14, 10, 9, face_kind=faces, ama=0.7)
-    vis = make_vis(re=300.0, pr=0.72, ref_t=250.0, scheme=scheme)
+    vis = make_vis(re=300.0, pr=0.72, ref_t=250.0, scheme=scheme, d0_bound=d0b)
     d, u, v, w, T = _prims(g, 20)
     for a in (u, v, w, T):
         oracle.ghost_fill(g, a)

@@ -139,9 +139,10 @@ def _metrics(m):
     return C.byref(mm)
 
 
-def viscous(re=500.0, pr=0.72, ref_t=288.15, scheme=8) -> WsViscous:
-    """ws_viscous: Reynolds and Prandtl numbers, Sutherland Ref_T, CD order 6 or 8."""
-    return WsViscous(re, pr, ref_t, scheme, 0)
+def viscous(re=500.0, pr=0.72, ref_t=288.15, scheme=8, d0_bound=(0,) * 6) -> WsViscous:
+    """ws_viscous: Reynolds and Prandtl numbers, Sutherland Ref_T, CD order 6 or 8,
+    and the per-face reduced boundary forms of the derivatives (DIF_BOUND)."""
+    return WsViscous(re, pr, ref_t, scheme, 0, (C.c_int32 * 6)(*[int(b) for b in d0_bound]))
 
 
 def _dp(a):

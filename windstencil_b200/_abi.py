@@ -56,7 +56,7 @@ class WsMetrics(C.Structure):
 
 class WsViscous(C.Structure):
     _fields_ = [("re", C.c_double), ("pr", C.c_double), ("ref_t", C.c_double),
-                ("scheme", C.c_int32), ("dummy0", C.c_int32)]
+                ("scheme", C.c_int32), ("dummy0", C.c_int32), ("d0_bound", C.c_int32 * 6)]
 
 
 class WsTile(C.Structure):

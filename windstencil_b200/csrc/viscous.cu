@@ -7,7 +7,8 @@
 // derivative kernels and four accumulation kernels (YF_Pe_XF) -- 40 launches
 // and 12 derivative fields in HBM.  Here:
 //   vis_flux_kernel: one pass over the interior computes the 12 first
-//     derivatives in registers (CD6/CD8 through the ghosts, value / h), the
+//     derivatives in registers (CD6/CD8 through the ghosts, value / h; the
+//     reference's reduced forms next to DIF_BOUND faces), the
 //     Sutherland viscosity (get_Amu_kernal, commen_kernel.cpp:123-132) and
 //     the viscous fluxes Ev1..4 of all three directions (12 LAP fields);
 //   ghost fill of those 12 fields by the face kinds (one launch per 8 fields);
@@ -32,8 +33,12 @@ struct VisArgs {
     uint32_t du_pitch, du_ly, du_lz;
     int nx, ny, nz;
     double rh[3];              // 1 / (h * the difference's divisor: 60 CD6, 840 CD8)
+    double h[3];               // grid spacing (the reduced boundary forms divide by it)
     double tsb, amu_c0, vfc;   // Sutherland constants, Cp/Pr
     int uniform, accumulate;
+    // DIF_BOUND: reduced forms next to the low / high face of direction d
+    // (the flag set and the face not EXTERNAL); any: some flag is on
+    int d0lo[3], d0hi[3], any_d0;
 };
 
 __device__ __forceinline__ size_t lapi(int X, int Y, int Z, uint32_t pitch, int ny) {
@@ -95,6 +100,32 @@ __device__ __forceinline__ double2 cd2_ring(const double2* w, int k, int stride)
                         cdv<R>(d[1][0], d[1][1], d[1][2], d[1][3]));
 }
 
+// The reference's reduced forms of the first difference next to a face whose
+// DIF_BOUND flag is set (OCFD_D0bound_scheme_kernel, OCFD_bound_Scheme.cpp:
+// 82-240), in its operation order: at distance e = 0..3 from the face a
+// one-sided difference, then 2nd-, 4th- and 6th-order central differences.
+// at(m) gives the stencil value at offset m (|m| <= 3).  Returns false where
+// the central scheme applies (the low face is tested first, as there).
+template <typename F>
+__device__ __forceinline__ bool d0_form(F at, int pos, int n, bool lo, bool hi, double& t) {
+    int e;
+    bool low;
+    if (lo && pos < 4) {
+        e = pos;
+        low = true;
+    } else if (hi && pos >= n - 4) {
+        e = n - 1 - pos;
+        low = false;
+    } else {
+        return false;
+    }
+    if (e == 0) t = low ? at(1) - at(0) : at(0) - at(-1);
+    else if (e == 1) t = (at(1) - at(-1)) * 0.5;
+    else if (e == 2) t = (at(-2) - 8.0 * at(-1) + 8.0 * at(1) - at(2)) / 12.0;
+    else t = (at(3) - at(-3) - 9.0 * (at(2) - at(-2)) + 45.0 * (at(1) - at(-1))) / 60.0;
+    return true;
+}
+
 struct VisItem {
     int x0, y0, k0, k1;
 };
@@ -128,7 +159,8 @@ constexpr size_t vis_div_smem() {   // two buffers of the Ev_x, Ev_y tiles and o
 // (get_Amu_kernal, commen_kernel.cpp:123-132) and the viscous fluxes
 // Ev1..4 of all three directions (vis_flux_ker, OCFD_NS_Jacobian3d.cpp:477-624)
 // at every interior cell.
-template <int R, bool UNI>
+// D0: compiled with the DIF_BOUND reduced forms (grids with a flag set)
+template <int R, bool UNI, bool D0>
 __global__ void __launch_bounds__(VNT, 2) vis_flux_kernel(const __grid_constant__ VisArgs a) {
     constexpr int W = 2 * R + 1, TX = VBX + 2 * R, TY = VBY + 2 * R, TYX = TY * TX;
     constexpr int PS = (TYX + VNT - 1) / VNT;     // tile positions a thread stages per field
@@ -214,6 +246,27 @@ __global__ void __launch_bounds__(VNT, 2) vis_flux_kernel(const __grid_constant_
                 g[2 * pr][2] = dz.x * a.rh[2];
                 g[2 * pr + 1][2] = dz.y * a.rh[2];
             }
+            if (D0) {           // DIF_BOUND: the reduced forms next to flagged faces
+#pragma unroll
+                for (int pr = 0; pr < 2; ++pr) {
+                    const double2* c = tile + (pr * TY + ly + R) * TX + lx + R;
+                    const double2* zr = ring + pr * VNT + tid;
+#pragma unroll
+                    for (int hh = 0; hh < 2; ++hh) {
+                        const int q = 2 * pr + hh;
+                        auto cx = [&](int m) { return hh ? c[m].y : c[m].x; };
+                        auto cy = [&](int m) { return hh ? c[m * TX].y : c[m * TX].x; };
+                        auto cz = [&](int m) {
+                            const double2 v = zr[((k + m + 2 * W) % W) * 2 * VNT];
+                            return hh ? v.y : v.x;
+                        };
+                        double t;
+                        if (d0_form(cx, i, a.nx, a.d0lo[0], a.d0hi[0], t)) g[q][0] = t / a.h[0];
+                        if (d0_form(cy, j, a.ny, a.d0lo[1], a.d0hi[1], t)) g[q][1] = t / a.h[1];
+                        if (d0_form(cz, k, a.nz, a.d0lo[2], a.d0hi[2], t)) g[q][2] = t / a.h[2];
+                    }
+                }
+            }
             const int Z = k + 4;
             double m[9], aj = 1.0;
             if (UNI) {
@@ -273,7 +326,7 @@ __device__ __forceinline__ void vcp_wait_all() { asm volatile("cp.async.wait_gro
 // The Ev_z window of a thread's column lives in registers; the next plane's
 // Ev_x / Ev_y tiles (and du, accumulating) arrive by cp.async into the other
 // of two shared-memory buffers while the current plane is processed.
-template <int R, bool UNI>
+template <int R, bool UNI, bool D0>
 __global__ void __launch_bounds__(VNT, 2) vis_div_kernel(const __grid_constant__ VisArgs a) {
     constexpr int W = 2 * R + 1, XW = VBX + 2 * R, YH = VBY + 2 * R;
     constexpr int XF = VBY * XW, YF = YH * VBX;               // x-rim, y-rim tile per field
@@ -365,8 +418,10 @@ __global__ void __launch_bounds__(VNT, 2) vis_div_kernel(const __grid_constant__
             const double2* yt = xt + 2 * XF;
 #pragma unroll
             for (int pr = 0; pr < 2; ++pr) {
-                const double2 dx = cd2<R>(xt + (pr * VBY + ly) * XW + lx + R, 1);
-                const double2 dy = cd2<R>(yt + (pr * YH + ly + R) * VBX + lx, VBX);
+                const double2* cxp = xt + (pr * VBY + ly) * XW + lx + R;
+                const double2* cyp = yt + (pr * YH + ly + R) * VBX + lx;
+                const double2 dx = cd2<R>(cxp, 1);
+                const double2 dy = cd2<R>(cyp, VBX);
                 const double ddx[2] = {dx.x, dx.y}, ddy[2] = {dy.x, dy.y};
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
@@ -374,10 +429,20 @@ __global__ void __launch_bounds__(VNT, 2) vis_div_kernel(const __grid_constant__
                     const double* z = zw[q];
                     const double dz = cdv<R>(z[R + 1] - z[R - 1], z[R + 2] - z[R - 2],
                                              z[R + 3] - z[R - 3], R == 4 ? z[R + 4] - z[0] : 0.0);
+                    double vx = ddx[h] * a.rh[0], vy = ddy[h] * a.rh[1], vz = dz * a.rh[2];
+                    if (D0) {           // DIF_BOUND: the reduced forms next to flagged faces
+                        auto fx = [&](int m) { return h ? cxp[m].y : cxp[m].x; };
+                        auto fy = [&](int m) { return h ? cyp[m * VBX].y : cyp[m * VBX].x; };
+                        auto fz = [&](int m) { return z[R + m]; };
+                        double t;
+                        if (d0_form(fx, i, a.nx, a.d0lo[0], a.d0hi[0], t)) vx = t / a.h[0];
+                        if (d0_form(fy, j, a.ny, a.d0lo[1], a.d0hi[1], t)) vy = t / a.h[1];
+                        if (d0_form(fz, k, a.nz, a.d0lo[2], a.d0hi[2], t)) vz = t / a.h[2];
+                    }
                     double acc = a.accumulate ? dus[(b * 4 + q) * VNT + tid] : 0.0;
-                    acc += aj * (ddx[h] * a.rh[0]);
-                    acc += aj * (ddy[h] * a.rh[1]);
-                    acc += aj * (dz * a.rh[2]);
+                    acc += aj * vx;
+                    acc += aj * vy;
+                    acc += aj * vz;
                     a.du[du_col + du_plane * k + du_var * (q + 1)] = acc;
                 }
             }
@@ -417,7 +482,7 @@ int launch_vis(K kernel, size_t smem, int* cache, const ws_grid* g, const VisArg
     return WS_OK;
 }
 
-int flux_cache[4][64], div_cache[4][64];
+int flux_cache[8][64], div_cache[8][64];
 
 }  // namespace
 
@@ -453,6 +518,13 @@ VisArgs vis_args(const ws_grid* g, const ws_viscous* vis, const ws_field* prims,
     a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
     const double dv = vis->scheme == 6 ? 60.0 : 840.0;
     a.rh[0] = 1.0 / (g->hx * dv); a.rh[1] = 1.0 / (g->hy * dv); a.rh[2] = 1.0 / (g->hz * dv);
+    a.h[0] = g->hx; a.h[1] = g->hy; a.h[2] = g->hz;
+    a.any_d0 = 0;
+    for (int d = 0; d < 3; ++d) {
+        a.d0lo[d] = vis->d0_bound[2 * d] && g->face_kind[2 * d] != WS_FACE_EXTERNAL;
+        a.d0hi[d] = vis->d0_bound[2 * d + 1] && g->face_kind[2 * d + 1] != WS_FACE_EXTERNAL;
+        a.any_d0 |= a.d0lo[d] | a.d0hi[d];
+    }
     // OCFD_init.cpp:380-396
     const double Cp = 1.0 / ((g->gamma - 1.0) * g->ama * g->ama);
     a.tsb = 110.4 / vis->ref_t;
@@ -473,11 +545,19 @@ void vis_flux_fields(const ws_grid* g, void* ws, ws_field ev[12]) {
 int launch_vis_flux(const ws_grid* g, const ws_viscous* vis, const ws_field prims[4],
                     const ws_metrics* m, void* ws, cudaStream_t st) {
     const VisArgs a = vis_args(g, vis, prims, m, ws_soa{}, ws, false);
-    const bool cd6 = vis->scheme == 6, uni = a.uniform != 0;
-    int rc = cd6 ? (uni ? launch_vis(vis_flux_kernel<3, true>, vis_flux_smem<3>(), flux_cache[0], g, a, st)
-                        : launch_vis(vis_flux_kernel<3, false>, vis_flux_smem<3>(), flux_cache[1], g, a, st))
-                 : (uni ? launch_vis(vis_flux_kernel<4, true>, vis_flux_smem<4>(), flux_cache[2], g, a, st)
-                        : launch_vis(vis_flux_kernel<4, false>, vis_flux_smem<4>(), flux_cache[3], g, a, st));
+    const bool cd6 = vis->scheme == 6, uni = a.uniform != 0, d0 = a.any_d0 != 0;
+    const int c = (cd6 ? 0 : 4) + (uni ? 0 : 2) + (d0 ? 1 : 0);
+    int rc;
+    switch (c) {
+        case 0: rc = launch_vis(vis_flux_kernel<3, true, false>, vis_flux_smem<3>(), flux_cache[c], g, a, st); break;
+        case 1: rc = launch_vis(vis_flux_kernel<3, true, true>, vis_flux_smem<3>(), flux_cache[c], g, a, st); break;
+        case 2: rc = launch_vis(vis_flux_kernel<3, false, false>, vis_flux_smem<3>(), flux_cache[c], g, a, st); break;
+        case 3: rc = launch_vis(vis_flux_kernel<3, false, true>, vis_flux_smem<3>(), flux_cache[c], g, a, st); break;
+        case 4: rc = launch_vis(vis_flux_kernel<4, true, false>, vis_flux_smem<4>(), flux_cache[c], g, a, st); break;
+        case 5: rc = launch_vis(vis_flux_kernel<4, true, true>, vis_flux_smem<4>(), flux_cache[c], g, a, st); break;
+        case 6: rc = launch_vis(vis_flux_kernel<4, false, false>, vis_flux_smem<4>(), flux_cache[c], g, a, st); break;
+        default: rc = launch_vis(vis_flux_kernel<4, false, true>, vis_flux_smem<4>(), flux_cache[c], g, a, st); break;
+    }
     if (rc) return rc;
     ws_field ef[12];
     vis_flux_fields(g, ws, ef);
@@ -488,11 +568,18 @@ int launch_vis_flux(const ws_grid* g, const ws_viscous* vis, const ws_field prim
 int launch_vis_div(const ws_grid* g, const ws_viscous* vis, const ws_metrics* m, ws_soa du,
                    void* ws, bool accumulate, cudaStream_t st) {
     const VisArgs a = vis_args(g, vis, nullptr, m, du, ws, accumulate);
-    const bool cd6 = vis->scheme == 6, uni = a.uniform != 0;
-    return cd6 ? (uni ? launch_vis(vis_div_kernel<3, true>, vis_div_smem<3>(), div_cache[0], g, a, st)
-                      : launch_vis(vis_div_kernel<3, false>, vis_div_smem<3>(), div_cache[1], g, a, st))
-               : (uni ? launch_vis(vis_div_kernel<4, true>, vis_div_smem<4>(), div_cache[2], g, a, st)
-                      : launch_vis(vis_div_kernel<4, false>, vis_div_smem<4>(), div_cache[3], g, a, st));
+    const bool cd6 = vis->scheme == 6, uni = a.uniform != 0, d0 = a.any_d0 != 0;
+    const int c = (cd6 ? 0 : 4) + (uni ? 0 : 2) + (d0 ? 1 : 0);
+    switch (c) {
+        case 0: return launch_vis(vis_div_kernel<3, true, false>, vis_div_smem<3>(), div_cache[c], g, a, st);
+        case 1: return launch_vis(vis_div_kernel<3, true, true>, vis_div_smem<3>(), div_cache[c], g, a, st);
+        case 2: return launch_vis(vis_div_kernel<3, false, false>, vis_div_smem<3>(), div_cache[c], g, a, st);
+        case 3: return launch_vis(vis_div_kernel<3, false, true>, vis_div_smem<3>(), div_cache[c], g, a, st);
+        case 4: return launch_vis(vis_div_kernel<4, true, false>, vis_div_smem<4>(), div_cache[c], g, a, st);
+        case 5: return launch_vis(vis_div_kernel<4, true, true>, vis_div_smem<4>(), div_cache[c], g, a, st);
+        case 6: return launch_vis(vis_div_kernel<4, false, false>, vis_div_smem<4>(), div_cache[c], g, a, st);
+        default: return launch_vis(vis_div_kernel<4, false, true>, vis_div_smem<4>(), div_cache[c], g, a, st);
+    }
 }
 
 // du[1..4] += (accumulate) or = viscous terms; du[0] = 0 when storing.
