@@ -438,9 +438,9 @@ struct PencilLauncher {
     static constexpr size_t SMEM = (size_t)WPB * PencilLayout<CT>::WARP * sizeof(CT);
     static constexpr int XW = 8;                       // warps of the cooperative x pass
     static constexpr size_t XSMEM = XW * PencilXLayout<CT, pencil_x_chunk<CT>()>::WARP_BYTES;
-    // the mixed form's stage pass holds more operands than 16 warps' 128
-    // registers allow: it runs with 12
-    static constexpr int SW = (sizeof(CT) == 4 && WPB > 12) ? 12 : WPB;
+    // the stage pass holds more operands than the other passes: the mixed
+    // form's runs with 12 warps (16 leave 128 registers), the FP64 one with 8
+    static constexpr int SW = sizeof(CT) == 4 ? (WPB > 12 ? 12 : WPB) : (WPB > 8 ? 8 : WPB);
     static constexpr size_t SSMEM = (size_t)SW * PencilLayout<CT>::WARP * sizeof(CT);
 
     // one grid (job of a)
