@@ -126,10 +126,14 @@ typedef struct ws_metrics {
     ws_field ajac;            /* Jacobian J    */
 } ws_metrics;
 
-/* Kernel tile shape: a CTA of `threads` threads owns tile_x x tile_y columns
- * and sweeps them along z; scan_z caps the planes of one sweep (0: no cap,
- * each persistent CTA sweeps its whole share of planes).  Zeroes in tile_x,
- * tile_y, threads select the tuned default. */
+/* Kernel selection.  All zeros (the default) and tile_x < 0 select the line
+ * passes: three barrier-free passes (x, y, z) in which each lane marches one
+ * grid line (with tile_x < 0, threads = 32 x warps per CTA, or 0 for the
+ * tuned count).  Any other tile_x, tile_y, threads select the fused tile
+ * sweep: a CTA of `threads` threads owns tile_x x tile_y columns and sweeps
+ * them along z; scan_z caps the planes of one sweep (0: no cap, each
+ * persistent CTA sweeps its whole share of planes).  Both give the same
+ * results, CLOSURE faces included. */
 typedef struct ws_tile {
     int32_t tile_x, tile_y, scan_z, threads;
 } ws_tile;

@@ -241,18 +241,14 @@ int tile_index(const ws_grid* g, ws_tile tile, bool stage, int* cfg) {
 
 // Fill RhsArgs and launch; shared by the drop-in entry and the solver.
 bool use_pencil(const ws_grid* g, ws_tile tile) {
+    (void)g;
     if (tile.tile_x < 0) return true;
-    if (tile.tile_x || tile.tile_y || tile.threads) return false;
-    for (int i = 0; i < 4; ++i)
-        if (g->face_kind[i] == WS_FACE_CLOSURE) return false;
-    return true;
+    return !(tile.tile_x || tile.tile_y || tile.threads);
 }
 
 namespace {
 int check_pencil(const ws_grid* g, ws_tile tile) {
-    for (int i = 0; i < 4; ++i)
-        if (g->face_kind[i] == WS_FACE_CLOSURE)
-            return fail(WS_ERR_UNSUPPORTED, "line passes: no CLOSURE faces");
+    (void)g;
     if (tile.threads % 32) return fail(WS_ERR_INVALID, "line passes: threads = 32 x warps");
     return WS_OK;
 }

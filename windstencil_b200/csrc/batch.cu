@@ -177,15 +177,12 @@ void BatchRunner::release(cudaStream_t st) {
 }
 
 int batch_kernel_cfg(const std::vector<GridState*>& grids, ws_tile tile) {
+    (void)grids;
     if (tile.tile_x < 0) return -1;
-    const int prec = grids.empty() ? WS_FP64 : grids[0]->g.precision;
     if (tile.tile_x || tile.tile_y || tile.threads) {
         const int c = find_tile_cfg(tile.tile_x, tile.tile_y, tile.threads);
         return c < 0 ? -2 : c;
     }
-    for (auto* s : grids)
-        for (int i = 0; i < 4; ++i)
-            if (s->g.face_kind[i] == WS_FACE_CLOSURE) return default_cfg(prec, true);
     return -1;
 }
 
@@ -320,7 +317,7 @@ int BatchRunner::enqueue_rhs(cudaStream_t st) {
     if (rc) return rc;
     if (pencil_)
         return launch_rhs_pencil_batch(d_rhs_[2 * parity_], d_woff_, (int)grids_.size(),
-                                       precision_, 0, st);
+                                       precision_, 0, closure_, st);
     return launch_rhs_batch(d_rhs_[2 * parity_], work_, precision_, true, closure_, cfg_, ctas_, 0,
                             st);
 }
@@ -333,7 +330,7 @@ int BatchRunner::enqueue_stage1(cudaStream_t st) {
     if (rc) return rc;
     if (pencil_)
         return launch_rhs_pencil_batch(d_rhs_[2 * parity_], d_woff_, (int)grids_.size(),
-                                       precision_, 1, st);
+                                       precision_, 1, closure_, st);
     return launch_rhs_batch(d_rhs_[2 * parity_], work_, precision_, true, closure_, cfg_, ctas_, 1,
                             st);
 }
@@ -345,7 +342,7 @@ int BatchRunner::enqueue_step(cudaStream_t st) {
         int rc = launch_ghost_fill_batch(d_ghost_[parity_ ^ two], d_gtab_, n_gtab_, st);
         if (rc) return rc;
         rc = pencil_ ? launch_rhs_pencil_batch(d_rhs_[2 * parity_ + two], d_woff_,
-                                               (int)grids_.size(), precision_, krk, st)
+                                               (int)grids_.size(), precision_, krk, closure_, st)
                      : launch_rhs_batch(d_rhs_[2 * parity_ + two], work_, precision_, true,
                                         closure_, cfg_, ctas_, krk, st);
         if (rc) return rc;
@@ -573,8 +570,8 @@ int ws_batch_status(ws_batch* b, int* status, ws_stream_t stream) {
 // Times the candidate kernels on the first RK stage of this batch (ghost
 // fill + RHS and stage update; the current state is left as it was) and
 // keeps the fastest; returns its tile selection in *chosen.  Candidates: the
-// line passes (tile_x = -1), unless a grid has CLOSURE faces, and every
-// compiled tile shape of the fused kernel with two sweep caps.
+// line passes (tile_x = -1) and every compiled tile shape of the fused
+// kernel with two sweep caps.
 int ws_batch_autotune(ws_batch* b, ws_tile* chosen, ws_stream_t stream) {
     if (!b) return fail(WS_ERR_INVALID, "batch is NULL");
     cudaStream_t st = (cudaStream_t)stream;
@@ -583,11 +580,7 @@ int ws_batch_autotune(ws_batch* b, ws_tile* chosen, ws_stream_t stream) {
     WS_CUDA(cudaEventCreate(&e1));
     float best = 1e30f;
     ws_tile best_tile{0, 0, 0, 0};
-    std::vector<ws_tile> cand;
-    bool closure = false;
-    for (auto& s : b->states)
-        for (int i = 0; i < 4; ++i) closure |= s.g.face_kind[i] == WS_FACE_CLOSURE;
-    if (!closure) cand.push_back(ws_tile{-1, 0, 0, 0});
+    std::vector<ws_tile> cand{ws_tile{-1, 0, 0, 0}};
     for (int c = 0; c < num_tile_cfgs(); ++c)
         for (int cap : {0, 32}) {
             const TileCfg tc = tile_cfg(c);

@@ -202,15 +202,10 @@ __device__ __forceinline__ double face_flux<float, false>(const float* bp, int p
 // value otherwise.  In y the ring kernel drops the M term of the last cell;
 // the face above it (f == n, used by that cell only) carries M of face n-1
 // instead of its own, which cancels the M term in that cell's difference.
-template <typename CT>
-__device__ __forceinline__ double closure_value(const CT* prow, const CT* mrow, int stride, int f,
-                                             int n, bool lo, bool hi, bool ydir) {
-    double sp[8], sm[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        sp[k] = (double)prow[k * stride];
-        sm[k] = (double)mrow[k * stride];
-    }
+// The same from the two stencils as arrays: sp[k] = F+ and sm[k] = F- of
+// cell f-4+k.
+__device__ __forceinline__ double closure_value_arr(const double sp[8], const double sm[8], int f,
+                                                    int n, bool lo, bool hi, bool ydir) {
     double P, M, num, den;
     if (lo && f == 0) P = sp[4];
     else if (lo && f == 1) P = w5::p_lift(sp + 1);
@@ -245,6 +240,18 @@ __device__ __forceinline__ double closure_value(const CT* prow, const CT* mrow, 
         M = sm[4] + num / den;
     }
     return P + M;
+}
+
+template <typename CT>
+__device__ __forceinline__ double closure_value(const CT* prow, const CT* mrow, int stride, int f,
+                                             int n, bool lo, bool hi, bool ydir) {
+    double sp[8], sm[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        sp[k] = (double)prow[k * stride];
+        sm[k] = (double)mrow[k * stride];
+    }
+    return closure_value_arr(sp, sm, f, n, lo, hi, ydir);
 }
 
 // face f of a direction with n cells needs a closure value

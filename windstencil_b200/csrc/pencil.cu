@@ -24,11 +24,13 @@ int launch_rhs_pencil(const RhsArgs& a, int precision, bool uniform, int wpb, in
 }
 
 // the batched form over the argument table g of n Cartesian grids (woff: the
-// x, y, z passes' work prefix tables, n + 1 entries each)
+// x, y, z passes' work prefix tables, n + 1 entries each; clo: some grid has
+// a CLOSURE face)
 int launch_rhs_pencil_batch(const RhsArgs* g, const long* woff, int n, int precision, int krk,
-                            cudaStream_t st) {
-    if (precision == WS_MIXED) return PencilLauncher<12, float, true>::batch(g, woff, n, krk, st);
-    return PencilLauncher<8, double, true>::batch(g, woff, n, krk, st);
+                            bool clo, cudaStream_t st) {
+    if (precision == WS_MIXED)
+        return PencilLauncher<12, float, true>::batch(g, woff, n, krk, clo, st);
+    return PencilLauncher<8, double, true>::batch(g, woff, n, krk, clo, st);
 }
 
 // work of pass dir over the interior of grid g: line groups x march length

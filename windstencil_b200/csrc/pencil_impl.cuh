@@ -24,6 +24,8 @@
 // through HBM between the passes, which the compute-bound passes absorb
 // (~320 B/cell against ~7.3 kFLOP/cell).
 #pragma once
+#include <type_traits>
+
 #include "bf3w_rhs_impl.cuh"
 
 namespace ws {
@@ -35,6 +37,31 @@ struct PencilLayout {
 };
 
 enum PencilMode { P_STORE = 0, P_ADD = 1, P_STAGE = 2 };
+
+// Face value of variable v of face f (direction of n cells, CLOSURE flags lo /
+// hi, ydir: the y forms) from a lane's ring column `col` of ns slots (slot
+// stride 10 x 32, the stencil from slot s0 on): the closure value next to a
+// CLOSURE face, the WENO7 value elsewhere.  Not inlined: the steps near the
+// line ends call it, and one copy keeps the march loops' code within the
+// instruction cache (inlined into those steps, the closure code doubled the
+// y pass's time through instruction fetch stalls).
+template <typename CT>
+__device__ __noinline__ double pencil_closure_face(const CT* col, int s0, int ns, int v, int f,
+                                                   int n, int lo, int hi, bool ydir) {
+    constexpr int RS = 10 * 32;
+    if (closure_face(f, n, lo, hi)) {
+        double sp[8], sm[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int sk = s0 + k < ns ? s0 + k : s0 + k - ns;
+            const CT* e = col + sk * RS;
+            sp[k] = (double)e[v * 32];
+            sm[k] = (double)e[(5 + v) * 32];
+        }
+        return closure_value_arr(sp, sm, f, n, lo, hi, ydir);
+    }
+    return face_flux<CT, true>(col + s0 * RS + v * 32, 5 * 32, RS, ns - s0, ns * RS);
+}
 
 // March length, first LAP position and line count of pass DIR over the job
 // of `a`; the pass's work is its line groups (32 lines) x positions.
@@ -48,11 +75,14 @@ __device__ __forceinline__ long pencil_work(const RhsArgs& a, int& L) {
 
 // One segment of pass DIR (0 x, 1 y, 2 z): positions p0 .. p0+len-1 of the
 // lines of group grp of the job of `a`, this lane's line marched with the
-// lane's ring column `ring`.
-template <int DIR, typename CT, bool UNI, int MODE>
+// lane's ring column `ring`.  CLO (y pass): faces next to a CLOSURE face of
+// the grid (a.clo) take the closure rules of closure_value_arr; the lanes of
+// a warp sit at the same y, so the branch is uniform.
+template <int DIR, typename CT, bool UNI, int MODE, bool CLO = false>
 __device__ __forceinline__ void pencil_segment(const RhsArgs& a, int krk, CT* ring, long grp,
                                                int p0, int len) {
     static_assert(MODE != P_STAGE || (DIR == 2 && UNI), "stage update: z pass, Cartesian");
+    static_assert(!CLO || DIR == 1, "closure faces: y pass (the x pass is pencil_x_segment)");
     constexpr bool ADD = MODE != P_STORE;
     using P = PencilLayout<CT>;
     const int lane = threadIdx.x & 31;
@@ -93,6 +123,17 @@ __device__ __forceinline__ void pencil_segment(const RhsArgs& a, int krk, CT* ri
                (size_t)a.du_pitch * ((size_t)(Y(m) - a.sy) + (size_t)a.du_ly * (size_t)(Z(m) - a.sz));
     };
     auto f_at = [&](int m) { return soa_index(a.fn, X(m) - 4, Y(m) - 4, Z(m) - 4, 0); };
+    // face value of variable v above march position m (ring stencil from
+    // slot s0 = (m - 3) & 7; face index m - 3 of the direction); the
+    // closure test is compiled only into the steps of the closure zones
+    const bool clo = CLO && (a.clo[2] | a.clo[3]);
+    auto face = [&](int s0, int m, int v, auto cl) -> double {
+        if constexpr (decltype(cl)::value)
+            return pencil_closure_face<CT>(ring, s0, 8, v, m - 3, a.ny, a.clo[2], a.clo[3], true);
+        else
+            return face_flux<CT, true>(ring + s0 * P::RS + v * 32, 5 * 32, P::RS, 8 - s0,
+                                       8 * P::RS);
+    };
 
     const int ms = m0 + p0;
     for (int m = ms - 4; m < ms + 4; ++m) {
@@ -123,10 +164,9 @@ __device__ __forceinline__ void pencil_segment(const RhsArgs& a, int krk, CT* ri
         const int s0 = (ms - 4) & 7;
 #pragma unroll
         for (int v = 0; v < 5; ++v)
-            fprev[v] = face_flux<CT, true>(ring + s0 * P::RS + v * 32, 5 * 32, P::RS, 8 - s0,
-                                           8 * P::RS);
+            fprev[v] = face(s0, ms - 1, v, std::integral_constant<bool, CLO>{});
     }
-    for (int m = ms; m < ms + len; ++m) {
+    auto step = [&](int m, auto cl) {
         double q[5], dc[5], fnc[5], fic[5];
 #pragma unroll
         for (int f = 0; f < 5; ++f) {
@@ -143,12 +183,11 @@ __device__ __forceinline__ void pencil_segment(const RhsArgs& a, int krk, CT* ri
         double r[5];
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
-            const double fc = face_flux<CT, true>(ring + s0 * P::RS + v * 32, 5 * 32, P::RS,
-                                                  8 - s0, 8 * P::RS);
+            const double fc = face(s0, m, v, cl);
             r[v] = -J * ((fc - fprev[v]) * rh);
             fprev[v] = fc;
         }
-        if (!valid) continue;
+        if (!valid) return;
         if (MODE == P_STAGE) {
             const size_t o = f_at(m);
             double qs[5];
@@ -163,12 +202,26 @@ __device__ __forceinline__ void pencil_segment(const RhsArgs& a, int krk, CT* ri
 #pragma unroll
             for (int v = 0; v < 5; ++v) a.du[o + v * vs] = ADD ? dc[v] + r[v] : r[v];
         }
+    };
+    // closure zones: faces m - 3 <= 3 next to the low face, m - 3 >= n - 3
+    // next to the high face (LAP positions m <= 6 and m >= n)
+    const int me = ms + len;
+    int z1 = ms, z2 = me;
+    if (clo) {
+        z1 = a.clo[2] ? max(ms, min(7, me)) : ms;
+        z2 = a.clo[3] ? max(z1, min(a.ny, me)) : me;
     }
+    int m = ms;
+    if constexpr (CLO)
+        for (; m < z1; ++m) step(m, std::true_type{});
+    for (; m < z2; ++m) step(m, std::false_type{});
+    if constexpr (CLO)
+        for (; m < me; ++m) step(m, std::true_type{});
 }
 
 // One pass along DIR over the job of `a`: every warp takes an equal
 // contiguous share of the (line group, position) space.
-template <int DIR, int WPB, typename CT, bool UNI, int MODE>
+template <int DIR, int WPB, typename CT, bool UNI, int MODE, bool CLO = false>
 __global__ void __launch_bounds__(WPB * 32, 1)
     pencil_rhs_kernel(const __grid_constant__ RhsArgs a, int krk) {
     using P = PencilLayout<CT>;
@@ -184,7 +237,7 @@ __global__ void __launch_bounds__(WPB * 32, 1)
         const long grp = pos / L;
         const int p0 = (int)(pos - grp * L);
         const int len = (int)min((long)(L - p0), end - pos);
-        pencil_segment<DIR, CT, UNI, MODE>(a, krk, ring, grp, p0, len);
+        pencil_segment<DIR, CT, UNI, MODE, CLO>(a, krk, ring, grp, p0, len);
         pos += len;
     }
 }
@@ -192,7 +245,7 @@ __global__ void __launch_bounds__(WPB * 32, 1)
 // The same pass over the grids of a batch: argument table `grids`, and
 // woff[i] the pass's work before grid i (woff[n] the total).  A warp's share
 // may cross grids.
-template <int DIR, int WPB, typename CT, int MODE>
+template <int DIR, int WPB, typename CT, int MODE, bool CLO = false>
 __global__ void __launch_bounds__(WPB * 32, 1)
     pencil_batch_kernel(const RhsArgs* __restrict__ grids, const long* __restrict__ woff, int n,
                         int krk) {
@@ -219,7 +272,7 @@ __global__ void __launch_bounds__(WPB * 32, 1)
         const long grp = local / L;
         const int p0 = (int)(local - grp * L);
         const int len = (int)min((long)(L - p0), end - pos);
-        pencil_segment<DIR, CT, true, MODE>(a, krk, ring, grp, p0, len);
+        pencil_segment<DIR, CT, true, MODE, CLO>(a, krk, ring, grp, p0, len);
         pos += len;
     }
 }
@@ -251,8 +304,10 @@ template <typename CT>
 constexpr int pencil_x_chunk() { return sizeof(CT) == 4 ? 4 : 2; }
 
 // One segment of the cooperative x pass (positions p0 .. p0+len-1 of the 32
-// lines of group grp); wbase: the warp's ring and du staging.
-template <typename CT, bool UNI, int MODE>
+// lines of group grp); wbase: the warp's ring and du staging.  CLO: faces
+// next to a CLOSURE x face take the closure rules (uniform across the warp,
+// whose lanes march the same x).
+template <typename CT, bool UNI, int MODE, bool CLO = false>
 __device__ __forceinline__ void pencil_x_segment(const RhsArgs& a, unsigned char* wbase,
                                                  long grp, int p0, int len) {
     static_assert(MODE != P_STAGE, "the x pass never applies the stage");
@@ -305,6 +360,17 @@ __device__ __forceinline__ void pencil_x_segment(const RhsArgs& a, unsigned char
             for (int c = 0; c < 10; ++c) dst[c * 32] = out[c];
         }
     };
+    const bool clo = CLO && (a.clo[0] | a.clo[1]);
+    // face value of variable v above point m (stencil from ring slot s0);
+    // the closure test is compiled only into the chunks of the closure zones
+    auto face = [&](int s0, int m, int v, auto cl) -> double {
+        if constexpr (decltype(cl)::value)
+            return pencil_closure_face<CT>(ring, s0, NS, v, m - 3, a.nx, a.clo[0], a.clo[1],
+                                           false);
+        else
+            return face_flux<CT, true>(ring + s0 * P::RS + v * 32, 5 * 32, P::RS, NS - s0,
+                                       NS * P::RS);
+    };
     const int ms = a.sx + p0;
     double qb[C][5];
     for (int p = ms - 4; p < ms + 4; p += C) {   // the first 8 points
@@ -318,26 +384,36 @@ __device__ __forceinline__ void pencil_x_segment(const RhsArgs& a, unsigned char
         const int s0 = (ms - 4) % NS;
 #pragma unroll
         for (int v = 0; v < 5; ++v)
-            fprev[v] = face_flux<CT, true>(ring + s0 * P::RS + v * 32, 5 * 32, P::RS,
-                                           NS - s0, NS * P::RS);
+            fprev[v] = face(s0, ms - 1, v, std::integral_constant<bool, CLO>{});
     }
-    for (int mc = ms; mc < ms + len; mc += C) {
-        const int cnt = min(C, ms + len - mc);
-        coop_split(mc + 4, cnt, qb);     // points mc+4 .. (slots of mc-4-C ..: dead)
-        __syncwarp();
-        if (mc + C < ms + len) coop_load(mc + C + 4, qb);
-        // faces of this lane's line, steps mc .. mc+cnt-1, into the staging
+    // faces of this lane's line, steps mc .. mc+cnt-1, into the staging
+    auto faces = [&](int mc, int cnt, auto cl) {
         for (int i = 0; i < cnt; ++i) {
             const int m = mc + i;
             const int s0 = (m - 3) % NS;
             const double J = UNI ? 1.0 : ldg_met(a, 9, m, oy, oz);
 #pragma unroll
             for (int v = 0; v < 5; ++v) {
-                const double fc = face_flux<CT, true>(ring + s0 * P::RS + v * 32, 5 * 32,
-                                                      P::RS, NS - s0, NS * P::RS);
+                const double fc = face(s0, m, v, cl);
                 dus[(v * C + i) * 32 + lane] = -J * ((fc - fprev[v]) * a.rhx);
                 fprev[v] = fc;
             }
+        }
+    };
+    for (int mc = ms; mc < ms + len; mc += C) {
+        const int cnt = min(C, ms + len - mc);
+        coop_split(mc + 4, cnt, qb);     // points mc+4 .. (slots of mc-4-C ..: dead)
+        __syncwarp();
+        if (mc + C < ms + len) coop_load(mc + C + 4, qb);
+        // closure zones: faces m - 3 <= 3 (LAP m <= 6) next to the low x face,
+        // m - 3 >= n - 3 (m >= n) next to the high one
+        if constexpr (CLO) {
+            if (clo && ((a.clo[0] && mc <= 6) || (a.clo[1] && mc + cnt - 1 >= a.nx)))
+                faces(mc, cnt, std::true_type{});
+            else
+                faces(mc, cnt, std::false_type{});
+        } else {
+            faces(mc, cnt, std::false_type{});
         }
         __syncwarp();
         // du of the chunk: point mc + xi of lines yi + LR r
@@ -362,7 +438,7 @@ __device__ __forceinline__ void pencil_x_segment(const RhsArgs& a, unsigned char
     __syncwarp();
 }
 
-template <int WPB, typename CT, bool UNI, int MODE>
+template <int WPB, typename CT, bool UNI, int MODE, bool CLO = false>
 __global__ void __launch_bounds__(WPB * 32, 1)
     pencil_x_coop_kernel(const __grid_constant__ RhsArgs a) {
     extern __shared__ __align__(16) unsigned char pencil_smem[];
@@ -377,12 +453,12 @@ __global__ void __launch_bounds__(WPB * 32, 1)
         const long grp = pos / L;
         const int p0 = (int)(pos - grp * L);
         const int len = (int)min((long)(L - p0), end - pos);
-        pencil_x_segment<CT, UNI, MODE>(a, wbase, grp, p0, len);
+        pencil_x_segment<CT, UNI, MODE, CLO>(a, wbase, grp, p0, len);
         pos += len;
     }
 }
 
-template <int WPB, typename CT, int MODE>
+template <int WPB, typename CT, int MODE, bool CLO = false>
 __global__ void __launch_bounds__(WPB * 32, 1)
     pencil_x_coop_batch_kernel(const RhsArgs* __restrict__ grids, const long* __restrict__ woff,
                                int n) {
@@ -408,7 +484,7 @@ __global__ void __launch_bounds__(WPB * 32, 1)
         const long grp = local / L;
         const int p0 = (int)(local - grp * L);
         const int len = (int)min((long)(L - p0), end - pos);
-        pencil_x_segment<CT, true, MODE>(a, wbase, grp, p0, len);
+        pencil_x_segment<CT, true, MODE, CLO>(a, wbase, grp, p0, len);
         pos += len;
     }
 }
@@ -444,56 +520,66 @@ struct PencilLauncher {
     static constexpr size_t SSMEM = (size_t)SW * PencilLayout<CT>::WARP * sizeof(CT);
 
     // one grid (job of a)
-    template <int DIR, int MODE>
+    template <int DIR, int MODE, bool CLO = false>
     static int one(const RhsArgs& a, int krk, cudaStream_t st) {
         constexpr int W = MODE == P_STAGE ? SW : WPB;
         static int blocks[64] = {0};
-        return pencil_launch(pencil_rhs_kernel<DIR, W, CT, UNI, MODE>, blocks, W * 32,
+        return pencil_launch(pencil_rhs_kernel<DIR, W, CT, UNI, MODE, CLO>, blocks, W * 32,
                              MODE == P_STAGE ? SSMEM : SMEM, st, a, krk);
     }
-    template <int MODE>
+    template <int MODE, bool CLO>
     static int xcoop(const RhsArgs& a, cudaStream_t st) {
         static int blocks[64] = {0};
-        return pencil_launch(pencil_x_coop_kernel<XW, CT, UNI, MODE>, blocks, XW * 32, XSMEM, st,
-                             a);
+        return pencil_launch(pencil_x_coop_kernel<XW, CT, UNI, MODE, CLO>, blocks, XW * 32,
+                             XSMEM, st, a);
     }
-    static int xpass(const RhsArgs& a, bool add_x, cudaStream_t st) {
-        return add_x ? xcoop<P_ADD>(a, st) : xcoop<P_STORE>(a, st);
+    // the x and y passes (each pass's closure instance when the grid has a
+    // CLOSURE face in its direction)
+    static int xy(const RhsArgs& a, bool add_x, cudaStream_t st) {
+        int rc;
+        if (a.clo[0] | a.clo[1])
+            rc = add_x ? xcoop<P_ADD, true>(a, st) : xcoop<P_STORE, true>(a, st);
+        else
+            rc = add_x ? xcoop<P_ADD, false>(a, st) : xcoop<P_STORE, false>(a, st);
+        if (rc) return rc;
+        return (a.clo[2] | a.clo[3]) ? one<1, P_ADD, true>(a, 0, st) : one<1, P_ADD>(a, 0, st);
     }
     // plain RHS: x (=, or += with add_x), y (+=), z (+=)
     static int rhs(const RhsArgs& a, bool add_x, cudaStream_t st) {
-        int rc = xpass(a, add_x, st);
-        if (rc || (rc = one<1, P_ADD>(a, 0, st))) return rc;
-        return one<2, P_ADD>(a, 0, st);
+        int rc = xy(a, add_x, st);
+        return rc ? rc : one<2, P_ADD>(a, 0, st);
     }
     // stage: x, y into du, then z with the stage update
     static int stage(const RhsArgs& a, bool add_x, int krk, cudaStream_t st) {
         if constexpr (UNI) {
-            int rc = xpass(a, add_x, st);
-            if (rc || (rc = one<1, P_ADD>(a, 0, st))) return rc;
-            return one<2, P_STAGE>(a, krk, st);
+            int rc = xy(a, add_x, st);
+            return rc ? rc : one<2, P_STAGE>(a, krk, st);
         } else {
             return fail(WS_ERR_UNSUPPORTED, "stage update needs Cartesian metrics");
         }
     }
 
     // a batch: argument table g of n grids, woff = the three passes' work
-    // prefix tables of n + 1 entries each (x, y, z); krk 0: RHS into each du
-    template <int DIR, int MODE>
+    // prefix tables of n + 1 entries each (x, y, z); krk 0: RHS into each du;
+    // clo: some grid has a CLOSURE face
+    template <int DIR, int MODE, bool CLO = false>
     static int one_batch(const RhsArgs* g, const long* woff, int n, int krk, cudaStream_t st) {
         constexpr int W = MODE == P_STAGE ? SW : WPB;
         static int blocks[64] = {0};
-        return pencil_launch(pencil_batch_kernel<DIR, W, CT, MODE>, blocks, W * 32,
+        return pencil_launch(pencil_batch_kernel<DIR, W, CT, MODE, CLO>, blocks, W * 32,
                              MODE == P_STAGE ? SSMEM : SMEM, st, g, woff, n, krk);
     }
-    static int batch(const RhsArgs* g, const long* woff, int n, int krk, cudaStream_t st) {
-        int rc;
-        {
-            static int blocks[64] = {0};
-            rc = pencil_launch(pencil_x_coop_batch_kernel<XW, CT, P_STORE>, blocks, XW * 32,
+    template <bool CLO>
+    static int xy_batch(const RhsArgs* g, const long* woff, int n, cudaStream_t st) {
+        static int blocks[64] = {0};
+        int rc = pencil_launch(pencil_x_coop_batch_kernel<XW, CT, P_STORE, CLO>, blocks, XW * 32,
                                XSMEM, st, g, woff, n);
-        }
-        if (rc || (rc = one_batch<1, P_ADD>(g, woff + (n + 1), n, 0, st))) return rc;
+        return rc ? rc : one_batch<1, P_ADD, CLO>(g, woff + (n + 1), n, 0, st);
+    }
+    static int batch(const RhsArgs* g, const long* woff, int n, int krk, bool clo,
+                     cudaStream_t st) {
+        int rc = clo ? xy_batch<true>(g, woff, n, st) : xy_batch<false>(g, woff, n, st);
+        if (rc) return rc;
         if (!krk) return one_batch<2, P_ADD>(g, woff + 2 * (n + 1), n, 0, st);
         // the batched mixed stage pass (arguments read from global memory)
         // needs the registers of 8 warps per CTA

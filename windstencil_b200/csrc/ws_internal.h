@@ -130,7 +130,8 @@ int find_tile_cfg(int bx, int by, int threads);   // index or -1
 int default_cfg(int precision, bool stage);       // tuned default shape (stage kernel or plain RHS)
 
 // The RHS as three line passes x, y, z (pencil_impl.cuh), wpb warps per CTA
-// (0: the default), one CTA per SM; no CLOSURE faces.  krk 0: the RHS into
+// (0: the default), one CTA per SM; CLOSURE faces of the grid (a.clo) run the
+// x and y passes' closure instances.  krk 0: the RHS into
 // a.du; krk 1..3: the RHS into a.du, the z pass applying stage krk (a.f_in,
 // a.fn -> a.f_out, primitives to a.p_out).  add_x: a.du already holds terms
 // the RHS adds to (the viscous terms).
@@ -138,13 +139,14 @@ int launch_rhs_pencil(const RhsArgs& a, int precision, bool uniform, int wpb, in
                       bool add_x, cudaStream_t st);
 // The line passes over a batch: g the argument table of n Cartesian grids
 // (each with its du), woff the x, y and z passes' work prefix tables (n + 1
-// entries each, pencil_pass_work); krk as launch_rhs_pencil (no add_x).
+// entries each, pencil_pass_work); krk as launch_rhs_pencil (no add_x); clo:
+// some grid has a CLOSURE face (the x and y passes' closure instances).
 int launch_rhs_pencil_batch(const RhsArgs* g, const long* woff, int n, int precision, int krk,
-                            cudaStream_t st);
+                            bool clo, cudaStream_t st);
 long pencil_pass_work(const ws_grid& g, int dir);
 // Whether a launch with tile selection `tile` runs the line passes: an
 // explicit request (tile_x < 0, threads = 32 x warps per CTA or 0), or the
-// default (all zeros) for grids without CLOSURE faces.
+// default (all zeros); an explicit fused tile runs the fused kernel.
 bool use_pencil(const ws_grid* g, ws_tile tile);
 
 // Launch the fused RHS for one grid; cfg indexes the compiled tile shapes.
@@ -227,8 +229,8 @@ int grid_state_derive(GridState& s, cudaStream_t st);
 
 // A set of grids stepped together: one batched launch per kernel per stage.
 // The kernel a batch of these grids runs for tile selection `tile`: -1 for
-// the line passes (the default, unless a grid has CLOSURE faces; or asked for
-// by tile_x < 0), else a fused tile configuration (-2: not compiled).
+// the line passes (the default, or asked for by tile_x < 0), else a fused
+// tile configuration (-2: not compiled).
 int batch_kernel_cfg(const std::vector<GridState*>& grids, ws_tile tile);
 
 class BatchRunner {
