@@ -110,8 +110,9 @@ size_t vis_workspace_bytes(const ws_grid* g);
 int check_viscous(const ws_viscous* vis);
 int launch_du_vis(const ws_grid* g, const ws_viscous* vis, const ws_field prims[4],
                   const ws_metrics* m, ws_soa du, void* ws, bool accumulate, cudaStream_t st);
-// the same in two passes: fluxes (+ their ghost fill by the face kinds), then
-// the divergence; between them a slab's caller exchanges the x-direction
+// the same in two passes: fluxes (+ the ghosts the divergence reads: each
+// direction's fluxes along their own axis, by the face kinds), then the
+// divergence; between them a slab's caller exchanges the x-direction
 // fluxes' halos (EXTERNAL faces).  The workspace's 12 flux fields: direction
 // dir, component q at ev[4 * dir + q].
 void vis_flux_fields(const ws_grid* g, void* ws, ws_field ev[12]);
