@@ -441,6 +441,8 @@ def bench_slabs_one_gpu(a, torch, ws, wl, stream, parts=2):
             "slab_overhead": ms_slabs / ms_whole - 1.0,
             "halo_bytes_per_stage_per_face": ws.halo_x_bytes(g, halo.HALO_FIELDS),
             "device_status": status,
+            "stepper": "C++ (ws_blocks_step: decomposition, pack, exchange, unpack and "
+                       "stages in the library)",
             "note": "slabs: per stage per slab a halo pack and unpack per shared face, "
                     "ghost fill, fused RHS + stage; the exchange between GPUs (NCCL) is "
                     "not in this number"}

@@ -98,7 +98,8 @@ enum ws_status {
     WS_ERR_BUDGET = 7,      /* admission would exceed the HBM budget         */
     WS_ERR_BUSY = 8,        /* object in use / queue full                    */
     WS_ERR_NOT_FOUND = 9,   /* unknown request id                            */
-    WS_ERR_IO = 10          /* file missing, short or not in the expected format */
+    WS_ERR_IO = 10,         /* file missing, short or not in the expected format */
+    WS_ERR_COMM = 11        /* a communication library call (NCCL) failed       */
 };
 
 /* Grid and physics constants.  Replaces the reference's __constant__ set
@@ -375,6 +376,61 @@ WS_API int  ws_solver_load(ws_solver* s, const char* path, int32_t* istep, doubl
  * A grid with WS_FACE_EXTERNAL faces then steps with ws_solver_stage_begin /
  * _end. */
 WS_API int  ws_solver_set_viscous(ws_solver* s, const ws_viscous* vis);
+
+/* ------------------------------------------------------------------------ */
+/* One grid split into blocks, stepped from C++                              */
+/* ------------------------------------------------------------------------ */
+/* Block `index` of g split into dims[0] x dims[1] x dims[2] blocks, the
+ * reference's MPI decomposition: rank = px + NPX0 * (py + NPY0 * pz)
+ * (OCFD_mpi.c:102-121); per axis n / P cells, the first n % P blocks one
+ * wider (:124-145); neighbours wrapped on a periodic axis, none (-1) at the
+ * ends of another or on an axis in one part (:176-197).  Faces shared with a
+ * neighbour are WS_FACE_EXTERNAL.  An axis must be periodic at both faces or
+ * at neither; g has no EXTERNAL faces; a block needs 4 cells per axis (8
+ * with a CLOSURE face on it). */
+typedef struct ws_block_info {
+    int32_t index, coords[3], origin[3], n[3];
+    int32_t nbr[3][2];      /* neighbour block per axis, low / high side; -1: none */
+    int32_t faces[6];       /* the block grid's face kinds */
+} ws_block_info;
+WS_API int ws_blocks_decompose(const ws_grid* g, const int32_t dims[3], int32_t index,
+                               ws_block_info* out);
+
+/* A set of blocks stepped with SSP-RK3 from C++ (the time loop of
+ * OCFD_NS_Solver.cpp:64-90): before every stage the halos of the stage's
+ * primitives (d, u, v, w, T, cc) are packed on the device, exchanged and
+ * unpacked into the neighbours' ghost planes (exchange_boundary_{x,y,z}_
+ * packed_dev, OCFD_mpi_dev.cpp:123-290); with viscous terms each direction's
+ * four fluxes are exchanged the same way between the flux pass and the
+ * divergence.  Everything is enqueued on the caller's stream.
+ *   nccl_id NULL: every block of the grid lives in this process, on the
+ *     current device; a block's ghosts come straight from its neighbour's
+ *     packed planes (a single-GPU stand-in for a multi-GPU run).
+ *   nccl_id (ws_nccl_unique_id on one rank, passed to all): this process
+ *     owns block `rank` of a job of dims[0] x dims[1] x dims[2] ranks, one
+ *     per GPU (the current device); the packed planes go to the neighbours
+ *     with NCCL point-to-point sends, one group per exchange.  NCCL is loaded
+ *     at run time (libnccl.so.2, the one already in the process if any).
+ * Block states are read and written through each block's solver
+ * (ws_blocks_solver; the block's part of the global state, ws_block_info). */
+typedef struct ws_blocks ws_blocks;
+WS_API int  ws_nccl_unique_id(void* id /* 128 bytes */);
+WS_API int  ws_blocks_create(const ws_grid* g, const int32_t dims[3], const void* nccl_id,
+                             int32_t rank, ws_blocks** out);
+WS_API void ws_blocks_destroy(ws_blocks* b);
+/* blocks in this process, and their descriptions / solvers (owned by b) */
+WS_API int  ws_blocks_count(ws_blocks* b, int32_t* count);
+WS_API int  ws_blocks_info(ws_blocks* b, int32_t i, ws_block_info* out);
+WS_API int  ws_blocks_solver(ws_blocks* b, int32_t i, ws_solver** s);
+/* Navier-Stokes on every block (NULL: Euler); every rank makes the same call */
+WS_API int  ws_blocks_set_viscous(ws_blocks* b, const ws_viscous* vis);
+/* nsteps SSP-RK3 steps of dt; every rank makes the same calls */
+WS_API int  ws_blocks_step(ws_blocks* b, double dt, int nsteps, ws_stream_t stream);
+/* global CFL time step: the minimum over all blocks (NCCL all-reduce over
+ * the ranks); synchronises `stream` */
+WS_API int  ws_blocks_compute_dt(ws_blocks* b, double cfl, double* dt, ws_stream_t stream);
+/* the largest status word of this process's blocks; synchronises `stream` */
+WS_API int  ws_blocks_status(ws_blocks* b, int* status, ws_stream_t stream);
 
 /* ------------------------------------------------------------------------ */
 /* Many independent grids, device-resident, stepped together: per RK stage   */

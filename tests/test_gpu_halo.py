@@ -378,3 +378,74 @@ def test_distributed_blocks_gloo_match_whole_grid(cuda):
     s.close()
     assert all(m[0] == dt and m[1] == 0 for m in meta)
     assert np.array_equal(got, want), rel_linf(got, want).max()
+
+
+# -- the C++ stepper (ws_blocks_*) against the Python stage sequence ---------
+NATIVE_CASES = [
+    ("slabs_3", (70, 20, 10), (PE,) * 6, (3, 1, 1), None),
+    ("closure_2x2", (48, 40, 10), (CL, CL, CL, CL, PE, PE), (2, 2, 1), None),
+    ("ns_2x1x2", (48, 16, 24), (EX, EX, PE, PE, PE, PE), (2, 1, 2),
+     dict(re=200.0, pr=0.72, ref_t=288.15, scheme=8)),
+]
+
+
+@pytest.mark.parametrize("case", NATIVE_CASES, ids=[c[0] for c in NATIVE_CASES])
+def test_native_stepper_matches_python_sequence(cuda, case):
+    """halo.in_process runs the library's C++ stepper; the Python sequence
+    (native=False) over the same kernels gives the same bits."""
+    _, shape, faces, dims, vis = case
+    g = ws.Grid(*shape, faces=faces)
+    f0 = wl.fourier_state(*shape, seed=37)
+    out = []
+    for native in (True, False):
+        st = halo.in_process(g, dims=dims, native=native)
+        try:
+            st.set_viscous(vis)
+            st.set_state(f0)
+            dt = st.compute_dt(0.3)
+            st.step(dt, 2)
+            out.append((dt, halo.join_state(st.get_state(), [r.block for r in st.runners])))
+            assert st.status() == 0
+        finally:
+            st.close()
+    assert out[0][0] == out[1][0]
+    assert np.array_equal(out[0][1], out[1][1]), rel_linf(out[0][1], out[1][1]).max()
+
+
+def test_native_stepper_one_rank_nccl(cuda):
+    """The C++ stepper's NCCL mode with a one-rank communicator on this GPU
+    (its all-reduce of the time step; one block has no neighbour) against
+    the whole-grid solver."""
+    shape, faces = (40, 24, 16), (PE,) * 6
+    g = ws.Grid(*shape, faces=faces)
+    f0 = wl.sod_state(*shape, seed=41)
+    whole = ws.Solver(g)
+    whole.set_state(f0)
+    dt = whole.compute_dt(0.5)
+    whole.step(dt, 3)
+    want = whole.get_state()
+    whole.close()
+    st = halo.NativeBlocks(g, (1, 1, 1), halo.nccl_unique_id(), 0)
+    try:
+        st.set_state(f0)
+        assert st.compute_dt(0.5) == dt
+        st.step(dt, 3)
+        got = st.get_state()[0]
+        assert st.status() == 0
+    finally:
+        st.close()
+    assert np.array_equal(got, want)
+
+
+def test_native_stepper_rejects_bad_input(cuda):
+    g = ws.Grid(32, 16, 8)
+    with pytest.raises(ws.WsError):
+        halo.NativeBlocks(g, (2, 1, 1), halo.nccl_unique_id(), 5)     # rank >= 2
+    with pytest.raises(ws.WsError):
+        halo.NativeBlocks(ws.Grid(12, 8, 8), (4, 1, 1))               # 3-cell slabs
+    st = halo.NativeBlocks(g, (2, 1, 1))
+    try:
+        with pytest.raises(ws.WsError):
+            st.step(0.0, 1)
+    finally:
+        st.close()

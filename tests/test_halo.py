@@ -67,6 +67,34 @@ def test_decompose_rejects_thin_or_mixed():
         decompose(Grid(32, 8, 8, faces=(FACE_PERIODIC, FACE_EXTRAP) + (0,) * 4), 2)
 
 
+@pytest.mark.parametrize("dims", [(2, 1, 1), (4, 1, 1), (3, 2, 1), (2, 2, 2), (1, 3, 2), (1, 1, 1)])
+@pytest.mark.parametrize("faces", [(FACE_PERIODIC,) * 6,
+                                   (FACE_CLOSURE, FACE_EXTRAP, FACE_PERIODIC, FACE_PERIODIC,
+                                    FACE_EXTRAP, FACE_EXTRAP),
+                                   (FACE_EXTRAP, FACE_EXTRAP, FACE_CLOSURE, FACE_CLOSURE,
+                                    FACE_PERIODIC, FACE_PERIODIC)])
+def test_native_decomposition_matches(dims, faces):
+    """ws_blocks_decompose (the C++ stepper's split) equals decompose_blocks:
+    extents, neighbours, face kinds, block order."""
+    from windstencil_b200.halo import native_decompose
+    g = Grid(67, 33, 19, faces=faces)
+    assert native_decompose(g, dims) == decompose_blocks(g, dims)
+
+
+def test_native_decomposition_rejects_like_python():
+    from windstencil_b200.halo import native_decompose
+    bad = [(Grid(12, 8, 8, faces=(FACE_PERIODIC,) * 6), (4, 1, 1)),
+           (Grid(28, 8, 8, faces=(FACE_CLOSURE, FACE_EXTRAP) + (0,) * 4), (4, 1, 1)),
+           (Grid(32, 8, 8, faces=(FACE_PERIODIC, FACE_EXTRAP) + (0,) * 4), (2, 1, 1)),
+           (Grid(32, 8, 8, faces=(FACE_EXTERNAL, FACE_EXTRAP) + (0,) * 4), (2, 1, 1)),
+           (Grid(32, 8, 8), (0, 1, 1))]
+    for g, dims in bad:
+        with pytest.raises(ValueError):
+            decompose_blocks(g, dims)
+        with pytest.raises(WsError):
+            native_decompose(g, dims)
+
+
 def test_abi_halo_argument_checks():
     """Halo entry points validate their arguments before any device work."""
     from windstencil_b200 import _abi

@@ -21,7 +21,7 @@ FP64, MIXED = 0, 1
 WS_OK = 0
 ERRORS = {1: "WS_ERR_INVALID", 2: "WS_ERR_CUDA", 3: "WS_ERR_ALLOC", 4: "WS_ERR_UNSUPPORTED",
           5: "WS_ERR_NONFINITE", 6: "WS_ERR_TIMEOUT", 7: "WS_ERR_BUDGET", 8: "WS_ERR_BUSY",
-          9: "WS_ERR_NOT_FOUND", 10: "WS_ERR_IO"}
+          9: "WS_ERR_NOT_FOUND", 10: "WS_ERR_IO", 11: "WS_ERR_COMM"}
 
 
 class WsField(C.Structure):
@@ -57,6 +57,11 @@ class WsMetrics(C.Structure):
 class WsViscous(C.Structure):
     _fields_ = [("re", C.c_double), ("pr", C.c_double), ("ref_t", C.c_double),
                 ("scheme", C.c_int32), ("dummy0", C.c_int32), ("d0_bound", C.c_int32 * 6)]
+
+
+class WsBlockInfo(C.Structure):
+    _fields_ = [("index", C.c_int32), ("coords", C.c_int32 * 3), ("origin", C.c_int32 * 3),
+                ("n", C.c_int32 * 3), ("nbr", (C.c_int32 * 2) * 3), ("faces", C.c_int32 * 6)]
 
 
 class WsTile(C.Structure):
@@ -137,6 +142,19 @@ SIGNATURES = {
     "ws_du_vis_workspace_bytes": (C.c_size_t, [C.POINTER(WsGrid)]),
     "ws_du_vis_jacobian3d": (_I, [C.POINTER(WsGrid), C.POINTER(WsViscous)] + [WsField] * 4 +
                              [C.POINTER(WsMetrics), WsSoa, _P, C.c_size_t, _P]),
+    "ws_blocks_decompose": (_I, [C.POINTER(WsGrid), C.POINTER(C.c_int32), C.c_int32,
+                                 C.POINTER(WsBlockInfo)]),
+    "ws_nccl_unique_id": (_I, [_P]),
+    "ws_blocks_create": (_I, [C.POINTER(WsGrid), C.POINTER(C.c_int32), _P, C.c_int32,
+                              C.POINTER(_P)]),
+    "ws_blocks_destroy": (None, [_P]),
+    "ws_blocks_count": (_I, [_P, C.POINTER(C.c_int32)]),
+    "ws_blocks_info": (_I, [_P, C.c_int32, C.POINTER(WsBlockInfo)]),
+    "ws_blocks_solver": (_I, [_P, C.c_int32, C.POINTER(_P)]),
+    "ws_blocks_set_viscous": (_I, [_P, C.POINTER(WsViscous)]),
+    "ws_blocks_step": (_I, [_P, C.c_double, _I, _P]),
+    "ws_blocks_compute_dt": (_I, [_P, C.c_double, C.POINTER(C.c_double), _P]),
+    "ws_blocks_status": (_I, [_P, C.POINTER(_I), _P]),
     "ws_batch_create": (_I, [C.POINTER(WsGrid), _I, C.POINTER(_P)]),
     "ws_batch_destroy": (None, [_P]),
     "ws_batch_size": (_I, [_P]),

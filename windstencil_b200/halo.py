@@ -35,13 +35,18 @@ viscous fluxes between their flux pass and their divergence, as the
 reference exchanges Ev1..4 between vis_flux_ker and their derivatives
 (OCFD_Stream.cpp:229-345).
 
-This module holds the decomposition, the exchange and the stage sequence;
-the per-block kernels live in libwindstencil_b200.so (CudaBlock).  Anything
-with CudaBlock's methods can stand in for it (the CPU tests run the oracle
-that way over gloo ranks).
+The stage sequence exists twice.  NativeBlocks drives the C++ stepper of
+libwindstencil_b200.so (ws_blocks_*: decomposition, pack, exchange, unpack
+and stages in C++; blocks in one process read each other's packs, blocks on
+separate GPUs exchange through NCCL loaded by the library).  SlabStepper is
+the same sequence in Python over CudaBlock runners and an exchange object;
+anything with CudaBlock's methods can stand in for a block (the CPU tests run
+the oracle that way over gloo ranks), and DistExchange moves the packs with
+torch.distributed.
 """
 from __future__ import annotations
 
+import ctypes as C
 import dataclasses
 from dataclasses import dataclass
 
@@ -49,6 +54,7 @@ import numpy as np
 
 from . import (FACE_CLOSURE, FACE_EXTERNAL, FACE_PERIODIC, Grid, Solver, halo_bytes, halo_pack,
                halo_unpack)
+from . import _abi
 
 HALO_FIELDS = 6          # d, u, v, w, T, cc
 FLUX_FIELDS = 4          # one direction's viscous fluxes Ev1..4
@@ -442,23 +448,167 @@ class SlabStepper:
 BlockStepper = SlabStepper
 
 
-def in_process(grid: Grid, parts=None, dims=None) -> SlabStepper:
+def in_process(grid: Grid, parts=None, dims=None, native: bool = True):
     """All blocks on the current CUDA device (a single-GPU stand-in for a
     multi-GPU run: same kernels, same halos, no waits between blocks):
-    `parts` x slabs, or a dims[0] x dims[1] x dims[2] process grid."""
-    dims = dims if dims is not None else (parts, 1, 1)
+    `parts` x slabs, or a dims[0] x dims[1] x dims[2] process grid.  native:
+    the library's C++ stepper (NativeBlocks), else the Python sequence."""
+    dims = tuple(dims) if dims is not None else (parts, 1, 1)
+    if native:
+        return NativeBlocks(grid, dims)
     return SlabStepper([CudaBlock(grid, b) for b in decompose_blocks(grid, dims)],
                        LocalExchange())
 
 
-def distributed(grid: Grid, group=None, dims=None) -> SlabStepper:
+def distributed(grid: Grid, group=None, dims=None, native: bool = False):
     """This rank's block of `grid` split over the ranks of `group` (one GPU
     per rank, the current CUDA device): x slabs, or `dims` whose product is
-    the group size."""
+    the group size.  native: the library's C++ stepper over its own NCCL
+    communicator (the id travels over `group`; NCCL ranks = group ranks),
+    else the Python sequence over torch.distributed."""
     import torch.distributed as dist
     world = dist.get_world_size(group)
     dims = tuple(dims) if dims is not None else (world, 1, 1)
     if dims[0] * dims[1] * dims[2] != world:
         raise ValueError(f"dims {dims} do not match {world} ranks")
-    block = decompose_blocks(grid, dims)[dist.get_rank(group)]
+    rank = dist.get_rank(group)
+    if native:
+        box = [nccl_unique_id() if rank == 0 else None]
+        dist.broadcast_object_list(box, src=dist.get_global_rank(group, 0) if group else 0,
+                                   group=group)
+        return NativeBlocks(grid, dims, box[0], rank)
+    block = decompose_blocks(grid, dims)[rank]
     return SlabStepper([CudaBlock(grid, block)], DistExchange(group))
+
+
+# ---- the C++ stepper ---------------------------------------------------------
+
+def _block_of(info, dims) -> Block:
+    nbr = tuple(tuple(None if info.nbr[ax][sd] < 0 else int(info.nbr[ax][sd])
+                      for sd in (LO, HI)) for ax in range(3))
+    return Block(int(info.index), tuple(dims), tuple(info.coords), tuple(info.origin),
+                 tuple(info.n), nbr, tuple(info.faces))
+
+
+def native_decompose(grid: Grid, dims) -> list[Block]:
+    """The library's decomposition (ws_blocks_decompose) of `grid` into
+    dims[0] x dims[1] x dims[2] blocks."""
+    from . import check, load
+    d = (C.c_int32 * 3)(*dims)
+    gc = grid.c()
+    out = []
+    for i in range(max(1, d[0] * d[1] * d[2])):      # index 0 also checks dims
+        info = _abi.WsBlockInfo()
+        check(load().ws_blocks_decompose(C.byref(gc), d, i, C.byref(info)))
+        out.append(_block_of(info, dims))
+    return out
+
+
+class _BlockSolver(Solver):
+    """A block's ws_solver, owned by the ws_blocks object."""
+
+    def __init__(self, g: Grid, handle):
+        self.g = g
+        self._gc = g.c()
+        self.h = handle
+
+    def close(self):
+        self.h = None
+
+
+class NativeRunner:
+    """One block of a NativeBlocks stepper in this process."""
+
+    def __init__(self, grid: Grid, block: Block, handle):
+        self.block = self.slab = block
+        self.grid = block_grid(grid, block)
+        self.solver = _BlockSolver(self.grid, handle)
+
+    def set_state(self, f_block: np.ndarray) -> None:
+        self.solver.set_state(f_block)
+
+    def get_state(self) -> np.ndarray:
+        return self.solver.get_state()
+
+
+class NativeBlocks:
+    """SSP-RK3 steps of `grid` split into dims[0] x dims[1] x dims[2] blocks,
+    stepped by the library's C++ stepper (ws_blocks_*).  nccl_id None: every
+    block in this process on the current device; else this process owns
+    block `rank` and exchanges with the other ranks over NCCL."""
+
+    def __init__(self, grid: Grid, dims, nccl_id: bytes | None = None, rank: int = 0):
+        from . import check, load
+        self.grid = grid
+        self.dims = tuple(int(v) for v in dims)
+        self._gc = grid.c()
+        d = (C.c_int32 * 3)(*self.dims)
+        h = C.c_void_p()
+        idbuf = None
+        if nccl_id is not None:
+            idbuf = C.create_string_buffer(bytes(nccl_id), 128)
+        check(load().ws_blocks_create(C.byref(self._gc), d, idbuf, int(rank), C.byref(h)))
+        self.h = h
+        n = C.c_int32()
+        check(load().ws_blocks_count(self.h, C.byref(n)))
+        self.runners = []
+        for i in range(n.value):
+            info = _abi.WsBlockInfo()
+            check(load().ws_blocks_info(self.h, i, C.byref(info)))
+            sh = C.c_void_p()
+            check(load().ws_blocks_solver(self.h, i, C.byref(sh)))
+            self.runners.append(NativeRunner(grid, _block_of(info, self.dims), sh))
+        self.viscous = False
+
+    def set_viscous(self, vis) -> None:
+        from . import check, load, viscous
+        if vis is None:
+            check(load().ws_blocks_set_viscous(self.h, None))
+        else:
+            v = vis if isinstance(vis, _abi.WsViscous) else viscous(**vis)
+            check(load().ws_blocks_set_viscous(self.h, C.byref(v)))
+        self.viscous = vis is not None
+
+    def step(self, dt: float, nsteps: int = 1, stream=None) -> None:
+        from . import _stream, check, load
+        check(load().ws_blocks_step(self.h, dt, nsteps, _stream(stream)))
+
+    def compute_dt(self, cfl: float, stream=None) -> float:
+        from . import _stream, check, load
+        dt = C.c_double()
+        check(load().ws_blocks_compute_dt(self.h, cfl, C.byref(dt), _stream(stream)))
+        return dt.value
+
+    def set_state(self, f_global: np.ndarray) -> None:
+        for r in self.runners:
+            r.set_state(split_state(f_global, r.block))
+
+    def get_state(self) -> list[np.ndarray]:
+        """This process's blocks' states, in block order."""
+        return [r.get_state() for r in self.runners]
+
+    def status(self, stream=None) -> int:
+        from . import _stream, check, load
+        s = C.c_int()
+        check(load().ws_blocks_status(self.h, C.byref(s), _stream(stream)))
+        return s.value
+
+    def close(self) -> None:
+        from . import load
+        if self.h:
+            load().ws_blocks_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def nccl_unique_id() -> bytes:
+    """A new NCCL communicator id (ws_nccl_unique_id), for NativeBlocks."""
+    from . import check, load
+    buf = C.create_string_buffer(128)
+    check(load().ws_nccl_unique_id(buf))
+    return buf.raw
