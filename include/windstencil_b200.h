@@ -415,6 +415,17 @@ WS_API int ws_blocks_decompose(const ws_grid* g, const int32_t dims[3], int32_t 
  * (ws_blocks_solver; the block's part of the global state, ws_block_info). */
 typedef struct ws_blocks ws_blocks;
 WS_API int  ws_nccl_unique_id(void* id /* 128 bytes */);
+/* The point-to-point messages block `index` posts in one exchange over
+ * NCCL, in posting order (kind 0 send of the planes next to face (axis,
+ * side), 1 receive into the ghosts beyond it; peer = block index): per axis
+ * the low planes' send, the high planes' send, the high ghosts' receive,
+ * the low ghosts' receive.  NCCL matches two ranks' messages in order, so
+ * every send lands in the ghosts it was packed for, a two-block periodic
+ * ring included.  *count = the number of messages (at most 12; ops holds the
+ * first cap). */
+typedef struct ws_p2p_op { int32_t kind, peer, axis, side; } ws_p2p_op;
+WS_API int  ws_blocks_exchange_plan(const ws_grid* g, const int32_t dims[3], int32_t index,
+                                    ws_p2p_op* ops, int32_t cap, int32_t* count);
 WS_API int  ws_blocks_create(const ws_grid* g, const int32_t dims[3], const void* nccl_id,
                              int32_t rank, ws_blocks** out);
 WS_API void ws_blocks_destroy(ws_blocks* b);

@@ -95,6 +95,39 @@ def test_native_decomposition_rejects_like_python():
             native_decompose(g, dims)
 
 
+@pytest.mark.parametrize("dims", [(2, 1, 1), (3, 1, 1), (2, 2, 1), (2, 2, 2), (1, 2, 3),
+                                  (4, 1, 2)])
+@pytest.mark.parametrize("periodic", [True, False])
+def test_native_nccl_plan_matches_in_order(dims, periodic):
+    """The C++ stepper's NCCL exchange posts each rank's messages in
+    ws_blocks_exchange_plan's order, and NCCL matches the messages between
+    two ranks in posting order.  Simulated over all ranks: every send finds a
+    receive, and the k-th send from a to b (planes next to face (axis, s))
+    meets the k-th receive at b from a, which fills the ghosts beyond face
+    (axis, 1 - s) -- the neighbour's opposite face -- along the same axis;
+    each shared face is received exactly once."""
+    from windstencil_b200.halo import native_exchange_plan
+    k = FACE_PERIODIC if periodic else FACE_EXTRAP
+    g = Grid(48, 40, 32, faces=(k,) * 6)
+    blocks = decompose_blocks(g, dims)
+    plans = [native_exchange_plan(g, dims, b.index) for b in blocks]
+    sends, recvs = {}, {}
+    for a, plan in enumerate(plans):
+        for kind, peer, axis, side in plan:
+            (sends if kind == "send" else recvs).setdefault((a, peer) if kind == "send"
+                                                            else (peer, a), []).append((axis, side))
+    assert sends.keys() == recvs.keys()
+    for (a, b), out in sends.items():
+        into = recvs[(a, b)]
+        assert len(out) == len(into)
+        for (ax_s, s), (ax_r, r) in zip(out, into):
+            assert ax_s == ax_r and r == 1 - s
+            assert blocks[a].nbr[ax_s][s] == b and blocks[b].nbr[ax_r][r] == a
+    for b, plan in zip(blocks, plans):
+        got = sorted((ax, sd) for kind, _, ax, sd in plan if kind == "recv")
+        assert got == sorted((ax, sd) for ax in range(3) for sd in b.sides(ax))
+
+
 def test_abi_halo_argument_checks():
     """Halo entry points validate their arguments before any device work."""
     from windstencil_b200 import _abi

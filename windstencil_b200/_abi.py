@@ -64,6 +64,11 @@ class WsBlockInfo(C.Structure):
                 ("n", C.c_int32 * 3), ("nbr", (C.c_int32 * 2) * 3), ("faces", C.c_int32 * 6)]
 
 
+class WsP2pOp(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("peer", C.c_int32), ("axis", C.c_int32),
+                ("side", C.c_int32)]
+
+
 class WsTile(C.Structure):
     _fields_ = [("tile_x", C.c_int32), ("tile_y", C.c_int32), ("scan_z", C.c_int32),
                 ("threads", C.c_int32)]
@@ -145,6 +150,8 @@ SIGNATURES = {
     "ws_blocks_decompose": (_I, [C.POINTER(WsGrid), C.POINTER(C.c_int32), C.c_int32,
                                  C.POINTER(WsBlockInfo)]),
     "ws_nccl_unique_id": (_I, [_P]),
+    "ws_blocks_exchange_plan": (_I, [C.POINTER(WsGrid), C.POINTER(C.c_int32), C.c_int32,
+                                     C.POINTER(WsP2pOp), C.c_int32, C.POINTER(C.c_int32)]),
     "ws_blocks_create": (_I, [C.POINTER(WsGrid), C.POINTER(C.c_int32), _P, C.c_int32,
                               C.POINTER(_P)]),
     "ws_blocks_destroy": (None, [_P]),

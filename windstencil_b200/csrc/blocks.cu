@@ -85,6 +85,33 @@ int nccl_fail(ncclResult_t r, const char* what) {
         if (r_ != ncclSuccess) return nccl_fail(r_, #call);        \
     } while (0)
 
+}  // namespace
+
+// The point-to-point messages of one exchange of a block, in the order they
+// are posted (one NCCL group): per axis, the send of the low planes, the
+// send of the high planes, the receive of the high ghosts, the receive of
+// the low ghosts.  NCCL matches the messages between two ranks in order, so
+// with a two-block periodic ring (the same peer on both sides) the first
+// message from the peer (its low planes) lands in the high ghosts and the
+// second in the low ones; every rank walks the axes in the same order.
+int exchange_plan(const ws_block_info& b, ws_p2p_op* ops, int cap) {
+    int n = 0;
+    auto put = [&](int kind, int peer, int axis, int side) {
+        if (n < cap) ops[n] = ws_p2p_op{kind, peer, axis, side};
+        ++n;
+    };
+    for (int ax = 0; ax < 3; ++ax) {
+        const int lo = b.nbr[ax][0], hi = b.nbr[ax][1];
+        if (lo >= 0) put(0, lo, ax, 0);
+        if (hi >= 0) put(0, hi, ax, 1);
+        if (hi >= 0) put(1, hi, ax, 1);
+        if (lo >= 0) put(1, lo, ax, 0);
+    }
+    return n;
+}
+
+namespace {
+
 // (first cell, cells) of part k of an axis of n cells split in P parts: the
 // first n % P parts one cell wider (OCFD_mpi.c:124-145)
 void part_extent(int n, int P, int k, int& first, int& cells) {
@@ -276,12 +303,8 @@ int exchange_local(ws_blocks* b, HaloKind kind, cudaStream_t st) {
     return WS_OK;
 }
 
-// One block per rank: pack every shared face, post all sends and receives
-// as one NCCL group, unpack.  Per axis the sends go low planes first and the
-// receives take the high ghosts first, so that with a two-block periodic
-// ring (the same peer on both sides) the k-th message from a peer lands in
-// the ghosts it was packed for (NCCL matches a pair's messages in order);
-// every rank walks the axes in the same order.
+// One block per rank: pack every shared face, post the sends and receives
+// of exchange_plan as one NCCL group, unpack.
 int exchange_nccl(ws_blocks* b, HaloKind kind, cudaStream_t st) {
     LocalBlock& l = b->blk[0];
     ws_field f[3][kPrimFields];
@@ -300,19 +323,16 @@ int exchange_nccl(ws_blocks* b, HaloKind kind, cudaStream_t st) {
                 return rc;
     }
     if (!any) return WS_OK;
+    ws_p2p_op ops[12];
+    const int nops = exchange_plan(l.info, ops, 12);
     Nccl& n = nccl();
     WS_NCCL(n.group_start());
     ncclResult_t r = ncclSuccess;
-    for (int ax = 0; ax < 3 && r == ncclSuccess; ++ax) {
-        const int lo = l.info.nbr[ax][0], hi = l.info.nbr[ax][1];
-        if (lo >= 0 && r == ncclSuccess)
-            r = n.send(l.send[ax][0], count[ax], ncclFloat64, lo, b->comm, st);
-        if (hi >= 0 && r == ncclSuccess)
-            r = n.send(l.send[ax][1], count[ax], ncclFloat64, hi, b->comm, st);
-        if (hi >= 0 && r == ncclSuccess)
-            r = n.recv(l.recv[ax][1], count[ax], ncclFloat64, hi, b->comm, st);
-        if (lo >= 0 && r == ncclSuccess)
-            r = n.recv(l.recv[ax][0], count[ax], ncclFloat64, lo, b->comm, st);
+    for (int i = 0; i < nops && r == ncclSuccess; ++i) {
+        const ws_p2p_op& o = ops[i];
+        r = o.kind == 0
+                ? n.send(l.send[o.axis][o.side], count[o.axis], ncclFloat64, o.peer, b->comm, st)
+                : n.recv(l.recv[o.axis][o.side], count[o.axis], ncclFloat64, o.peer, b->comm, st);
     }
     const ncclResult_t re = n.group_end();       // closes the group in every case
     if (r != ncclSuccess) return nccl_fail(r, "ncclSend / ncclRecv");
@@ -350,6 +370,15 @@ extern "C" {
 int ws_blocks_decompose(const ws_grid* g, const int32_t dims[3], int32_t index,
                         ws_block_info* out) {
     return decompose_block(g, dims, index, out);
+}
+
+int ws_blocks_exchange_plan(const ws_grid* g, const int32_t dims[3], int32_t index,
+                            ws_p2p_op* ops, int32_t cap, int32_t* count) {
+    if (!count || (cap > 0 && !ops)) return fail(WS_ERR_INVALID, "NULL argument");
+    ws_block_info b{};
+    if (int rc = decompose_block(g, dims, index, &b)) return rc;
+    *count = exchange_plan(b, ops, cap);
+    return WS_OK;
 }
 
 int ws_nccl_unique_id(void* id) {

@@ -504,6 +504,19 @@ def native_decompose(grid: Grid, dims) -> list[Block]:
     return out
 
 
+def native_exchange_plan(grid: Grid, dims, index: int) -> list[tuple]:
+    """The messages block `index` posts in one NCCL exchange of the C++
+    stepper (ws_blocks_exchange_plan), in order: (kind "send" / "recv",
+    peer block, axis, side)."""
+    from . import check, load
+    d = (C.c_int32 * 3)(*dims)
+    gc = grid.c()
+    ops = (_abi.WsP2pOp * 12)()
+    n = C.c_int32()
+    check(load().ws_blocks_exchange_plan(C.byref(gc), d, index, ops, 12, C.byref(n)))
+    return [("send" if o.kind == 0 else "recv", o.peer, o.axis, o.side) for o in ops[:n.value]]
+
+
 class _BlockSolver(Solver):
     """A block's ws_solver, owned by the ws_blocks object."""
 
