@@ -88,6 +88,10 @@ def parse():
                     help="process group of --gpus N > 1; gloo stages the halos through "
                          "host memory, so ranks may share a GPU (a test of the "
                          "multi-rank path on one device)")
+    ap.add_argument("--halo", default="torch", choices=["torch", "native"],
+                    help="with --gpus N > 1: the stage sequence in Python with the halos "
+                         "over torch.distributed (torch), or the library's C++ stepper "
+                         "with its own NCCL communicator (native; needs --backend nccl)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--batch-grids", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=50)
@@ -702,7 +706,9 @@ def run_ours(a, rank, world, dist):
         dims = process_dims(a, world)
         gg = ws.Grid(a.nx * dims[0], a.ny * dims[1], a.nz * dims[2], faces=faces)
         with torch.cuda.stream(stream):
-            stepper = halo.distributed(gg, dims=dims)
+            if a.halo == "native" and a.backend != "nccl":
+                raise SystemExit("--halo native needs --backend nccl (one GPU per rank)")
+            stepper = halo.distributed(gg, dims=dims, native=a.halo == "native")
             runner = stepper.runners[0]
             runner.set_state(f0)
             dt = stepper.compute_dt(0.5)
@@ -832,9 +838,11 @@ def run_ours(a, rank, world, dist):
                 "gpu_launches": launches_per_step * a.steps, "clocks": clk.summary(),
                 "device_status": status}
         if world > 1:
-            line["halo_transport"] = ("NCCL point-to-point, device buffers"
-                                      if a.backend == "nccl"
-                                      else "gloo, staged through pinned host memory")
+            line["halo_transport"] = (
+                "NCCL point-to-point, device buffers, stage sequence in C++ (ws_blocks_step)"
+                if a.halo == "native" else
+                "NCCL point-to-point, device buffers, stage sequence in Python"
+                if a.backend == "nccl" else "gloo, staged through pinned host memory")
         line.update(extra)
         print(json.dumps(line), flush=True)
 
