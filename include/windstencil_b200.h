@@ -321,6 +321,12 @@ WS_API void ws_solver_destroy(ws_solver* s);
 WS_API int  ws_solver_set_state(ws_solver* s, const double* f_host, ws_stream_t stream);
 /* Downloads the conserved state; synchronises `stream`. */
 WS_API int  ws_solver_get_state(ws_solver* s, double* f_host, ws_stream_t stream);
+/* The same download, only enqueued on `stream` (the host does not wait): f_host
+ * must stay valid, and is complete, once the stream has passed the copy (the
+ * caller synchronises).  With pinned f_host the copy runs on a copy engine
+ * beside kernels of other streams, so a caller with several solvers can
+ * overlap one's transfers with another's steps. */
+WS_API int  ws_solver_get_state_async(ws_solver* s, double* f_host, ws_stream_t stream);
 /* Downloads du of the last ws_solver_rhs() (a step uses du as its
  * accumulator, so read it before stepping); synchronises `stream`. */
 WS_API int  ws_solver_get_rhs(ws_solver* s, double* du_host, ws_stream_t stream);

@@ -147,3 +147,40 @@ def test_c_sequence_extrap_x(oracle, cuda):
     out, _, flags = _c_time_loop(cuda, g, f0, dt, 4)
     assert flags == 0
     assert rel_linf(out, oracle.rk3_steps(og, f0, dt, 4)).max() <= TOL
+
+
+def test_get_state_async_matches_get_state(cuda):
+    """ws_solver_get_state_async enqueues the download only: after the
+    caller synchronises the stream, the pinned buffer holds the same state as
+    ws_solver_get_state's; two solvers on two streams, stepped in turn with
+    their downloads in flight, give the states they give alone."""
+    shape = (40, 24, 16)
+    g = ws.Grid(*shape, faces=(ws.FACE_EXTRAP, ws.FACE_EXTRAP, 0, 0, 0, 0))
+    f0 = wl.sod_state(*shape, seed=43)
+    lib = ws.load()
+    ref = ws.Solver(g)
+    ref.set_state(f0)
+    dt = ref.compute_dt(0.5)
+    ref.step(dt, 2)
+    want = ref.get_state()
+    ref.close()
+    streams = [cuda.cuda.Stream(), cuda.cuda.Stream()]
+    solvers = [ws.Solver(g), ws.Solver(g)]
+    inp = cuda.from_numpy(np.ascontiguousarray(f0)).pin_memory()
+    outs = [cuda.empty(f0.shape, dtype=cuda.float64).pin_memory() for _ in range(2)]
+    try:
+        for k in (0, 1):
+            ws.check(lib.ws_solver_set_state(solvers[k].h, inp.numpy().ctypes.data,
+                                             streams[k].cuda_stream))
+            solvers[k].step(dt, 2, stream=streams[k])
+            ws.check(lib.ws_solver_get_state_async(solvers[k].h, outs[k].numpy().ctypes.data,
+                                                   streams[k].cuda_stream))
+        for st in streams:
+            st.synchronize()
+        for k in (0, 1):
+            assert np.array_equal(outs[k].numpy(), want)
+        with pytest.raises(ws.WsError):
+            ws.check(lib.ws_solver_get_state_async(solvers[0].h, None, None))
+    finally:
+        for s in solvers:
+            s.close()

@@ -123,6 +123,7 @@ SIGNATURES = {
     "ws_solver_destroy": (None, [_P]),
     "ws_solver_set_state": (_I, [_P, _P, _P]),
     "ws_solver_get_state": (_I, [_P, _P, _P]),
+    "ws_solver_get_state_async": (_I, [_P, _P, _P]),
     "ws_solver_get_rhs": (_I, [_P, _P, _P]),
     "ws_solver_fields": (_I, [_P, C.POINTER(WsSoa), C.POINTER(WsSoa), C.POINTER(WsField)]),
     "ws_solver_compute_dt": (_I, [_P, C.c_double, C.POINTER(C.c_double), _P]),

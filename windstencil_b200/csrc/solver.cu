@@ -250,6 +250,11 @@ int ws_solver_get_state(ws_solver* s, double* f_host, ws_stream_t stream) {
     return WS_OK;
 }
 
+int ws_solver_get_state_async(ws_solver* s, double* f_host, ws_stream_t stream) {
+    if (!s || !f_host) return fail(WS_ERR_INVALID, "NULL argument");
+    return grid_state_download(s->s, f_host, (cudaStream_t)stream);
+}
+
 int ws_solver_get_rhs(ws_solver* s, double* du_host, ws_stream_t stream) {
     if (!s || !du_host) return fail(WS_ERR_INVALID, "NULL argument");
     cudaStream_t st = (cudaStream_t)stream;
