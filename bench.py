@@ -678,37 +678,42 @@ def max_over_ranks(torch, dist, x):
     return float(t.item())
 
 
-def pipelined_e2e(a, torch, ws, g, f0, dt, host, cells, n_steps):
-    """The e2e leg with the transfers overlapped: two solvers on two streams
-    take the steps in turn; each step uploads its input state from pinned
-    host memory (ws_solver_set_state), takes one SSP-RK3 step and downloads
-    its result into its own pinned buffer (ws_solver_get_state_async), so one
-    solver's upload and download run on the copy engines while the other
-    steps.  Every step still moves its whole state both ways."""
+def pipelined_e2e(a, torch, ws, g, f0, dt, host, cells, n_steps, nsolv=3):
+    """The e2e leg with the transfers overlapped: nsolv solvers on their own
+    streams take the steps in turn; each step uploads its input state from
+    pinned host memory (ws_solver_set_state), takes one SSP-RK3 step and
+    downloads its result into its solver's pinned buffer
+    (ws_solver_get_state_async), so the solvers' uploads and downloads run on
+    the copy engines while another steps (per stream the three are in series,
+    hence more than two solvers).  Every step still moves its whole state
+    both ways."""
     lib = ws.load()
-    st = [torch.cuda.Stream(), torch.cuda.Stream()]
-    solvers = [ws.Solver(g), ws.Solver(g)]
-    outs = [torch.empty_like(host).pin_memory() for _ in range(2)]
+    st = [torch.cuda.Stream() for _ in range(nsolv)]
+    solvers = [ws.Solver(g) for _ in range(nsolv)]
+    outs = [torch.empty_like(host).pin_memory() for _ in range(nsolv)]
     inp = host.numpy().ctypes.data
     try:
         def one(i):
-            k = i % 2
+            k = i % nsolv
             ws._abi.check(lib.ws_solver_set_state(solvers[k].h, inp, st[k].cuda_stream))
             solvers[k].step(dt, 1, stream=st[k])
             ws._abi.check(lib.ws_solver_get_state_async(
                 solvers[k].h, outs[k].numpy().ctypes.data, st[k].cuda_stream))
-        for i in range(2):          # graphs captured, buffers touched
+        for i in range(nsolv):      # graphs captured, buffers touched
             one(i)
         torch.cuda.synchronize()
         q0, q1 = _events(torch)
-        qb = torch.cuda.Event()
         w0 = time.perf_counter()
         q0.record(st[0])
-        st[1].wait_event(q0)
-        for i in range(2 * n_steps):
+        for x in st[1:]:
+            x.wait_event(q0)
+        steps = nsolv * n_steps
+        for i in range(steps):
             one(i)
-        qb.record(st[1])
-        st[0].wait_event(qb)
+        for x in st[1:]:
+            qb = torch.cuda.Event()
+            qb.record(x)
+            st[0].wait_event(qb)
         q1.record(st[0])
         q1.synchronize()
         wall = time.perf_counter() - w0
@@ -717,14 +722,14 @@ def pipelined_e2e(a, torch, ws, g, f0, dt, host, cells, n_steps):
     finally:
         for s in solvers:
             s.close()
-    return {"value": cells * 3 * 2 * n_steps / (ms * 1e-3) / 1e9, "steps": 2 * n_steps,
-            "wall_s": wall, "pipelined": True, "device_status_ok": ok,
-            "note": "two solvers on two streams take the steps in turn; every step: its "
+    return {"value": cells * 3 * steps / (ms * 1e-3) / 1e9, "steps": steps,
+            "wall_s": wall, "pipelined": True, "solvers": nsolv, "device_status_ok": ok,
+            "note": f"{nsolv} solvers on their own streams take the steps in turn; every step: its "
                     "input state pinned host -> device (ws_solver_set_state), one SSP-RK3 "
                     "step, its result device -> its own pinned host buffer "
-                    "(ws_solver_get_state_async); one solver's transfers overlap the "
-                    "other's step. serial_value: the same with one solver, each step "
-                    "waiting for its download"}
+                    "(ws_solver_get_state_async); one solver's transfers overlap another's "
+                    "step. serial_value: the same with one solver, each step waiting for "
+                    "its download"}
 
 
 def run_ours(a, rank, world, dist):
