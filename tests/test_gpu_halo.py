@@ -449,3 +449,28 @@ def test_native_stepper_rejects_bad_input(cuda):
             st.step(0.0, 1)
     finally:
         st.close()
+
+
+@pytest.mark.parametrize("nccl", [False, True])
+def test_native_stepper_dt_failure_is_collective(cuda, nccl):
+    """A non-finite state makes ws_blocks_compute_dt fail; in NCCL mode the
+    failing rank still takes the all-reduce (so no other rank would wait in
+    it for good) and the communicator serves the next call."""
+    shape = (32, 16, 8)
+    g = ws.Grid(*shape)
+    f0 = wl.fourier_state(*shape, seed=47)
+    bad = f0.copy()
+    bad[4, 3, 5, 7] = np.nan
+    st = (halo.NativeBlocks(g, (1, 1, 1), halo.nccl_unique_id(), 0) if nccl
+          else halo.NativeBlocks(g, (2, 1, 1)))
+    try:
+        st.set_state(bad)
+        with pytest.raises(ws.WsError):
+            st.compute_dt(0.5)
+        st.set_state(f0)
+        whole = ws.Solver(g)
+        whole.set_state(f0)
+        assert st.compute_dt(0.5) == whole.compute_dt(0.5)
+        whole.close()
+    finally:
+        st.close()

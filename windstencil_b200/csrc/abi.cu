@@ -18,6 +18,7 @@ namespace ws {
 static thread_local std::string g_last_error;
 
 void set_error(const std::string& msg) { g_last_error = msg; }
+std::string last_error_message() { return g_last_error; }
 int fail(int code, const std::string& msg) {
     g_last_error = msg;
     return code;

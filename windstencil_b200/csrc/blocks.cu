@@ -488,18 +488,28 @@ int ws_blocks_compute_dt(ws_blocks* b, double cfl, double* dt, ws_stream_t strea
     if (!b || !dt) return fail(WS_ERR_INVALID, "NULL argument");
     double m = 0.0;
     bool first = true;
+    int rc = WS_OK;
     for (auto& l : b->blk) {
         double d = 0.0;
-        if (int rc = ws_solver_compute_dt(l.s, cfl, &d, stream)) return rc;
+        if ((rc = ws_solver_compute_dt(l.s, cfl, &d, stream))) break;
         m = first ? d : std::min(m, d);
         first = false;
     }
     if (b->comm) {
+        // every rank takes the all-reduce, also after a local failure (which
+        // contributes -1), so that no rank waits in it for good; then all of
+        // them return an error
+        const std::string local_error = rc ? last_error_message() : std::string();
+        if (rc) m = -1.0;
         cudaStream_t st = (cudaStream_t)stream;
         WS_CUDA(cudaMemcpyAsync(b->d_min, &m, sizeof m, cudaMemcpyHostToDevice, st));
         WS_NCCL(nccl().all_reduce(b->d_min, b->d_min, 1, ncclFloat64, ncclMin, b->comm, st));
         WS_CUDA(cudaMemcpyAsync(&m, b->d_min, sizeof m, cudaMemcpyDeviceToHost, st));
         WS_CUDA(cudaStreamSynchronize(st));
+        if (rc) return fail(rc, local_error);
+        if (!(m > 0)) return fail(WS_ERR_NONFINITE, "another rank's time step failed");
+    } else if (rc) {
+        return rc;
     }
     *dt = m;
     return WS_OK;

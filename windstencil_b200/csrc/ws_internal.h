@@ -39,6 +39,7 @@ int launch_halo(const ws_grid* g, const ws_field* f, int nf, int axis, int side,
 
 // Error reporting: the message of the last failure, per host thread.
 void set_error(const std::string& msg);
+std::string last_error_message();       // this thread's last failure message
 int fail(int code, const std::string& msg);
 int cuda_fail(cudaError_t e, const char* what);
 #define WS_CUDA(call)                                        \
