@@ -289,6 +289,50 @@ def test_gloo_ranks_match_whole_grid(oracle, case):
     assert np.array_equal(got, want)
 
 
+def _dt_failure_rank_main(rank, world, port, out_dir):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import datetime
+
+    import torch.distributed as dist
+    from oracle.oracle import Oracle
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        oracle = Oracle()
+        oracle.set_threads(1)
+        g = Grid(32, 12, 8, faces=(FACE_PERIODIC,) * 6)
+
+        class FailingSlab(OracleSlab):          # a block whose dt fails, planted on the CPU
+            def local_dt(self, cfl):
+                raise WsError(5, "planted: non-finite wave speed")
+
+        slab = decompose(g, world)[rank]
+        runner = (FailingSlab if rank == 1 else OracleSlab)(oracle, g, slab)
+        st = SlabStepper([runner], DistExchange())
+        st.set_state(_state(g))
+        try:
+            st.compute_dt(0.5)
+            outcome = "returned"
+        except WsError:
+            outcome = "raised"
+        with open(os.path.join(out_dir, f"rank{rank}.txt"), "w") as fh:
+            fh.write(outcome)
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_dt_failure_is_collective():
+    """A rank whose block's time step fails still takes the dt reduction
+    (contributing -1), so the other rank does not wait in it for good, and
+    every rank raises."""
+    with tempfile.TemporaryDirectory() as d:
+        mp.start_processes(_dt_failure_rank_main, args=(2, _free_port(), d), nprocs=2,
+                           join=True, start_method="spawn")
+        got = [open(os.path.join(d, f"rank{r}.txt")).read() for r in range(2)]
+    assert got == ["raised", "raised"]
+
+
 def _block_rank_main(rank, world, port, case, out_dir):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     import datetime

@@ -19,6 +19,7 @@ FACE_PERIODIC, FACE_EXTRAP, FACE_CLOSURE, FACE_EXTERNAL = 0, 1, 2, 3
 FP64, MIXED = 0, 1
 
 WS_OK = 0
+WS_ERR_NONFINITE = 5
 ERRORS = {1: "WS_ERR_INVALID", 2: "WS_ERR_CUDA", 3: "WS_ERR_ALLOC", 4: "WS_ERR_UNSUPPORTED",
           5: "WS_ERR_NONFINITE", 6: "WS_ERR_TIMEOUT", 7: "WS_ERR_BUDGET", 8: "WS_ERR_BUSY",
           9: "WS_ERR_NOT_FOUND", 10: "WS_ERR_IO", 11: "WS_ERR_COMM"}

@@ -52,8 +52,8 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from . import (FACE_CLOSURE, FACE_EXTERNAL, FACE_PERIODIC, Grid, Solver, halo_bytes, halo_pack,
-               halo_unpack)
+from . import (FACE_CLOSURE, FACE_EXTERNAL, FACE_PERIODIC, Grid, Solver, WsError, halo_bytes,
+               halo_pack, halo_unpack)
 from . import _abi
 
 HALO_FIELDS = 6          # d, u, v, w, T, cc
@@ -426,8 +426,23 @@ class SlabStepper:
 
     def compute_dt(self, cfl: float) -> float:
         """Global CFL time step: the minimum of the blocks' (the maximum wave
-        speed over the whole grid)."""
-        return self.exchange.min(min(r.local_dt(cfl) for r in self.runners))
+        speed over the whole grid).  Every rank takes the reduction, also when
+        its own blocks fail (they contribute -1), so that no rank waits in it
+        for good; then every rank raises."""
+        err = None
+        try:
+            local = min(r.local_dt(cfl) for r in self.runners)
+        except WsError as e:
+            local, err = -1.0, e
+        if not local > 0:                      # NaN or a failure
+            local = -1.0
+        dt = self.exchange.min(local)
+        if err is not None:
+            raise err
+        if not dt > 0:
+            raise WsError(_abi.WS_ERR_NONFINITE, "a block's maximum wave speed is not finite "
+                                                 "and positive")
+        return dt
 
     def set_state(self, f_global: np.ndarray) -> None:
         for r in self.runners:
