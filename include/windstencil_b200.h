@@ -201,7 +201,9 @@ typedef struct ws_viscous {
     int32_t d0_bound[6];
 } ws_viscous;
 
-/* Device workspace that ws_du_vis_jacobian3d needs for grid g (bytes). */
+/* Device workspace that ws_du_vis_jacobian3d needs for grid g (bytes): the
+ * viscous flux fields as LAP arrays, 12 of them, or 9 on a Cartesian grid
+ * (metrics_uniform), where the symmetric stress entries share a field. */
 WS_API size_t ws_du_vis_workspace_bytes(const ws_grid* g);
 
 /* du[1..4] (SoA, whole interior) += viscous terms of momentum and energy from

@@ -364,7 +364,7 @@ __global__ void __launch_bounds__(VNT, 2) vis_div_kernel(const __grid_constant__
         const int i = w.x0 + lx, j = w.y0 + ly;
         const bool own = i < a.nx && j < a.ny;
         const int X = min(i, a.nx - 1) + 4, Y = min(j, a.ny - 1) + 4;
-        // in-plane offsets (the 12 flux fields share one pitch): this column,
+        // in-plane offsets (the flux fields share one pitch): this column,
         // the x-rim and y-rim tile positions (clamped into the array)
         const int col = X + (int)a.epitch * Y;
         int xo[PX], yo[PY];
