@@ -302,7 +302,8 @@ def _peak(ws, name):
 
 
 def time_rhs_kernel(torch, ws, g, solver, stream, reps):
-    """Mean device time of the fused RHS through the drop-in entry point."""
+    """Mean device time of one RHS (the line passes, the default kernel) through
+    the drop-in entry point."""
     import ctypes as C
     _, du_desc, prims = solver.fields()
     gc = g.c()
@@ -448,7 +449,7 @@ def bench_slabs_one_gpu(a, torch, ws, wl, stream, parts=2):
             "stepper": "C++ (ws_blocks_step: decomposition, pack, exchange, unpack and "
                        "stages in the library)",
             "note": "slabs: per stage per slab a halo pack and unpack per shared face, "
-                    "ghost fill, fused RHS + stage; the exchange between GPUs (NCCL) is "
+                    "ghost fill, RHS line passes with the stage; the exchange between GPUs (NCCL) is "
                     "not in this number"}
 
 
@@ -743,7 +744,7 @@ def run_ours(a, rank, world, dist):
     f0 = wl.sod_state(a.nx, a.ny, a.nz, seed=2 + rank)
     stream = torch.cuda.Stream()
     if world == 1:
-        # one grid: the step's two graphs (ghost fill + fused RHS/stage, x3)
+        # one grid: the step's graphs (ghost fill + x, y, z line passes with the stage, x3)
         g = ws.Grid(a.nx, a.ny, a.nz, faces=faces)
         s = ws.Solver(g)
         s.set_state(f0, stream=stream)
