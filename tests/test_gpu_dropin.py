@@ -84,6 +84,21 @@ def test_init_empty_job_writes_nothing(oracle, cuda):
     assert bool(cuda.isnan(cc[:, :, :g.nx + 8]).all())
 
 
+@pytest.mark.parametrize("tile", [None, (-1, 0, 0, 0), (16, 8, 0, 704)])
+def test_rhs_empty_job_writes_nothing(cuda, tile):
+    """A job with no cells in one direction returns WS_OK and launches
+    nothing, on the line passes and the tile sweep alike."""
+    g = ws.Grid(12, 8, 8)
+    prims = [ws.lap_tensor(g, fill=1.0) for _ in range(5)]
+    du = cuda.full((5, 4, 4, 4), np.nan, dtype=cuda.float64, device="cuda")
+    for job in (ws.WsJob(ws.WsDim3(6, 6, 6), ws.WsDim3(6, 10, 10)),
+                ws.WsJob(ws.WsDim3(6, 6, 6), ws.WsDim3(10, 6, 10)),
+                ws.WsJob(ws.WsDim3(6, 6, 6), ws.WsDim3(10, 10, 6))):
+        ws.du_invis_jacobian3d(g, job, *prims, du, tile=tile)
+    cuda.cuda.synchronize()
+    assert bool(cuda.isnan(du).all())
+
+
 def _c_time_loop(torch, g, f0, dt, nsteps):
     """INTEGRATION's drop-in sequence through the C ABI, on one stream."""
     lib = ws.load()
